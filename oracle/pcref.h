@@ -1,0 +1,27 @@
+// ORACLE -- test infrastructure only (see pcref.cpp).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace pcref {
+
+struct NodeRecord {
+	std::string name;
+	int64_t byteOffset, byteSize, numPoints;
+};
+
+struct Result {
+	std::vector<uint8_t> octree, hierarchy, metadata;
+	std::vector<std::string> chunkIds;    // chunk (file-name) order
+	std::vector<int64_t> chunkCounts;
+	std::vector<NodeRecord> nodes;        // completion order
+};
+
+// Converts one uncompressed LAS file image; method is "poisson",
+// "poisson_average" or "random"; name goes to metadata.json; seed is the
+// random sampler's pinned seed.
+bool convert(const uint8_t* las, size_t size, const std::string& method, const std::string& name,
+             uint32_t seed, Result& res, std::string& err);
+
+}  // namespace pcref

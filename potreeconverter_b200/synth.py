@@ -1,0 +1,268 @@
+"""Seeded synthetic LAS generator for the benchmark and parity workloads.
+
+The reference's published numbers use real scans that are not available
+here, so every workload is a seeded synthetic cloud with the shapes, sizes
+and value distributions of the named configurations:
+
+* ``terrain``  -- 2.5D ground: x, y ~ U[0, extent]; z = three seeded sinusoids
+  (amplitudes 2-10 m) + N(0, 0.05 m); 10 % of the points on vertical facades
+  5-30 m tall. LAS 1.2, point format 2. RGB is a height ramp +/- 2000.
+* ``hotspots`` -- LAS 1.4, point format 3 (GPS time, monotone with 1e-5 s
+  jitter) plus one float32 extra-bytes attribute ~ N(0, 1); a 2 x 2 km x 50 m
+  slab with 20 Gaussian hot-spots (sigma 5-40 m) at 100x background density.
+* ``lattice``  -- precision stress: a jittered cubic lattice whose pitch is
+  the level-3 node spacing (cube / 1024), every coordinate moved by +/-1-3
+  quantization units. Point format 2.
+* ``strips``   -- aerial strips: overlapping 300 m flight strips over a seeded
+  value-noise heightfield, 15 % canopy points; point format 3.
+
+All coordinates are quantized to scale 0.001, and the header bounding box is
+the exact min/max of the quantized coordinates (the reference rejects points
+outside the header box, chunker_countsort_laszip.cpp:236-251).
+"""
+
+from __future__ import annotations
+
+import struct
+
+import numpy as np
+
+SCALE = 0.001
+
+# LAS point record dtypes (little endian, packed)
+_PDRF2 = np.dtype([
+    ("X", "<i4"), ("Y", "<i4"), ("Z", "<i4"), ("intensity", "<u2"),
+    ("bits", "u1"), ("classification", "u1"), ("scan_angle_rank", "i1"),
+    ("user_data", "u1"), ("point_source_id", "<u2"),
+    ("red", "<u2"), ("green", "<u2"), ("blue", "<u2"),
+])
+_PDRF3 = np.dtype([
+    ("X", "<i4"), ("Y", "<i4"), ("Z", "<i4"), ("intensity", "<u2"),
+    ("bits", "u1"), ("classification", "u1"), ("scan_angle_rank", "i1"),
+    ("user_data", "u1"), ("point_source_id", "<u2"), ("gps_time", "<f8"),
+    ("red", "<u2"), ("green", "<u2"), ("blue", "<u2"),
+])
+assert _PDRF2.itemsize == 26 and _PDRF3.itemsize == 34
+
+
+def _record_dtype(pdrf: int, extra_float: bool) -> np.dtype:
+    base = {2: _PDRF2, 3: _PDRF3}[pdrf]
+    if not extra_float:
+        return base
+    fields = [(n, base.fields[n][0]) for n in base.names] + [("extra", "<f4")]
+    return np.dtype(fields)
+
+
+def _extra_bytes_vlr(name: str = "extra", description: str = "N(0,1) float") -> bytes:
+    """One extra-bytes descriptor (record id 4, 192 bytes) for a float32."""
+    rec = bytearray(192)
+    rec[2] = 9  # data type 9 = float
+    rec[3] = 0  # options: no scale/offset/min/max
+    nb = name.encode()[:31]
+    rec[4:4 + len(nb)] = nb
+    db = description.encode()[:31]
+    rec[160:160 + len(db)] = db
+    hdr = bytearray(54)
+    hdr[2:2 + 9] = b"LASF_Spec"
+    struct.pack_into("<HH", hdr, 18, 4, 192)
+    d = b"Extra bytes"
+    hdr[22:22 + len(d)] = d
+    return bytes(hdr) + bytes(rec)
+
+
+def write_las(X, Y, Z, attrs: dict, *, pdrf: int, version_minor: int,
+              extra=None) -> bytes:
+    """Serialize quantized points into an uncompressed LAS file image."""
+    n = int(X.shape[0])
+    dt = _record_dtype(pdrf, extra is not None)
+    recs = np.zeros(n, dtype=dt)
+    recs["X"], recs["Y"], recs["Z"] = X, Y, Z
+    for k, v in attrs.items():
+        recs[k] = v
+    if extra is not None:
+        recs["extra"] = extra
+    header_size = 227 if version_minor <= 2 else 375
+    vlrs = _extra_bytes_vlr() if extra is not None else b""
+    offset_to_points = header_size + len(vlrs)
+
+    xs = X.astype(np.float64) * SCALE
+    ys = Y.astype(np.float64) * SCALE
+    zs = Z.astype(np.float64) * SCALE
+    h = bytearray(header_size)
+    h[0:4] = b"LASF"
+    h[24], h[25] = 1, version_minor
+    h[26:26 + 9] = b"synthetic"
+    h[58:58 + 19] = b"potreeconverter_b200"[:19]
+    struct.pack_into("<HH", h, 90, 1, 2024)
+    struct.pack_into("<H", h, 94, header_size)
+    struct.pack_into("<I", h, 96, offset_to_points)
+    struct.pack_into("<I", h, 100, 1 if extra is not None else 0)
+    struct.pack_into("<B", h, 104, pdrf)
+    struct.pack_into("<H", h, 105, dt.itemsize)
+    struct.pack_into("<I", h, 107, n if n < 2**32 else 0)
+    ret = (recs["bits"] & 7).astype(np.int64)
+    byret = np.bincount(np.clip(ret, 1, 5) - 1, minlength=5)[:5] if n else np.zeros(5, np.int64)
+    struct.pack_into("<5I", h, 111, *[int(v) if n < 2**32 else 0 for v in byret])
+    struct.pack_into("<3d", h, 131, SCALE, SCALE, SCALE)
+    struct.pack_into("<3d", h, 155, 0.0, 0.0, 0.0)
+    if n:
+        struct.pack_into("<6d", h, 179, xs.max(), xs.min(), ys.max(), ys.min(), zs.max(), zs.min())
+    if version_minor >= 4:
+        struct.pack_into("<Q", h, 235, 0)
+        struct.pack_into("<I", h, 243, 0)
+        struct.pack_into("<Q", h, 247, n)
+        struct.pack_into("<15Q", h, 255, *([int(v) for v in byret] + [0] * 10))
+    return bytes(h) + vlrs + recs.tobytes()
+
+
+def _common_attrs(rng, n, z):
+    nret = rng.integers(1, 6, n)
+    ret = np.minimum(rng.integers(1, 6, n), nret)
+    bits = (ret | (nret << 3)).astype(np.uint8)
+    zr = (z - z.min()) / max(float(np.ptp(z)), 1e-9)
+    ramp = np.stack([zr * 50000, (1 - np.abs(zr - 0.5) * 2) * 50000, (1 - zr) * 50000], 1)
+    rgb = np.clip(ramp + rng.uniform(-2000, 2000, (n, 3)) + 6000, 0, 65535).astype(np.uint16)
+    return {
+        "intensity": rng.integers(0, 65536, n, dtype=np.uint16),
+        "bits": bits,
+        "classification": rng.integers(0, 32, n, dtype=np.uint8),
+        "scan_angle_rank": rng.integers(-30, 31, n).astype(np.int8),
+        "user_data": rng.integers(0, 256, n, dtype=np.uint8),
+        "point_source_id": rng.integers(0, 64, n, dtype=np.uint16),
+        "red": rgb[:, 0], "green": rgb[:, 1], "blue": rgb[:, 2],
+    }
+
+
+def _quantize(x):
+    return np.round(np.asarray(x, dtype=np.float64) / SCALE).astype(np.int32)
+
+
+def terrain(n: int, seed: int, extent: float = 500.0) -> bytes:
+    """Config-0 style 2.5D terrain with facades, LAS 1.2 point format 2."""
+    rng = np.random.default_rng(seed)
+    n_fac = n // 10
+    n_gnd = n - n_fac
+    amps = rng.uniform(2.0, 10.0, 3)
+    freqs = rng.uniform(0.5, 3.0, (3, 2)) * (2 * np.pi / extent)
+    phases = rng.uniform(0, 2 * np.pi, 3)
+
+    def height(x, y):
+        h = np.zeros_like(x)
+        for a, (fx, fy), p in zip(amps, freqs, phases):
+            h += a * np.sin(fx * x + fy * y + p)
+        return h
+
+    x = rng.uniform(0, extent, n_gnd)
+    y = rng.uniform(0, extent, n_gnd)
+    z = height(x, y) + rng.normal(0, 0.05, n_gnd)
+    # vertical facades: axis-aligned wall segments
+    nwalls = max(1, n_fac // 5000 + 4)
+    wx0 = rng.uniform(0.05 * extent, 0.95 * extent, nwalls)
+    wy0 = rng.uniform(0.05 * extent, 0.95 * extent, nwalls)
+    wlen = rng.uniform(0.02 * extent, 0.08 * extent, nwalls)
+    whgt = rng.uniform(5.0, 30.0, nwalls)
+    wdir = rng.integers(0, 2, nwalls)
+    w = rng.integers(0, nwalls, n_fac)
+    t = rng.uniform(0, 1, n_fac) * wlen[w]
+    fx = np.clip(np.where(wdir[w] == 0, wx0[w] + t, wx0[w]), 0, extent)
+    fy = np.clip(np.where(wdir[w] == 0, wy0[w], wy0[w] + t), 0, extent)
+    fz = height(fx, fy) + rng.uniform(0, 1, n_fac) * whgt[w]
+    xs = np.concatenate([x, fx])
+    ys = np.concatenate([y, fy])
+    zs = np.concatenate([z, fz])
+    perm = rng.permutation(n)
+    xs, ys, zs = xs[perm], ys[perm], zs[perm]
+    X, Y, Z = _quantize(xs), _quantize(ys), _quantize(zs)
+    attrs = _common_attrs(rng, n, zs)
+    return write_las(X, Y, Z, attrs, pdrf=2, version_minor=2)
+
+
+def hotspots(n: int, seed: int, extent: float = 2000.0, height: float = 50.0,
+             n_spots: int = 20) -> bytes:
+    """Config-1 style clustered slab, LAS 1.4 point format 3 + float extra."""
+    rng = np.random.default_rng(seed)
+    sig = rng.uniform(5.0, 40.0, n_spots)
+    cx = rng.uniform(0.1 * extent, 0.9 * extent, n_spots)
+    cy = rng.uniform(0.1 * extent, 0.9 * extent, n_spots)
+    # 100x background density inside each spot's 1-sigma disc
+    area_bg = extent * extent
+    w_spot = 100.0 * np.pi * sig ** 2
+    p_bg = area_bg / (area_bg + w_spot.sum())
+    n_bg = int(round(n * p_bg))
+    n_sp = n - n_bg
+    which = rng.choice(n_spots, n_sp, p=w_spot / w_spot.sum())
+    xs = np.concatenate([rng.uniform(0, extent, n_bg), cx[which] + rng.normal(0, 1, n_sp) * sig[which]])
+    ys = np.concatenate([rng.uniform(0, extent, n_bg), cy[which] + rng.normal(0, 1, n_sp) * sig[which]])
+    zs = np.concatenate([rng.uniform(0, height, n_bg),
+                         np.clip(height * 0.5 + rng.normal(0, 1, n_sp) * sig[which] * 0.3, 0, height)])
+    xs = np.clip(xs, 0, extent)
+    ys = np.clip(ys, 0, extent)
+    perm = rng.permutation(n)
+    xs, ys, zs = xs[perm], ys[perm], zs[perm]
+    X, Y, Z = _quantize(xs), _quantize(ys), _quantize(zs)
+    attrs = _common_attrs(rng, n, zs)
+    attrs["gps_time"] = np.arange(n, dtype=np.float64) * 1e-4 + 3.0e5 + rng.uniform(-1e-5, 1e-5, n)
+    extra = rng.normal(0, 1, n).astype(np.float32)
+    return write_las(X, Y, Z, attrs, pdrf=3, version_minor=4, extra=extra)
+
+
+def lattice(n: int, seed: int, cube: float = 1024.0) -> bytes:
+    """Config-2 style jittered lattice with pitch = cube/1024 (level-3 spacing)."""
+    rng = np.random.default_rng(seed)
+    pitch = cube / 1024.0
+    side_xy = 1024
+    nz = max(1, int(np.ceil(n / (side_xy * side_xy))))
+    idx = rng.choice(side_xy * side_xy * nz, n, replace=False) if n < side_xy * side_xy * nz else np.arange(n)
+    ix = idx % side_xy
+    iy = (idx // side_xy) % side_xy
+    iz = idx // (side_xy * side_xy)
+    X = _quantize(ix * pitch) + rng.choice([-3, -2, -1, 1, 2, 3], n)
+    Y = _quantize(iy * pitch) + rng.choice([-3, -2, -1, 1, 2, 3], n)
+    Z = _quantize(iz * pitch) + rng.choice([-3, -2, -1, 1, 2, 3], n)
+    perm = rng.permutation(n)
+    X, Y, Z = X[perm].astype(np.int32), Y[perm].astype(np.int32), Z[perm].astype(np.int32)
+    attrs = _common_attrs(rng, n, Z.astype(np.float64) * SCALE)
+    return write_las(X, Y, Z, attrs, pdrf=2, version_minor=2)
+
+
+def _value_noise(rng, x, y, extent, octaves=6):
+    h = np.zeros_like(x)
+    amp, freq, total = 1.0, 4.0 / extent, 0.0
+    for _ in range(octaves):
+        g = rng.uniform(0, 1, (66, 66))
+        gx = np.clip(x * freq, 0, 64.999)
+        gy = np.clip(y * freq, 0, 64.999)
+        i0, j0 = np.floor(gx).astype(np.int64) % 65, np.floor(gy).astype(np.int64) % 65
+        fx, fy = gx - np.floor(gx), gy - np.floor(gy)
+        sx, sy = fx * fx * (3 - 2 * fx), fy * fy * (3 - 2 * fy)
+        v = (g[i0, j0] * (1 - sx) * (1 - sy) + g[i0 + 1, j0] * sx * (1 - sy)
+             + g[i0, j0 + 1] * (1 - sx) * sy + g[i0 + 1, j0 + 1] * sx * sy)
+        h += amp * v
+        total += amp
+        amp *= 0.5
+        freq = min(freq * 2.0, 64.0 / extent)
+    return h / total
+
+
+def strips(n: int, seed: int, extent: float = 20000.0, n_strips: int = 40,
+           width: float = 300.0) -> bytes:
+    """Config-3 style aerial strips over value-noise terrain, point format 3."""
+    rng = np.random.default_rng(seed)
+    centers = np.linspace(width / 2, extent - width / 2, n_strips)
+    s = rng.integers(0, n_strips, n)
+    xs = np.clip(centers[s] + rng.uniform(-width / 2, width / 2, n) * 1.4, 0, extent)
+    ys = rng.uniform(0, extent, n)
+    zs = _value_noise(np.random.default_rng(seed + 1), xs, ys, extent) * 400.0
+    canopy = rng.uniform(0, 1, n) < 0.15
+    zs = zs + canopy * rng.uniform(0, 30.0, n)
+    X, Y, Z = _quantize(xs), _quantize(ys), _quantize(zs)
+    attrs = _common_attrs(rng, n, zs)
+    attrs["gps_time"] = np.arange(n, dtype=np.float64) * 1e-5 + 1.0e5
+    return write_las(X, Y, Z, attrs, pdrf=3, version_minor=4)
+
+
+GENERATORS = {"terrain": terrain, "hotspots": hotspots, "lattice": lattice, "strips": strips}
+
+
+def generate(kind: str, n: int, seed: int, **kw) -> bytes:
+    return GENERATORS[kind](n, seed, **kw)
