@@ -1,0 +1,136 @@
+/*
+ * pcgpu.h -- C ABI of the B200-native octree LOD builder (libpcgpu.so).
+ *
+ * The library converts an uncompressed LAS file image into the three files
+ * PotreeConverter 2.0 writes (octree.bin, hierarchy.bin, metadata.json),
+ * byte-identical to a determinism-pinned reference build, with every stage of
+ * the build running as CUDA kernels for sm_100a on one GPU.
+ *
+ * Reference interfaces replaced (paths relative to the PotreeConverter
+ * source tree):
+ *   pcg_convert      main.cpp:345-393 chunking() + indexing(), i.e.
+ *                    chunker_countsort_laszip::doChunking
+ *                    (include/chunker_countsort_laszip.h:19) followed by
+ *                    indexer::doIndexing (include/indexer.h:379) with the
+ *                    Sampler chosen by -m (main.cpp:377-392).
+ *   pcg_method       the three Sampler plug-ins (include/structures.h:152-164):
+ *                    SamplerPoisson, SamplerPoissonAverage, SamplerRandom.
+ *   pcg_submit/poll  no counterpart: request loop for conversion jobs.
+ *   pcg_kernel_*     single-kernel entry points used by the parity tests; each
+ *                    names the reference code it reproduces.
+ *
+ * Conventions: every call returns a pcg_status (the reference calls exit()).
+ * The caller owns all host memory it passes in; buffers in a pcg_result are
+ * owned by the library until pcg_result_free. The context owns all device
+ * memory; all device work runs on the context's stream. A context is
+ * internally locked, so it may be shared between host threads.
+ */
+#ifndef PCGPU_H
+#define PCGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pcg_status {
+	PCG_OK = 0,
+	PCG_BAD_INPUT = 1,    /* malformed or unsupported LAS input            */
+	PCG_OUT_OF_BOX = 2,   /* point outside the header bounding box (the
+	                         reference's exit(123), chunker_countsort_laszip.cpp:236-251) */
+	PCG_OOM = 3,          /* device or host allocation failed             */
+	PCG_TIMEOUT = 4,      /* a bounded device wait gave up                */
+	PCG_INTERNAL = 5,     /* inconsistent device result                   */
+	PCG_CUDA = 6,         /* CUDA runtime error                           */
+	PCG_NOT_FOUND = 7     /* unknown job id                               */
+} pcg_status;
+
+typedef enum pcg_method {
+	PCG_POISSON = 0,          /* sampler_poisson.h        */
+	PCG_POISSON_AVERAGE = 1,  /* sampler_poisson_average.h */
+	PCG_RANDOM = 2            /* sampler_random.h          */
+} pcg_method;
+
+typedef enum pcg_form {
+	PCG_FORM_BATCHED = 0, /* one launch per octree level over all nodes, FP32
+	                         neighbour tests with an FP64 guard band          */
+	PCG_FORM_PLAIN = 1    /* one launch per node, every neighbour test FP64  */
+} pcg_form;
+
+typedef struct pcg_opts {
+	int32_t device;        /* CUDA device ordinal                            */
+	uint32_t random_seed;  /* seed of the random sampler's leaf shuffle; the
+	                          pinned reference uses 1592614637               */
+	int32_t form;          /* pcg_form                                        */
+	int32_t reserved;
+} pcg_opts;
+
+typedef struct pcg_job {
+	const void* las;       /* uncompressed LAS file image (host memory)      */
+	uint64_t las_size;
+	int32_t method;        /* pcg_method                                      */
+	int32_t reserved;
+	const char* name;      /* metadata.json "name" (the reference uses the
+	                          input file's stem, main.cpp:171-173)            */
+	const char* projection;/* metadata.json "projection" (may be NULL)       */
+} pcg_job;
+
+typedef struct pcg_stats {
+	int64_t num_points;           /* points in the LAS file                 */
+	int64_t num_chunks;
+	int64_t num_nodes;            /* hierarchy records written              */
+	int64_t output_points;
+	int64_t octree_depth;
+	int64_t escalated_pairs;      /* FP32 tests re-decided in FP64          */
+	int64_t heapsort_fallbacks;   /* introsort depth-limit hits             */
+	double ms_total;              /* wall time of pcg_convert               */
+	double ms_h2d, ms_chunking, ms_octree, ms_sampling, ms_output, ms_d2h, ms_host_writers;
+	int64_t gpu_launches;         /* kernels launched for this job          */
+} pcg_stats;
+
+typedef struct pcg_result {
+	uint8_t* octree;       uint64_t octree_size;
+	uint8_t* hierarchy;    uint64_t hierarchy_size;
+	char* metadata;        uint64_t metadata_size;   /* NUL terminated */
+	pcg_stats stats;
+} pcg_result;
+
+typedef struct pcg_ctx pcg_ctx;
+
+/* Context lifecycle. opts may be NULL (device 0, pinned seed, batched). */
+pcg_status pcg_create(pcg_ctx** ctx, const pcg_opts* opts);
+void pcg_destroy(pcg_ctx* ctx);
+const char* pcg_last_error(const pcg_ctx* ctx);
+const char* pcg_status_string(pcg_status s);
+
+/* Synchronous conversion (replaces chunking() + indexing(), main.cpp:345-393). */
+pcg_status pcg_convert(pcg_ctx* ctx, const pcg_job* job, pcg_result* out);
+void pcg_result_free(pcg_result* r);
+
+/* Writes out->{octree,hierarchy,metadata} as <dir>/octree.bin etc. */
+pcg_status pcg_write_files(const pcg_result* r, const char* dir);
+
+/* Request loop: jobs are admitted by device-memory footprint and run as
+ * device work interleaves; pcg_wait blocks until the job finished. */
+pcg_status pcg_submit(pcg_ctx* ctx, const pcg_job* job, uint64_t* job_id);
+pcg_status pcg_poll(pcg_ctx* ctx, uint64_t job_id, int32_t* done);
+pcg_status pcg_wait(pcg_ctx* ctx, uint64_t job_id, pcg_result* out);
+
+/* ---- single-kernel entry points (device-agnostic host buffers) ---------- */
+
+/* Sorts n keys ascending with the exact element order std::sort (libstdc++
+ * introsort: median-of-3 pivot, threshold 16, heapsort at the depth limit)
+ * produces for the comparator "a < b" -- the sort the samplers call
+ * (sampler_poisson.h:183-203). perm_out[i] = input index of the i-th element. */
+pcg_status pcg_kernel_sort_keys(pcg_ctx* ctx, const double* keys, int64_t n, int32_t* perm_out);
+
+/* perm_out[i] = index that std::shuffle(0..n-1, std::default_random_engine(seed))
+ * leaves at position i (sampler_random.h:97-104). */
+pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* perm_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PCGPU_H */

@@ -1349,3 +1349,20 @@ void pcref_free(pcref_output* out) {
 }
 
 }  // extern "C"
+
+// Test hooks: the library behaviour the samplers rely on, straight from
+// libstdc++ (the same standard library the reference links).
+extern "C" void pcref_std_sort_perm(const double* keys, int64_t n, int32_t* perm) {
+	struct E { double k; int32_t i; };
+	std::vector<E> v(n);
+	for (int64_t i = 0; i < n; i++) v[i] = {keys[i], (int32_t)i};
+	std::sort(v.begin(), v.end(), [](const E& a, const E& b) { return a.k < b.k; });
+	for (int64_t i = 0; i < n; i++) perm[i] = v[i].i;
+}
+
+extern "C" void pcref_std_shuffle(int64_t n, uint32_t seed, int32_t* perm) {
+	std::vector<int> v(n);
+	for (int64_t i = 0; i < n; i++) v[i] = (int)i;
+	std::shuffle(v.begin(), v.end(), std::default_random_engine(seed));
+	for (int64_t i = 0; i < n; i++) perm[i] = v[i];
+}

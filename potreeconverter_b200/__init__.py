@@ -1,0 +1,225 @@
+"""B200-native octree LOD builder with PotreeConverter 2.0's output format.
+
+The conversion runs as CUDA kernels for sm_100a inside ``libpcgpu.so``; this
+package is a thin ctypes layer over its C ABI (``include/pcgpu.h``), mirroring
+the reference's conversion entry (``PotreeConverter <in.las> -o <dir> -m
+poisson|poisson_average|random``, main.cpp:497-569) as :func:`convert`.
+
+There is no CPU fallback: importing works without a GPU, but every call that
+converts or launches a kernel raises if the CUDA library or a device is
+missing.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpcgpu.so")
+
+METHODS = {"poisson": 0, "poisson_average": 1, "random": 2}
+FORMS = {"batched": 0, "plain": 1}
+PINNED_SEED = 1592614637
+
+STATUS = {0: "ok", 1: "bad input", 2: "point outside bounding box", 3: "out of memory", 4: "timeout",
+          5: "internal error", 6: "cuda error", 7: "not found"}
+
+
+class PcgError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("random_seed", ctypes.c_uint32), ("form", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class _Job(ctypes.Structure):
+    _fields_ = [("las", ctypes.c_void_p), ("las_size", ctypes.c_uint64), ("method", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("name", ctypes.c_char_p), ("projection", ctypes.c_char_p)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("num_points", ctypes.c_int64), ("num_chunks", ctypes.c_int64), ("num_nodes", ctypes.c_int64),
+                ("output_points", ctypes.c_int64), ("octree_depth", ctypes.c_int64),
+                ("escalated_pairs", ctypes.c_int64), ("heapsort_fallbacks", ctypes.c_int64),
+                ("ms_total", ctypes.c_double), ("ms_h2d", ctypes.c_double), ("ms_chunking", ctypes.c_double),
+                ("ms_octree", ctypes.c_double), ("ms_sampling", ctypes.c_double), ("ms_output", ctypes.c_double),
+                ("ms_d2h", ctypes.c_double), ("ms_host_writers", ctypes.c_double), ("gpu_launches", ctypes.c_int64)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("octree", ctypes.POINTER(ctypes.c_uint8)), ("octree_size", ctypes.c_uint64),
+                ("hierarchy", ctypes.POINTER(ctypes.c_uint8)), ("hierarchy_size", ctypes.c_uint64),
+                ("metadata", ctypes.c_char_p), ("metadata_size", ctypes.c_uint64), ("stats", _Stats)]
+
+
+# every symbol include/pcgpu.h declares
+EXPORTS = ["pcg_create", "pcg_destroy", "pcg_last_error", "pcg_status_string", "pcg_convert", "pcg_result_free",
+           "pcg_write_files", "pcg_submit", "pcg_poll", "pcg_wait", "pcg_kernel_sort_keys", "pcg_kernel_shuffle"]
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libpcgpu.so (built by ``python -m potreeconverter_b200.build``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libpcgpu.so not found at {path}; build it with python -m potreeconverter_b200.build")
+    lib = ctypes.CDLL(path)
+    c = ctypes
+    lib.pcg_create.argtypes = [c.POINTER(c.c_void_p), c.POINTER(_Opts)]
+    lib.pcg_destroy.argtypes = [c.c_void_p]
+    lib.pcg_last_error.argtypes = [c.c_void_p]
+    lib.pcg_last_error.restype = c.c_char_p
+    lib.pcg_status_string.argtypes = [c.c_int]
+    lib.pcg_status_string.restype = c.c_char_p
+    lib.pcg_convert.argtypes = [c.c_void_p, c.POINTER(_Job), c.POINTER(_Result)]
+    lib.pcg_result_free.argtypes = [c.POINTER(_Result)]
+    lib.pcg_write_files.argtypes = [c.POINTER(_Result), c.c_char_p]
+    lib.pcg_submit.argtypes = [c.c_void_p, c.POINTER(_Job), c.POINTER(c.c_uint64)]
+    lib.pcg_poll.argtypes = [c.c_void_p, c.c_uint64, c.POINTER(c.c_int32)]
+    lib.pcg_wait.argtypes = [c.c_void_p, c.c_uint64, c.POINTER(_Result)]
+    lib.pcg_kernel_sort_keys.argtypes = [c.c_void_p, c.c_void_p, c.c_int64, c.c_void_p]
+    lib.pcg_kernel_shuffle.argtypes = [c.c_void_p, c.c_int64, c.c_uint32, c.c_void_p]
+    _lib = lib
+    return lib
+
+
+@dataclass
+class Conversion:
+    """The three PotreeConverter outputs plus run statistics."""
+    octree: bytes
+    hierarchy: bytes
+    metadata: str
+    stats: dict
+
+    def write(self, outdir: str) -> None:
+        os.makedirs(outdir, exist_ok=True)
+        with open(os.path.join(outdir, "octree.bin"), "wb") as f:
+            f.write(self.octree)
+        with open(os.path.join(outdir, "hierarchy.bin"), "wb") as f:
+            f.write(self.hierarchy)
+        with open(os.path.join(outdir, "metadata.json"), "w", newline="") as f:
+            f.write(self.metadata)
+
+
+def _take(lib, res: _Result) -> Conversion:
+    octree = ctypes.string_at(res.octree, res.octree_size) if res.octree_size else b""
+    hierarchy = ctypes.string_at(res.hierarchy, res.hierarchy_size) if res.hierarchy_size else b""
+    metadata = ctypes.string_at(res.metadata, res.metadata_size).decode() if res.metadata_size else ""
+    stats = {name: getattr(res.stats, name) for name, _ in _Stats._fields_}
+    lib.pcg_result_free(ctypes.byref(res))
+    return Conversion(octree, hierarchy, metadata, stats)
+
+
+class Context:
+    """A device context (pcg_create/pcg_destroy)."""
+
+    def __init__(self, device: int = 0, seed: int = PINNED_SEED, form: str = "batched"):
+        self._lib = load_library()
+        opts = _Opts(device, seed, FORMS[form], 0)
+        h = ctypes.c_void_p()
+        st = self._lib.pcg_create(ctypes.byref(h), ctypes.byref(opts))
+        if st != 0:
+            raise PcgError(st, "pcg_create failed")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pcg_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _err(self, st):
+        return PcgError(st, self._lib.pcg_last_error(self._h).decode(errors="replace"))
+
+    @staticmethod
+    def _job(las, method, name, projection, keep):
+        if isinstance(las, (bytes, bytearray, memoryview)):
+            buf = (ctypes.c_uint8 * len(las)).from_buffer_copy(las) if isinstance(las, bytes) else \
+                (ctypes.c_uint8 * len(las)).from_buffer(las)
+            keep.append(buf)
+            ptr, size = ctypes.addressof(buf), len(las)
+        else:  # (pointer, size), e.g. pinned host memory
+            ptr, size = las
+        nm = name.encode()
+        pj = projection.encode()
+        keep.extend([nm, pj])
+        return _Job(ptr, size, METHODS[method], 0, nm, pj)
+
+    def convert(self, las, method: str = "poisson", name: str = "cloud", projection: str = "") -> Conversion:
+        """Converts one LAS file image (bytes, or (host pointer, size))."""
+        keep = []
+        job = self._job(las, method, name, projection, keep)
+        res = _Result()
+        st = self._lib.pcg_convert(self._h, ctypes.byref(job), ctypes.byref(res))
+        if st != 0:
+            raise self._err(st)
+        return _take(self._lib, res)
+
+    def submit(self, las, method: str = "poisson", name: str = "cloud", projection: str = "") -> int:
+        keep = []
+        job = self._job(las, method, name, projection, keep)
+        jid = ctypes.c_uint64()
+        st = self._lib.pcg_submit(self._h, ctypes.byref(job), ctypes.byref(jid))
+        if st != 0:
+            raise self._err(st)
+        return jid.value
+
+    def poll(self, job_id: int) -> bool:
+        done = ctypes.c_int32()
+        st = self._lib.pcg_poll(self._h, job_id, ctypes.byref(done))
+        if st != 0:
+            raise self._err(st)
+        return bool(done.value)
+
+    def wait(self, job_id: int) -> Conversion:
+        res = _Result()
+        st = self._lib.pcg_wait(self._h, job_id, ctypes.byref(res))
+        if st != 0:
+            raise self._err(st)
+        return _take(self._lib, res)
+
+    def sort_keys(self, keys):
+        """Permutation std::sort produces for FP64 keys (device kernel)."""
+        import numpy as np
+        k = np.ascontiguousarray(keys, dtype=np.float64)
+        perm = np.empty(k.shape[0], dtype=np.int32)
+        st = self._lib.pcg_kernel_sort_keys(self._h, k.ctypes.data, k.shape[0], perm.ctypes.data)
+        if st != 0:
+            raise self._err(st)
+        return perm
+
+    def shuffle(self, n: int, seed: int = PINNED_SEED):
+        """Index order std::shuffle(iota(n), default_random_engine(seed)) gives (device kernel)."""
+        import numpy as np
+        perm = np.empty(n, dtype=np.int32)
+        st = self._lib.pcg_kernel_shuffle(self._h, n, seed, perm.ctypes.data)
+        if st != 0:
+            raise self._err(st)
+        return perm
+
+
+def convert(las, method: str = "poisson", name: str = "cloud", form: str = "batched", seed: int = PINNED_SEED,
+            device: int = 0) -> Conversion:
+    """One-shot conversion: PotreeConverter <in.las> -m method."""
+    with Context(device=device, seed=seed, form=form) as ctx:
+        return ctx.convert(las, method=method, name=name)

@@ -1,0 +1,310 @@
+// Chunker on the device: LAS record decode + quantize + count grid
+// (countPointsInCells, chunker_countsort_laszip.cpp:131-361, and the decode
+// half of distributePoints, :749-803 with the handlers of :380-658), the
+// pyramid cell merge (createLUT, :1074-1204) and the chunk lookup that feeds
+// the stable scatter (:837-904).
+//
+// All FP64 expressions are evaluated in the reference's order; the library
+// is compiled with --fmad=false so no multiply-add is contracted, matching
+// x86-64 SSE2 code without FMA.
+
+#include <math_constants.h>
+
+#include "kernels.h"
+
+namespace pcg {
+
+namespace {
+
+__device__ __forceinline__ unsigned long long ordered(double d) {
+	unsigned long long b = (unsigned long long)__double_as_longlong(d);
+	return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+template <class T> __device__ __forceinline__ T ld(const uint8_t* p) {
+	T v;
+	memcpy(&v, p, sizeof(T));
+	return v;
+}
+
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min(a, b)
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max(a, b)
+
+constexpr int kDecodeThreads = 256;
+
+struct IntRange {
+	int mn, mx;
+	__device__ void init() { mn = 0x7fffffff; mx = -0x7fffffff - 1; }
+	__device__ void add(int v) { mn = v < mn ? v : mn; mx = v > mx ? v : mx; }
+};
+
+__device__ void flush_int(AttrStatsDev* st, int comp, const IntRange& r, unsigned long long* smem_mn, unsigned long long* smem_mx) {
+	if (r.mn <= r.mx) {
+		atomicMin(smem_mn + comp, ordered((double)r.mn));
+		atomicMax(smem_mx + comp, ordered((double)r.mx));
+	}
+}
+
+// One thread per point (grid-stride). Writes the quantized position SoA and
+// the count-grid cell, counts into the grid with warp-aggregated atomics and
+// reduces attribute min/max (in registers, then shared memory, then one
+// global atomic per block and statistic).
+__global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(const uint8_t* __restrict__ recs, DecodeParams p,
+                                                                    uint32_t* __restrict__ grid, ChunkingOut out) {
+	// shared statistics: [attr][comp] ordered min / max
+	__shared__ unsigned long long s_mn[MAX_ATTRS][3];
+	__shared__ unsigned long long s_mx[MAX_ATTRS][3];
+	__shared__ unsigned int s_hist[256];
+	for (int i = threadIdx.x; i < MAX_ATTRS * 3; i += blockDim.x) {
+		(&s_mn[0][0])[i] = ~0ull;
+		(&s_mx[0][0])[i] = 0ull;
+	}
+	for (int i = threadIdx.x; i < 256; i += blockDim.x) s_hist[i] = 0;
+	__syncthreads();
+
+	double pmn[3] = {CUDART_INF, CUDART_INF, CUDART_INF}, pmx[3] = {-CUDART_INF, -CUDART_INF, -CUDART_INF};
+	double gmn = CUDART_INF, gmx = -CUDART_INF;
+	IntRange r_int, r_ret, r_nret, r_cls, r_sar, r_user, r_psid, r_r, r_g, r_b;
+	r_int.init(); r_ret.init(); r_nret.init(); r_cls.init(); r_sar.init(); r_user.init(); r_psid.init(); r_r.init(); r_g.init(); r_b.init();
+
+	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+	const int G = p.grid;
+	const double dG = (double)G;
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride) {
+		const uint8_t* r = recs + i * p.rec_len;
+		int32_t Xi = ld<int32_t>(r), Yi = ld<int32_t>(r + 4), Zi = ld<int32_t>(r + 8);
+		// laszip_get_coordinates (laszip_dll.cpp:1137-1139)
+		double x = p.in_scale[0] * (double)Xi + p.in_offset[0];
+		double y = p.in_scale[1] * (double)Yi + p.in_offset[1];
+		double z = p.in_scale[2] * (double)Zi + p.in_offset[2];
+		// quantize (chunker_countsort_laszip.cpp:228-230, 781-783)
+		int32_t X = (int32_t)((x - p.pos_offset[0]) / p.pos_scale[0]);
+		int32_t Y = (int32_t)((y - p.pos_offset[1]) / p.pos_scale[1]);
+		int32_t Z = (int32_t)((z - p.pos_offset[2]) / p.pos_scale[2]);
+		// unit cube coordinates and cell (:232-257)
+		double ux = ((double)X * p.pos_scale[0] + p.pos_offset[0] - p.cmin[0]) / p.csize;
+		double uy = ((double)Y * p.pos_scale[1] + p.pos_offset[1] - p.cmin[1]) / p.csize;
+		double uz = ((double)Z * p.pos_scale[2] + p.pos_offset[2] - p.cmin[2]) / p.csize;
+		bool in_box = ux >= 0.0 && uy >= 0.0 && uz >= 0.0 && ux <= 1.0 && uy <= 1.0 && uz <= 1.0;
+		uint32_t cell = 0;
+		if (!in_box) {
+			atomicCAS((unsigned long long*)&out.error[0], 0ull, (unsigned long long)(i + 1));
+		} else {
+			int64_t ix = (int64_t)dmin(dG * ux, dG - 1.0);
+			int64_t iy = (int64_t)dmin(dG * uy, dG - 1.0);
+			int64_t iz = (int64_t)dmin(dG * uz, dG - 1.0);
+			cell = (uint32_t)(ix + iy * G + iz * (int64_t)G * G);
+		}
+		out.X[i] = X;
+		out.Y[i] = Y;
+		out.Z[i] = Z;
+		out.cell[i] = cell;
+		// warp-aggregated increment of the count grid
+		{
+			unsigned active = __activemask();
+			unsigned key = in_box ? cell : 0xffffffffu;
+			unsigned peers = __match_any_sync(active, key);
+			if (in_box && (__ffs(peers) - 1) == (int)(threadIdx.x & 31)) atomicAdd(grid + cell, (uint32_t)__popc(peers));
+		}
+		// attribute statistics (handlers, :391-545); position uses the
+		// unquantized coordinate (:789-795)
+		pmn[0] = dmin(pmn[0], x); pmn[1] = dmin(pmn[1], y); pmn[2] = dmin(pmn[2], z);
+		pmx[0] = dmax(pmx[0], x); pmx[1] = dmax(pmx[1], y); pmx[2] = dmax(pmx[2], z);
+		if (p.stat_intensity >= 0) r_int.add(ld<uint16_t>(r + 12));
+		uint8_t bits = r[14];
+		if (p.stat_retnum >= 0) r_ret.add(bits & 7);
+		if (p.stat_nret >= 0) r_nret.add((bits >> 3) & 7);
+		if (p.stat_class >= 0) {
+			int c = r[15] & 31;
+			r_cls.add(c);
+			atomicAdd(&s_hist[c], 1u);
+		}
+		if (p.stat_sar >= 0) r_sar.add((int8_t)r[16]);
+		if (p.stat_user >= 0) r_user.add(r[17]);
+		if (p.stat_psid >= 0) r_psid.add(ld<uint16_t>(r + 18));
+		if (p.stat_gps >= 0) {
+			double g = ld<double>(r + p.src_gps);
+			gmn = dmin(gmn, g);
+			gmx = dmax(gmx, g);
+		}
+		if (p.stat_rgb >= 0) {
+			r_r.add(ld<uint16_t>(r + p.src_rgb));
+			r_g.add(ld<uint16_t>(r + p.src_rgb + 2));
+			r_b.add(ld<uint16_t>(r + p.src_rgb + 4));
+		}
+		for (int e = 0; e < p.n_extra; e++) {
+			const ExtraDesc& d = p.extra[e];
+			for (int c = 0; c < d.num_elements && c < 3; c++) {
+				const uint8_t* q = r + d.src_off + c * d.element_size;
+				double v = 0.0;
+				switch (d.type) {
+				case 0: v = (double)ld<int8_t>(q); break;
+				case 1: v = (double)ld<int16_t>(q); break;
+				case 2: v = (double)ld<int32_t>(q); break;
+				case 3: v = (double)ld<int64_t>(q); break;
+				case 10: v = (double)ld<uint8_t>(q); break;
+				case 11: v = (double)ld<uint16_t>(q); break;
+				case 12: v = (double)ld<uint32_t>(q); break;
+				case 13: v = (double)ld<uint64_t>(q); break;
+				case 20: v = (double)ld<float>(q); break;
+				case 21: v = ld<double>(q); break;
+				default: v = 0.0;
+				}
+				atomicMin(&s_mn[d.stat_index][c], ordered(v));
+				atomicMax(&s_mx[d.stat_index][c], ordered(v));
+			}
+		}
+	}
+	// block reduction of the register accumulators
+	if (pmn[0] <= pmx[0]) {
+		for (int c = 0; c < 3; c++) {
+			atomicMin(&s_mn[p.stat_pos][c], ordered(pmn[c]));
+			atomicMax(&s_mx[p.stat_pos][c], ordered(pmx[c]));
+		}
+	}
+	if (p.stat_intensity >= 0) flush_int(out.stats, 0, r_int, s_mn[p.stat_intensity], s_mx[p.stat_intensity]);
+	if (p.stat_retnum >= 0) flush_int(out.stats, 0, r_ret, s_mn[p.stat_retnum], s_mx[p.stat_retnum]);
+	if (p.stat_nret >= 0) flush_int(out.stats, 0, r_nret, s_mn[p.stat_nret], s_mx[p.stat_nret]);
+	if (p.stat_class >= 0) flush_int(out.stats, 0, r_cls, s_mn[p.stat_class], s_mx[p.stat_class]);
+	if (p.stat_sar >= 0) flush_int(out.stats, 0, r_sar, s_mn[p.stat_sar], s_mx[p.stat_sar]);
+	if (p.stat_user >= 0) flush_int(out.stats, 0, r_user, s_mn[p.stat_user], s_mx[p.stat_user]);
+	if (p.stat_psid >= 0) flush_int(out.stats, 0, r_psid, s_mn[p.stat_psid], s_mx[p.stat_psid]);
+	if (p.stat_rgb >= 0) {
+		flush_int(out.stats, 0, r_r, s_mn[p.stat_rgb], s_mx[p.stat_rgb]);
+		flush_int(out.stats, 1, r_g, s_mn[p.stat_rgb], s_mx[p.stat_rgb]);
+		flush_int(out.stats, 2, r_b, s_mn[p.stat_rgb], s_mx[p.stat_rgb]);
+	}
+	if (p.stat_gps >= 0 && gmn <= gmx) {
+		atomicMin(&s_mn[p.stat_gps][0], ordered(gmn));
+		atomicMax(&s_mx[p.stat_gps][0], ordered(gmx));
+	}
+	__syncthreads();
+	for (int i = threadIdx.x; i < MAX_ATTRS * 3; i += blockDim.x) {
+		int a = i / 3, c = i % 3;
+		unsigned long long vmn = s_mn[a][c], vmx = s_mx[a][c];
+		if (vmn != ~0ull) atomicMin(&out.stats[a].mn[c], vmn);
+		if (vmx != 0ull) atomicMax(&out.stats[a].mx[c], vmx);
+	}
+	for (int i = threadIdx.x; i < 256; i += blockDim.x)
+		if (s_hist[i]) atomicAdd(&out.histogram[i], (unsigned long long)s_hist[i]);
+}
+
+// One pyramid level of createLUT: low cell (x, y, z) merges its 8 high
+// cells unless one of them is already split (-1) or the sum exceeds the
+// chunk capacity; then every non-empty high cell becomes a chunk.
+template <class TH>
+__global__ void lut_merge_kernel(const TH* __restrict__ high, int64_t* __restrict__ low, int level_low, int g_low,
+                                 int64_t max_points, ChunkCell* __restrict__ chunks, int32_t* __restrict__ num_chunks, int capacity) {
+	int64_t cells = (int64_t)g_low * g_low * g_low;
+	int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= cells) return;
+	int x = (int)(t % g_low), y = (int)((t / g_low) % g_low), z = (int)(t / ((int64_t)g_low * g_low));
+	int g_high = 2 * g_low;
+	int64_t vals[8];
+	int64_t sum = 0;
+	bool unmergeable = false;
+	for (int j = 0; j < 8; j++) {
+		int nx = 2 * x + ((j & 4) >> 2), ny = 2 * y + ((j & 2) >> 1), nz = 2 * z + (j & 1);
+		int64_t v = (int64_t)high[nx + (int64_t)ny * g_high + (int64_t)nz * g_high * g_high];
+		if (sizeof(TH) == 4) v = (int64_t)(uint32_t)v;
+		vals[j] = v;
+		if (v == -1) unmergeable = true; else sum += v;
+	}
+	int64_t idx_low = x + (int64_t)y * g_low + (int64_t)z * g_low * g_low;
+	if (unmergeable || sum > max_points) {
+		for (int j = 0; j < 8; j++) {
+			if (vals[j] > 0) {
+				int k = atomicAdd(num_chunks, 1);
+				if (k < capacity) {
+					ChunkCell c;
+					c.level = level_low + 1;
+					c.x = 2 * x + ((j & 4) >> 2);
+					c.y = 2 * y + ((j & 2) >> 1);
+					c.z = 2 * z + (j & 1);
+					c.count = vals[j];
+					chunks[k] = c;
+				}
+			}
+		}
+		low[idx_low] = -1;
+	} else {
+		low[idx_low] = sum;
+	}
+}
+
+__global__ void lut_fill_kernel(const ChunkCell* __restrict__ chunks, int grid_size, int level_max, int32_t* __restrict__ lut) {
+	ChunkCell c = chunks[blockIdx.x];
+	int size = 1 << (level_max - c.level);
+	int64_t cells = (int64_t)size * size * size;
+	for (int64_t t = threadIdx.x; t < cells; t += blockDim.x) {
+		int ox = (int)(t % size), oy = (int)((t / size) % size), oz = (int)(t / ((int64_t)size * size));
+		int64_t x = (int64_t)size * c.x + ox, y = (int64_t)size * c.y + oy, z = (int64_t)size * c.z + oz;
+		lut[x + y * grid_size + z * (int64_t)grid_size * grid_size] = (int32_t)blockIdx.x;
+	}
+}
+
+__global__ void assign_kernel(const uint32_t* __restrict__ cell, const int32_t* __restrict__ lut, int64_t n,
+                              uint32_t* __restrict__ chunk_of, uint32_t* __restrict__ ids, int64_t* error) {
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	int32_t c = lut[cell[i]];
+	if (c < 0) {
+		atomicCAS((unsigned long long*)&error[1], 0ull, (unsigned long long)(i + 1));
+		c = 0;
+	}
+	chunk_of[i] = (uint32_t)c;
+	ids[i] = (uint32_t)i;
+}
+
+}  // namespace
+
+void launch_decode_count(const uint8_t* d_recs, const DecodeParams& p, uint32_t* grid, ChunkingOut& out, DeviceMem& mem) {
+	if (p.n == 0) return;
+	int dev = 0;
+	PCG_CUDA(cudaGetDevice(&dev));
+	int sms = 0;
+	PCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+	int64_t blocks = ceil_div(p.n, kDecodeThreads * 4);
+	int64_t cap = (int64_t)sms * 8;
+	if (blocks > cap) blocks = cap;
+	if (blocks < 1) blocks = 1;
+	decode_count_kernel<<<(unsigned)blocks, kDecodeThreads, 0, mem.stream()>>>(d_recs, p, grid, out);
+	PCG_LAUNCHED();
+}
+
+void launch_lut_merge(const uint32_t* grid, int grid_size, int64_t max_points_per_chunk, ChunkCell* chunks,
+                      int32_t* num_chunks, int capacity, DeviceMem& mem) {
+	cudaStream_t s = mem.stream();
+	int level_max = bits_for((uint64_t)grid_size) - 1;
+	int64_t* prev = nullptr;
+	for (int level_low = level_max - 1; level_low >= 0; level_low--) {
+		int g_low = 1 << level_low;
+		int64_t cells = (int64_t)g_low * g_low * g_low;
+		int64_t* low = mem.alloc<int64_t>(cells);
+		unsigned blocks = (unsigned)ceil_div(cells, 256);
+		if (level_low == level_max - 1)
+			lut_merge_kernel<uint32_t><<<blocks, 256, 0, s>>>(grid, low, level_low, g_low, max_points_per_chunk, chunks, num_chunks, capacity);
+		else
+			lut_merge_kernel<int64_t><<<blocks, 256, 0, s>>>(prev, low, level_low, g_low, max_points_per_chunk, chunks, num_chunks, capacity);
+		PCG_LAUNCHED();
+		if (prev) mem.free(prev);
+		prev = low;
+	}
+	if (prev) mem.free(prev);
+}
+
+void launch_lut_fill(const ChunkCell* chunks, int num_chunks, int grid_size, int32_t* lut, DeviceMem& mem) {
+	if (num_chunks == 0) return;
+	int level_max = bits_for((uint64_t)grid_size) - 1;
+	lut_fill_kernel<<<num_chunks, 256, 0, mem.stream()>>>(chunks, grid_size, level_max, lut);
+	PCG_LAUNCHED();
+}
+
+void launch_assign_chunks(const uint32_t* cell, const int32_t* lut, int64_t n, uint32_t* chunk_of, uint32_t* ids,
+                          int64_t* error, DeviceMem& mem) {
+	if (n == 0) return;
+	assign_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(cell, lut, n, chunk_of, ids, error);
+	PCG_LAUNCHED();
+}
+
+}  // namespace pcg

@@ -1,0 +1,58 @@
+// Host-callable launchers of the pipeline kernels (one per CUDA unit).
+#pragma once
+
+#include "dev.h"
+
+namespace pcg {
+
+// ------------------------------------------------------------- chunking.cu
+struct ChunkCell {      // one chunk found by the LUT merge
+	int32_t level, x, y, z;
+	int64_t count;
+};
+
+struct ChunkingOut {
+	int32_t* X; int32_t* Y; int32_t* Z;     // quantized positions, input order
+	uint32_t* cell;                          // count-grid cell per point
+	AttrStatsDev* stats;                     // per attribute
+	unsigned long long* histogram;           // 256 bins (classification)
+	int64_t* error;                          // [0] = first failing point + 1 (out of box), [1] = lookup failure
+};
+
+void launch_decode_count(const uint8_t* d_recs, const DecodeParams& p, uint32_t* grid, ChunkingOut& out, DeviceMem& mem);
+// Pyramid merge of the count grid (createLUT, chunker_countsort_laszip.cpp:1074-1204).
+void launch_lut_merge(const uint32_t* grid, int grid_size, int64_t max_points_per_chunk, ChunkCell* chunks,
+                      int32_t* num_chunks, int capacity, DeviceMem& mem);
+// Fills the LUT: chunk k owns cells of chunks[k] (already in chunk order).
+void launch_lut_fill(const ChunkCell* chunks, int num_chunks, int grid_size, int32_t* lut, DeviceMem& mem);
+void launch_assign_chunks(const uint32_t* cell, const int32_t* lut, int64_t n, uint32_t* chunk_of, uint32_t* ids,
+                          int64_t* error, DeviceMem& mem);
+
+// --------------------------------------------------------------- octree.cu
+struct SegmentDesc {        // one node to split with a 32^3 counting sort
+	int64_t start;           // range in the working id array
+	int64_t count;
+	int64_t coff;            // offset in the compacted round array
+	double min[3], size[3];  // node box (min, max - min)
+};
+
+struct NodeCand {           // createNodes output (indexer.cpp:732-817)
+	int32_t seg;
+	int32_t level;           // 0..5 below the segment node
+	int32_t path;            // 3 bits per level, first level in the high bits
+	int32_t pad;
+	int64_t start;           // relative to the segment start
+	int64_t count;
+};
+
+struct PosParams {
+	double scale[3], offset[3];
+};
+
+void launch_octree_round(uint32_t* ids, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParams& pp,
+                         const SegmentDesc* d_segs, int num_segs, int64_t total, NodeCand* cands, int32_t* num_cands,
+                         int64_t cand_capacity, DeviceMem& mem);
+// number of distinct (X, Y, Z) among ids[0..n)
+int64_t count_unique_positions(const uint32_t* ids, int64_t n, const int32_t* X, const int32_t* Y, const int32_t* Z, DeviceMem& mem);
+
+}  // namespace pcg

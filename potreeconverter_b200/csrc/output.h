@@ -1,0 +1,25 @@
+// Output-stage and partition launchers.
+#pragma once
+
+#include "dev.h"
+
+namespace pcg {
+
+struct PayloadItem {        // one completed node with points
+	const uint32_t* ids;
+	const uint64_t* cols;    // packed colours or null
+	int64_t count;
+	int64_t out_offset;      // in points
+};
+
+void launch_write_payloads(const uint8_t* d_recs, const DecodeParams& p, const int32_t* X, const int32_t* Y, const int32_t* Z,
+                           const PayloadItem* items, int num_items, uint8_t* out, DeviceMem& mem);
+void launch_fill_colors(const uint8_t* d_recs, int rec_len, int src_rgb, const uint32_t* ids, int64_t n, uint64_t* cols, DeviceMem& mem);
+void launch_gather_u32(const uint32_t* src, const int64_t* idx, int64_t n, uint32_t* dst, DeviceMem& mem);
+// Stable split of candidates by accepted flag: pre = exclusive prefix of the
+// flags (n + 1 entries), accepted ids (and colours) compacted in order into
+// acc_ids, rejected ids into rej_ids (skipped when rej_ids is null).
+void launch_split(const uint8_t* accepted, int64_t n, const uint32_t* ids, const uint64_t* cols, uint32_t* pre, uint32_t* acc_ids,
+                  uint64_t* acc_cols, uint32_t* rej_ids, DeviceMem& mem);
+
+}  // namespace pcg

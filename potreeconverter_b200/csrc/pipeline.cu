@@ -1,0 +1,1060 @@
+// Host orchestration of one conversion job and the C ABI (include/pcgpu.h).
+//
+// Stage map (reference files relative to the PotreeConverter source tree):
+//   decode + count grid   chunking.cu   chunker_countsort_laszip.cpp:131-361, 749-803
+//   LUT merge             chunking.cu   chunker_countsort_laszip.cpp:1074-1204
+//   stable scatter        radix.cu      chunker_countsort_laszip.cpp:837-904
+//   per-chunk octree      octree.cu     indexer.cpp:691-1109
+//   samplers              sampling.cu   sampler_poisson.h, sampler_poisson_average.h, sampler_random.h
+//   completion order      here          indexer.cpp:1581-1745 (chunks, chunk-root tasks, root)
+//   octree.bin            output.cu     indexer.cpp:1453-1516
+//   hierarchy/metadata    writers.cpp   indexer.h:120-244, HierarchyBuilder.h, indexer.cpp:354-524
+//
+// The reference hands chunks to the indexer through files; here every
+// intermediate stays in device memory and only point ids move between
+// stages. Sampling runs level by level (deepest first) over all nodes of the
+// level at once; the reference's node completion order, which fixes the
+// octree.bin layout, is recomputed on the host from the final tree.
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <fstream>
+#include <functional>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "../../include/pcgpu.h"
+#include "kernels.h"
+#include "output.h"
+#include "sampling.h"
+#include "writers.h"
+
+namespace pcg {
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+double ms_since(Clock::time_point t) { return std::chrono::duration<double, std::milli>(Clock::now() - t).count(); }
+
+constexpr int64_t kMaxNodePoints = 10'000;          // indexer.h:47
+constexpr int kChunkRootMergeThreshold = 5'000'000; // indexer.cpp:241
+
+struct TNode {
+	std::string name;
+	int parent = -1;
+	int child[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+	Vec3d min, max;
+	int depth = 0;
+	int chunk = -1;             // chunk whose subtree holds the node; -1 above chunk roots
+	bool chunk_root = false;
+	// leaf payload from the octree build: range of the working id array
+	int64_t leaf_start = 0, leaf_count = 0;
+	// current buffer (what the parent's sampler sees)
+	const uint32_t* buf_ids = nullptr;
+	const uint64_t* buf_cols = nullptr;
+	int64_t buf_count = 0;
+	// state after the parent's sampling
+	const uint32_t* fin_ids = nullptr;
+	const uint64_t* fin_cols = nullptr;
+	int64_t fin_count = 0;
+	bool completed = false;     // gets a hierarchy record
+	bool unlinked = false;      // removed from the parent's child list
+	bool has_children() const {
+		for (int c : child) if (c >= 0) return true;
+		return false;
+	}
+};
+
+struct Tree {
+	std::vector<TNode> nodes;
+	int add(const std::string& name, int parent, const Vec3d& mn, const Vec3d& mx) {
+		TNode n;
+		n.name = name;
+		n.parent = parent;
+		n.min = mn;
+		n.max = mx;
+		n.depth = (int)name.size() - 1;
+		nodes.push_back(n);
+		return (int)nodes.size() - 1;
+	}
+	int child_of(int p, int idx, int chunk) {
+		if (nodes[p].child[idx] >= 0) return nodes[p].child[idx];
+		Vec3d mn, mx;
+		child_box(nodes[p].min, nodes[p].max, idx, mn, mx);
+		int c = add(nodes[p].name + char('0' + idx), p, mn, mx);
+		nodes[c].chunk = chunk;
+		nodes[p].child[idx] = c;
+		return c;
+	}
+};
+
+std::string chunk_id(const ChunkCell& c, int grid) {  // toNodeID, chunker_countsort_laszip.cpp:82-115
+	std::string id = "r";
+	int cur = grid;
+	int lx = c.x, ly = c.y, lz = c.z;
+	for (int i = 0; i < c.level; i++) {
+		int index = 0;
+		if (lx >= cur / 2) { index += 4; lx -= cur / 2; }
+		if (ly >= cur / 2) { index += 2; ly -= cur / 2; }
+		if (lz >= cur / 2) { index += 1; lz -= cur / 2; }
+		id += char('0' + index);
+		cur /= 2;
+	}
+	return id;
+}
+
+double decode_ordered(unsigned long long k) {
+	unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+	double d;
+	memcpy(&d, &b, 8);
+	return d;
+}
+
+template <class T>
+T* upload(const std::vector<T>& v, DeviceMem& mem) {
+	T* d = mem.alloc<T>(v.size() ? v.size() : 1);
+	if (!v.empty()) PCG_CUDA(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, mem.stream()));
+	return d;
+}
+
+template <class T>
+std::vector<T> download(const T* d, size_t n, cudaStream_t s) {
+	std::vector<T> v(n);
+	if (n) PCG_CUDA(cudaMemcpyAsync(v.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+	PCG_CUDA(cudaStreamSynchronize(s));
+	return v;
+}
+
+struct JobResult {
+	std::vector<uint8_t> hierarchy;
+	std::string metadata;
+	uint8_t* octree = nullptr;  // pinned host memory
+	uint64_t octree_size = 0;
+	pcg_stats stats{};
+};
+
+struct Converter {
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	uint32_t seed = 1592614637u;
+	int form = PCG_FORM_BATCHED;
+
+	void run(const pcg_job& job, JobResult& res) {
+		auto t0 = Clock::now();
+		g_launch_count = 0;
+		PCG_CUDA(cudaSetDevice(device));
+		std::string err;
+		LasInfo info;
+		const uint8_t* las = static_cast<const uint8_t*>(job.las);
+		if (!las || !parse_las(las, job.las_size, info, err)) throw PcgError(PCG_BAD_INPUT, err.empty() ? "no input" : err);
+		Setup s;
+		if (!make_setup(info, s, err)) throw PcgError(PCG_BAD_INPUT, err);
+		if (job.method < 0 || job.method > 2) throw PcgError(PCG_BAD_INPUT, "unknown sampling method");
+		if (s.total_points < 2) throw PcgError(PCG_BAD_INPUT, "need at least two points");
+		if (s.total_points >= (int64_t(1) << 31)) throw PcgError(PCG_BAD_INPUT, "more than 2^31 points per job");
+		const int64_t N = s.total_points;
+		const int method = job.method;
+		DeviceMem mem(stream);
+		res.stats.num_points = N;
+
+		// ---------------------------------------------------------- input
+		auto t_h2d = Clock::now();
+		const int64_t rec_bytes = N * (int64_t)info.record_length;
+		uint8_t* d_recs = mem.alloc<uint8_t>(rec_bytes);
+		PCG_CUDA(cudaMemcpyAsync(d_recs, las + info.offset_to_points, rec_bytes, cudaMemcpyHostToDevice, stream));
+		PCG_CUDA(cudaStreamSynchronize(stream));
+		res.stats.ms_h2d = ms_since(t_h2d);
+
+		// ------------------------------------------------------- chunking
+		auto t_chunk = Clock::now();
+		DecodeParams p = decode_params(s);
+		const int G = s.grid_size;
+		const int64_t cells = (int64_t)G * G * G;
+		uint32_t* grid = mem.alloc<uint32_t>(cells);
+		PCG_CUDA(cudaMemsetAsync(grid, 0, cells * sizeof(uint32_t), stream));
+		ChunkingOut co;
+		co.X = mem.alloc<int32_t>(N);
+		co.Y = mem.alloc<int32_t>(N);
+		co.Z = mem.alloc<int32_t>(N);
+		co.cell = mem.alloc<uint32_t>(N);
+		std::vector<AttrStatsDev> st_init(MAX_ATTRS);
+		for (auto& a : st_init) for (int c = 0; c < 3; c++) { a.mn[c] = ~0ull; a.mx[c] = 0ull; }
+		co.stats = upload(st_init, mem);
+		co.histogram = mem.alloc<unsigned long long>(256);
+		PCG_CUDA(cudaMemsetAsync(co.histogram, 0, 256 * 8, stream));
+		co.error = mem.alloc<int64_t>(2);
+		PCG_CUDA(cudaMemsetAsync(co.error, 0, 16, stream));
+		launch_decode_count(d_recs, p, grid, co, mem);
+
+		const int chunk_cap = 1 << 20;
+		ChunkCell* d_chunks = mem.alloc<ChunkCell>(chunk_cap);
+		int32_t* d_nchunks = mem.alloc<int32_t>(1);
+		PCG_CUDA(cudaMemsetAsync(d_nchunks, 0, 4, stream));
+		launch_lut_merge(grid, G, s.max_points_per_chunk, d_chunks, d_nchunks, chunk_cap, mem);
+		auto errs = download(co.error, 2, stream);
+		if (errs[0]) throw PcgError(PCG_OUT_OF_BOX, "point " + std::to_string(errs[0] - 1) + " lies outside the header bounding box");
+		int nchunks = download(d_nchunks, 1, stream)[0];
+		if (nchunks > chunk_cap) throw PcgError(PCG_INTERNAL, "too many chunks");
+		auto cells_found = download(d_chunks, (size_t)nchunks, stream);
+		// chunk order = chunk file-name order (the oracle's sorted directory scan)
+		std::vector<std::pair<std::string, ChunkCell>> chunks;
+		for (auto& c : cells_found) chunks.push_back({chunk_id(c, G), c});
+		std::sort(chunks.begin(), chunks.end(), [](const auto& a, const auto& b) { return a.first + ".bin" < b.first + ".bin"; });
+		std::vector<ChunkCell> sorted_cells;
+		for (auto& c : chunks) sorted_cells.push_back(c.second);
+		ChunkCell* d_sorted = upload(sorted_cells, mem);
+		int32_t* lut = mem.alloc<int32_t>(cells);
+		PCG_CUDA(cudaMemsetAsync(lut, 0xff, cells * sizeof(int32_t), stream));
+		launch_lut_fill(d_sorted, nchunks, G, lut, mem);
+		uint32_t* chunk_of = mem.alloc<uint32_t>(N);
+		uint32_t* ids = mem.alloc<uint32_t>(N);
+		launch_assign_chunks(co.cell, lut, N, chunk_of, ids, co.error, mem);
+		{
+			uint32_t* kt = mem.alloc<uint32_t>(N);
+			uint32_t* vt = mem.alloc<uint32_t>(N);
+			radix_sort_pairs(chunk_of, ids, kt, vt, N, 0, std::max(1, bits_for((uint64_t)std::max(nchunks - 1, 0))), mem);
+			mem.free(kt);
+			mem.free(vt);
+		}
+		errs = download(co.error, 2, stream);
+		if (errs[1]) throw PcgError(PCG_INTERNAL, "point to chunk lookup failed");
+		mem.free(chunk_of);
+		mem.free(lut);
+		mem.free(grid);
+		mem.free(co.cell);
+		res.stats.num_chunks = nchunks;
+		res.stats.ms_chunking = ms_since(t_chunk);
+
+		// ---------------------------------------------------- octree build
+		auto t_oct = Clock::now();
+		Tree tree;
+		const Vec3d rmin = s.cube_min, rmax = s.root_max;
+		tree.add("r", -1, rmin, rmax);
+		std::vector<int> chunk_roots;
+		int64_t off = 0;
+		for (int k = 0; k < nchunks; k++) {
+			const std::string& id = chunks[k].first;
+			int cur = 0;
+			for (size_t i = 1; i < id.size(); i++) cur = tree.child_of(cur, id[i] - '0', i + 1 == id.size() ? k : -1);
+			TNode& cr = tree.nodes[cur];
+			cr.chunk = k;
+			cr.chunk_root = true;
+			cr.leaf_start = off;
+			cr.leaf_count = chunks[k].second.count;
+			off += cr.leaf_count;
+			chunk_roots.push_back(cur);
+		}
+		if (off != N) throw PcgError(PCG_INTERNAL, "chunk counts do not add up");
+		int64_t octree_depth = 0;
+		PosParams pp;
+		for (int a = 0; a < 3; a++) { pp.scale[a] = (&s.pos_scale.x)[a]; pp.offset[a] = (&s.pos_offset.x)[a]; }
+		// nodes to split this round: (node, count of the parent call for the
+		// duplicate test, indexer.cpp:1002)
+		struct Pending { int node; int64_t parent_count; };
+		std::vector<Pending> pending;
+		for (int cr : chunk_roots)
+			if (tree.nodes[cr].leaf_count >= kMaxNodePoints) pending.push_back({cr, -1});
+		NodeCand* d_cands = nullptr;
+		int32_t* d_ncands = mem.alloc<int32_t>(1);
+		int64_t cand_cap = 0;
+		while (!pending.empty()) {
+			std::vector<SegmentDesc> segs;
+			int64_t total = 0;
+			for (auto& pd : pending) {
+				TNode& n = tree.nodes[pd.node];
+				SegmentDesc d;
+				d.start = n.leaf_start;
+				d.count = n.leaf_count;
+				d.coff = total;
+				Vec3d size = n.max - n.min;
+				d.min[0] = n.min.x; d.min[1] = n.min.y; d.min[2] = n.min.z;
+				d.size[0] = size.x; d.size[1] = size.y; d.size[2] = size.z;
+				segs.push_back(d);
+				total += d.count;
+			}
+			if (total > cand_cap) {
+				if (d_cands) mem.free(d_cands);
+				cand_cap = total;
+				d_cands = mem.alloc<NodeCand>(cand_cap);
+			}
+			SegmentDesc* d_segs = upload(segs, mem);
+			PCG_CUDA(cudaMemsetAsync(d_ncands, 0, 4, stream));
+			launch_octree_round(ids, co.X, co.Y, co.Z, pp, d_segs, (int)segs.size(), total, d_cands, d_ncands, cand_cap, mem);
+			int ncand = download(d_ncands, 1, stream)[0];
+			if (ncand > cand_cap) throw PcgError(PCG_INTERNAL, "octree round overflow");
+			auto cands = download(d_cands, (size_t)ncand, stream);
+			mem.free(d_segs);
+			// deterministic handling order: by segment, then path
+			std::sort(cands.begin(), cands.end(), [](const NodeCand& a, const NodeCand& b) {
+				if (a.seg != b.seg) return a.seg < b.seg;
+				if (a.level != b.level) return a.level < b.level;
+				return a.path < b.path;
+			});
+			std::vector<Pending> next;
+			std::vector<int64_t> seg_depth(segs.size(), 0);
+			for (auto& c : cands) {
+				int sn = pending[c.seg].node;
+				int cur = sn;
+				for (int l = 0; l < c.level; l++) {
+					int digit = (c.path >> (3 * (c.level - 1 - l))) & 7;
+					cur = tree.child_of(cur, digit, tree.nodes[sn].chunk);
+				}
+				TNode& rn = tree.nodes[cur];
+				rn.leaf_start = tree.nodes[sn].leaf_start + c.start;
+				rn.leaf_count = c.count;
+				octree_depth = std::max<int64_t>(octree_depth, rn.depth);
+				if (rn.leaf_count > kMaxNodePoints) next.push_back({cur, tree.nodes[sn].leaf_count});
+			}
+			// the split node's own points now live in its children (or in the
+			// node itself when createNodes kept it whole)
+			for (auto& pd : pending) {
+				TNode& n = tree.nodes[pd.node];
+				if (n.has_children()) n.leaf_count = 0;
+			}
+			// duplicate handling for nodes that did not split
+			std::vector<Pending> refined;
+			for (auto& nx : next) {
+				TNode& sub = tree.nodes[nx.node];
+				if (sub.leaf_count == nx.parent_count) {
+					int64_t uniq = count_unique_positions(ids + sub.leaf_start, sub.leaf_count, co.X, co.Y, co.Z, mem);
+					int64_t dups = sub.leaf_count - uniq;
+					if (dups >= kMaxNodePoints / 2) {
+						// the reference keeps the first `uniq` records (indexer.cpp:1088-1090)
+						sub.leaf_count = uniq;
+					}
+				}
+				if (sub.leaf_count >= kMaxNodePoints) refined.push_back({nx.node, sub.leaf_count});
+			}
+			pending.swap(refined);
+		}
+		res.stats.octree_depth = octree_depth;
+		res.stats.ms_octree = ms_since(t_oct);
+
+		// --------------------------------------------------------- sampling
+		auto t_samp = Clock::now();
+		SampleStats* d_st = mem.alloc<SampleStats>(1);
+		PCG_CUDA(cudaMemsetAsync(d_st, 0, sizeof(SampleStats), stream));
+		PosParamsS pps;
+		for (int a = 0; a < 3; a++) { pps.scale[a] = pp.scale[a]; pps.offset[a] = pp.offset[a]; }
+		const double base_spacing = (rmax - rmin).x / 128.0;  // indexer.cpp:1603
+		const uint32_t* leaf_ids = ids;
+		uint64_t* leaf_cols = nullptr;
+		if (method == PCG_RANDOM) {
+			// every leaf is shuffled when the sampler visits it (sampler_random.h:89-121)
+			std::vector<int64_t> loff, lcnt;
+			for (auto& n : tree.nodes)
+				if (!n.has_children() && n.leaf_count > 0) { loff.push_back(n.leaf_start); lcnt.push_back(n.leaf_count); }
+			uint32_t* shuffled = mem.alloc<uint32_t>(N);
+			int32_t* scratch = mem.alloc<int32_t>(N);
+			int64_t* d_off = upload(loff, mem);
+			int64_t* d_cnt = upload(lcnt, mem);
+			launch_shuffle_leaves(d_off, d_cnt, (int)loff.size(), ids, shuffled, scratch, seed, mem);
+			leaf_ids = shuffled;
+		}
+		if (method == PCG_POISSON_AVERAGE) {
+			if (p.off_rgb < 0) throw PcgError(PCG_BAD_INPUT, "poisson_average needs an rgb attribute");
+			leaf_cols = mem.alloc<uint64_t>(N);
+			launch_fill_colors(d_recs, info.record_length, p.src_rgb, ids, N, leaf_cols, mem);
+		}
+		for (auto& n : tree.nodes) {
+			if (!n.has_children()) {
+				n.buf_ids = leaf_ids + n.leaf_start;
+				n.buf_cols = leaf_cols ? leaf_cols + n.leaf_start : nullptr;
+				n.buf_count = n.leaf_count;
+			}
+		}
+		int max_depth = 0;
+		for (auto& n : tree.nodes) max_depth = std::max(max_depth, n.depth);
+		for (int d = max_depth - 1; d >= 0; d--) {
+			std::vector<int> level_nodes;
+			for (int i = 0; i < (int)tree.nodes.size(); i++)
+				if (tree.nodes[i].depth == d && tree.nodes[i].has_children()) level_nodes.push_back(i);
+			if (level_nodes.empty()) continue;
+			sample_level(tree, level_nodes, method, base_spacing, pps, co, d_recs, p, d_st, mem, res);
+		}
+		// the root's final payload is its accepted buffer
+		TNode& root = tree.nodes[0];
+		root.fin_ids = root.buf_ids;
+		root.fin_cols = root.buf_cols;
+		root.fin_count = root.buf_count;
+		auto hst = download(d_st, 1, stream)[0];
+		if (hst.timeouts) throw PcgError(PCG_TIMEOUT, "a bounded device loop gave up");
+		res.stats.escalated_pairs = (int64_t)hst.escalated;
+		res.stats.heapsort_fallbacks = (int64_t)hst.heapsorts;
+		res.stats.ms_sampling = ms_since(t_samp);
+
+		// ------------------------------------------------ completion order
+		auto t_out = Clock::now();
+		std::vector<int> order = completion_order(tree, chunk_roots, method);
+		std::vector<HierRecord> recs;
+		std::vector<PayloadItem> items;
+		int64_t out_points = 0;
+		for (int ni : order) {
+			TNode& n = tree.nodes[ni];
+			HierRecord r;
+			r.name = n.name;
+			r.num_points = n.fin_count;
+			if (n.fin_count > 0) {
+				r.byte_offset = out_points * s.bpp;
+				r.byte_size = n.fin_count * s.bpp;
+				items.push_back({n.fin_ids, n.fin_cols, n.fin_count, out_points});
+				out_points += n.fin_count;
+			}
+			recs.push_back(r);
+		}
+		uint8_t* d_out = mem.alloc<uint8_t>(out_points * s.bpp);
+		PayloadItem* d_items = upload(items, mem);
+		launch_write_payloads(d_recs, p, co.X, co.Y, co.Z, d_items, (int)items.size(), d_out, mem);
+		PCG_CUDA(cudaStreamSynchronize(stream));
+		res.stats.ms_output = ms_since(t_out);
+		auto t_d2h = Clock::now();
+		res.octree_size = (uint64_t)(out_points * s.bpp);
+		PCG_CUDA(cudaMallocHost((void**)&res.octree, res.octree_size ? res.octree_size : 1));
+		if (res.octree_size) PCG_CUDA(cudaMemcpyAsync(res.octree, d_out, res.octree_size, cudaMemcpyDeviceToHost, stream));
+		auto stats_dev = download(co.stats, MAX_ATTRS, stream);
+		auto hist = download(co.histogram, 256, stream);
+		res.stats.ms_d2h = ms_since(t_d2h);
+
+		// ---------------------------------------------------- host writers
+		auto t_w = Clock::now();
+		int64_t first_chunk = 0;
+		if (!build_hierarchy(recs, res.hierarchy, first_chunk, err)) throw PcgError(PCG_INTERNAL, err);
+		std::vector<AttrStats> astats(s.attrs.size());
+		for (size_t i = 0; i < s.attrs.size(); i++) {
+			const auto& sd = stats_dev[i];
+			astats[i].min = {decode_ordered(sd.mn[0]), decode_ordered(sd.mn[1]), decode_ordered(sd.mn[2])};
+			astats[i].max = {decode_ordered(sd.mx[0]), decode_ordered(sd.mx[1]), decode_ordered(sd.mx[2])};
+			astats[i].histogram.assign(256, 0);
+			if (s.attrs[i].kind == AK_CLASSIFICATION)
+				for (int k = 0; k < 256; k++) astats[i].histogram[k] = (int64_t)hist[k];
+		}
+		res.metadata = build_metadata(job.name ? job.name : "", job.projection ? job.projection : "", N, first_chunk, octree_depth, s,
+		                              astats, base_spacing);
+		res.stats.ms_host_writers = ms_since(t_w);
+		res.stats.num_nodes = (int64_t)recs.size();
+		res.stats.output_points = out_points;
+		res.stats.gpu_launches = g_launch_count;
+		res.stats.ms_total = ms_since(t0);
+	}
+
+	static DecodeParams decode_params(const Setup& s) {
+		DecodeParams p{};
+		const LasInfo& L = s.las;
+		for (int a = 0; a < 3; a++) {
+			p.in_scale[a] = (&L.scale.x)[a];
+			p.in_offset[a] = (&L.offset.x)[a];
+			p.pos_scale[a] = (&s.pos_scale.x)[a];
+			p.pos_offset[a] = (&s.pos_offset.x)[a];
+			p.cmin[a] = (&s.cube_min.x)[a];
+		}
+		p.csize = s.chunk_cube_size;
+		p.n = s.total_points;
+		p.rec_len = L.record_length;
+		p.pdrf = L.pdrf;
+		p.bpp = s.bpp;
+		p.grid = s.grid_size;
+		p.off_intensity = p.off_retnum = p.off_nret = p.off_class = p.off_sar = p.off_user = p.off_psid = p.off_gps = p.off_rgb = -1;
+		p.stat_intensity = p.stat_retnum = p.stat_nret = p.stat_class = p.stat_sar = p.stat_user = p.stat_psid = p.stat_gps = p.stat_rgb = -1;
+		p.src_gps = 20;
+		p.src_rgb = (L.pdrf == 2) ? 20 : 28;
+		p.n_extra = 0;
+		for (int i = 0; i < (int)s.attrs.size(); i++) {
+			const AttrDesc& a = s.attrs[i];
+			switch (a.kind) {
+			case AK_POSITION: p.stat_pos = i; break;
+			case AK_INTENSITY: p.off_intensity = a.out_offset; p.stat_intensity = i; break;
+			case AK_RETURN_NUMBER: p.off_retnum = a.out_offset; p.stat_retnum = i; break;
+			case AK_NUMBER_OF_RETURNS: p.off_nret = a.out_offset; p.stat_nret = i; break;
+			case AK_CLASSIFICATION: p.off_class = a.out_offset; p.stat_class = i; break;
+			case AK_SCAN_ANGLE_RANK: p.off_sar = a.out_offset; p.stat_sar = i; break;
+			case AK_USER_DATA: p.off_user = a.out_offset; p.stat_user = i; break;
+			case AK_POINT_SOURCE_ID: p.off_psid = a.out_offset; p.stat_psid = i; break;
+			case AK_GPS_TIME: p.off_gps = a.out_offset; p.stat_gps = i; break;
+			case AK_RGB: p.off_rgb = a.out_offset; p.stat_rgb = i; break;
+			default: {
+				if (p.n_extra >= MAX_EXTRA) throw PcgError(PCG_BAD_INPUT, "too many extra attributes");
+				ExtraDesc& e = p.extra[p.n_extra++];
+				e.src_off = a.src_offset;
+				e.dst_off = a.out_offset;
+				e.size = a.size;
+				e.type = (int)a.type;
+				e.num_elements = a.numElements;
+				e.element_size = a.elementSize;
+				e.stat_index = i;
+				e.pad = 0;
+			}
+			}
+		}
+		if ((int)s.attrs.size() > MAX_ATTRS) throw PcgError(PCG_BAD_INPUT, "too many attributes");
+		return p;
+	}
+
+	void sample_level(Tree& tree, const std::vector<int>& level_nodes, int method, double base_spacing, const PosParamsS& pps,
+	                  const ChunkingOut& co, const uint8_t* d_recs, const DecodeParams& p, SampleStats* d_st, DeviceMem& mem,
+	                  JobResult& res) {
+		(void)d_recs;
+		(void)p;
+		(void)res;
+		const int K = (int)level_nodes.size();
+		std::vector<LevelNode> ln(K);
+		std::vector<GatherItem> items;
+		struct ChildSlot { int node; int64_t start, count; };
+		std::vector<ChildSlot> child_slots;  // per (node, child) in gather order
+		int64_t M = 0, H = 0;
+		for (int k = 0; k < K; k++) {
+			TNode& n = tree.nodes[level_nodes[k]];
+			LevelNode& l = ln[k];
+			l.cand_off = M;
+			for (int c = 0; c < 8; c++) {
+				int ci = n.child[c];
+				if (ci < 0) continue;
+				TNode& ch = tree.nodes[ci];
+				if (ch.buf_count > 0) items.push_back({ch.buf_ids, ch.buf_cols, M, ch.buf_count, c, k});
+				child_slots.push_back({ci, M, ch.buf_count});
+				M += ch.buf_count;
+			}
+			l.count = M - l.cand_off;
+			int64_t cap = 64;
+			while (cap < 2 * l.count) cap <<= 1;
+			l.hash_off = H;
+			l.hash_cap = cap;
+			H += cap;
+			l.min[0] = n.min.x; l.min[1] = n.min.y; l.min[2] = n.min.z;
+			l.max[0] = n.max.x; l.max[1] = n.max.y; l.max[2] = n.max.z;
+			l.level = n.depth;
+			l.spacing = base_spacing / std::pow(2.0, (double)n.depth);  // sampler_poisson.h:114
+			l.pad = 0;
+		}
+		cudaStream_t s = stream;
+		LevelBuffers lb;
+		lb.M = M;
+		lb.K = K;
+		lb.ids = mem.alloc<uint32_t>(M);
+		lb.cols = method == PCG_POISSON_AVERAGE ? mem.alloc<uint64_t>(M) : nullptr;
+		lb.child = mem.alloc<uint8_t>(M);
+		lb.node_of = mem.alloc<int32_t>(M);
+		lb.count_in_child = mem.alloc<int32_t>(M);
+		lb.accepted = mem.alloc<uint8_t>(M);
+		LevelNode* d_nodes = upload(ln, mem);
+		GatherItem* d_items = upload(items, mem);
+		launch_gather(d_items, (int)items.size(), lb, mem);
+		// node order for the warp-per-node kernels: largest first
+		std::vector<int32_t> order(K);
+		for (int k = 0; k < K; k++) order[k] = k;
+		std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ln[a].count > ln[b].count; });
+		int32_t* d_order = upload(order, mem);
+		uint64_t* hkeys = mem.alloc<uint64_t>(H);
+		int32_t* hvals = mem.alloc<int32_t>(H);
+		if (method == PCG_RANDOM) {
+			launch_random_accept_sized(d_nodes, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, H, d_st, mem);
+		} else {
+			lb.keys = mem.alloc<double>(M);
+			lb.perm = mem.alloc<int32_t>(M);
+			lb.pos = mem.alloc<int32_t>(M);
+			lb.acc_rank = mem.alloc<int32_t>(M);
+			launch_keys(d_nodes, co.X, co.Y, co.Z, pps, lb, mem);
+			double* axyz = mem.alloc<double>(3 * M);
+			double* akey = mem.alloc<double>(M);
+			int32_t* anext = mem.alloc<int32_t>(M);
+			int32_t* apos = mem.alloc<int32_t>(M);
+			const int mode = method == PCG_POISSON ? 0 : 1;
+			const bool guard = form == PCG_FORM_BATCHED;
+			if (form == PCG_FORM_PLAIN) {
+				for (int k = 0; k < K; k++) {
+					launch_node_sort(d_nodes, d_order, K, lb, d_st, mem, k, k + 1);
+					launch_greedy(mode, false, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, k, k + 1);
+				}
+			} else {
+				launch_node_sort(d_nodes, d_order, K, lb, d_st, mem);
+				launch_greedy(mode, guard, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem);
+			}
+			if (method == PCG_POISSON_AVERAGE) {
+				long long* sums = mem.alloc<long long>(4 * M);
+				launch_average_colors(d_nodes, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, anext, apos, nullptr, sums, mem);
+				mem.free(sums);
+			}
+			mem.free(axyz); mem.free(akey); mem.free(anext); mem.free(apos);
+			mem.free(lb.keys); mem.free(lb.perm); mem.free(lb.pos); mem.free(lb.acc_rank);
+		}
+		mem.free(hkeys);
+		mem.free(hvals);
+		// split candidates into the parents' buffers and the children's payloads
+		uint32_t* pre = mem.alloc<uint32_t>(M + 1);
+		uint32_t* acc_ids = mem.alloc<uint32_t>(M);
+		uint64_t* acc_cols = lb.cols ? mem.alloc<uint64_t>(M) : nullptr;
+		uint32_t* rej_ids = method == PCG_POISSON_AVERAGE ? nullptr : mem.alloc<uint32_t>(M);
+		launch_split(lb.accepted, M, lb.ids, lb.cols, pre, acc_ids, acc_cols, rej_ids, mem);
+		// prefix values at node and child boundaries
+		std::vector<int64_t> bidx;
+		for (int k = 0; k < K; k++) { bidx.push_back(ln[k].cand_off); bidx.push_back(ln[k].cand_off + ln[k].count); }
+		for (auto& cs : child_slots) { bidx.push_back(cs.start); bidx.push_back(cs.start + cs.count); }
+		int64_t* d_bidx = upload(bidx, mem);
+		uint32_t* d_bval = mem.alloc<uint32_t>(bidx.size());
+		launch_gather_u32(pre, d_bidx, (int64_t)bidx.size(), d_bval, mem);
+		auto bval = download(d_bval, bidx.size(), s);
+		// parents
+		for (int k = 0; k < K; k++) {
+			TNode& n = tree.nodes[level_nodes[k]];
+			uint32_t a0 = bval[2 * k], a1 = bval[2 * k + 1];
+			n.buf_ids = acc_ids + a0;
+			n.buf_cols = acc_cols ? acc_cols + a0 : nullptr;
+			n.buf_count = (int64_t)(a1 - a0);
+		}
+		// children (sampler_poisson.h:247-291, sampler_poisson_average.h:418-475, sampler_random.h:184-225)
+		size_t base = 2 * (size_t)K;
+		for (size_t i = 0; i < child_slots.size(); i++) {
+			const ChildSlot& cs = child_slots[i];
+			TNode& ch = tree.nodes[cs.node];
+			uint32_t a0 = bval[base + 2 * i], a1 = bval[base + 2 * i + 1];
+			int64_t accepted = (int64_t)(a1 - a0);
+			int64_t rejected = cs.count - accepted;
+			if (method == PCG_POISSON_AVERAGE) {
+				if (rejected == 0) {
+					ch.unlinked = true;  // dropped, never completed (:465-466)
+				} else {
+					ch.completed = true;
+					ch.fin_ids = lb.ids + cs.start;
+					ch.fin_cols = lb.cols + cs.start;
+					ch.fin_count = cs.count;  // the child keeps all of its points
+				}
+			} else {
+				ch.completed = true;
+				if (rejected == 0) {
+					if (!ch.has_children()) ch.unlinked = true;
+					ch.fin_count = 0;
+				} else {
+					ch.fin_ids = rej_ids + (cs.start - a0);
+					ch.fin_cols = nullptr;
+					ch.fin_count = rejected;
+				}
+			}
+		}
+		mem.free(d_bidx);
+		mem.free(d_bval);
+		mem.free(pre);
+		mem.free(d_nodes);
+		mem.free(d_items);
+		mem.free(d_order);
+		mem.free(lb.child);
+		mem.free(lb.node_of);
+		mem.free(lb.count_in_child);
+		mem.free(lb.accepted);
+		if (method != PCG_POISSON_AVERAGE) mem.free(lb.ids);
+	}
+
+	// The single-threaded reference's completion order (doIndexing,
+	// indexer.cpp:1639-1745): chunks in file-name order, each sampled in
+	// post-order; then the merged chunk-root tasks (processChunkRoots,
+	// :202-281) in pre-order; then the root.
+	static std::vector<int> completion_order(Tree& tree, const std::vector<int>& chunk_roots, int method) {
+		std::vector<int> order;
+		std::vector<char> sampled(tree.nodes.size(), 0);
+		std::vector<char> cleared(tree.nodes.size(), 0);  // children.clear() was called
+		auto complete_children = [&](int ni) {
+			const TNode& n = tree.nodes[ni];
+			for (int c = 0; c < 8; c++) {
+				int ci = n.child[c];
+				if (ci < 0) continue;
+				const TNode& ch = tree.nodes[ci];
+				if (method == PCG_POISSON_AVERAGE && ch.unlinked) continue;
+				order.push_back(ci);
+			}
+		};
+		std::function<void(int)> post = [&](int ni) {
+			if (!cleared[ni]) {
+				for (int c = 0; c < 8; c++) {
+					int ci = tree.nodes[ni].child[c];
+					if (ci >= 0 && !sampled[ci]) post(ci);
+				}
+			}
+			sampled[ni] = 1;
+			if (!cleared[ni] && tree.nodes[ni].has_children()) complete_children(ni);
+		};
+		for (int cr : chunk_roots) {
+			post(cr);
+			cleared[cr] = 1;
+		}
+		// chunk-root tasks
+		struct CR { int node; std::vector<int> kids; std::vector<int> fcrs; int num_points = 0; bool cleared = false; };
+		std::vector<CR> crs;
+		std::unordered_map<int, int> cr_of;
+		std::function<void(int)> build = [&](int ni) {
+			int me = (int)crs.size();
+			crs.push_back(CR{ni, {}, {}, 0, false});
+			cr_of[ni] = me;
+			if (cleared[ni]) return;
+			for (int c = 0; c < 8; c++) {
+				int ci = tree.nodes[ni].child[c];
+				if (ci >= 0) {
+					build(ci);
+					crs[me].kids.push_back(cr_of[ci]);
+				}
+			}
+		};
+		build(0);
+		for (int cr : chunk_roots) {
+			auto it = cr_of.find(cr);
+			if (it == cr_of.end()) continue;
+			crs[it->second].fcrs.push_back(cr);
+			// numPoints of the chunk root after its chunk was sampled
+			crs[it->second].num_points += (int)tree.nodes[cr].buf_count;
+		}
+		std::function<void(int)> merge = [&](int ci) {
+			CR& c = crs[ci];
+			for (int k : c.kids) merge(k);
+			if (c.kids.empty()) return;
+			int np = 0;
+			for (int k : crs[ci].kids) np += crs[k].num_points;
+			crs[ci].num_points = np;
+			if (np < kChunkRootMergeThreshold) {
+				std::vector<int> f = crs[ci].fcrs;
+				for (int k : crs[ci].kids) f.insert(f.end(), crs[k].fcrs.begin(), crs[k].fcrs.end());
+				crs[ci].fcrs = f;
+				crs[ci].kids.clear();
+			}
+		};
+		merge(0);
+		std::vector<int> tasks;
+		std::function<void(int)> pre = [&](int ci) {
+			if (!crs[ci].fcrs.empty()) tasks.push_back(crs[ci].node);
+			for (int k : crs[ci].kids) pre(k);
+		};
+		pre(0);
+		for (int t : tasks) {
+			post(t);
+			cleared[t] = 1;
+		}
+		if (!sampled[0]) post(0);
+		order.push_back(0);
+		return order;
+	}
+};
+
+}  // namespace
+
+}  // namespace pcg
+
+// ====================================================================== C ABI
+
+struct pcg_ctx {
+	pcg::Converter conv;
+	std::mutex mtx;
+	std::string last_error;
+	// request loop
+	struct Job {
+		uint64_t id;
+		std::vector<uint8_t> las;
+		std::string name, projection;
+		int32_t method;
+		bool done = false;
+		pcg_status status = PCG_OK;
+		std::string error;
+		pcg::JobResult result;
+		size_t footprint = 0;
+	};
+	std::mutex qmtx;
+	std::condition_variable qcv;
+	std::deque<std::shared_ptr<Job>> queue;
+	std::unordered_map<uint64_t, std::shared_ptr<Job>> jobs;
+	std::vector<std::thread> workers;
+	std::vector<cudaStream_t> worker_streams;
+	size_t budget = 0, in_use = 0;
+	uint64_t next_id = 1;
+	bool stopping = false;
+};
+
+namespace {
+
+pcg_status fail(pcg_ctx* ctx, pcg_status st, const std::string& msg) {
+	if (ctx) ctx->last_error = msg;
+	return st;
+}
+
+template <class F>
+pcg_status guarded(pcg_ctx* ctx, F&& f) {
+	try {
+		f();
+		return PCG_OK;
+	} catch (const pcg::PcgError& e) {
+		return fail(ctx, (pcg_status)e.status, e.what());
+	} catch (const pcg::CudaError& e) {
+		cudaGetLastError();
+		return fail(ctx, e.code == cudaErrorMemoryAllocation ? PCG_OOM : PCG_CUDA, e.what());
+	} catch (const std::bad_alloc&) {
+		return fail(ctx, PCG_OOM, "host allocation failed");
+	} catch (const std::exception& e) {
+		return fail(ctx, PCG_INTERNAL, e.what());
+	}
+}
+
+void move_result(pcg::JobResult& r, pcg_result* out) {
+	memset(out, 0, sizeof(*out));
+	out->octree = r.octree;
+	out->octree_size = r.octree_size;
+	r.octree = nullptr;
+	out->hierarchy = (uint8_t*)malloc(r.hierarchy.size() + 1);
+	if (!r.hierarchy.empty()) memcpy(out->hierarchy, r.hierarchy.data(), r.hierarchy.size());
+	out->hierarchy_size = r.hierarchy.size();
+	out->metadata = (char*)malloc(r.metadata.size() + 1);
+	memcpy(out->metadata, r.metadata.data(), r.metadata.size());
+	out->metadata[r.metadata.size()] = 0;
+	out->metadata_size = r.metadata.size();
+	out->stats = r.stats;
+}
+
+size_t estimate_footprint(const pcg_job& job) {
+	// point records + positions/ids/keys per point, plus headroom
+	return (size_t)job.las_size * 3 + (size_t)(job.las_size / 20) * 64 + (size_t(64) << 20);
+}
+
+void worker_main(pcg_ctx* ctx, int wi) {
+	pcg::Converter conv = ctx->conv;
+	conv.stream = ctx->worker_streams[wi];
+	while (true) {
+		std::shared_ptr<pcg_ctx::Job> job;
+		{
+			std::unique_lock<std::mutex> lk(ctx->qmtx);
+			ctx->qcv.wait(lk, [&] {
+				if (ctx->stopping) return true;
+				return !ctx->queue.empty() && (ctx->in_use == 0 || ctx->in_use + ctx->queue.front()->footprint <= ctx->budget);
+			});
+			if (ctx->stopping && ctx->queue.empty()) return;
+			if (ctx->queue.empty()) continue;
+			job = ctx->queue.front();
+			ctx->queue.pop_front();
+			ctx->in_use += job->footprint;
+		}
+		pcg_job pj{};
+		pj.las = job->las.data();
+		pj.las_size = job->las.size();
+		pj.method = job->method;
+		pj.name = job->name.c_str();
+		pj.projection = job->projection.c_str();
+		std::string err;
+		pcg_status st = PCG_OK;
+		try {
+			conv.run(pj, job->result);
+		} catch (const pcg::PcgError& e) {
+			st = (pcg_status)e.status; err = e.what();
+		} catch (const pcg::CudaError& e) {
+			cudaGetLastError(); st = PCG_CUDA; err = e.what();
+		} catch (const std::exception& e) {
+			st = PCG_INTERNAL; err = e.what();
+		}
+		{
+			std::lock_guard<std::mutex> lk(ctx->qmtx);
+			job->status = st;
+			job->error = err;
+			job->done = true;
+			ctx->in_use -= job->footprint;
+		}
+		ctx->qcv.notify_all();
+	}
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pcg_status_string(pcg_status s) {
+	switch (s) {
+	case PCG_OK: return "ok";
+	case PCG_BAD_INPUT: return "bad input";
+	case PCG_OUT_OF_BOX: return "point outside bounding box";
+	case PCG_OOM: return "out of memory";
+	case PCG_TIMEOUT: return "timeout";
+	case PCG_INTERNAL: return "internal error";
+	case PCG_CUDA: return "cuda error";
+	case PCG_NOT_FOUND: return "not found";
+	}
+	return "unknown";
+}
+
+pcg_status pcg_create(pcg_ctx** out, const pcg_opts* opts) {
+	if (!out) return PCG_BAD_INPUT;
+	*out = nullptr;
+	pcg_ctx* ctx = new (std::nothrow) pcg_ctx();
+	if (!ctx) return PCG_OOM;
+	pcg_status st = guarded(ctx, [&] {
+		if (opts) {
+			ctx->conv.device = opts->device;
+			ctx->conv.seed = opts->random_seed;
+			ctx->conv.form = opts->form;
+		}
+		int n = 0;
+		PCG_CUDA(cudaGetDeviceCount(&n));
+		if (ctx->conv.device < 0 || ctx->conv.device >= n) throw pcg::PcgError(PCG_BAD_INPUT, "no such CUDA device");
+		PCG_CUDA(cudaSetDevice(ctx->conv.device));
+		PCG_CUDA(cudaStreamCreateWithFlags(&ctx->conv.stream, cudaStreamNonBlocking));
+		cudaMemPool_t pool;
+		PCG_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctx->conv.device));
+		uint64_t threshold = UINT64_MAX;
+		PCG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+	});
+	if (st != PCG_OK) {
+		fprintf(stderr, "pcg_create: %s\n", ctx->last_error.c_str());
+		delete ctx;
+		return st;
+	}
+	*out = ctx;
+	return PCG_OK;
+}
+
+void pcg_destroy(pcg_ctx* ctx) {
+	if (!ctx) return;
+	{
+		std::lock_guard<std::mutex> lk(ctx->qmtx);
+		ctx->stopping = true;
+	}
+	ctx->qcv.notify_all();
+	for (auto& t : ctx->workers) t.join();
+	for (auto& kv : ctx->jobs) if (kv.second->result.octree) cudaFreeHost(kv.second->result.octree);
+	cudaSetDevice(ctx->conv.device);
+	for (auto s : ctx->worker_streams) cudaStreamDestroy(s);
+	if (ctx->conv.stream) {
+		cudaStreamSynchronize(ctx->conv.stream);
+		cudaStreamDestroy(ctx->conv.stream);
+	}
+	delete ctx;
+}
+
+const char* pcg_last_error(const pcg_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+
+pcg_status pcg_convert(pcg_ctx* ctx, const pcg_job* job, pcg_result* out) {
+	if (!ctx || !job || !out) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->mtx);
+	memset(out, 0, sizeof(*out));
+	pcg::JobResult r;
+	pcg_status st = guarded(ctx, [&] { ctx->conv.run(*job, r); });
+	if (st != PCG_OK) {
+		if (r.octree) cudaFreeHost(r.octree);
+		return st;
+	}
+	move_result(r, out);
+	return PCG_OK;
+}
+
+void pcg_result_free(pcg_result* r) {
+	if (!r) return;
+	if (r->octree) cudaFreeHost(r->octree);
+	free(r->hierarchy);
+	free(r->metadata);
+	memset(r, 0, sizeof(*r));
+}
+
+pcg_status pcg_write_files(const pcg_result* r, const char* dir) {
+	if (!r || !dir) return PCG_BAD_INPUT;
+	auto wr = [&](const char* name, const void* data, uint64_t size) {
+		std::ofstream f(std::string(dir) + "/" + name, std::ios::binary);
+		if (!f) return false;
+		f.write((const char*)data, (std::streamsize)size);
+		return (bool)f;
+	};
+	if (!wr("octree.bin", r->octree, r->octree_size)) return PCG_BAD_INPUT;
+	if (!wr("hierarchy.bin", r->hierarchy, r->hierarchy_size)) return PCG_BAD_INPUT;
+	if (!wr("metadata.json", r->metadata, r->metadata_size)) return PCG_BAD_INPUT;
+	return PCG_OK;
+}
+
+pcg_status pcg_submit(pcg_ctx* ctx, const pcg_job* job, uint64_t* job_id) {
+	if (!ctx || !job || !job_id || !job->las) return PCG_BAD_INPUT;
+	return guarded(ctx, [&] {
+		std::lock_guard<std::mutex> lk(ctx->qmtx);
+		if (ctx->workers.empty()) {
+			size_t free_b = 0, total_b = 0;
+			PCG_CUDA(cudaSetDevice(ctx->conv.device));
+			PCG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+			ctx->budget = (size_t)(free_b * 0.8);
+			const int nworkers = 4;
+			for (int i = 0; i < nworkers; i++) {
+				cudaStream_t s;
+				PCG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+				ctx->worker_streams.push_back(s);
+			}
+			for (int i = 0; i < nworkers; i++) ctx->workers.emplace_back(worker_main, ctx, i);
+		}
+		auto j = std::make_shared<pcg_ctx::Job>();
+		j->id = ctx->next_id++;
+		j->las.assign((const uint8_t*)job->las, (const uint8_t*)job->las + job->las_size);
+		j->name = job->name ? job->name : "";
+		j->projection = job->projection ? job->projection : "";
+		j->method = job->method;
+		j->footprint = estimate_footprint(*job);
+		ctx->jobs[j->id] = j;
+		ctx->queue.push_back(j);
+		*job_id = j->id;
+		ctx->qcv.notify_all();
+	});
+}
+
+pcg_status pcg_poll(pcg_ctx* ctx, uint64_t job_id, int32_t* done) {
+	if (!ctx || !done) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->qmtx);
+	auto it = ctx->jobs.find(job_id);
+	if (it == ctx->jobs.end()) return PCG_NOT_FOUND;
+	*done = it->second->done ? 1 : 0;
+	return PCG_OK;
+}
+
+pcg_status pcg_wait(pcg_ctx* ctx, uint64_t job_id, pcg_result* out) {
+	if (!ctx || !out) return PCG_BAD_INPUT;
+	std::shared_ptr<pcg_ctx::Job> j;
+	{
+		std::unique_lock<std::mutex> lk(ctx->qmtx);
+		auto it = ctx->jobs.find(job_id);
+		if (it == ctx->jobs.end()) return PCG_NOT_FOUND;
+		j = it->second;
+		ctx->qcv.wait(lk, [&] { return j->done; });
+		ctx->jobs.erase(job_id);
+	}
+	memset(out, 0, sizeof(*out));
+	if (j->status != PCG_OK) {
+		ctx->last_error = j->error;
+		return j->status;
+	}
+	move_result(j->result, out);
+	return PCG_OK;
+}
+
+pcg_status pcg_kernel_sort_keys(pcg_ctx* ctx, const double* keys, int64_t n, int32_t* perm_out) {
+	if (!ctx || (n > 0 && (!keys || !perm_out)) || n < 0 || n >= (int64_t(1) << 31)) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->mtx);
+	return guarded(ctx, [&] {
+		if (n == 0) return;
+		PCG_CUDA(cudaSetDevice(ctx->conv.device));
+		pcg::DeviceMem mem(ctx->conv.stream);
+		double* dk = mem.alloc<double>(n);
+		int32_t* dv = mem.alloc<int32_t>(n);
+		pcg::SampleStats* st = mem.alloc<pcg::SampleStats>(1);
+		PCG_CUDA(cudaMemsetAsync(st, 0, sizeof(pcg::SampleStats), mem.stream()));
+		PCG_CUDA(cudaMemcpyAsync(dk, keys, n * sizeof(double), cudaMemcpyHostToDevice, mem.stream()));
+		std::vector<int32_t> iota(n);
+		for (int64_t i = 0; i < n; i++) iota[i] = (int32_t)i;
+		PCG_CUDA(cudaMemcpyAsync(dv, iota.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, mem.stream()));
+		pcg::launch_sort_keys_single(dk, dv, n, mem, st);
+		PCG_CUDA(cudaMemcpyAsync(perm_out, dv, n * sizeof(int32_t), cudaMemcpyDeviceToHost, mem.stream()));
+		PCG_CUDA(cudaStreamSynchronize(mem.stream()));
+	});
+}
+
+pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* perm_out) {
+	if (!ctx || n < 0 || (n > 0 && !perm_out) || n >= (int64_t(1) << 31)) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->mtx);
+	return guarded(ctx, [&] {
+		if (n == 0) return;
+		PCG_CUDA(cudaSetDevice(ctx->conv.device));
+		pcg::DeviceMem mem(ctx->conv.stream);
+		int32_t* dp = mem.alloc<int32_t>(n);
+		pcg::launch_shuffle_single(n, seed, dp, mem);
+		PCG_CUDA(cudaMemcpyAsync(perm_out, dp, n * sizeof(int32_t), cudaMemcpyDeviceToHost, mem.stream()));
+		PCG_CUDA(cudaStreamSynchronize(mem.stream()));
+	});
+}
+
+}  // extern "C"

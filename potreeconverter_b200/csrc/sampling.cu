@@ -1,0 +1,826 @@
+// Sampler kernels. One launch covers one octree level across all of its
+// inner nodes (the batched form) or a single node (the plain form).
+//
+//  * node_sort_kernel   -- std::sort of the candidates by FP64 squared
+//    distance to the node centre (sampler_poisson.h:183-203), reproduced
+//    element for element: the libstdc++ introsort partitions are replayed by
+//    one warp per node. Hoare's pairing of the k-th left stop with the k-th
+//    right stop is computed from stop ranks (ballot/popc), so a partition is
+//    two coalesced passes instead of a sequential two-pointer walk; the final
+//    insertion sort is a stable sort of each <=16-element block.
+//  * greedy_kernel      -- the sequential acceptance scan of
+//    sampler_poisson.h:133-245 (and the grid variant of
+//    sampler_poisson_average.h:184-281), one warp per node, 32 candidates
+//    per step. Each lane looks up conflicts among the already accepted
+//    points through a per-node spatial hash (cells of two spacings, so 8
+//    cells cover the spacing ball), conflicts inside the step come from
+//    lane shuffles, and the 32 decisions are resolved in order. The
+//    reference's early exit (accepted points closer to the centre than
+//    |c| - s stop the scan) and its 10,001-check cap become two static
+//    conditions on a conflicting accepted point a of candidate p:
+//    key(a) >= (sqrt(key(p)) - s)^2, and at most 10,000 points accepted
+//    after a. Together they give exactly the reference's decision.
+//  * average_colors     -- poisson_average's colour sums
+//    (sampler_poisson_average.h:357-416) in closed form: every rejected
+//    candidate adds its colour to each accepted point within the spacing,
+//    doubled when it precedes that point in sorted order (the reference
+//    doubles an accepted point's running sum when its own turn comes), and
+//    every accepted point adds twice its own colour.
+//  * random_accept      -- sampler_random.h:146-178: a point is accepted if
+//    its child holds < 100 points, or if it is the first point of its
+//    128^3 cell that is eligible; first-eligible is an atomicMin per cell.
+//  * shuffle_leaves     -- std::shuffle(..., std::default_random_engine(seed))
+//    of sampler_random.h:97-118, libstdc++'s two-draws-per-call variant.
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "sampling.h"
+
+namespace pcg {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr uint64_t EMPTY_KEY = ~0ull;
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+	uint32_t m;
+	asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+	return m;
+}
+
+// ---------------------------------------------------------------- gather
+__global__ void gather_kernel(const GatherItem* __restrict__ items, LevelBuffers lb) {
+	const GatherItem it = items[blockIdx.x];
+	for (int64_t t = threadIdx.x; t < it.count; t += blockDim.x) {
+		int64_t j = it.dst_off + t;
+		lb.ids[j] = it.src_ids[t];
+		if (lb.cols) lb.cols[j] = it.src_cols ? it.src_cols[t] : 0ull;
+		lb.child[j] = (uint8_t)it.child;
+		lb.node_of[j] = it.node;
+		lb.count_in_child[j] = (int32_t)it.count;
+	}
+}
+
+__device__ __forceinline__ void point_xyz(const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp, uint32_t id,
+                                          double& x, double& y, double& z) {
+	// (xyz[0] * scale.x) + offset.x, sampler_poisson.h:99-101
+	x = ((double)X[id] * pp.scale[0]) + pp.offset[0];
+	y = ((double)Y[id] * pp.scale[1]) + pp.offset[1];
+	z = ((double)Z[id] * pp.scale[2]) + pp.offset[2];
+}
+
+__global__ void keys_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
+                            const int32_t* __restrict__ Z, PosParamsS pp, LevelBuffers lb) {
+	int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const LevelNode& nd = nodes[lb.node_of[j]];
+	double x, y, z;
+	point_xyz(X, Y, Z, pp, lb.ids[j], x, y, z);
+	// center = (min + max) * 0.5 (sampler_poisson.h:127)
+	double cx = (nd.min[0] + nd.max[0]) * 0.5, cy = (nd.min[1] + nd.max[1]) * 0.5, cz = (nd.min[2] + nd.max[2]) * 0.5;
+	double ax = x - cx, ay = y - cy, az = z - cz;
+	lb.keys[j] = ax * ax + ay * ay + az * az;
+	lb.perm[j] = (int32_t)(j - nd.cand_off);
+}
+
+// ------------------------------------------------------ std::sort replay
+struct SortScratch {
+	int32_t* SL;   // [M] left stop positions
+	int32_t* SR;   // [M] right stop positions
+	int32_t* blk;  // [2M] final blocks (start, end)
+};
+
+__device__ void heap_adjust(double* key, int32_t* val, int64_t hole, int64_t len, double vk, int32_t vv) {
+	// std::__adjust_heap followed by std::__push_heap (stl_heap.h)
+	const int64_t top = hole;
+	int64_t second = hole;
+	while (second < (len - 1) / 2) {
+		second = 2 * (second + 1);
+		if (key[second] < key[second - 1]) second--;
+		key[hole] = key[second];
+		val[hole] = val[second];
+		hole = second;
+	}
+	if ((len & 1) == 0 && second == (len - 2) / 2) {
+		second = 2 * (second + 1);
+		key[hole] = key[second - 1];
+		val[hole] = val[second - 1];
+		hole = second - 1;
+	}
+	int64_t parent = (hole - 1) / 2;
+	while (hole > top && key[parent] < vk) {
+		key[hole] = key[parent];
+		val[hole] = val[parent];
+		hole = parent;
+		parent = (hole - 1) / 2;
+	}
+	key[hole] = vk;
+	val[hole] = vv;
+}
+
+// std::__partial_sort(first, last, last): make_heap + sort_heap
+__device__ void heap_sort(double* key, int32_t* val, int64_t len) {
+	if (len >= 2) {
+		int64_t parent = (len - 2) / 2;
+		while (true) {
+			heap_adjust(key, val, parent, len, key[parent], val[parent]);
+			if (parent == 0) break;
+			parent--;
+		}
+	}
+	int64_t last = len;
+	while (last > 1) {
+		--last;
+		double vk = key[last];
+		int32_t vv = val[last];
+		key[last] = key[0];
+		val[last] = val[0];
+		heap_adjust(key, val, 0, last, vk, vv);
+	}
+}
+
+// One Hoare partition of [f, l) after the median-of-three pivot move
+// (std::__unguarded_partition_pivot). Returns the cut.
+__device__ int64_t warp_partition(double* key, int32_t* val, int64_t f, int64_t l, int32_t* SL, int32_t* SR) {
+	const int lane = threadIdx.x & 31;
+	if (lane == 0) {
+		int64_t a = f + 1, b = f + (l - f) / 2, c = l - 1;
+		double ka = key[a], kb = key[b], kc = key[c];
+		int64_t m;
+		if (ka < kb) {
+			if (kb < kc) m = b;
+			else if (ka < kc) m = c;
+			else m = a;
+		} else if (ka < kc) m = a;
+		else if (kb < kc) m = c;
+		else m = b;
+		double tk = key[f]; key[f] = key[m]; key[m] = tk;
+		int32_t tv = val[f]; val[f] = val[m]; val[m] = tv;
+	}
+	__syncwarp();
+	const double P = key[f];
+	const uint32_t lt = lanemask_lt();
+	int cL = 0, cR = 0;
+	for (int64_t base = f + 1; base < l; base += 32) {
+		int64_t p = base + lane;
+		bool valid = p < l;
+		double k = valid ? key[p] : 0.0;
+		bool isL = valid && !(k < P);
+		bool isR = valid && !(P < k);
+		uint32_t bL = __ballot_sync(FULL, isL), bR = __ballot_sync(FULL, isR);
+		if (isL) SL[cL + __popc(bL & lt)] = (int32_t)(p - f);
+		if (isR) SR[cR + __popc(bR & lt)] = (int32_t)(p - f);
+		cL += __popc(bL);
+		cR += __popc(bR);
+	}
+	__syncwarp();
+	const int m = cL < cR ? cL : cR;
+	int K = m;
+	for (int kb = 0; kb < m; kb += 32) {
+		int k = kb + lane;
+		bool stop = k < m && !(SL[k] < SR[cR - 1 - k]);
+		uint32_t b = __ballot_sync(FULL, stop);
+		if (b) { K = kb + __ffs(b) - 1; break; }
+	}
+	for (int k = lane; k < K; k += 32) {
+		int64_t i = f + SL[k], j = f + SR[cR - 1 - k];
+		double tk = key[i]; key[i] = key[j]; key[j] = tk;
+		int32_t tv = val[i]; val[i] = val[j]; val[j] = tv;
+	}
+	int64_t c1 = K < cL ? (int64_t)SL[K] : INT64_MAX;
+	int64_t c2 = K >= 1 ? (int64_t)SR[cR - K] : INT64_MAX;
+	__syncwarp();
+	return f + (c1 < c2 ? c1 : c2);
+}
+
+struct Seg { int64_t f, l; int32_t d; int32_t pad; };
+
+// Replays std::sort (std::__sort) on key/val[0..n) with one warp.
+__device__ void warp_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL, int32_t* SR, int32_t* blk, Seg* stack,
+                              SampleStats* st) {
+	const int lane = threadIdx.x & 31;
+	int nblk = 0;
+	if (n > 1) {
+		int sp = 0;
+		if (lane == 0) stack[0] = {0, n, 2 * (63 - __clzll((long long)n)), 0};
+		sp = 1;
+		__syncwarp();
+		while (sp > 0) {
+			Seg s = stack[sp - 1];
+			sp--;
+			__syncwarp();
+			int64_t f = s.f, l = s.l;
+			int d = s.d;
+			bool heaped = false;
+			while (l - f > 16) {
+				if (d == 0) {
+					if (lane == 0) {
+						heap_sort(key + f, val + f, l - f);
+						atomicAdd(&st->heapsorts, 1ull);
+					}
+					__syncwarp();
+					heaped = true;
+					break;
+				}
+				d--;
+				int64_t cut = warp_partition(key, val, f, l, SL + f, SR + f);
+				if (lane == 0) stack[sp] = {cut, l, d, 0};
+				sp++;
+				__syncwarp();
+				l = cut;
+			}
+			if (!heaped && l - f > 1) {
+				if (lane == 0) { blk[2 * nblk] = (int32_t)f; blk[2 * nblk + 1] = (int32_t)l; }
+				nblk++;
+			}
+		}
+	}
+	__syncwarp();
+	// final insertion sort == stable sort inside each block
+	for (int b = lane; b < nblk; b += 32) {
+		int64_t s = blk[2 * b], e = blk[2 * b + 1];
+		for (int64_t i = s + 1; i < e; i++) {
+			double vk = key[i];
+			int32_t vv = val[i];
+			int64_t j = i;
+			while (j > s && vk < key[j - 1]) {
+				key[j] = key[j - 1];
+				val[j] = val[j - 1];
+				j--;
+			}
+			key[j] = vk;
+			val[j] = vv;
+		}
+	}
+	__syncwarp();
+}
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kStackDepth = 128;
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) node_sort_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order,
+                                                                       int node_begin, int node_end, LevelBuffers lb, SortScratch sc,
+                                                                       SampleStats* st, int* next_node) {
+	__shared__ Seg stacks[kWarpsPerBlock][kStackDepth];
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	while (true) {
+		int idx = 0;
+		if (lane == 0) idx = atomicAdd(next_node, 1);
+		idx = __shfl_sync(FULL, idx, 0) + node_begin;
+		if (idx >= node_end) break;
+		const LevelNode nd = nodes[order[idx]];
+		double* key = lb.keys + nd.cand_off;
+		int32_t* val = lb.perm + nd.cand_off;
+		warp_std_sort(key, val, nd.count, sc.SL + nd.cand_off, sc.SR + nd.cand_off, sc.blk + 2 * nd.cand_off, stacks[warp], st);
+		for (int64_t t = lane; t < nd.count; t += 32) lb.pos[nd.cand_off + val[t]] = (int32_t)t;
+	}
+}
+
+__global__ void sort_single_kernel(double* key, int32_t* val, int64_t n, SortScratch sc, SampleStats* st) {
+	__shared__ Seg stack[kStackDepth];
+	if (threadIdx.x >= 32) return;
+	warp_std_sort(key, val, n, sc.SL, sc.SR, sc.blk, stack, st);
+}
+
+// --------------------------------------------------------------- hashing
+__device__ __forceinline__ uint64_t hash_slot(uint64_t k, int64_t cap) {
+	return ((k * 0x9E3779B97F4A7C15ull) >> 17) & (uint64_t)(cap - 1);
+}
+
+// cells of 2*spacing*(1+1e-6): points closer than the spacing are in
+// neighbouring cells along each axis, and a candidate needs 8 cells
+struct CellGrid {
+	double min[3];
+	double inv;
+};
+
+__device__ __forceinline__ void cell_of(const CellGrid& g, double x, double y, double z, int c[3], double fr[3]) {
+	double u[3] = {(x - g.min[0]) * g.inv, (y - g.min[1]) * g.inv, (z - g.min[2]) * g.inv};
+	for (int a = 0; a < 3; a++) {
+		double fl = floor(u[a]);
+		fl = fl < -1000.0 ? -1000.0 : (fl > 1000.0 ? 1000.0 : fl);
+		c[a] = (int)fl;
+		fr[a] = u[a] - fl;
+	}
+}
+
+__device__ __forceinline__ uint64_t cell_key(int cx, int cy, int cz) {
+	return ((uint64_t)(cx + 1024) << 22) | ((uint64_t)(cy + 1024) << 11) | (uint64_t)(cz + 1024);
+}
+
+__device__ __forceinline__ int32_t hash_find(const uint64_t* keys, const int32_t* heads, int64_t cap, uint64_t k) {
+	uint64_t s = hash_slot(k, cap);
+	for (int64_t probe = 0; probe < cap; probe++) {
+		uint64_t kk = keys[s];
+		if (kk == k) return heads[s];
+		if (kk == EMPTY_KEY) return -1;
+		s = (s + 1) & (uint64_t)(cap - 1);
+	}
+	return -1;
+}
+
+// inserts item into the cell's list; returns false if the table is full
+__device__ __forceinline__ bool hash_push(uint64_t* keys, int32_t* heads, int32_t* next, int64_t cap, uint64_t k, int32_t item) {
+	uint64_t s = hash_slot(k, cap);
+	for (int64_t probe = 0; probe < cap; probe++) {
+		uint64_t prev = atomicCAS((unsigned long long*)&keys[s], (unsigned long long)EMPTY_KEY, (unsigned long long)k);
+		if (prev == EMPTY_KEY || prev == k) {
+			next[item] = atomicExch(&heads[s], item);
+			return true;
+		}
+		s = (s + 1) & (uint64_t)(cap - 1);
+	}
+	return false;
+}
+
+// ------------------------------------------------------------- greedy
+struct GreedyArgs {
+	uint64_t* hkeys;
+	int32_t* hheads;
+	double* axyz;   // accepted positions, 3 per slot (slot = cand_off + rank)
+	double* akey;   // accepted sort keys
+	int32_t* anext; // per-cell list links
+	int32_t* apos;  // accepted sorted positions
+};
+
+__device__ __forceinline__ double sqdist(double ax, double ay, double az, double bx, double by, double bz) {
+	// squaredDistance(point, candidate), sampler_poisson.h:117-125
+	double dx = ax - bx, dy = ay - by, dz = az - bz;
+	return dx * dx + dy * dy + dz * dz;
+}
+
+template <int MODE, bool GUARD>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) greedy_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order,
+                                                                    int node_begin, int node_end, const int32_t* __restrict__ X,
+                                                                    const int32_t* __restrict__ Y, const int32_t* __restrict__ Z,
+                                                                    PosParamsS pp, LevelBuffers lb, GreedyArgs ga, SampleStats* st,
+                                                                    int* next_node) {
+	const int lane = threadIdx.x & 31;
+	const uint32_t lt = lanemask_lt();
+	while (true) {
+		int idx = 0;
+		if (lane == 0) idx = atomicAdd(next_node, 1);
+		idx = __shfl_sync(FULL, idx, 0) + node_begin;
+		if (idx >= node_end) break;
+		const LevelNode nd = nodes[order[idx]];
+		const int64_t n = nd.count, co = nd.cand_off;
+		uint64_t* hk = ga.hkeys + nd.hash_off;
+		int32_t* hh = ga.hheads + nd.hash_off;
+		for (int64_t s = lane; s < nd.hash_cap; s += 32) { hk[s] = EMPTY_KEY; hh[s] = -1; }
+		__syncwarp();
+		const double sp = nd.spacing;
+		const double s2 = sp * sp;
+		const double cx = (nd.min[0] + nd.max[0]) * 0.5, cy = (nd.min[1] + nd.max[1]) * 0.5, cz = (nd.min[2] + nd.max[2]) * 0.5;
+		CellGrid g;
+		g.min[0] = nd.min[0]; g.min[1] = nd.min[1]; g.min[2] = nd.min[2];
+		g.inv = 1.0 / (2.0 * sp * 1.000001);
+		// FP32 guard band: node-relative float coordinates decide pairs whose
+		// squared distance is clearly away from s^2; the rest are re-decided
+		// in FP64 exactly as the reference computes them.
+		const float s2f = (float)s2;
+		const float lo = s2f * (1.0f - 2e-3f), hi = s2f * (1.0f + 2e-3f);
+		int64_t cnt = 0;  // accepted so far
+		unsigned long long escalated = 0;
+		for (int64_t b0 = 0; b0 < n; b0 += 32) {
+			const int64_t t = b0 + lane;
+			const bool valid = t < n;
+			double x = 0, y = 0, z = 0, key = 0, lim = -CUDART_INF;
+			int32_t local = 0;
+			if (valid) {
+				local = lb.perm[co + t];
+				point_xyz(X, Y, Z, pp, lb.ids[co + local], x, y, z);
+				key = lb.keys[co + t];
+				if (MODE == 0) {
+					// cd = sqrt(cdd); limit = cd - spacing (sampler_poisson.h:135-141)
+					double cd = sqrt(key);
+					double limit = cd - sp;
+					lim = limit * limit;
+				}
+			}
+			const float xf = (float)(x - cx), yf = (float)(y - cy), zf = (float)(z - cz);
+			// 1) conflicts with points accepted before this step
+			int64_t maxrank = -1;
+			if (valid) {
+				int c[3];
+				double fr[3];
+				cell_of(g, x, y, z, c, fr);
+				int o[3];
+				for (int a = 0; a < 3; a++) o[a] = fr[a] < 0.5 ? -1 : 1;
+#pragma unroll
+				for (int q = 0; q < 8; q++) {
+					int qx = c[0] + ((q & 4) ? o[0] : 0), qy = c[1] + ((q & 2) ? o[1] : 0), qz = c[2] + ((q & 1) ? o[2] : 0);
+					int32_t r = hash_find(hk, hh, nd.hash_cap, cell_key(qx, qy, qz));
+					int64_t guard = 0;
+					while (r >= 0 && guard++ <= n) {
+						const int64_t slot = co + r;
+						if (MODE == 1 || ga.akey[slot] >= lim) {
+							double ax = ga.axyz[3 * slot], ay = ga.axyz[3 * slot + 1], az = ga.axyz[3 * slot + 2];
+							bool conflict;
+							if (GUARD) {
+								float dxf = (float)(ax - cx) - xf, dyf = (float)(ay - cy) - yf, dzf = (float)(az - cz) - zf;
+								float ddf = dxf * dxf + dyf * dyf + dzf * dzf;
+								if (ddf < lo) conflict = true;
+								else if (ddf > hi) conflict = false;
+								else { conflict = sqdist(ax, ay, az, x, y, z) < s2; escalated++; }
+							} else {
+								conflict = sqdist(ax, ay, az, x, y, z) < s2;
+							}
+							if (conflict && r > maxrank) maxrank = r;
+						}
+						r = ga.anext[slot];
+					}
+					if (guard > n + 1) atomicAdd(&st->timeouts, 1ull);
+				}
+			}
+			// 2) conflicts inside the step: earlier lanes that would be
+			//    accepted before this candidate
+			uint32_t mask = 0;
+			for (int j = 0; j < 32; j++) {
+				double xj = __shfl_sync(FULL, x, j), yj = __shfl_sync(FULL, y, j), zj = __shfl_sync(FULL, z, j);
+				double kj = __shfl_sync(FULL, key, j);
+				if (valid && j < lane) {
+					if (MODE == 1 || kj >= lim) {
+						if (sqdist(xj, yj, zj, x, y, z) < s2) mask |= 1u << j;
+					}
+				}
+			}
+			// 3) decisions in sorted order
+			uint32_t accmask = 0;
+			const int nvalid = (int)((n - b0) < 32 ? (n - b0) : 32);
+			bool acc = false;
+			for (int i = 0; i < nvalid; i++) {
+				bool dec = false;
+				if (lane == i) {
+					int64_t m_i = __popc(accmask);
+					bool old_conflict = maxrank >= 0 && (MODE == 1 || maxrank >= cnt + m_i - 10001);
+					bool new_conflict = (mask & accmask) != 0;
+					dec = !old_conflict && !new_conflict;
+					acc = dec;
+				}
+				dec = __shfl_sync(FULL, dec, i);
+				if (dec) accmask |= 1u << i;
+			}
+			// 4) publish accepted points
+			if (valid) {
+				lb.accepted[co + local] = acc ? 1 : 0;
+				if (acc) {
+					int32_t rank = (int32_t)(cnt + __popc(accmask & lt));
+					lb.acc_rank[co + local] = rank;
+					const int64_t slot = co + rank;
+					ga.axyz[3 * slot] = x;
+					ga.axyz[3 * slot + 1] = y;
+					ga.axyz[3 * slot + 2] = z;
+					ga.akey[slot] = key;
+					ga.apos[slot] = (int32_t)t;
+					int c[3];
+					double fr[3];
+					cell_of(g, x, y, z, c, fr);
+					if (!hash_push(hk, hh, ga.anext + co, nd.hash_cap, cell_key(c[0], c[1], c[2]), rank)) atomicAdd(&st->timeouts, 1ull);
+				}
+			}
+			cnt += __popc(accmask);
+			__syncwarp();
+		}
+		if (GUARD) {
+			for (int o = 16; o > 0; o >>= 1) escalated += __shfl_down_sync(FULL, escalated, o);
+			if (lane == 0 && escalated) atomicAdd(&st->escalated, escalated);
+		}
+	}
+}
+
+// --------------------------------------------------- poisson_average colours
+__global__ void average_colors_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
+                                      const int32_t* __restrict__ Z, PosParamsS pp, LevelBuffers lb, GreedyArgs ga,
+                                      long long* __restrict__ sums) {
+	int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const LevelNode& nd = nodes[lb.node_of[j]];
+	const int64_t co = nd.cand_off;
+	const uint64_t col = lb.cols[j];
+	const long long r = (long long)(col & 0xffff), g = (long long)((col >> 16) & 0xffff), b = (long long)((col >> 32) & 0xffff);
+	if (lb.accepted[j]) {
+		long long* s = sums + 4 * (co + lb.acc_rank[j]);
+		atomicAdd((unsigned long long*)&s[0], (unsigned long long)(2 * r));
+		atomicAdd((unsigned long long*)&s[1], (unsigned long long)(2 * g));
+		atomicAdd((unsigned long long*)&s[2], (unsigned long long)(2 * b));
+		atomicAdd((unsigned long long*)&s[3], 2ull);
+		return;
+	}
+	double x, y, z;
+	point_xyz(X, Y, Z, pp, lb.ids[j], x, y, z);
+	const double s2 = nd.spacing * nd.spacing;
+	const int32_t my_pos = lb.pos[j];
+	CellGrid gr;
+	gr.min[0] = nd.min[0]; gr.min[1] = nd.min[1]; gr.min[2] = nd.min[2];
+	gr.inv = 1.0 / (2.0 * nd.spacing * 1.000001);
+	int c[3];
+	double fr[3];
+	cell_of(gr, x, y, z, c, fr);
+	int o[3];
+	for (int a = 0; a < 3; a++) o[a] = fr[a] < 0.5 ? -1 : 1;
+	const uint64_t* hk = ga.hkeys + nd.hash_off;
+	const int32_t* hh = ga.hheads + nd.hash_off;
+	for (int q = 0; q < 8; q++) {
+		int qx = c[0] + ((q & 4) ? o[0] : 0), qy = c[1] + ((q & 2) ? o[1] : 0), qz = c[2] + ((q & 1) ? o[2] : 0);
+		int32_t a = hash_find(hk, hh, nd.hash_cap, cell_key(qx, qy, qz));
+		int64_t guard = 0;
+		while (a >= 0 && guard++ <= nd.count) {
+			const int64_t slot = co + a;
+			if (sqdist(ga.axyz[3 * slot], ga.axyz[3 * slot + 1], ga.axyz[3 * slot + 2], x, y, z) < s2) {
+				long long f = my_pos < ga.apos[slot] ? 2 : 1;
+				long long* s = sums + 4 * slot;
+				atomicAdd((unsigned long long*)&s[0], (unsigned long long)(f * r));
+				atomicAdd((unsigned long long*)&s[1], (unsigned long long)(f * g));
+				atomicAdd((unsigned long long*)&s[2], (unsigned long long)(f * b));
+				atomicAdd((unsigned long long*)&s[3], (unsigned long long)f);
+			}
+			a = ga.anext[slot];
+		}
+	}
+}
+
+__global__ void average_finish_kernel(const LevelNode* __restrict__ nodes, LevelBuffers lb, const long long* __restrict__ sums) {
+	int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M || !lb.accepted[j]) return;
+	const int64_t slot = nodes[lb.node_of[j]].cand_off + lb.acc_rank[j];
+	const long long* s = sums + 4 * slot;
+	// rgbTarget = p.r / p.w (sampler_poisson_average.h:443-445)
+	uint64_t r = (uint16_t)(s[0] / s[3]), g = (uint16_t)(s[1] / s[3]), b = (uint16_t)(s[2] / s[3]);
+	lb.cols[j] = r | (g << 16) | (b << 32);
+}
+
+// ---------------------------------------------------------------- random
+__device__ __forceinline__ void random_cell(const LevelNode& nd, double x, double y, double z, int64_t& index, double& distance) {
+	// toCellIndex, sampler_random.h:64-87
+	const double G = 128.0;
+	double sx = nd.max[0] - nd.min[0], sy = nd.max[1] - nd.min[1], sz = nd.max[2] - nd.min[2];
+	double nx = (x - nd.min[0]) / sx, ny = (y - nd.min[1]) / sy, nz = (z - nd.min[2]) / sz;
+	double lx = 2.0 * fmod(G * nx, 1.0) - 1.0;
+	double ly = 2.0 * fmod(G * ny, 1.0) - 1.0;
+	double lz = 2.0 * fmod(G * nz, 1.0) - 1.0;
+	distance = sqrt(lx * lx + ly * ly + lz * lz);
+	int64_t cx = (int64_t)(G * nx), cy = (int64_t)(G * ny), cz = (int64_t)(G * nz);
+	cx = cx < 0 ? 0 : (cx > 127 ? 127 : cx);
+	cy = cy < 0 ? 0 : (cy > 127 ? 127 : cy);
+	cz = cz < 0 ? 0 : (cz > 127 ? 127 : cz);
+	index = cx + cy * 128 + cz * 128 * 128;
+}
+
+__global__ void random_first_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
+                                    const int32_t* __restrict__ Z, PosParamsS pp, LevelBuffers lb, uint64_t* hkeys, int32_t* hvals,
+                                    SampleStats* st) {
+	int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const LevelNode& nd = nodes[lb.node_of[j]];
+	double x, y, z;
+	point_xyz(X, Y, Z, pp, lb.ids[j], x, y, z);
+	int64_t index;
+	double distance;
+	random_cell(nd, x, y, z, index, distance);
+	const double all = sqrt(3.0);
+	bool small = lb.count_in_child[j] < 100;
+	bool dist_ok = distance < 0.7 * all;
+	if (!(small || dist_ok)) return;
+	uint64_t* hk = hkeys + nd.hash_off;
+	int32_t* hv = hvals + nd.hash_off;
+	uint64_t k = (uint64_t)index;
+	uint64_t s = hash_slot(k, nd.hash_cap);
+	const int32_t me = (int32_t)(j - nd.cand_off);
+	for (int64_t probe = 0; probe < nd.hash_cap; probe++) {
+		uint64_t prev = atomicCAS((unsigned long long*)&hk[s], (unsigned long long)EMPTY_KEY, (unsigned long long)k);
+		if (prev == EMPTY_KEY || prev == k) {
+			atomicMin(&hv[s], me);
+			return;
+		}
+		s = (s + 1) & (uint64_t)(nd.hash_cap - 1);
+	}
+	atomicAdd(&st->timeouts, 1ull);
+}
+
+__global__ void random_accept_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
+                                     const int32_t* __restrict__ Z, PosParamsS pp, LevelBuffers lb, const uint64_t* hkeys,
+                                     const int32_t* hvals) {
+	int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const LevelNode& nd = nodes[lb.node_of[j]];
+	double x, y, z;
+	point_xyz(X, Y, Z, pp, lb.ids[j], x, y, z);
+	int64_t index;
+	double distance;
+	random_cell(nd, x, y, z, index, distance);
+	const double all = sqrt(3.0);
+	bool small = lb.count_in_child[j] < 100;
+	bool dist_ok = distance < 0.7 * all;
+	bool acc = small;
+	if (!acc && dist_ok) {
+		int32_t first = hash_find(hkeys + nd.hash_off, hvals + nd.hash_off, nd.hash_cap, (uint64_t)index);
+		acc = first == (int32_t)(j - nd.cand_off);
+	}
+	lb.accepted[j] = acc ? 1 : 0;
+}
+
+__global__ void clear_hash_kernel(uint64_t* keys, int32_t* vals, int64_t n, int32_t fill) {
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) { keys[i] = EMPTY_KEY; vals[i] = fill; }
+}
+
+// --------------------------------------------------------------- shuffle
+// std::default_random_engine = minstd_rand0 (16807, 0, 2^31 - 1)
+struct MinStd {
+	uint64_t x;
+	__device__ explicit MinStd(uint32_t seed) {
+		uint64_t s = (uint64_t)seed % 2147483647ull;
+		x = s == 0 ? 1 : s;
+	}
+	__device__ uint64_t operator()() {
+		x = (x * 16807ull) % 2147483647ull;
+		return x;
+	}
+};
+
+// uniform_int_distribution<unsigned long>{a, b}(minstd), downscaling branch
+__device__ __forceinline__ uint64_t uniform(MinStd& g, uint64_t a, uint64_t b) {
+	const uint64_t urngrange = 2147483646ull - 1ull;
+	const uint64_t urange = b - a;
+	uint64_t ret;
+	if (urngrange > urange) {
+		const uint64_t uerange = urange + 1;
+		const uint64_t scaling = urngrange / uerange;
+		const uint64_t past = uerange * scaling;
+		do ret = g() - 1ull; while (ret >= past);
+		ret /= scaling;
+	} else {
+		ret = g() - 1ull;  // urange == urngrange; larger ranges do not occur (n < 46341)
+	}
+	return ret + a;
+}
+
+__device__ void std_shuffle(int32_t* v, int64_t n, uint32_t seed) {
+	if (n == 0) return;
+	MinStd g(seed);
+	const uint64_t urngrange = 2147483645ull;
+	const uint64_t urange = (uint64_t)n;
+	if (urngrange / urange >= urange) {
+		int64_t i = 1;
+		if ((urange % 2) == 0) {
+			int64_t k = (int64_t)uniform(g, 0, 1);
+			int32_t t = v[i]; v[i] = v[k]; v[k] = t;
+			i++;
+		}
+		while (i != n) {
+			const uint64_t swap_range = (uint64_t)i + 1;
+			uint64_t xx = uniform(g, 0, swap_range * (swap_range + 1) - 1);
+			int64_t p1 = (int64_t)(xx / (swap_range + 1)), p2 = (int64_t)(xx % (swap_range + 1));
+			int32_t t = v[i]; v[i] = v[p1]; v[p1] = t;
+			i++;
+			t = v[i]; v[i] = v[p2]; v[p2] = t;
+			i++;
+		}
+	} else {
+		for (int64_t i = 1; i < n; i++) {
+			int64_t k = (int64_t)uniform(g, 0, (uint64_t)i);
+			int32_t t = v[i]; v[i] = v[k]; v[k] = t;
+		}
+	}
+}
+
+__global__ void shuffle_leaves_kernel(const int64_t* __restrict__ off, const int64_t* __restrict__ cnt, int num, const uint32_t* __restrict__ in,
+                                      uint32_t* __restrict__ out, int32_t* scratch, uint32_t seed) {
+	int l = blockIdx.x * blockDim.x + threadIdx.x;
+	if (l >= num) return;
+	const int64_t o = off[l], n = cnt[l];
+	int32_t* idx = scratch + o;
+	for (int64_t i = 0; i < n; i++) idx[i] = (int32_t)i;
+	std_shuffle(idx, n, seed);
+	// buffer[indices[i]] = points[i] (sampler_random.h:106-115)
+	for (int64_t i = 0; i < n; i++) out[o + idx[i]] = in[o + i];
+}
+
+__global__ void shuffle_single_kernel(int64_t n, uint32_t seed, int32_t* perm) {
+	for (int64_t i = 0; i < n; i++) perm[i] = (int32_t)i;
+	std_shuffle(perm, n, seed);
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------- launchers
+void launch_gather(const GatherItem* items, int num_items, LevelBuffers& lb, DeviceMem& mem) {
+	if (num_items == 0) return;
+	gather_kernel<<<num_items, 256, 0, mem.stream()>>>(items, lb);
+	PCG_LAUNCHED();
+}
+
+void launch_keys(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
+                 LevelBuffers& lb, DeviceMem& mem) {
+	if (lb.M == 0) return;
+	keys_kernel<<<(unsigned)ceil_div(lb.M, 256), 256, 0, mem.stream()>>>(nodes, X, Y, Z, pp, lb);
+	PCG_LAUNCHED();
+}
+
+static int sm_count() {
+	int dev = 0, sms = 0;
+	PCG_CUDA(cudaGetDevice(&dev));
+	PCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+	return sms;
+}
+
+void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, LevelBuffers& lb, SampleStats* st, DeviceMem& mem,
+                      int node_begin, int node_end) {
+	if (node_end < 0) node_end = K;
+	if (node_end <= node_begin || lb.M == 0) return;
+	SortScratch sc;
+	sc.SL = mem.alloc<int32_t>(lb.M);
+	sc.SR = mem.alloc<int32_t>(lb.M);
+	sc.blk = mem.alloc<int32_t>(2 * lb.M);
+	int* counter = mem.alloc<int>(1);
+	PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), mem.stream()));
+	int nodes_here = node_end - node_begin;
+	int blocks = (int)ceil_div(nodes_here, kWarpsPerBlock);
+	int cap = sm_count() * 16;
+	if (blocks > cap) blocks = cap;
+	node_sort_kernel<<<blocks, kWarpsPerBlock * 32, 0, mem.stream()>>>(nodes, order, node_begin, node_end, lb, sc, st, counter);
+	PCG_LAUNCHED();
+	mem.free(sc.SL);
+	mem.free(sc.SR);
+	mem.free(sc.blk);
+	mem.free(counter);
+}
+
+void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int32_t* order, int K, const int32_t* X, const int32_t* Y,
+                   const int32_t* Z, const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads,
+                   double* acc_xyz, double* acc_key, int32_t* acc_next, int32_t* acc_pos, SampleStats* st, DeviceMem& mem,
+                   int node_begin, int node_end) {
+	if (node_end < 0) node_end = K;
+	if (node_end <= node_begin || lb.M == 0) return;
+	GreedyArgs ga{hash_keys, hash_heads, acc_xyz, acc_key, acc_next, acc_pos};
+	int* counter = mem.alloc<int>(1);
+	PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), mem.stream()));
+	int nodes_here = node_end - node_begin;
+	int blocks = (int)ceil_div(nodes_here, kWarpsPerBlock);
+	int cap = sm_count() * 16;
+	if (blocks > cap) blocks = cap;
+	dim3 grid(blocks), block(kWarpsPerBlock * 32);
+	cudaStream_t s = mem.stream();
+	if (mode == 0 && fp32_guard) greedy_kernel<0, true><<<grid, block, 0, s>>>(nodes, order, node_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
+	else if (mode == 0) greedy_kernel<0, false><<<grid, block, 0, s>>>(nodes, order, node_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
+	else if (fp32_guard) greedy_kernel<1, true><<<grid, block, 0, s>>>(nodes, order, node_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
+	else greedy_kernel<1, false><<<grid, block, 0, s>>>(nodes, order, node_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
+	PCG_LAUNCHED();
+	mem.free(counter);
+}
+
+void launch_average_colors(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
+                           LevelBuffers& lb, const uint64_t* hash_keys, const int32_t* hash_heads, const double* acc_xyz,
+                           const int32_t* acc_next, const int32_t* acc_pos, const int64_t* /*acc_base*/, long long* sums,
+                           DeviceMem& mem) {
+	if (lb.M == 0) return;
+	GreedyArgs ga{const_cast<uint64_t*>(hash_keys), const_cast<int32_t*>(hash_heads), const_cast<double*>(acc_xyz), nullptr,
+	              const_cast<int32_t*>(acc_next), const_cast<int32_t*>(acc_pos)};
+	PCG_CUDA(cudaMemsetAsync(sums, 0, sizeof(long long) * 4 * lb.M, mem.stream()));
+	unsigned blocks = (unsigned)ceil_div(lb.M, 256);
+	average_colors_kernel<<<blocks, 256, 0, mem.stream()>>>(nodes, X, Y, Z, pp, lb, ga, sums);
+	PCG_LAUNCHED();
+	average_finish_kernel<<<blocks, 256, 0, mem.stream()>>>(nodes, lb, sums);
+	PCG_LAUNCHED();
+}
+
+void launch_random_accept_sized(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
+                                LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_vals, int64_t hash_total, SampleStats* st,
+                                DeviceMem& mem) {
+	if (lb.M == 0) return;
+	clear_hash_kernel<<<(unsigned)ceil_div(hash_total, 256), 256, 0, mem.stream()>>>(hash_keys, hash_vals, hash_total, 0x7fffffff);
+	PCG_LAUNCHED();
+	unsigned blocks = (unsigned)ceil_div(lb.M, 256);
+	random_first_kernel<<<blocks, 256, 0, mem.stream()>>>(nodes, X, Y, Z, pp, lb, hash_keys, hash_vals, st);
+	PCG_LAUNCHED();
+	random_accept_kernel<<<blocks, 256, 0, mem.stream()>>>(nodes, X, Y, Z, pp, lb, hash_keys, hash_vals);
+	PCG_LAUNCHED();
+}
+
+void launch_shuffle_leaves(const int64_t* leaf_off, const int64_t* leaf_cnt, int num_leaves, const uint32_t* ids_in,
+                           uint32_t* ids_out, int32_t* scratch, uint32_t seed, DeviceMem& mem) {
+	if (num_leaves == 0) return;
+	shuffle_leaves_kernel<<<(unsigned)ceil_div(num_leaves, 64), 64, 0, mem.stream()>>>(leaf_off, leaf_cnt, num_leaves, ids_in, ids_out,
+	                                                                                    scratch, seed);
+	PCG_LAUNCHED();
+}
+
+void launch_sort_keys_single(double* keys, int32_t* vals, int64_t n, DeviceMem& mem, SampleStats* st) {
+	if (n <= 0) return;
+	SortScratch sc;
+	sc.SL = mem.alloc<int32_t>(n);
+	sc.SR = mem.alloc<int32_t>(n);
+	sc.blk = mem.alloc<int32_t>(2 * n);
+	sort_single_kernel<<<1, 32, 0, mem.stream()>>>(keys, vals, n, sc, st);
+	PCG_LAUNCHED();
+}
+
+void launch_shuffle_single(int64_t n, uint32_t seed, int32_t* perm, DeviceMem& mem) {
+	if (n <= 0) return;
+	shuffle_single_kernel<<<1, 1, 0, mem.stream()>>>(n, seed, perm);
+	PCG_LAUNCHED();
+}
+
+}  // namespace pcg

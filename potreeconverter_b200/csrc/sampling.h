@@ -1,0 +1,80 @@
+// Sampler kernels (one octree level across all its nodes per launch).
+#pragma once
+
+#include "dev.h"
+
+namespace pcg {
+
+struct LevelNode {          // one inner node sampled at this level
+	int64_t cand_off;        // first candidate (gather order: child 0..7, index order)
+	int64_t count;
+	int64_t hash_off;        // first slot of the node's hash table
+	int64_t hash_cap;        // power of two
+	double min[3], max[3];   // node box
+	double spacing;          // baseSpacing / 2^level
+	int32_t level;
+	int32_t pad;
+};
+
+struct GatherItem {         // copy `count` ids (and colours) of one child buffer
+	const uint32_t* src_ids;
+	const uint64_t* src_cols; // packed r | g << 16 | b << 32, or null
+	int64_t dst_off;
+	int64_t count;
+	int32_t child;
+	int32_t node;
+};
+
+struct LevelBuffers {
+	int64_t M = 0;                 // candidates at this level
+	int K = 0;                     // nodes at this level
+	uint32_t* ids = nullptr;       // [M] candidate point ids
+	uint64_t* cols = nullptr;      // [M] packed colours (poisson_average)
+	uint8_t* child = nullptr;      // [M] child index
+	int32_t* node_of = nullptr;    // [M] node index
+	int32_t* count_in_child = nullptr; // [M] size of the candidate's child buffer (random)
+	double* keys = nullptr;        // [M] FP64 squared distance to the node centre
+	int32_t* perm = nullptr;       // [M] sorted position t -> local candidate index
+	int32_t* pos = nullptr;        // [M] local candidate index -> sorted position
+	uint8_t* accepted = nullptr;   // [M]
+	int32_t* acc_rank = nullptr;   // [M] acceptance rank for accepted candidates
+};
+
+struct PosParamsS {
+	double scale[3], offset[3];
+};
+
+struct SampleStats {
+	unsigned long long escalated;  // FP32 decisions re-made in FP64
+	unsigned long long heapsorts;  // introsort depth-limit fallbacks
+	unsigned long long timeouts;   // bounded loops that gave up
+	unsigned long long pad;
+};
+
+void launch_gather(const GatherItem* items, int num_items, LevelBuffers& lb, DeviceMem& mem);
+void launch_keys(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
+                 LevelBuffers& lb, DeviceMem& mem);
+// std::sort emulation per node; `order` lists node indices, largest first.
+void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, LevelBuffers& lb, SampleStats* st, DeviceMem& mem,
+                      int node_begin = 0, int node_end = -1);
+// mode 0 = poisson (early exit + 10,001-check window), 1 = poisson_average (pure greedy)
+void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int32_t* order, int K, const int32_t* X, const int32_t* Y,
+                   const int32_t* Z, const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads,
+                   double* acc_xyz, double* acc_key, int32_t* acc_next, int32_t* acc_pos, SampleStats* st, DeviceMem& mem,
+                   int node_begin = 0, int node_end = -1);
+// poisson_average colour sums: new packed colour per accepted candidate
+void launch_average_colors(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
+                           LevelBuffers& lb, const uint64_t* hash_keys, const int32_t* hash_heads, const double* acc_xyz,
+                           const int32_t* acc_next, const int32_t* acc_pos, const int64_t* acc_base, long long* sums,
+                           DeviceMem& mem);
+void launch_random_accept_sized(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
+                                LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_vals, int64_t hash_total, SampleStats* st,
+                                DeviceMem& mem);
+// leaf shuffle of the random sampler; leaves given as (offset, count) ranges of ids
+void launch_shuffle_leaves(const int64_t* leaf_off, const int64_t* leaf_cnt, int num_leaves, const uint32_t* ids_in,
+                           uint32_t* ids_out, int32_t* scratch, uint32_t seed, DeviceMem& mem);
+// stand-alone entry points for the parity tests
+void launch_sort_keys_single(double* keys, int32_t* vals, int64_t n, DeviceMem& mem, SampleStats* st);
+void launch_shuffle_single(int64_t n, uint32_t seed, int32_t* perm, DeviceMem& mem);
+
+}  // namespace pcg

@@ -1,0 +1,162 @@
+// Host-side FP64 set-up: LAS header, attribute schema, scale/offset, cubic
+// bounding box and chunk-grid parameters, evaluated with the same
+// expressions (and therefore the same rounding) as the reference.
+
+#include <cmath>
+#include <cstring>
+
+#include "pcg_internal.h"
+
+namespace pcg {
+
+const char* attr_type_name(AttrType t) {  // Attributes.h:51-78
+	switch (t) {
+	case AttrType::INT8: return "int8";
+	case AttrType::INT16: return "int16";
+	case AttrType::INT32: return "int32";
+	case AttrType::INT64: return "int64";
+	case AttrType::UINT8: return "uint8";
+	case AttrType::UINT16: return "uint16";
+	case AttrType::UINT32: return "uint32";
+	case AttrType::UINT64: return "uint64";
+	case AttrType::FLOAT: return "float";
+	case AttrType::DOUBLE: return "double";
+	case AttrType::UNDEFINED: return "undefined";
+	}
+	return "error";
+}
+
+int attr_type_size(AttrType t) {  // Attributes.h:33-49
+	switch (t) {
+	case AttrType::UINT8: case AttrType::INT8: return 1;
+	case AttrType::UINT16: case AttrType::INT16: return 2;
+	case AttrType::UINT32: case AttrType::INT32: case AttrType::FLOAT: return 4;
+	case AttrType::UINT64: case AttrType::INT64: case AttrType::DOUBLE: return 8;
+	default: return 0;
+	}
+}
+
+template <class T> static T get(const uint8_t* p) { T v; std::memcpy(&v, p, sizeof(T)); return v; }
+
+// Header fields as LASzip reports them for an uncompressed file
+// (LasLoader.cpp:72-128).
+bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& err) {
+	if (size < 227 || std::memcmp(las, "LASF", 4) != 0) { err = "input is not a LAS file"; return false; }
+	info.version_minor = las[25];
+	uint16_t header_size = get<uint16_t>(las + 94);
+	info.offset_to_points = get<uint32_t>(las + 96);
+	uint32_t num_vlrs = get<uint32_t>(las + 100);
+	uint8_t fmt = las[104];
+	if (fmt & 0xC0) { err = "compressed (LAZ) point data is not supported"; return false; }
+	info.pdrf = fmt & 0x3f;
+	info.record_length = get<uint16_t>(las + 105);
+	uint64_t legacy = get<uint32_t>(las + 107);
+	info.scale = {get<double>(las + 131), get<double>(las + 139), get<double>(las + 147)};
+	info.offset = {get<double>(las + 155), get<double>(las + 163), get<double>(las + 171)};
+	info.max.x = get<double>(las + 179); info.min.x = get<double>(las + 187);
+	info.max.y = get<double>(las + 195); info.min.y = get<double>(las + 203);
+	info.max.z = get<double>(las + 211); info.min.z = get<double>(las + 219);
+	uint64_t ext = 0;
+	if (info.version_minor >= 4 && header_size >= 375 && size >= 255) ext = get<uint64_t>(las + 247);
+	info.num_points = (int64_t)(ext > legacy ? ext : legacy);  // LasLoader.cpp:103
+	uint64_t pos = header_size;
+	for (uint32_t i = 0; i < num_vlrs; i++) {
+		if (pos + 54 > size) { err = "truncated variable length record"; return false; }
+		LasInfo::Vlr v;
+		v.record_id = get<uint16_t>(las + pos + 18);
+		uint16_t len = get<uint16_t>(las + pos + 20);
+		if (pos + 54 + len > size) { err = "truncated variable length record"; return false; }
+		v.data.assign(las + pos + 54, las + pos + 54 + len);
+		info.vlrs.push_back(std::move(v));
+		pos += 54 + len;
+	}
+	if (info.offset_to_points + (uint64_t)info.num_points * (uint64_t)info.record_length > size) {
+		err = "truncated point data";
+		return false;
+	}
+	return true;
+}
+
+static void las_type_info(int type_id, AttrType& type, int& num_elements) {  // LasLoader.cpp:7-69
+	static const AttrType base[] = {AttrType::UNDEFINED, AttrType::UINT8, AttrType::INT8, AttrType::UINT16, AttrType::INT16,
+	                                AttrType::UINT32, AttrType::INT32, AttrType::UINT64, AttrType::INT64, AttrType::FLOAT, AttrType::DOUBLE};
+	if (type_id == 0) { type = AttrType::UNDEFINED; num_elements = 1; return; }
+	type = base[(type_id - 1) % 10 + 1];
+	num_elements = type_id <= 10 ? 1 : (type_id <= 20 ? 2 : 3);
+}
+
+bool make_setup(const LasInfo& info, Setup& s, std::string& err) {
+	s.las = info;
+	auto mk = [](const char* name, int size, int ne, int es, AttrType t, int kind) {
+		AttrDesc a; a.name = name; a.size = size; a.numElements = ne; a.elementSize = es; a.type = t; a.kind = kind; return a;
+	};
+	AttrDesc xyz = mk("position", 12, 3, 4, AttrType::INT32, AK_POSITION);
+	AttrDesc intensity = mk("intensity", 2, 1, 2, AttrType::UINT16, AK_INTENSITY);
+	AttrDesc retnum = mk("return number", 1, 1, 1, AttrType::UINT8, AK_RETURN_NUMBER);
+	AttrDesc nret = mk("number of returns", 1, 1, 1, AttrType::UINT8, AK_NUMBER_OF_RETURNS);
+	AttrDesc cls = mk("classification", 1, 1, 1, AttrType::UINT8, AK_CLASSIFICATION);
+	AttrDesc sar = mk("scan angle rank", 1, 1, 1, AttrType::UINT8, AK_SCAN_ANGLE_RANK);
+	AttrDesc user = mk("user data", 1, 1, 1, AttrType::UINT8, AK_USER_DATA);
+	AttrDesc psid = mk("point source id", 2, 1, 2, AttrType::UINT16, AK_POINT_SOURCE_ID);
+	AttrDesc gps = mk("gps-time", 8, 1, 8, AttrType::DOUBLE, AK_GPS_TIME);
+	AttrDesc rgb = mk("rgb", 6, 3, 2, AttrType::UINT16, AK_RGB);
+	// attribute order per point format, PotreeConverter.h:160-181
+	switch (info.pdrf) {
+	case 0: s.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid}; s.std_record_length = 20; break;
+	case 1: s.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid, gps}; s.std_record_length = 28; break;
+	case 2: s.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid, rgb}; s.std_record_length = 26; break;
+	case 3: s.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid, gps, rgb}; s.std_record_length = 34; break;
+	default: err = "unsupported LAS point data format " + std::to_string(info.pdrf) + " (0-3 are supported)"; return false;
+	}
+	s.first_extra_index = (int)s.attrs.size();  // chunker_countsort_laszip.cpp:551-560
+	if (info.record_length < s.std_record_length) { err = "point record length shorter than its format"; return false; }
+	// extra bytes, PotreeConverter.h:80-133
+	int src = s.std_record_length;
+	for (auto& vlr : info.vlrs) {
+		if (vlr.record_id != 4) continue;
+		int num = (int)vlr.data.size() / 192;
+		for (int i = 0; i < num; i++) {
+			const uint8_t* r = vlr.data.data() + i * 192;
+			char name[33] = {0}, desc[33] = {0};
+			std::memcpy(name, r + 4, 32);
+			std::memcpy(desc, r + 160, 32);
+			AttrType t; int ne;
+			las_type_info(r[2], t, ne);
+			int es = attr_type_size(t);
+			AttrDesc a = mk(name, ne * es, ne, es, t, AK_EXTRA);
+			a.description = desc;
+			if (r[3] & 0b01000) std::memcpy(&a.scale, r + 112, 24);
+			if (r[3] & 0b10000) std::memcpy(&a.offset, r + 136, 24);
+			a.src_offset = src;
+			src += a.size;
+			s.attrs.push_back(a);
+		}
+	}
+	if (src > info.record_length) { err = "extra bytes exceed the point record length"; return false; }
+	int off = 0;
+	for (auto& a : s.attrs) { a.out_offset = off; off += a.size; }
+	s.bpp = off;
+
+	// computeScaleOffset with a single source, PotreeConverter.h:29-76
+	Vec3d mn = info.min, mx = info.max;
+	Vec3d size = mx - mn;
+	double msx = size.x / std::pow(2.0, 30.0), msy = size.y / std::pow(2.0, 30.0), msz = size.z / std::pow(2.0, 30.0);
+	s.pos_scale = {info.scale.x < msx ? msx : info.scale.x, info.scale.y < msy ? msy : info.scale.y, info.scale.z < msz ? msz : info.scale.z};
+	s.pos_offset = mn;
+	// computeStats, main.cpp:215-284
+	double cube = vmax3(mx - mn);
+	if (cube == 0.0) { err = "invalid bounding box: at least one axis has a size of zero"; return false; }
+	s.cube_min = mn;
+	s.cube_max = mn + cube;
+	if ((s.cube_max - mn).x == 0.0) { err = "invalid bounding box"; return false; }
+	// main.cpp:273-281 rejects a box with any zero-size cubic axis
+	s.chunk_cube_size = vmax3(s.cube_max - s.cube_min);  // chunker_countsort_laszip.cpp:205-207
+	s.root_max = s.cube_min + vmax3(s.cube_max - s.cube_min);  // :1252-1254
+	s.total_points = info.num_points;
+	int64_t t20 = s.total_points / 20;
+	s.max_points_per_chunk = (int)(t20 < 10'000'000 ? t20 : 10'000'000);
+	s.grid_size = s.total_points < 100'000'000 ? 128 : (s.total_points < 500'000'000 ? 256 : 512);
+	return true;
+}
+
+}  // namespace pcg

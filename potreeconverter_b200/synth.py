@@ -266,3 +266,31 @@ GENERATORS = {"terrain": terrain, "hotspots": hotspots, "lattice": lattice, "str
 
 def generate(kind: str, n: int, seed: int, **kw) -> bytes:
     return GENERATORS[kind](n, seed, **kw)
+
+
+def duplicates(n: int, seed: int, extent: float = 100.0, dup_fraction: float = 0.3,
+               n_sites: int = 3) -> bytes:
+    """Terrain with exact duplicate positions piled on a few sites.
+
+    Each site holds many points with identical XYZ (and differing attributes),
+    which drives the per-chunk octree into its duplicate-handling path
+    (indexer.cpp:1002-1099)."""
+    rng = np.random.default_rng(seed)
+    n_dup = int(n * dup_fraction)
+    n_base = n - n_dup
+    x = rng.uniform(0, extent, n_base)
+    y = rng.uniform(0, extent, n_base)
+    z = np.sin(x * 0.05) * 3 + rng.normal(0, 0.05, n_base)
+    site = rng.integers(0, n_sites, n_dup)
+    sx, sy, sz = rng.uniform(0, extent, n_sites), rng.uniform(0, extent, n_sites), rng.uniform(0, 3, n_sites)
+    xs = np.concatenate([x, sx[site]])
+    ys = np.concatenate([y, sy[site]])
+    zs = np.concatenate([z, sz[site]])
+    perm = rng.permutation(n)
+    xs, ys, zs = xs[perm], ys[perm], zs[perm]
+    X, Y, Z = _quantize(xs), _quantize(ys), _quantize(zs)
+    attrs = _common_attrs(rng, n, zs)
+    return write_las(X, Y, Z, attrs, pdrf=2, version_minor=2)
+
+
+GENERATORS["duplicates"] = duplicates

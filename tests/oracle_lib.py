@@ -1,0 +1,101 @@
+"""Test-side access to the oracle (oracle/pcref.cpp, the single-threaded
+CPU restatement of the reference pipeline) and to the golden fixtures the
+pinned reference produced (tests/golden/golden.json). Test infrastructure
+only: nothing in the library imports this module."""
+
+from __future__ import annotations
+
+import ctypes
+import functools
+import hashlib
+import json
+import os
+import subprocess
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(REPO, "oracle")
+ORACLE_LIB = os.path.join(ORACLE_DIR, "_build", "libpcref.so")
+GOLDEN = os.path.join(REPO, "tests", "golden", "golden.json")
+PINNED_SEED = 1592614637
+
+
+class _Out(ctypes.Structure):
+    _fields_ = [("octree", ctypes.POINTER(ctypes.c_uint8)), ("octree_size", ctypes.c_uint64),
+                ("hierarchy", ctypes.POINTER(ctypes.c_uint8)), ("hierarchy_size", ctypes.c_uint64),
+                ("metadata", ctypes.c_char_p), ("metadata_size", ctypes.c_uint64),
+                ("num_chunks", ctypes.c_int32), ("chunk_ids", ctypes.c_void_p),
+                ("chunk_counts", ctypes.POINTER(ctypes.c_int64)), ("error", ctypes.c_char * 256)]
+
+
+def build_oracle():
+    if not os.path.exists(ORACLE_LIB):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, "restatement"], check=True)
+
+
+class Oracle:
+    def __init__(self):
+        build_oracle()
+        lib = ctypes.CDLL(ORACLE_LIB)
+        lib.pcref_convert.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_char_p,
+                                      ctypes.c_uint32, ctypes.POINTER(_Out)]
+        lib.pcref_free.argtypes = [ctypes.POINTER(_Out)]
+        lib.pcref_std_sort_perm.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+        lib.pcref_std_shuffle.argtypes = [ctypes.c_int64, ctypes.c_uint32, ctypes.c_void_p]
+        self.lib = lib
+
+    def convert(self, las: bytes, method: str, name: str = "cloud", seed: int = PINNED_SEED):
+        buf = (ctypes.c_uint8 * len(las)).from_buffer_copy(las)
+        out = _Out()
+        rc = self.lib.pcref_convert(ctypes.addressof(buf), len(las), method.encode(), name.encode(), seed,
+                                    ctypes.byref(out))
+        if rc != 0:
+            raise RuntimeError(out.error.decode())
+        res = {
+            "octree.bin": ctypes.string_at(out.octree, out.octree_size),
+            "hierarchy.bin": ctypes.string_at(out.hierarchy, out.hierarchy_size),
+            "metadata.json": ctypes.string_at(out.metadata, out.metadata_size),
+        }
+        p = out.chunk_ids
+        chunk_ids = []
+        off = 0
+        for _ in range(out.num_chunks):
+            s = ctypes.string_at(p + off)
+            chunk_ids.append(s.decode())
+            off += len(s) + 1
+        res["chunks"] = list(zip(chunk_ids, [out.chunk_counts[i] for i in range(out.num_chunks)]))
+        self.lib.pcref_free(ctypes.byref(out))
+        return res
+
+    def sort_perm(self, keys):
+        k = np.ascontiguousarray(keys, dtype=np.float64)
+        perm = np.empty(k.shape[0], dtype=np.int32)
+        self.lib.pcref_std_sort_perm(k.ctypes.data, k.shape[0], perm.ctypes.data)
+        return perm
+
+    def shuffle(self, n, seed=PINNED_SEED):
+        perm = np.empty(n, dtype=np.int32)
+        self.lib.pcref_std_shuffle(n, seed, perm.ctypes.data)
+        return perm
+
+
+def load_golden():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+@functools.lru_cache(maxsize=16)
+def case_las(kind: str, n: int, seed: int, kwargs_json: str) -> bytes:
+    from potreeconverter_b200 import synth
+    return synth.generate(kind, n, seed, **json.loads(kwargs_json))
+
+
+def las_for(case: dict) -> bytes:
+    las = case_las(case["kind"], case["points"], case["seed"], json.dumps(case["kwargs"], sort_keys=True))
+    assert hashlib.md5(las).hexdigest() == case["las_md5"], "synthetic generator output changed"
+    return las
+
+
+def md5(b: bytes) -> str:
+    return hashlib.md5(b).hexdigest()

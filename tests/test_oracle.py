@@ -1,0 +1,35 @@
+"""The oracle (CPU restatement) is pinned against the reference: its three
+output files must match, byte for byte, the digests the pinned reference
+converter produced for the same seeded inputs (tests/golden/golden.json)."""
+
+import pytest
+
+from tests.oracle_lib import las_for, load_golden, md5
+
+CASES = [(c, m) for c in load_golden()["cases"] for m in c["outputs"]]
+
+
+@pytest.mark.parametrize("case,method", CASES, ids=[f"{c['name']}-{m}" for c, m in CASES])
+def test_oracle_matches_pinned_reference(oracle, case, method):
+    out = oracle.convert(las_for(case), method, name=case["name"])
+    for f in ("octree.bin", "hierarchy.bin", "metadata.json"):
+        assert len(out[f]) == case["outputs"][method][f]["size"], f
+        assert md5(out[f]) == case["outputs"][method][f]["md5"], f
+
+
+def test_oracle_std_sort_ties_are_deterministic(oracle):
+    import numpy as np
+    rng = np.random.default_rng(5)
+    keys = rng.integers(0, 7, 5000).astype(np.float64)
+    p1, p2 = oracle.sort_perm(keys), oracle.sort_perm(keys)
+    assert (p1 == p2).all()
+    assert (np.diff(keys[p1]) >= 0).all()
+    # ties are not in input order: std::sort is not stable
+    assert not (p1 == np.argsort(keys, kind="stable")).all()
+
+
+def test_oracle_shuffle_is_a_permutation(oracle):
+    import numpy as np
+    for n in (0, 1, 2, 3, 10, 9999, 10000):
+        p = oracle.shuffle(n)
+        assert sorted(p.tolist()) == list(range(n))
