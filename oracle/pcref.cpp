@@ -1312,6 +1312,9 @@ struct pcref_output {
 	char* chunk_ids;         // num_chunks NUL-terminated ids, concatenated
 	int64_t* chunk_counts;   // points per chunk, chunk (file-name) order
 	char error[256];
+	int64_t num_nodes;       // completed nodes, completion order
+	char* node_names;        // NUL-terminated names, concatenated
+	int64_t* node_info;      // per node: byte offset, byte size, point count
 };
 
 int pcref_convert(const void* las, uint64_t size, const char* method, const char* name, uint32_t seed, pcref_output* out) {
@@ -1340,11 +1343,24 @@ int pcref_convert(const void* las, uint64_t size, const char* method, const char
 	for (auto& s : res.chunkIds) { memcpy(out->chunk_ids + p, s.c_str(), s.size() + 1); p += s.size() + 1; }
 	out->chunk_counts = (int64_t*)malloc(sizeof(int64_t) * (res.chunkCounts.size() + 1));
 	for (size_t i = 0; i < res.chunkCounts.size(); i++) out->chunk_counts[i] = res.chunkCounts[i];
+	out->num_nodes = (int64_t)res.nodes.size();
+	size_t nameBytes = 0;
+	for (auto& n : res.nodes) nameBytes += n.name.size() + 1;
+	out->node_names = (char*)malloc(nameBytes + 1);
+	out->node_info = (int64_t*)malloc(sizeof(int64_t) * 3 * (res.nodes.size() + 1));
+	p = 0;
+	for (size_t i = 0; i < res.nodes.size(); i++) {
+		memcpy(out->node_names + p, res.nodes[i].name.c_str(), res.nodes[i].name.size() + 1);
+		p += res.nodes[i].name.size() + 1;
+		out->node_info[3 * i] = res.nodes[i].byteOffset;
+		out->node_info[3 * i + 1] = res.nodes[i].byteSize;
+		out->node_info[3 * i + 2] = res.nodes[i].numPoints;
+	}
 	return 0;
 }
 
 void pcref_free(pcref_output* out) {
-	free(out->octree); free(out->hierarchy); free(out->metadata); free(out->chunk_ids); free(out->chunk_counts);
+	free(out->octree); free(out->hierarchy); free(out->metadata); free(out->chunk_ids); free(out->chunk_counts); free(out->node_names); free(out->node_info);
 	memset(out, 0, sizeof(*out));
 }
 

@@ -94,9 +94,11 @@ struct Tree {
 	}
 };
 
-std::string chunk_id(const ChunkCell& c, int grid) {  // toNodeID, chunker_countsort_laszip.cpp:82-115
+// toNodeID(level, gridSize, x, y, z), chunker_countsort_laszip.cpp:82-115,
+// called with the grid size of the chunk's own level (:1162)
+std::string chunk_id(const ChunkCell& c) {
 	std::string id = "r";
-	int cur = grid;
+	int cur = 1 << c.level;
 	int lx = c.x, ly = c.y, lz = c.z;
 	for (int i = 0; i < c.level; i++) {
 		int index = 0;
@@ -204,7 +206,7 @@ struct Converter {
 		auto cells_found = download(d_chunks, (size_t)nchunks, stream);
 		// chunk order = chunk file-name order (the oracle's sorted directory scan)
 		std::vector<std::pair<std::string, ChunkCell>> chunks;
-		for (auto& c : cells_found) chunks.push_back({chunk_id(c, G), c});
+		for (auto& c : cells_found) chunks.push_back({chunk_id(c), c});
 		std::sort(chunks.begin(), chunks.end(), [](const auto& a, const auto& b) { return a.first + ".bin" < b.first + ".bin"; });
 		std::vector<ChunkCell> sorted_cells;
 		for (auto& c : chunks) sorted_cells.push_back(c.second);

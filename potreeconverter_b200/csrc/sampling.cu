@@ -195,6 +195,9 @@ __device__ int64_t warp_partition(double* key, int32_t* val, int64_t f, int64_t 
 	return f + (c1 < c2 ? c1 : c2);
 }
 
+constexpr int kWarpsPerBlock = 4;
+constexpr int kStackDepth = 128;
+
 struct Seg { int64_t f, l; int32_t d; int32_t pad; };
 
 // Replays std::sort (std::__sort) on key/val[0..n) with one warp.
@@ -226,6 +229,12 @@ __device__ void warp_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL,
 				}
 				d--;
 				int64_t cut = warp_partition(key, val, f, l, SL + f, SR + f);
+				if (cut <= f || cut >= l || sp >= kStackDepth) {
+					// cannot happen for comparable keys (the median-of-three
+					// guarantees stops on both sides); record and stop
+					if (lane == 0) atomicAdd(&st->timeouts, 1ull);
+					break;
+				}
 				if (lane == 0) stack[sp] = {cut, l, d, 0};
 				sp++;
 				__syncwarp();
@@ -257,8 +266,6 @@ __device__ void warp_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL,
 	__syncwarp();
 }
 
-constexpr int kWarpsPerBlock = 4;
-constexpr int kStackDepth = 128;
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) node_sort_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order,
                                                                        int node_begin, int node_end, LevelBuffers lb, SortScratch sc,

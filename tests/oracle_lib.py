@@ -26,7 +26,8 @@ class _Out(ctypes.Structure):
                 ("hierarchy", ctypes.POINTER(ctypes.c_uint8)), ("hierarchy_size", ctypes.c_uint64),
                 ("metadata", ctypes.c_char_p), ("metadata_size", ctypes.c_uint64),
                 ("num_chunks", ctypes.c_int32), ("chunk_ids", ctypes.c_void_p),
-                ("chunk_counts", ctypes.POINTER(ctypes.c_int64)), ("error", ctypes.c_char * 256)]
+                ("chunk_counts", ctypes.POINTER(ctypes.c_int64)), ("error", ctypes.c_char * 256),
+                ("num_nodes", ctypes.c_int64), ("node_names", ctypes.c_void_p), ("node_info", ctypes.POINTER(ctypes.c_int64))]
 
 
 def build_oracle():
@@ -65,6 +66,13 @@ class Oracle:
             chunk_ids.append(s.decode())
             off += len(s) + 1
         res["chunks"] = list(zip(chunk_ids, [out.chunk_counts[i] for i in range(out.num_chunks)]))
+        nodes = []
+        off = 0
+        for i in range(out.num_nodes):
+            s = ctypes.string_at(out.node_names + off)
+            off += len(s) + 1
+            nodes.append((s.decode(), out.node_info[3 * i], out.node_info[3 * i + 1], out.node_info[3 * i + 2]))
+        res["nodes"] = nodes  # completion order: (name, byte offset, byte size, points)
         self.lib.pcref_free(ctypes.byref(out))
         return res
 

@@ -1,0 +1,37 @@
+"""Single-kernel parity: the device replay of std::sort and std::shuffle
+against libstdc++ itself (through the oracle library)."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 15, 16, 17, 33, 100, 1000, 4097, 100_000])
+@pytest.mark.parametrize("ties", ["none", "few", "many", "all"])
+def test_sort_matches_std_sort(gpu_ctx, oracle, n, ties):
+    rng = np.random.default_rng(n * 7 + len(ties))
+    if ties == "none":
+        keys = rng.random(n)
+    elif ties == "few":
+        keys = rng.integers(0, max(1, n), n).astype(np.float64)
+    elif ties == "many":
+        keys = rng.integers(0, 5, n).astype(np.float64)
+    else:
+        keys = np.zeros(n)
+    assert (gpu_ctx.sort_keys(keys) == oracle.sort_perm(keys)).all()
+
+
+@pytest.mark.parametrize("pattern", ["sorted", "reversed", "organ", "sawtooth"])
+def test_sort_adversarial_orders(gpu_ctx, oracle, pattern):
+    n = 50_000
+    i = np.arange(n, dtype=np.float64)
+    keys = {"sorted": i, "reversed": i[::-1].copy(), "organ": np.minimum(i, n - i),
+            "sawtooth": i % 97}[pattern]
+    assert (gpu_ctx.sort_keys(keys) == oracle.sort_perm(keys)).all()
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 3, 4, 99, 100, 101, 5000, 9999, 10000])
+@pytest.mark.parametrize("seed", [1592614637, 0, 1, 2147483647, 4294967295])
+def test_shuffle_matches_std_shuffle(gpu_ctx, oracle, n, seed):
+    assert (gpu_ctx.shuffle(n, seed) == oracle.shuffle(n, seed)).all()
