@@ -64,16 +64,27 @@ typedef struct pcg_opts {
 	                          pinned reference uses 1592614637               */
 	int32_t form;          /* pcg_form                                        */
 	int32_t reserved;
+	void* stream;          /* cudaStream_t for all device work, or NULL for a
+	                          stream owned by the context                     */
 } pcg_opts;
 
+enum {
+	PCG_JOB_OCTREE_ON_DEVICE = 1  /* leave octree.bin in device memory:
+	                                 pcg_result.octree is then a device pointer */
+};
+
 typedef struct pcg_job {
-	const void* las;       /* uncompressed LAS file image (host memory)      */
+	const void* las;       /* uncompressed LAS file image (host memory); with
+	                          device_records set, only its header and VLRs
+	                          are read                                        */
 	uint64_t las_size;
 	int32_t method;        /* pcg_method                                      */
-	int32_t reserved;
+	int32_t flags;         /* PCG_JOB_* bits                                  */
 	const char* name;      /* metadata.json "name" (the reference uses the
 	                          input file's stem, main.cpp:171-173)            */
 	const char* projection;/* metadata.json "projection" (may be NULL)       */
+	const void* device_records; /* point records already in device memory
+	                          (record_length * point count bytes), or NULL    */
 } pcg_job;
 
 typedef struct pcg_stats {
@@ -87,10 +98,14 @@ typedef struct pcg_stats {
 	double ms_total;              /* wall time of pcg_convert               */
 	double ms_h2d, ms_chunking, ms_octree, ms_sampling, ms_output, ms_d2h, ms_host_writers;
 	int64_t gpu_launches;         /* kernels launched for this job          */
+	double ms_sort, ms_greedy;    /* device time of the sampler sort / acceptance kernels */
+	int64_t sampled_nodes;        /* inner nodes sampled                    */
+	int64_t candidates;           /* candidate points over all sampled nodes */
 } pcg_stats;
 
 typedef struct pcg_result {
-	uint8_t* octree;       uint64_t octree_size;
+	uint8_t* octree;       uint64_t octree_size;     /* host memory unless the
+	                                                    job asked for device */
 	uint8_t* hierarchy;    uint64_t hierarchy_size;
 	char* metadata;        uint64_t metadata_size;   /* NUL terminated */
 	pcg_stats stats;

@@ -35,12 +35,16 @@ class PcgError(RuntimeError):
 
 class _Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("random_seed", ctypes.c_uint32), ("form", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("reserved", ctypes.c_int32), ("stream", ctypes.c_void_p)]
 
 
 class _Job(ctypes.Structure):
     _fields_ = [("las", ctypes.c_void_p), ("las_size", ctypes.c_uint64), ("method", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("name", ctypes.c_char_p), ("projection", ctypes.c_char_p)]
+                ("flags", ctypes.c_int32), ("name", ctypes.c_char_p), ("projection", ctypes.c_char_p),
+                ("device_records", ctypes.c_void_p)]
+
+
+OCTREE_ON_DEVICE = 1
 
 
 class _Stats(ctypes.Structure):
@@ -49,7 +53,9 @@ class _Stats(ctypes.Structure):
                 ("escalated_pairs", ctypes.c_int64), ("heapsort_fallbacks", ctypes.c_int64),
                 ("ms_total", ctypes.c_double), ("ms_h2d", ctypes.c_double), ("ms_chunking", ctypes.c_double),
                 ("ms_octree", ctypes.c_double), ("ms_sampling", ctypes.c_double), ("ms_output", ctypes.c_double),
-                ("ms_d2h", ctypes.c_double), ("ms_host_writers", ctypes.c_double), ("gpu_launches", ctypes.c_int64)]
+                ("ms_d2h", ctypes.c_double), ("ms_host_writers", ctypes.c_double), ("gpu_launches", ctypes.c_int64),
+                ("ms_sort", ctypes.c_double), ("ms_greedy", ctypes.c_double), ("sampled_nodes", ctypes.c_int64),
+                ("candidates", ctypes.c_int64)]
 
 
 class _Result(ctypes.Structure):
@@ -122,9 +128,9 @@ def _take(lib, res: _Result) -> Conversion:
 class Context:
     """A device context (pcg_create/pcg_destroy)."""
 
-    def __init__(self, device: int = 0, seed: int = PINNED_SEED, form: str = "batched"):
+    def __init__(self, device: int = 0, seed: int = PINNED_SEED, form: str = "batched", stream: int | None = None):
         self._lib = load_library()
-        opts = _Opts(device, seed, FORMS[form], 0)
+        opts = _Opts(device, seed, FORMS[form], 0, stream)
         h = ctypes.c_void_p()
         st = self._lib.pcg_create(ctypes.byref(h), ctypes.byref(opts))
         if st != 0:
@@ -152,7 +158,7 @@ class Context:
         return PcgError(st, self._lib.pcg_last_error(self._h).decode(errors="replace"))
 
     @staticmethod
-    def _job(las, method, name, projection, keep):
+    def _job(las, method, name, projection, keep, device_records=None, flags=0):
         if isinstance(las, (bytes, bytearray, memoryview)):
             buf = (ctypes.c_uint8 * len(las)).from_buffer_copy(las) if isinstance(las, bytes) else \
                 (ctypes.c_uint8 * len(las)).from_buffer(las)
@@ -163,7 +169,7 @@ class Context:
         nm = name.encode()
         pj = projection.encode()
         keep.extend([nm, pj])
-        return _Job(ptr, size, METHODS[method], 0, nm, pj)
+        return _Job(ptr, size, METHODS[method], flags, nm, pj, device_records)
 
     def convert(self, las, method: str = "poisson", name: str = "cloud", projection: str = "") -> Conversion:
         """Converts one LAS file image (bytes, or (host pointer, size))."""
@@ -174,6 +180,34 @@ class Context:
         if st != 0:
             raise self._err(st)
         return _take(self._lib, res)
+
+    def convert_stats(self, las, method: str = "poisson", name: str = "cloud") -> dict:
+        """Converts like :meth:`convert` (octree.bin lands in pinned host
+        memory) but returns only the statistics, releasing the outputs."""
+        keep = []
+        job = self._job(las, method, name, "", keep)
+        res = _Result()
+        st = self._lib.pcg_convert(self._h, ctypes.byref(job), ctypes.byref(res))
+        if st != 0:
+            raise self._err(st)
+        stats = {n: getattr(res.stats, n) for n, _ in _Stats._fields_}
+        stats["octree_size"] = res.octree_size
+        self._lib.pcg_result_free(ctypes.byref(res))
+        return stats
+
+    def convert_resident(self, header, device_records: int, method: str = "poisson", name: str = "cloud") -> dict:
+        """Converts point records already in device memory; octree.bin stays
+        on the device and is released at once. Returns the run statistics."""
+        keep = []
+        job = self._job(header, method, name, "", keep, device_records=device_records, flags=OCTREE_ON_DEVICE)
+        res = _Result()
+        st = self._lib.pcg_convert(self._h, ctypes.byref(job), ctypes.byref(res))
+        if st != 0:
+            raise self._err(st)
+        stats = {n: getattr(res.stats, n) for n, _ in _Stats._fields_}
+        stats["octree_size"] = res.octree_size
+        self._lib.pcg_result_free(ctypes.byref(res))
+        return stats
 
     def submit(self, las, method: str = "poisson", name: str = "cloud", projection: str = "") -> int:
         keep = []

@@ -90,7 +90,9 @@ struct Setup {
 	int first_extra_index = 0;
 };
 
-bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& err);
+// points_elsewhere: the point records are not part of this buffer (they are
+// already in device memory), so only the header and VLRs must be present.
+bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& err, bool points_elsewhere = false);
 bool make_setup(const LasInfo& info, Setup& s, std::string& err);
 
 // ---------------------------------------------------------- device params

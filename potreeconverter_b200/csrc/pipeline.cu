@@ -133,11 +133,84 @@ std::vector<T> download(const T* d, size_t n, cudaStream_t s) {
 	return v;
 }
 
+// Pinned host buffers for octree.bin images, recycled between jobs so the
+// device-to-host copy runs at link speed instead of paying for page locking
+// every time. Buffers handed out in a pcg_result come back in pcg_result_free.
+class PinnedPool {
+public:
+	uint8_t* take(size_t n) {
+		std::lock_guard<std::mutex> lk(m_);
+		if (n == 0) n = 1;
+		auto it = free_.lower_bound(n);
+		if (it != free_.end() && it->first <= 2 * n + (size_t(64) << 20)) {
+			void* p = it->second;
+			cached_ -= it->first;
+			free_.erase(it);
+			return static_cast<uint8_t*>(p);
+		}
+		void* p = nullptr;
+		if (cudaMallocHost(&p, n) != cudaSuccess) {
+			cudaGetLastError();
+			return nullptr;
+		}
+		owned_[p] = n;
+		return static_cast<uint8_t*>(p);
+	}
+	bool give(void* p) {
+		std::lock_guard<std::mutex> lk(m_);
+		auto it = owned_.find(p);
+		if (it == owned_.end()) return false;
+		free_.insert({it->second, p});
+		cached_ += it->second;
+		while (cached_ > kMaxCached && !free_.empty()) {  // drop the largest
+			auto last = std::prev(free_.end());
+			cached_ -= last->first;
+			owned_.erase(last->second);
+			cudaFreeHost(last->second);
+			free_.erase(last);
+		}
+		return true;
+	}
+
+private:
+	static constexpr size_t kMaxCached = size_t(8) << 30;
+	std::mutex m_;
+	std::multimap<size_t, void*> free_;
+	std::unordered_map<void*, size_t> owned_;
+	size_t cached_ = 0;
+};
+
+PinnedPool g_pinned;
+
+// octree.bin images left in device memory (PCG_JOB_OCTREE_ON_DEVICE)
+std::mutex g_dev_mtx;
+std::unordered_map<void*, int> g_dev_results;  // pointer -> device
+
+void release_octree(void* p) {
+	if (!p) return;
+	int dev = -1;
+	{
+		std::lock_guard<std::mutex> lk(g_dev_mtx);
+		auto it = g_dev_results.find(p);
+		if (it != g_dev_results.end()) { dev = it->second; g_dev_results.erase(it); }
+	}
+	if (dev >= 0) {
+		int cur = 0;
+		cudaGetDevice(&cur);
+		cudaSetDevice(dev);
+		cudaFree(p);
+		cudaSetDevice(cur);
+	} else if (!g_pinned.give(p)) {
+		cudaFreeHost(p);
+	}
+}
+
 struct JobResult {
 	std::vector<uint8_t> hierarchy;
 	std::string metadata;
-	uint8_t* octree = nullptr;  // pinned host memory
+	uint8_t* octree = nullptr;  // pinned host memory, or device memory
 	uint64_t octree_size = 0;
+	bool octree_on_device = false;
 	pcg_stats stats{};
 };
 
@@ -146,6 +219,7 @@ struct Converter {
 	cudaStream_t stream = nullptr;
 	uint32_t seed = 1592614637u;
 	int form = PCG_FORM_BATCHED;
+	PinnedPool* host_buffers = &g_pinned;
 
 	void run(const pcg_job& job, JobResult& res) {
 		auto t0 = Clock::now();
@@ -154,7 +228,8 @@ struct Converter {
 		std::string err;
 		LasInfo info;
 		const uint8_t* las = static_cast<const uint8_t*>(job.las);
-		if (!las || !parse_las(las, job.las_size, info, err)) throw PcgError(PCG_BAD_INPUT, err.empty() ? "no input" : err);
+		if (!las || !parse_las(las, job.las_size, info, err, job.device_records != nullptr))
+			throw PcgError(PCG_BAD_INPUT, err.empty() ? "no input" : err);
 		Setup s;
 		if (!make_setup(info, s, err)) throw PcgError(PCG_BAD_INPUT, err);
 		if (job.method < 0 || job.method > 2) throw PcgError(PCG_BAD_INPUT, "unknown sampling method");
@@ -168,9 +243,14 @@ struct Converter {
 		// ---------------------------------------------------------- input
 		auto t_h2d = Clock::now();
 		const int64_t rec_bytes = N * (int64_t)info.record_length;
-		uint8_t* d_recs = mem.alloc<uint8_t>(rec_bytes);
-		PCG_CUDA(cudaMemcpyAsync(d_recs, las + info.offset_to_points, rec_bytes, cudaMemcpyHostToDevice, stream));
-		PCG_CUDA(cudaStreamSynchronize(stream));
+		uint8_t* d_recs = nullptr;
+		if (job.device_records) {
+			d_recs = static_cast<uint8_t*>(const_cast<void*>(job.device_records));
+		} else {
+			d_recs = mem.alloc<uint8_t>(rec_bytes);
+			PCG_CUDA(cudaMemcpyAsync(d_recs, las + info.offset_to_points, rec_bytes, cudaMemcpyHostToDevice, stream));
+			PCG_CUDA(cudaStreamSynchronize(stream));
+		}
 		res.stats.ms_h2d = ms_since(t_h2d);
 
 		// ------------------------------------------------------- chunking
@@ -410,15 +490,27 @@ struct Converter {
 			}
 			recs.push_back(r);
 		}
-		uint8_t* d_out = mem.alloc<uint8_t>(out_points * s.bpp);
+		const bool keep_on_device = (job.flags & PCG_JOB_OCTREE_ON_DEVICE) != 0;
+		res.octree_size = (uint64_t)(out_points * s.bpp);
+		uint8_t* d_out = nullptr;
+		if (keep_on_device) {
+			// outlives the job's allocations; released by pcg_result_free
+			PCG_CUDA(cudaMallocAsync((void**)&d_out, res.octree_size ? res.octree_size : 1, stream));
+			res.octree = d_out;
+			res.octree_on_device = true;
+		} else {
+			d_out = mem.alloc<uint8_t>(res.octree_size);
+		}
 		PayloadItem* d_items = upload(items, mem);
 		launch_write_payloads(d_recs, p, co.X, co.Y, co.Z, d_items, (int)items.size(), d_out, mem);
 		PCG_CUDA(cudaStreamSynchronize(stream));
 		res.stats.ms_output = ms_since(t_out);
 		auto t_d2h = Clock::now();
-		res.octree_size = (uint64_t)(out_points * s.bpp);
-		PCG_CUDA(cudaMallocHost((void**)&res.octree, res.octree_size ? res.octree_size : 1));
-		if (res.octree_size) PCG_CUDA(cudaMemcpyAsync(res.octree, d_out, res.octree_size, cudaMemcpyDeviceToHost, stream));
+		if (!keep_on_device) {
+			res.octree = host_buffers ? host_buffers->take(res.octree_size) : nullptr;
+			if (!res.octree) PCG_CUDA(cudaMallocHost((void**)&res.octree, res.octree_size ? res.octree_size : 1));
+			if (res.octree_size) PCG_CUDA(cudaMemcpyAsync(res.octree, d_out, res.octree_size, cudaMemcpyDeviceToHost, stream));
+		}
 		auto stats_dev = download(co.stats, MAX_ATTRS, stream);
 		auto hist = download(co.histogram, 256, stream);
 		res.stats.ms_d2h = ms_since(t_d2h);
@@ -533,6 +625,8 @@ struct Converter {
 			l.spacing = base_spacing / std::pow(2.0, (double)n.depth);  // sampler_poisson.h:114
 			l.pad = 0;
 		}
+		res.stats.sampled_nodes += K;
+		res.stats.candidates += M;
 		cudaStream_t s = stream;
 		LevelBuffers lb;
 		lb.M = M;
@@ -567,15 +661,29 @@ struct Converter {
 			int32_t* apos = mem.alloc<int32_t>(M);
 			const int mode = method == PCG_POISSON ? 0 : 1;
 			const bool guard = form == PCG_FORM_BATCHED;
+			int num_big = 0;
+			while (num_big < K && ln[order[num_big]].count >= kBigNodeCandidates) num_big++;
+			cudaEvent_t ev[3];
+			for (auto& e : ev) PCG_CUDA(cudaEventCreate(&e));
+			PCG_CUDA(cudaEventRecord(ev[0], s));
 			if (form == PCG_FORM_PLAIN) {
-				for (int k = 0; k < K; k++) {
-					launch_node_sort(d_nodes, d_order, K, lb, d_st, mem, k, k + 1);
-					launch_greedy(mode, false, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, k, k + 1);
-				}
+				for (int k = 0; k < K; k++) launch_node_sort(d_nodes, d_order, K, lb, d_st, mem, k, k + 1, num_big);
+				PCG_CUDA(cudaEventRecord(ev[1], s));
+				for (int k = 0; k < K; k++)
+					launch_greedy(mode, false, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, k, k + 1, num_big);
 			} else {
-				launch_node_sort(d_nodes, d_order, K, lb, d_st, mem);
-				launch_greedy(mode, guard, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem);
+				launch_node_sort(d_nodes, d_order, K, lb, d_st, mem, 0, -1, num_big);
+				PCG_CUDA(cudaEventRecord(ev[1], s));
+				launch_greedy(mode, guard, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, 0, -1, num_big);
 			}
+			PCG_CUDA(cudaEventRecord(ev[2], s));
+			PCG_CUDA(cudaEventSynchronize(ev[2]));
+			float t_sort = 0, t_greedy = 0;
+			PCG_CUDA(cudaEventElapsedTime(&t_sort, ev[0], ev[1]));
+			PCG_CUDA(cudaEventElapsedTime(&t_greedy, ev[1], ev[2]));
+			res.stats.ms_sort += t_sort;
+			res.stats.ms_greedy += t_greedy;
+			for (auto& e : ev) cudaEventDestroy(e);
 			if (method == PCG_POISSON_AVERAGE) {
 				long long* sums = mem.alloc<long long>(4 * M);
 				launch_average_colors(d_nodes, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, anext, apos, nullptr, sums, mem);
@@ -769,6 +877,7 @@ struct pcg_ctx {
 	size_t budget = 0, in_use = 0;
 	uint64_t next_id = 1;
 	bool stopping = false;
+	bool own_stream = true;
 };
 
 namespace {
@@ -795,8 +904,12 @@ pcg_status guarded(pcg_ctx* ctx, F&& f) {
 	}
 }
 
-void move_result(pcg::JobResult& r, pcg_result* out) {
+void move_result(pcg::JobResult& r, pcg_result* out, int device) {
 	memset(out, 0, sizeof(*out));
+	if (r.octree_on_device && r.octree) {
+		std::lock_guard<std::mutex> lk(pcg::g_dev_mtx);
+		pcg::g_dev_results[r.octree] = device;
+	}
 	out->octree = r.octree;
 	out->octree_size = r.octree_size;
 	r.octree = nullptr;
@@ -893,7 +1006,12 @@ pcg_status pcg_create(pcg_ctx** out, const pcg_opts* opts) {
 		PCG_CUDA(cudaGetDeviceCount(&n));
 		if (ctx->conv.device < 0 || ctx->conv.device >= n) throw pcg::PcgError(PCG_BAD_INPUT, "no such CUDA device");
 		PCG_CUDA(cudaSetDevice(ctx->conv.device));
-		PCG_CUDA(cudaStreamCreateWithFlags(&ctx->conv.stream, cudaStreamNonBlocking));
+		if (opts && opts->stream) {
+			ctx->conv.stream = static_cast<cudaStream_t>(opts->stream);
+			ctx->own_stream = false;
+		} else {
+			PCG_CUDA(cudaStreamCreateWithFlags(&ctx->conv.stream, cudaStreamNonBlocking));
+		}
 		cudaMemPool_t pool;
 		PCG_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctx->conv.device));
 		uint64_t threshold = UINT64_MAX;
@@ -916,12 +1034,13 @@ void pcg_destroy(pcg_ctx* ctx) {
 	}
 	ctx->qcv.notify_all();
 	for (auto& t : ctx->workers) t.join();
-	for (auto& kv : ctx->jobs) if (kv.second->result.octree) cudaFreeHost(kv.second->result.octree);
+	for (auto& kv : ctx->jobs)
+		if (kv.second->result.octree && !pcg::g_pinned.give(kv.second->result.octree)) cudaFreeHost(kv.second->result.octree);
 	cudaSetDevice(ctx->conv.device);
 	for (auto s : ctx->worker_streams) cudaStreamDestroy(s);
 	if (ctx->conv.stream) {
 		cudaStreamSynchronize(ctx->conv.stream);
-		cudaStreamDestroy(ctx->conv.stream);
+		if (ctx->own_stream) cudaStreamDestroy(ctx->conv.stream);
 	}
 	delete ctx;
 }
@@ -935,16 +1054,17 @@ pcg_status pcg_convert(pcg_ctx* ctx, const pcg_job* job, pcg_result* out) {
 	pcg::JobResult r;
 	pcg_status st = guarded(ctx, [&] { ctx->conv.run(*job, r); });
 	if (st != PCG_OK) {
-		if (r.octree) cudaFreeHost(r.octree);
+		if (r.octree_on_device && r.octree) cudaFree(r.octree);
+		else if (r.octree && !pcg::g_pinned.give(r.octree)) cudaFreeHost(r.octree);
 		return st;
 	}
-	move_result(r, out);
+	move_result(r, out, ctx->conv.device);
 	return PCG_OK;
 }
 
 void pcg_result_free(pcg_result* r) {
 	if (!r) return;
-	if (r->octree) cudaFreeHost(r->octree);
+	pcg::release_octree(r->octree);
 	free(r->hierarchy);
 	free(r->metadata);
 	memset(r, 0, sizeof(*r));
@@ -1020,7 +1140,7 @@ pcg_status pcg_wait(pcg_ctx* ctx, uint64_t job_id, pcg_result* out) {
 		ctx->last_error = j->error;
 		return j->status;
 	}
-	move_result(j->result, out);
+	move_result(j->result, out, ctx->conv.device);
 	return PCG_OK;
 }
 

@@ -200,55 +200,62 @@ constexpr int kStackDepth = 128;
 
 struct Seg { int64_t f, l; int32_t d; int32_t pad; };
 
-// Replays std::sort (std::__sort) on key/val[0..n) with one warp.
-__device__ void warp_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL, int32_t* SR, int32_t* blk, Seg* stack,
-                              SampleStats* st) {
+__device__ __forceinline__ int introsort_depth(int64_t n) { return 2 * (63 - __clzll((long long)n)); }  // std::__lg(n) * 2
+
+// Replays std::__introsort_loop on [f0, l0) with depth budget d0, one warp.
+// The <= 16-element segments the loop leaves behind are appended to blk
+// (counter nblk); heap-sorted segments need no final pass.
+__device__ void warp_introsort(double* key, int32_t* val, int64_t f0, int64_t l0, int d0, int32_t* SL, int32_t* SR, int32_t* blk,
+                               int* nblk, Seg* stack, SampleStats* st, int stack_cap = kStackDepth) {
 	const int lane = threadIdx.x & 31;
-	int nblk = 0;
-	if (n > 1) {
-		int sp = 0;
-		if (lane == 0) stack[0] = {0, n, 2 * (63 - __clzll((long long)n)), 0};
-		sp = 1;
+	if (lane == 0) stack[0] = {f0, l0, d0, 0};
+	int sp = 1;
+	__syncwarp();
+	while (sp > 0) {
+		Seg s = stack[sp - 1];
+		sp--;
 		__syncwarp();
-		while (sp > 0) {
-			Seg s = stack[sp - 1];
-			sp--;
-			__syncwarp();
-			int64_t f = s.f, l = s.l;
-			int d = s.d;
-			bool heaped = false;
-			while (l - f > 16) {
-				if (d == 0) {
-					if (lane == 0) {
-						heap_sort(key + f, val + f, l - f);
-						atomicAdd(&st->heapsorts, 1ull);
-					}
-					__syncwarp();
-					heaped = true;
-					break;
+		int64_t f = s.f, l = s.l;
+		int d = s.d;
+		bool done = false;
+		while (l - f > 16) {
+			if (d == 0) {
+				if (lane == 0) {
+					heap_sort(key + f, val + f, l - f);
+					atomicAdd(&st->heapsorts, 1ull);
 				}
-				d--;
-				int64_t cut = warp_partition(key, val, f, l, SL + f, SR + f);
-				if (cut <= f || cut >= l || sp >= kStackDepth) {
-					// cannot happen for comparable keys (the median-of-three
-					// guarantees stops on both sides); record and stop
-					if (lane == 0) atomicAdd(&st->timeouts, 1ull);
-					break;
-				}
-				if (lane == 0) stack[sp] = {cut, l, d, 0};
-				sp++;
 				__syncwarp();
-				l = cut;
+				done = true;
+				break;
 			}
-			if (!heaped && l - f > 1) {
-				if (lane == 0) { blk[2 * nblk] = (int32_t)f; blk[2 * nblk + 1] = (int32_t)l; }
-				nblk++;
+			d--;
+			int64_t cut = warp_partition(key, val, f, l, SL + f, SR + f);
+			if (cut <= f || cut >= l || sp >= stack_cap) {
+				// cannot happen for comparable keys (the median-of-three
+				// guarantees stops on both sides, and a path holds at most
+				// depth-budget pending segments); record and stop
+				if (lane == 0) atomicAdd(&st->timeouts, 1ull);
+				done = true;
+				break;
 			}
+			if (lane == 0) stack[sp] = {cut, l, d, 0};
+			sp++;
+			__syncwarp();
+			l = cut;
+		}
+		if (!done && l - f > 1 && lane == 0) {
+			int b = atomicAdd(nblk, 1);
+			blk[2 * b] = (int32_t)f;
+			blk[2 * b + 1] = (int32_t)l;
 		}
 	}
 	__syncwarp();
-	// final insertion sort == stable sort inside each block
-	for (int b = lane; b < nblk; b += 32) {
+}
+
+// std::__final_insertion_sort: on the block structure the introsort loop
+// leaves, it equals a stable insertion sort inside every block.
+__device__ void insertion_blocks(double* key, int32_t* val, const int32_t* blk, int nblk, int tid, int nthreads) {
+	for (int b = tid; b < nblk; b += nthreads) {
 		int64_t s = blk[2 * b], e = blk[2 * b + 1];
 		for (int64_t i = s + 1; i < e; i++) {
 			double vk = key[i];
@@ -263,14 +270,25 @@ __device__ void warp_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL,
 			val[j] = vv;
 		}
 	}
-	__syncwarp();
 }
 
+// std::sort on key/val[0..n) with one warp.
+__device__ void warp_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL, int32_t* SR, int32_t* blk, Seg* stack, int* nblk,
+                              SampleStats* st) {
+	const int lane = threadIdx.x & 31;
+	if (lane == 0) *nblk = 0;
+	__syncwarp();
+	if (n > 1) warp_introsort(key, val, 0, n, introsort_depth(n), SL, SR, blk, nblk, stack, st);
+	__syncwarp();
+	insertion_blocks(key, val, blk, *nblk, lane, 32);
+	__syncwarp();
+}
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) node_sort_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order,
                                                                        int node_begin, int node_end, LevelBuffers lb, SortScratch sc,
                                                                        SampleStats* st, int* next_node) {
 	__shared__ Seg stacks[kWarpsPerBlock][kStackDepth];
+	__shared__ int nblk[kWarpsPerBlock];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	while (true) {
 		int idx = 0;
@@ -280,15 +298,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) node_sort_kernel(const Le
 		const LevelNode nd = nodes[order[idx]];
 		double* key = lb.keys + nd.cand_off;
 		int32_t* val = lb.perm + nd.cand_off;
-		warp_std_sort(key, val, nd.count, sc.SL + nd.cand_off, sc.SR + nd.cand_off, sc.blk + 2 * nd.cand_off, stacks[warp], st);
+		warp_std_sort(key, val, nd.count, sc.SL + nd.cand_off, sc.SR + nd.cand_off, sc.blk + 2 * nd.cand_off, stacks[warp], &nblk[warp], st);
 		for (int64_t t = lane; t < nd.count; t += 32) lb.pos[nd.cand_off + val[t]] = (int32_t)t;
 	}
 }
 
 __global__ void sort_single_kernel(double* key, int32_t* val, int64_t n, SortScratch sc, SampleStats* st) {
 	__shared__ Seg stack[kStackDepth];
+	__shared__ int nblk;
 	if (threadIdx.x >= 32) return;
-	warp_std_sort(key, val, n, sc.SL, sc.SR, sc.blk, stack, st);
+	warp_std_sort(key, val, n, sc.SL, sc.SR, sc.blk, stack, &nblk, st);
 }
 
 // --------------------------------------------------------------- hashing
@@ -710,6 +729,419 @@ __global__ void shuffle_single_kernel(int64_t n, uint32_t seed, int32_t* perm) {
 	std_shuffle(perm, n, seed);
 }
 
+// ============================================ one CTA per large node
+// Nodes with many candidates (upper octree levels, dense 3D data) would keep
+// a single warp busy for a long time while the GPU idles. They get a whole
+// CTA: the sort partitions large segments with the block, and the greedy
+// decides 512 candidates per round.
+
+constexpr int kBigThreads = 512;
+constexpr int kBigWarps = kBigThreads / 32;
+constexpr int kBigSortMin = 4096;    // segments this long are partitioned by the whole CTA
+constexpr int kSmallQueue = 256;
+
+struct BlockScratch {
+	unsigned long long warp_sums[kBigWarps];
+	int64_t first_true;
+	int64_t bracket;
+};
+
+// exclusive scan of a packed (hi:lo) 64-bit count over the CTA
+__device__ unsigned long long block_scan_u64(unsigned long long v, unsigned long long& total, BlockScratch& sh) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	unsigned long long x = v;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		unsigned long long y = __shfl_up_sync(FULL, x, o);
+		if (lane >= o) x += y;
+	}
+	if (lane == 31) sh.warp_sums[warp] = x;
+	__syncthreads();
+	if (warp == 0) {
+		unsigned long long w = lane < kBigWarps ? sh.warp_sums[lane] : 0ull;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			unsigned long long y = __shfl_up_sync(FULL, w, o);
+			if (lane >= o) w += y;
+		}
+		if (lane < kBigWarps) sh.warp_sums[lane] = w;
+	}
+	__syncthreads();
+	unsigned long long before = warp > 0 ? sh.warp_sums[warp - 1] : 0ull;
+	total = sh.warp_sums[kBigWarps - 1];
+	__syncthreads();
+	return before + x - v;
+}
+
+// The same partition as warp_partition, computed by the whole CTA.
+__device__ int64_t block_partition(double* key, int32_t* val, int64_t f, int64_t l, int32_t* SL, int32_t* SR, BlockScratch& sh) {
+	const int tid = threadIdx.x;
+	if (tid == 0) {
+		int64_t a = f + 1, b = f + (l - f) / 2, c = l - 1;
+		double ka = key[a], kb = key[b], kc = key[c];
+		int64_t m;
+		if (ka < kb) {
+			if (kb < kc) m = b;
+			else if (ka < kc) m = c;
+			else m = a;
+		} else if (ka < kc) m = a;
+		else if (kb < kc) m = c;
+		else m = b;
+		double tk = key[f]; key[f] = key[m]; key[m] = tk;
+		int32_t tv = val[f]; val[f] = val[m]; val[m] = tv;
+	}
+	__syncthreads();
+	const double P = key[f];
+	int64_t cL = 0, cR = 0;
+	constexpr int IPT = 4;
+	for (int64_t base = f + 1; base < l; base += (int64_t)kBigThreads * IPT) {
+		const int64_t p0 = base + (int64_t)tid * IPT;
+		unsigned lm = 0, rm = 0;
+		uint32_t lc = 0, rc = 0;
+#pragma unroll
+		for (int k = 0; k < IPT; k++) {
+			int64_t p = p0 + k;
+			if (p < l) {
+				double kk = key[p];
+				if (!(kk < P)) { lm |= 1u << k; lc++; }
+				if (!(P < kk)) { rm |= 1u << k; rc++; }
+			}
+		}
+		unsigned long long total;
+		unsigned long long pre = block_scan_u64(((unsigned long long)rc << 32) | lc, total, sh);
+		int64_t lpos = cL + (int64_t)(pre & 0xffffffffull), rpos = cR + (int64_t)(pre >> 32);
+#pragma unroll
+		for (int k = 0; k < IPT; k++) {
+			if (lm & (1u << k)) SL[lpos++] = (int32_t)(p0 + k - f);
+			if (rm & (1u << k)) SR[rpos++] = (int32_t)(p0 + k - f);
+		}
+		cL += (int64_t)(total & 0xffffffffull);
+		cR += (int64_t)(total >> 32);
+	}
+	__syncthreads();
+	const int64_t m = cL < cR ? cL : cR;
+	// first k with !(SL[k] < SR[cR-1-k]); the predicate is monotone in k
+	if (tid == 0) { sh.first_true = m; sh.bracket = 0; }
+	__syncthreads();
+	const int64_t stride = (m + kBigThreads - 1) / kBigThreads;
+	if (m > 0) {
+		int64_t k = (int64_t)tid * stride;
+		if (k < m && !(SL[k] < SR[cR - 1 - k])) atomicMin((unsigned long long*)&sh.first_true, (unsigned long long)k);
+	}
+	__syncthreads();
+	const int64_t coarse = sh.first_true;  // a k where the predicate holds, or m
+	const int64_t lo = coarse >= stride ? coarse - stride + 1 : 0;
+	for (int64_t k = lo + tid; k < coarse && k < m; k += kBigThreads)
+		if (!(SL[k] < SR[cR - 1 - k])) atomicMin((unsigned long long*)&sh.first_true, (unsigned long long)k);
+	__syncthreads();
+	const int64_t K = sh.first_true;
+	for (int64_t k = tid; k < K; k += kBigThreads) {
+		int64_t i = f + SL[k], j = f + SR[cR - 1 - k];
+		double tk = key[i]; key[i] = key[j]; key[j] = tk;
+		int32_t tv = val[i]; val[i] = val[j]; val[j] = tv;
+	}
+	int64_t c1 = K < cL ? (int64_t)SL[K] : INT64_MAX;
+	int64_t c2 = K >= 1 ? (int64_t)SR[cR - K] : INT64_MAX;
+	__syncthreads();
+	return f + (c1 < c2 ? c1 : c2);
+}
+
+// std::sort on key/val[0..n) with one CTA: segments of at least
+// kBigSortMin elements are partitioned by the block, shorter ones by warps.
+__device__ void block_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL, int32_t* SR, int32_t* blk, SampleStats* st) {
+	__shared__ Seg bstack[kStackDepth];
+	__shared__ Seg queue[kSmallQueue];
+	__shared__ Seg wstacks[kBigWarps][64];
+	__shared__ int qn, nblk;
+	__shared__ BlockScratch sh;
+	const int tid = threadIdx.x, warp = tid >> 5;
+	if (tid == 0) { qn = 0; nblk = 0; }
+	__syncthreads();
+	auto drain = [&]() {
+		// warps take the queued small segments
+		for (int q = warp; q < qn; q += kBigWarps)
+			warp_introsort(key, val, queue[q].f, queue[q].l, queue[q].d, SL, SR, blk, &nblk, wstacks[warp], st, 64);
+		__syncthreads();
+		if (tid == 0) qn = 0;
+		__syncthreads();
+	};
+	if (n > 1) {
+		int sp = 1;
+		if (tid == 0) bstack[0] = {0, n, introsort_depth(n), 0};
+		__syncthreads();
+		while (sp > 0) {
+			Seg s = bstack[sp - 1];
+			sp--;
+			__syncthreads();
+			int64_t f = s.f, l = s.l;
+			int d = s.d;
+			bool done = false;
+			while (l - f > 16) {
+				if (l - f < kBigSortMin) {
+					if (tid == 0) queue[qn++] = {f, l, d, 0};
+					__syncthreads();
+					if (qn == kSmallQueue) drain();
+					done = true;
+					break;
+				}
+				if (d == 0) {
+					if (tid == 0) {
+						heap_sort(key + f, val + f, l - f);
+						atomicAdd(&st->heapsorts, 1ull);
+					}
+					__syncthreads();
+					done = true;
+					break;
+				}
+				d--;
+				int64_t cut = block_partition(key, val, f, l, SL + f, SR + f, sh);
+				if (cut <= f || cut >= l || sp >= kStackDepth) {
+					if (tid == 0) atomicAdd(&st->timeouts, 1ull);
+					done = true;
+					break;
+				}
+				if (tid == 0) bstack[sp] = {cut, l, d, 0};
+				sp++;
+				__syncthreads();
+				l = cut;
+			}
+			if (!done && l - f > 1 && tid == 0) {
+				int b = atomicAdd(&nblk, 1);
+				blk[2 * b] = (int32_t)f;
+				blk[2 * b + 1] = (int32_t)l;
+			}
+			__syncthreads();
+		}
+		drain();
+	}
+	insertion_blocks(key, val, blk, nblk, tid, kBigThreads);
+	__syncthreads();
+}
+
+__global__ void __launch_bounds__(kBigThreads) node_sort_big_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order,
+                                                                   int node_begin, LevelBuffers lb, SortScratch sc, SampleStats* st) {
+	const LevelNode nd = nodes[order[node_begin + blockIdx.x]];
+	int32_t* val = lb.perm + nd.cand_off;
+	block_std_sort(lb.keys + nd.cand_off, val, nd.count, sc.SL + nd.cand_off, sc.SR + nd.cand_off, sc.blk + 2 * nd.cand_off, st);
+	for (int64_t t = threadIdx.x; t < nd.count; t += kBigThreads) lb.pos[nd.cand_off + val[t]] = (int32_t)t;
+}
+
+__global__ void __launch_bounds__(kBigThreads) sort_single_big_kernel(double* key, int32_t* val, int64_t n, SortScratch sc, SampleStats* st) {
+	block_std_sort(key, val, n, sc.SL, sc.SR, sc.blk, st);
+}
+
+// Greedy acceptance, 512 candidates per round and CTA:
+//  A. each thread looks up its candidate's conflicts among the points
+//     accepted before the round (global spatial hash);
+//  B. conflicts among the round's own candidates are found through a shared
+//     memory hash of the round (earlier candidates within the spacing);
+//  C. warp 0 decides the round in sorted order, 32 candidates per step;
+//  D. the round's accepted points are appended and hashed.
+constexpr int kRound = kBigThreads;
+constexpr int kRoundHash = 2 * kRound;
+constexpr int kMaxLocal = 12;
+
+struct RoundShared {
+	double x[kRound], y[kRound], z[kRound], key[kRound], lim[kRound];
+	int32_t maxrank[kRound];
+	int32_t local[kRound];
+	uint64_t hkey[kRoundHash];
+	int16_t hhead[kRoundHash];
+	int16_t hnext[kRound];
+	int16_t conf[kRound][kMaxLocal];
+	uint8_t nconf[kRound];
+	uint8_t acc[kRound];
+	int32_t cnt;          // accepted before this round
+	int32_t round_acc;
+	unsigned long long warp_sums[kBigWarps];
+};
+
+__device__ __forceinline__ uint32_t round_slot(uint64_t k) { return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> 53) & (kRoundHash - 1); }
+
+template <int MODE>
+__global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order, int node_begin,
+                                                                const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
+                                                                const int32_t* __restrict__ Z, PosParamsS pp, LevelBuffers lb, GreedyArgs ga,
+                                                                SampleStats* st) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	RoundShared& R = *reinterpret_cast<RoundShared*>(smem_raw);
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const LevelNode nd = nodes[order[node_begin + blockIdx.x]];
+	const int64_t n = nd.count, co = nd.cand_off;
+	uint64_t* hk = ga.hkeys + nd.hash_off;
+	int32_t* hh = ga.hheads + nd.hash_off;
+	for (int64_t s = tid; s < nd.hash_cap; s += kBigThreads) { hk[s] = EMPTY_KEY; hh[s] = -1; }
+	if (tid == 0) R.cnt = 0;
+	__syncthreads();
+	const double sp = nd.spacing, s2 = sp * sp;
+	CellGrid g;
+	g.min[0] = nd.min[0]; g.min[1] = nd.min[1]; g.min[2] = nd.min[2];
+	g.inv = 1.0 / (2.0 * sp * 1.000001);
+	const uint32_t lt = lanemask_lt();
+	for (int64_t r0 = 0; r0 < n; r0 += kRound) {
+		const int64_t t = r0 + tid;
+		const bool valid = t < n;
+		const int nr = (int)((n - r0) < kRound ? (n - r0) : kRound);
+		// ---- A
+		double x = 0, y = 0, z = 0, key = 0, lim = -CUDART_INF;
+		int32_t local = 0, maxrank = -1;
+		int c[3] = {0, 0, 0};
+		double fr[3] = {0, 0, 0};
+		if (valid) {
+			local = lb.perm[co + t];
+			point_xyz(X, Y, Z, pp, lb.ids[co + local], x, y, z);
+			key = lb.keys[co + t];
+			if (MODE == 0) {
+				double cd = sqrt(key);
+				double limit = cd - sp;
+				lim = limit * limit;
+			}
+			cell_of(g, x, y, z, c, fr);
+			int o[3];
+			for (int a = 0; a < 3; a++) o[a] = fr[a] < 0.5 ? -1 : 1;
+#pragma unroll
+			for (int q = 0; q < 8; q++) {
+				int qx = c[0] + ((q & 4) ? o[0] : 0), qy = c[1] + ((q & 2) ? o[1] : 0), qz = c[2] + ((q & 1) ? o[2] : 0);
+				int32_t rr = hash_find(hk, hh, nd.hash_cap, cell_key(qx, qy, qz));
+				int64_t guard = 0;
+				while (rr >= 0 && guard++ <= n) {
+					const int64_t slot = co + rr;
+					if (MODE == 1 || ga.akey[slot] >= lim) {
+						if (sqdist(ga.axyz[3 * slot], ga.axyz[3 * slot + 1], ga.axyz[3 * slot + 2], x, y, z) < s2 && rr > maxrank) maxrank = rr;
+					}
+					rr = ga.anext[slot];
+				}
+				if (guard > n + 1) atomicAdd(&st->timeouts, 1ull);
+			}
+		}
+		R.x[tid] = x; R.y[tid] = y; R.z[tid] = z; R.key[tid] = key; R.lim[tid] = lim;
+		R.maxrank[tid] = maxrank;
+		R.local[tid] = local;
+		R.acc[tid] = 0;
+		R.nconf[tid] = 0;
+		for (int s = tid; s < kRoundHash; s += kBigThreads) { R.hkey[s] = EMPTY_KEY; R.hhead[s] = -1; }
+		__syncthreads();
+		// ---- B: hash the round by cell, then collect earlier conflicting candidates
+		if (valid) {
+			uint64_t k = cell_key(c[0], c[1], c[2]);
+			uint32_t s = round_slot(k);
+			for (int probe = 0; probe < kRoundHash; probe++) {
+				unsigned long long prev = atomicCAS((unsigned long long*)&R.hkey[s], (unsigned long long)EMPTY_KEY, (unsigned long long)k);
+				if (prev == EMPTY_KEY || prev == k) break;
+				s = (s + 1) & (kRoundHash - 1);
+			}
+			// lists are pushed with atomicExch on 16-bit heads via 32-bit CAS
+			int32_t* word = reinterpret_cast<int32_t*>(&R.hhead[s & ~1u]);
+			int shift = (s & 1u) ? 16 : 0;
+			while (true) {
+				int32_t old = *word;
+				int16_t head = (int16_t)((old >> shift) & 0xffff);
+				int32_t neu = (old & ~(0xffff << shift)) | ((int32_t)(uint16_t)tid << shift);
+				R.hnext[tid] = head;
+				if (atomicCAS(word, old, neu) == old) break;
+			}
+		}
+		__syncthreads();
+		if (valid) {
+			int o[3];
+			for (int a = 0; a < 3; a++) o[a] = fr[a] < 0.5 ? -1 : 1;
+			int nc = 0;
+			for (int q = 0; q < 8; q++) {
+				int qx = c[0] + ((q & 4) ? o[0] : 0), qy = c[1] + ((q & 2) ? o[1] : 0), qz = c[2] + ((q & 1) ? o[2] : 0);
+				uint64_t k = cell_key(qx, qy, qz);
+				uint32_t s = round_slot(k);
+				int16_t j = -1;
+				for (int probe = 0; probe < kRoundHash; probe++) {
+					uint64_t kk = R.hkey[s];
+					if (kk == k) { j = R.hhead[s]; break; }
+					if (kk == EMPTY_KEY) break;
+					s = (s + 1) & (kRoundHash - 1);
+				}
+				while (j >= 0) {
+					if (j < tid && (MODE == 1 || R.key[j] >= lim) && sqdist(R.x[j], R.y[j], R.z[j], x, y, z) < s2) {
+						if (nc < kMaxLocal) R.conf[tid][nc] = j;
+						nc++;
+					}
+					j = R.hnext[j];
+				}
+			}
+			R.nconf[tid] = (uint8_t)(nc < 255 ? nc : 255);
+		}
+		__syncthreads();
+		// ---- C: in-order decisions by warp 0
+		if (warp == 0) {
+			int32_t cnt = R.cnt;
+			for (int cb = 0; cb < nr; cb += 32) {
+				const int i = cb + lane;
+				const bool v = i < nr;
+				bool prev_conflict = false;
+				uint32_t mask = 0;
+				if (v) {
+					int nc = R.nconf[i];
+					if (nc <= kMaxLocal) {
+						for (int e = 0; e < nc; e++) {
+							int j = R.conf[i][e];
+							if (j < cb) prev_conflict |= R.acc[j] != 0;
+							else mask |= 1u << (j - cb);
+						}
+					} else {  // list overflow: check every earlier candidate of the round
+						for (int j = 0; j < i; j++) {
+							if ((MODE == 1 || R.key[j] >= R.lim[i]) && sqdist(R.x[j], R.y[j], R.z[j], R.x[i], R.y[i], R.z[i]) < s2) {
+								if (j < cb) prev_conflict |= R.acc[j] != 0;
+								else mask |= 1u << (j - cb);
+							}
+						}
+					}
+				}
+				uint32_t accmask = 0;
+				const int mr = R.maxrank[v ? i : 0];
+				const int nvalid = nr - cb < 32 ? nr - cb : 32;
+				for (int b = 0; b < nvalid; b++) {
+					bool dec = false;
+					if (lane == b) {
+						int32_t m_i = cnt + __popc(accmask);
+						bool old_conflict = mr >= 0 && (MODE == 1 || mr >= m_i - 10001);
+						dec = !old_conflict && !prev_conflict && !(mask & accmask);
+					}
+					dec = __shfl_sync(FULL, dec, b);
+					if (dec) accmask |= 1u << b;
+				}
+				if (v) R.acc[i] = (accmask >> lane) & 1u;
+				cnt += __popc(accmask);
+				__syncwarp();
+			}
+		}
+		__syncthreads();
+		// ---- D: publish
+		const bool acc = valid && R.acc[tid];
+		unsigned long long total;
+		unsigned long long pre;
+		{
+			BlockScratch& bs = *reinterpret_cast<BlockScratch*>(R.warp_sums);
+			pre = block_scan_u64(acc ? 1ull : 0ull, total, bs);
+		}
+		const int32_t base = R.cnt;
+		if (valid) {
+			lb.accepted[co + local] = acc ? 1 : 0;
+			if (acc) {
+				int32_t rank = base + (int32_t)pre;
+				lb.acc_rank[co + local] = rank;
+				const int64_t slot = co + rank;
+				ga.axyz[3 * slot] = x;
+				ga.axyz[3 * slot + 1] = y;
+				ga.axyz[3 * slot + 2] = z;
+				ga.akey[slot] = key;
+				ga.apos[slot] = (int32_t)t;
+				if (!hash_push(hk, hh, ga.anext + co, nd.hash_cap, cell_key(c[0], c[1], c[2]), rank)) atomicAdd(&st->timeouts, 1ull);
+			}
+		}
+		__syncthreads();
+		if (tid == 0) R.cnt = base + (int32_t)total;
+		__syncthreads();
+		(void)lt;
+	}
+}
+
 }  // namespace
 
 // ----------------------------------------------------------------- launchers
@@ -734,48 +1166,70 @@ static int sm_count() {
 }
 
 void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, LevelBuffers& lb, SampleStats* st, DeviceMem& mem,
-                      int node_begin, int node_end) {
+                      int node_begin, int node_end, int num_big) {
 	if (node_end < 0) node_end = K;
 	if (node_end <= node_begin || lb.M == 0) return;
 	SortScratch sc;
 	sc.SL = mem.alloc<int32_t>(lb.M);
 	sc.SR = mem.alloc<int32_t>(lb.M);
 	sc.blk = mem.alloc<int32_t>(2 * lb.M);
-	int* counter = mem.alloc<int>(1);
-	PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), mem.stream()));
-	int nodes_here = node_end - node_begin;
-	int blocks = (int)ceil_div(nodes_here, kWarpsPerBlock);
-	int cap = sm_count() * 16;
-	if (blocks > cap) blocks = cap;
-	node_sort_kernel<<<blocks, kWarpsPerBlock * 32, 0, mem.stream()>>>(nodes, order, node_begin, node_end, lb, sc, st, counter);
-	PCG_LAUNCHED();
+	// nodes order[0..num_big) get a CTA each, the rest a warp each
+	const int big_end = num_big < node_end ? num_big : node_end;
+	if (big_end > node_begin) {
+		node_sort_big_kernel<<<big_end - node_begin, kBigThreads, 0, mem.stream()>>>(nodes, order, node_begin, lb, sc, st);
+		PCG_LAUNCHED();
+	}
+	const int small_begin = node_begin > num_big ? node_begin : num_big;
+	if (node_end > small_begin) {
+		int* counter = mem.alloc<int>(1);
+		PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), mem.stream()));
+		int blocks = (int)ceil_div(node_end - small_begin, kWarpsPerBlock);
+		int cap = sm_count() * 16;
+		if (blocks > cap) blocks = cap;
+		node_sort_kernel<<<blocks, kWarpsPerBlock * 32, 0, mem.stream()>>>(nodes, order, small_begin, node_end, lb, sc, st, counter);
+		PCG_LAUNCHED();
+		mem.free(counter);
+	}
 	mem.free(sc.SL);
 	mem.free(sc.SR);
 	mem.free(sc.blk);
-	mem.free(counter);
 }
 
 void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int32_t* order, int K, const int32_t* X, const int32_t* Y,
                    const int32_t* Z, const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads,
                    double* acc_xyz, double* acc_key, int32_t* acc_next, int32_t* acc_pos, SampleStats* st, DeviceMem& mem,
-                   int node_begin, int node_end) {
+                   int node_begin, int node_end, int num_big) {
 	if (node_end < 0) node_end = K;
 	if (node_end <= node_begin || lb.M == 0) return;
 	GreedyArgs ga{hash_keys, hash_heads, acc_xyz, acc_key, acc_next, acc_pos};
-	int* counter = mem.alloc<int>(1);
-	PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), mem.stream()));
-	int nodes_here = node_end - node_begin;
-	int blocks = (int)ceil_div(nodes_here, kWarpsPerBlock);
-	int cap = sm_count() * 16;
-	if (blocks > cap) blocks = cap;
-	dim3 grid(blocks), block(kWarpsPerBlock * 32);
 	cudaStream_t s = mem.stream();
-	if (mode == 0 && fp32_guard) greedy_kernel<0, true><<<grid, block, 0, s>>>(nodes, order, node_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
-	else if (mode == 0) greedy_kernel<0, false><<<grid, block, 0, s>>>(nodes, order, node_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
-	else if (fp32_guard) greedy_kernel<1, true><<<grid, block, 0, s>>>(nodes, order, node_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
-	else greedy_kernel<1, false><<<grid, block, 0, s>>>(nodes, order, node_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
-	PCG_LAUNCHED();
-	mem.free(counter);
+	const int big_end = num_big < node_end ? num_big : node_end;
+	if (big_end > node_begin) {
+		size_t smem = sizeof(RoundShared);
+		if (mode == 0) {
+			PCG_CUDA(cudaFuncSetAttribute(greedy_big_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			greedy_big_kernel<0><<<big_end - node_begin, kBigThreads, smem, s>>>(nodes, order, node_begin, X, Y, Z, pp, lb, ga, st);
+		} else {
+			PCG_CUDA(cudaFuncSetAttribute(greedy_big_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			greedy_big_kernel<1><<<big_end - node_begin, kBigThreads, smem, s>>>(nodes, order, node_begin, X, Y, Z, pp, lb, ga, st);
+		}
+		PCG_LAUNCHED();
+	}
+	const int small_begin = node_begin > num_big ? node_begin : num_big;
+	if (node_end > small_begin) {
+		int* counter = mem.alloc<int>(1);
+		PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), s));
+		int blocks = (int)ceil_div(node_end - small_begin, kWarpsPerBlock);
+		int cap = sm_count() * 16;
+		if (blocks > cap) blocks = cap;
+		dim3 grid(blocks), block(kWarpsPerBlock * 32);
+		if (mode == 0 && fp32_guard) greedy_kernel<0, true><<<grid, block, 0, s>>>(nodes, order, small_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
+		else if (mode == 0) greedy_kernel<0, false><<<grid, block, 0, s>>>(nodes, order, small_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
+		else if (fp32_guard) greedy_kernel<1, true><<<grid, block, 0, s>>>(nodes, order, small_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
+		else greedy_kernel<1, false><<<grid, block, 0, s>>>(nodes, order, small_begin, node_end, X, Y, Z, pp, lb, ga, st, counter);
+		PCG_LAUNCHED();
+		mem.free(counter);
+	}
 }
 
 void launch_average_colors(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
@@ -820,7 +1274,8 @@ void launch_sort_keys_single(double* keys, int32_t* vals, int64_t n, DeviceMem& 
 	sc.SL = mem.alloc<int32_t>(n);
 	sc.SR = mem.alloc<int32_t>(n);
 	sc.blk = mem.alloc<int32_t>(2 * n);
-	sort_single_kernel<<<1, 32, 0, mem.stream()>>>(keys, vals, n, sc, st);
+	if (n >= kBigSortMin) sort_single_big_kernel<<<1, kBigThreads, 0, mem.stream()>>>(keys, vals, n, sc, st);
+	else sort_single_kernel<<<1, 32, 0, mem.stream()>>>(keys, vals, n, sc, st);
 	PCG_LAUNCHED();
 }
 

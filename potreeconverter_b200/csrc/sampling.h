@@ -55,13 +55,15 @@ void launch_gather(const GatherItem* items, int num_items, LevelBuffers& lb, Dev
 void launch_keys(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
                  LevelBuffers& lb, DeviceMem& mem);
 // std::sort emulation per node; `order` lists node indices, largest first.
+// Nodes order[0..num_big) (the largest) get one CTA each, the rest one warp.
+constexpr int64_t kBigNodeCandidates = 16384;
 void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, LevelBuffers& lb, SampleStats* st, DeviceMem& mem,
-                      int node_begin = 0, int node_end = -1);
+                      int node_begin = 0, int node_end = -1, int num_big = 0);
 // mode 0 = poisson (early exit + 10,001-check window), 1 = poisson_average (pure greedy)
 void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int32_t* order, int K, const int32_t* X, const int32_t* Y,
                    const int32_t* Z, const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads,
                    double* acc_xyz, double* acc_key, int32_t* acc_next, int32_t* acc_pos, SampleStats* st, DeviceMem& mem,
-                   int node_begin = 0, int node_end = -1);
+                   int node_begin = 0, int node_end = -1, int num_big = 0);
 // poisson_average colour sums: new packed colour per accepted candidate
 void launch_average_colors(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
                            LevelBuffers& lb, const uint64_t* hash_keys, const int32_t* hash_heads, const double* acc_xyz,

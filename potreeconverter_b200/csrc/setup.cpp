@@ -40,7 +40,7 @@ template <class T> static T get(const uint8_t* p) { T v; std::memcpy(&v, p, size
 
 // Header fields as LASzip reports them for an uncompressed file
 // (LasLoader.cpp:72-128).
-bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& err) {
+bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& err, bool points_elsewhere) {
 	if (size < 227 || std::memcmp(las, "LASF", 4) != 0) { err = "input is not a LAS file"; return false; }
 	info.version_minor = las[25];
 	uint16_t header_size = get<uint16_t>(las + 94);
@@ -70,7 +70,7 @@ bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& er
 		info.vlrs.push_back(std::move(v));
 		pos += 54 + len;
 	}
-	if (info.offset_to_points + (uint64_t)info.num_points * (uint64_t)info.record_length > size) {
+	if (!points_elsewhere && info.offset_to_points + (uint64_t)info.num_points * (uint64_t)info.record_length > size) {
 		err = "truncated point data";
 		return false;
 	}

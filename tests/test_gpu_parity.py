@@ -54,9 +54,11 @@ def test_out_of_box_point_is_reported(gpu_ctx):
     from potreeconverter_b200 import synth
     import struct
     las = bytearray(synth.terrain(5000, 9))
-    # shrink the header's max x below the data
-    mx = struct.unpack_from("<d", las, 179)[0]
-    struct.pack_into("<d", las, 179, mx * 0.5)
+    # the reference checks points against the cubic box min + max extent
+    # (chunker_countsort_laszip.cpp:205-251): halving every header maximum
+    # halves the cube, and points beyond it must be reported
+    for off in (179, 195, 211):
+        struct.pack_into("<d", las, off, struct.unpack_from("<d", las, off)[0] * 0.5)
     with pytest.raises(pc.PcgError) as e:
         gpu_ctx.convert(bytes(las))
     assert e.value.status in (2,)
