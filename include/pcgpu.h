@@ -144,6 +144,25 @@ pcg_status pcg_kernel_sort_keys(pcg_ctx* ctx, const double* keys, int64_t n, int
  * leaves at position i (sampler_random.h:97-104). */
 pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* perm_out);
 
+/* ---- the same sort for callers that cannot allocate ---------------------
+ * No counterpart in the reference. pcg_kernel_sort_keys_noalloc is
+ * pcg_kernel_sort_keys for code that must not allocate device memory, e.g. a
+ * plugin whose host framework owns every device allocation, or code
+ * enqueuing work while a stream is captured (cudaMalloc is not allowed
+ * there). Keys (n doubles) and the output permutation (n int32) are device
+ * buffers the caller provides; all scratch lives in a static device array of
+ * 28 * PCG_NOALLOC_SORT_MAX + 256 bytes that every GPU loading the library
+ * holds until the process exits. No cudaMalloc/cudaFree is called.
+ *  - n > PCG_NOALLOC_SORT_MAX returns PCG_BAD_INPUT and does nothing;
+ *  - the first call on a device looks up the array's device address (set-up
+ *    per device); make that first call before any stream capture;
+ *  - work runs on `stream` (a cudaStream_t, NULL = legacy default) and the
+ *    call waits for it to finish;
+ *  - all calls share the one array: calls that overlap on the GPU (other
+ *    streams or host threads) race and must be serialized by the caller. */
+#define PCG_NOALLOC_SORT_MAX 262144
+pcg_status pcg_kernel_sort_keys_noalloc(const double* d_keys, int64_t n, int32_t* d_perm, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

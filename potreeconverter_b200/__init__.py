@@ -66,7 +66,8 @@ class _Result(ctypes.Structure):
 
 # every symbol include/pcgpu.h declares
 EXPORTS = ["pcg_create", "pcg_destroy", "pcg_last_error", "pcg_status_string", "pcg_convert", "pcg_result_free",
-           "pcg_write_files", "pcg_submit", "pcg_poll", "pcg_wait", "pcg_kernel_sort_keys", "pcg_kernel_shuffle"]
+           "pcg_write_files", "pcg_submit", "pcg_poll", "pcg_wait", "pcg_kernel_sort_keys", "pcg_kernel_shuffle",
+           "pcg_kernel_sort_keys_noalloc"]
 
 _lib = None
 
@@ -94,6 +95,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pcg_wait.argtypes = [c.c_void_p, c.c_uint64, c.POINTER(_Result)]
     lib.pcg_kernel_sort_keys.argtypes = [c.c_void_p, c.c_void_p, c.c_int64, c.c_void_p]
     lib.pcg_kernel_shuffle.argtypes = [c.c_void_p, c.c_int64, c.c_uint32, c.c_void_p]
+    lib.pcg_kernel_sort_keys_noalloc.argtypes = [c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p]
     _lib = lib
     return lib
 

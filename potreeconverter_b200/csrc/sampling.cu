@@ -1286,3 +1286,101 @@ void launch_shuffle_single(int64_t n, uint32_t seed, int32_t* perm, DeviceMem& m
 }
 
 }  // namespace pcg
+
+// ================================================= sort without allocation
+// pcg_kernel_sort_keys_noalloc: the std::sort replay for callers that cannot
+// allocate device memory themselves or let a library do it -- code running
+// inside a host framework that owns every device allocation (a plugin under
+// a fixed memory budget), or code enqueuing work while a stream is being
+// captured, where cudaMalloc is not permitted. Its scratch is this
+// file-scope array, reserved on every GPU that loads the library until the
+// process exits.
+
+#include "../../include/pcgpu.h"
+
+#include <mutex>
+
+namespace pcg {
+
+constexpr int64_t kNoAllocSortMax = PCG_NOALLOC_SORT_MAX;
+// per key: working key (8 B), permutation (4 B), left and right stop lists
+// (4 + 4 B), final blocks (8 B); then the error counters
+constexpr size_t kNoAllocKeyBytes = 28;
+constexpr size_t kNoAllocSortBytes = (size_t)kNoAllocSortMax * kNoAllocKeyBytes + 256;
+static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[kNoAllocSortBytes];
+
+namespace {
+
+std::mutex g_noalloc_mtx;
+constexpr int kMaxDevices = 128;
+void* g_noalloc_base[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the array's name is only a host-side handle).
+cudaError_t noalloc_scratch(int dev, void** out) {
+	std::lock_guard<std::mutex> lk(g_noalloc_mtx);
+	if (!g_noalloc_base[dev]) {
+		void* p = nullptr;
+		cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
+		if (e != cudaSuccess) return e;
+		g_noalloc_base[dev] = p;
+	}
+	*out = g_noalloc_base[dev];
+	return cudaSuccess;
+}
+
+__global__ void noalloc_prepare_kernel(const double* __restrict__ in, int64_t n, double* __restrict__ key, int32_t* __restrict__ val) {
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) {
+		key[i] = in[i];
+		val[i] = (int32_t)i;
+	}
+}
+
+__global__ void noalloc_finish_kernel(const int32_t* __restrict__ val, int64_t n, int32_t* __restrict__ out) {
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = val[i];
+}
+
+}  // namespace
+}  // namespace pcg
+
+extern "C" pcg_status pcg_kernel_sort_keys_noalloc(const double* d_keys, int64_t n, int32_t* d_perm, void* stream) {
+	using namespace pcg;
+	if (n < 0 || n > kNoAllocSortMax || (n > 0 && (!d_keys || !d_perm))) return PCG_BAD_INPUT;
+	if (n == 0) return PCG_OK;
+	int dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+		cudaGetLastError();
+		return PCG_CUDA;
+	}
+	void* base = nullptr;
+	if (noalloc_scratch(dev, &base) != cudaSuccess) {
+		cudaGetLastError();
+		return PCG_CUDA;
+	}
+	unsigned char* b = static_cast<unsigned char*>(base);
+	double* key = reinterpret_cast<double*>(b);
+	int32_t* val = reinterpret_cast<int32_t*>(b + 8 * kNoAllocSortMax);
+	SortScratch sc;
+	sc.SL = reinterpret_cast<int32_t*>(b + 12 * kNoAllocSortMax);
+	sc.SR = reinterpret_cast<int32_t*>(b + 16 * kNoAllocSortMax);
+	sc.blk = reinterpret_cast<int32_t*>(b + 20 * kNoAllocSortMax);
+	SampleStats* st = reinterpret_cast<SampleStats*>(b + kNoAllocKeyBytes * kNoAllocSortMax);
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	// the array keeps the previous call's contents: only the error counters
+	// must start at zero, every other byte is written before it is read
+	if (cudaMemsetAsync(st, 0, sizeof(SampleStats), s) != cudaSuccess) { cudaGetLastError(); return PCG_CUDA; }
+	const unsigned blocks = (unsigned)ceil_div(n, 256);
+	noalloc_prepare_kernel<<<blocks, 256, 0, s>>>(d_keys, n, key, val);
+	if (n >= kBigSortMin) sort_single_big_kernel<<<1, kBigThreads, 0, s>>>(key, val, n, sc, st);
+	else sort_single_kernel<<<1, 32, 0, s>>>(key, val, n, sc, st);
+	noalloc_finish_kernel<<<blocks, 256, 0, s>>>(val, n, d_perm);
+	SampleStats h{};
+	if (cudaGetLastError() != cudaSuccess || cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+	    cudaStreamSynchronize(s) != cudaSuccess) {
+		cudaGetLastError();
+		return PCG_CUDA;
+	}
+	return h.timeouts ? PCG_INTERNAL : PCG_OK;
+}
