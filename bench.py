@@ -239,9 +239,11 @@ def main():
     e_start = torch.cuda.Event(enable_timing=True)
     e_end = torch.cuda.Event(enable_timing=True)
     octree_bytes = 0
+    e_stats = None
     e_start.record(stream)
     for _ in range(args.steps):
-        octree_bytes = ctx.convert_stats((pinned.data_ptr(), pinned.numel()), method="poisson", name="bench")["octree_size"]
+        e_stats = ctx.convert_stats((pinned.data_ptr(), pinned.numel()), method="poisson", name="bench")
+        octree_bytes = e_stats["octree_size"]
     e_end.record(stream)
     e_end.synchronize()
     barrier(dist, device)
@@ -284,6 +286,8 @@ def main():
                          "pipeline_achieved": whole_bytes / (ms * 1e-3) / 1e9, "pipeline_bytes_per_step": whole_bytes},
             "stages_ms": {k: round(s[k], 3) for k in ("ms_chunking", "ms_octree", "ms_sampling", "ms_sort", "ms_greedy",
                                                      "ms_output", "ms_host_writers")},
+            "e2e_stages_ms": {k: round(e_stats[k], 3) for k in ("ms_total", "ms_h2d", "ms_sampling", "ms_output", "ms_d2h",
+                                                                  "ms_host_writers")},
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "escalated_pairs": int(s["escalated_pairs"]),

@@ -592,6 +592,8 @@ struct Converter {
 	void sample_level(Tree& tree, const std::vector<int>& level_nodes, int method, double base_spacing, const PosParamsS& pps,
 	                  const ChunkingOut& co, const uint8_t* d_recs, const DecodeParams& p, SampleStats* d_st, DeviceMem& mem,
 	                  JobResult& res) {
+		int sms = 148;
+		PCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
 		(void)d_recs;
 		(void)p;
 		(void)res;
@@ -661,8 +663,11 @@ struct Converter {
 			int32_t* apos = mem.alloc<int32_t>(M);
 			const int mode = method == PCG_POISSON ? 0 : 1;
 			const bool guard = form == PCG_FORM_BATCHED;
+			// large nodes get a CTA each; on levels with few nodes every node
+			// of some size does, so the GPU is not left to a handful of warps
 			int num_big = 0;
-			while (num_big < K && ln[order[num_big]].count >= kBigNodeCandidates) num_big++;
+			const int64_t big_min = K < 2 * sms ? kSmallLevelCtaCandidates : kBigNodeCandidates;
+			while (num_big < K && ln[order[num_big]].count >= big_min) num_big++;
 			cudaEvent_t ev[3];
 			for (auto& e : ev) PCG_CUDA(cudaEventCreate(&e));
 			PCG_CUDA(cudaEventRecord(ev[0], s));

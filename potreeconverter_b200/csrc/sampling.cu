@@ -930,16 +930,36 @@ __global__ void __launch_bounds__(kBigThreads) sort_single_big_kernel(double* ke
 	block_std_sort(key, val, n, sc.SL, sc.SR, sc.blk, st);
 }
 
-// Greedy acceptance, 512 candidates per round and CTA:
+// Greedy acceptance for a large node, one CTA, 512 candidates per round:
 //  A. each thread looks up its candidate's conflicts among the points
-//     accepted before the round (global spatial hash);
+//     accepted in earlier rounds. They live in a dense grid over the node
+//     box (64^3 cells of two spacings, 7 acceptance ranks inline per cell,
+//     overflow in a list), so a lookup is two dependent loads per cell;
 //  B. conflicts among the round's own candidates are found through a shared
 //     memory hash of the round (earlier candidates within the spacing);
-//  C. warp 0 decides the round in sorted order, 32 candidates per step;
-//  D. the round's accepted points are appended and hashed.
+//  C. decisions: parallel passes decide every candidate whose earlier
+//     conflicts are all decided (accepted once none of them is accepted,
+//     rejected once one is); warp 0 then decides what is left in sorted
+//     order -- candidates whose old conflict sits at the edge of the
+//     10,001-check window, which depends on how many were accepted before;
+//  D. the round's accepted points get their ranks and enter the grid.
 constexpr int kRound = kBigThreads;
 constexpr int kRoundHash = 2 * kRound;
 constexpr int kMaxLocal = 12;
+constexpr int kGridDim = 64;  // node box = 128 spacings = 64 cells of 2 spacings
+constexpr int64_t kGridCells = (int64_t)kGridDim * kGridDim * kGridDim;
+constexpr int kCellSlots = 7;
+
+struct alignas(32) AccCell {
+	int32_t count;
+	int32_t slot[kCellSlots];
+};
+
+struct GridArena {
+	AccCell* cells;  // kGridCells per CTA slot
+	int32_t* ovf;    // overflow list heads, kGridCells per CTA slot
+	int32_t* link;   // overflow list links, one per candidate (cand_off + rank)
+};
 
 struct RoundShared {
 	double x[kRound], y[kRound], z[kRound], key[kRound], lim[kRound];
@@ -950,43 +970,59 @@ struct RoundShared {
 	int16_t hnext[kRound];
 	int16_t conf[kRound][kMaxLocal];
 	uint8_t nconf[kRound];
-	uint8_t acc[kRound];
-	int32_t cnt;          // accepted before this round
-	int32_t round_acc;
+	uint8_t state[kRound];   // 0 undecided, 1 accepted, 2 rejected
+	uint8_t old[kRound];     // old-window status: 0 no conflict, 1 conflict, 2 depends on the count
+	int32_t cnt;             // accepted before this round
+	int32_t changed;
 	unsigned long long warp_sums[kBigWarps];
 };
 
 __device__ __forceinline__ uint32_t round_slot(uint64_t k) { return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> 53) & (kRoundHash - 1); }
 
+__device__ __forceinline__ int grid_clamp(int c) { return c < 0 ? 0 : (c >= kGridDim ? kGridDim - 1 : c); }
+__device__ __forceinline__ int64_t grid_index(int cx, int cy, int cz) {
+	return ((int64_t)grid_clamp(cz) * kGridDim + grid_clamp(cy)) * kGridDim + grid_clamp(cx);
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order, int node_begin,
                                                                 const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
                                                                 const int32_t* __restrict__ Z, PosParamsS pp, LevelBuffers lb, GreedyArgs ga,
-                                                                SampleStats* st) {
+                                                                GridArena arena, SampleStats* st) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	RoundShared& R = *reinterpret_cast<RoundShared*>(smem_raw);
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	const LevelNode nd = nodes[order[node_begin + blockIdx.x]];
 	const int64_t n = nd.count, co = nd.cand_off;
+	AccCell* cells = arena.cells + (int64_t)blockIdx.x * kGridCells;
+	int32_t* ovf = arena.ovf + (int64_t)blockIdx.x * kGridCells;
+	{
+		int4* c4 = reinterpret_cast<int4*>(cells);
+		const int64_t n4 = kGridCells * (int64_t)sizeof(AccCell) / 16;
+		for (int64_t i = tid; i < n4; i += kBigThreads) c4[i] = make_int4(0, 0, 0, 0);
+		for (int64_t i = tid; i < kGridCells; i += kBigThreads) ovf[i] = -1;
+	}
 	uint64_t* hk = ga.hkeys + nd.hash_off;
 	int32_t* hh = ga.hheads + nd.hash_off;
-	for (int64_t s = tid; s < nd.hash_cap; s += kBigThreads) { hk[s] = EMPTY_KEY; hh[s] = -1; }
+	if (MODE == 1) {
+		// poisson_average's colour pass finds accepted points through the hash
+		for (int64_t i = tid; i < nd.hash_cap; i += kBigThreads) { hk[i] = EMPTY_KEY; hh[i] = -1; }
+	}
 	if (tid == 0) R.cnt = 0;
 	__syncthreads();
 	const double sp = nd.spacing, s2 = sp * sp;
 	CellGrid g;
 	g.min[0] = nd.min[0]; g.min[1] = nd.min[1]; g.min[2] = nd.min[2];
 	g.inv = 1.0 / (2.0 * sp * 1.000001);
-	const uint32_t lt = lanemask_lt();
 	for (int64_t r0 = 0; r0 < n; r0 += kRound) {
 		const int64_t t = r0 + tid;
 		const bool valid = t < n;
 		const int nr = (int)((n - r0) < kRound ? (n - r0) : kRound);
+		const int32_t cnt0 = R.cnt;
 		// ---- A
 		double x = 0, y = 0, z = 0, key = 0, lim = -CUDART_INF;
 		int32_t local = 0, maxrank = -1;
-		int c[3] = {0, 0, 0};
-		double fr[3] = {0, 0, 0};
+		int c[3] = {0, 0, 0}, o[3] = {1, 1, 1};
 		if (valid) {
 			local = lb.perm[co + t];
 			point_xyz(X, Y, Z, pp, lb.ids[co + local], x, y, z);
@@ -996,29 +1032,57 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 				double limit = cd - sp;
 				lim = limit * limit;
 			}
+			double fr[3];
 			cell_of(g, x, y, z, c, fr);
-			int o[3];
 			for (int a = 0; a < 3; a++) o[a] = fr[a] < 0.5 ? -1 : 1;
+			int64_t cidx[8];
+			int32_t ccount[8];
 #pragma unroll
 			for (int q = 0; q < 8; q++) {
-				int qx = c[0] + ((q & 4) ? o[0] : 0), qy = c[1] + ((q & 2) ? o[1] : 0), qz = c[2] + ((q & 1) ? o[2] : 0);
-				int32_t rr = hash_find(hk, hh, nd.hash_cap, cell_key(qx, qy, qz));
-				int64_t guard = 0;
-				while (rr >= 0 && guard++ <= n) {
+				cidx[q] = grid_index(c[0] + ((q & 4) ? o[0] : 0), c[1] + ((q & 2) ? o[1] : 0), c[2] + ((q & 1) ? o[2] : 0));
+				ccount[q] = cells[cidx[q]].count;
+			}
+#pragma unroll
+			for (int q = 0; q < 8; q++) {
+				// a clamped neighbour may repeat a cell; scanning it twice is harmless
+				const AccCell& cell = cells[cidx[q]];
+				const int inl = ccount[q] < kCellSlots ? ccount[q] : kCellSlots;
+				for (int k = 0; k < inl; k++) {
+					const int32_t rr = cell.slot[k];
 					const int64_t slot = co + rr;
 					if (MODE == 1 || ga.akey[slot] >= lim) {
 						if (sqdist(ga.axyz[3 * slot], ga.axyz[3 * slot + 1], ga.axyz[3 * slot + 2], x, y, z) < s2 && rr > maxrank) maxrank = rr;
 					}
-					rr = ga.anext[slot];
 				}
-				if (guard > n + 1) atomicAdd(&st->timeouts, 1ull);
+				if (ccount[q] > kCellSlots) {
+					int32_t rr = ovf[cidx[q]];
+					int64_t guard = 0;
+					while (rr >= 0 && guard++ <= n) {
+						const int64_t slot = co + rr;
+						if (MODE == 1 || ga.akey[slot] >= lim) {
+							if (sqdist(ga.axyz[3 * slot], ga.axyz[3 * slot + 1], ga.axyz[3 * slot + 2], x, y, z) < s2 && rr > maxrank) maxrank = rr;
+						}
+						rr = arena.link[slot];
+					}
+					if (guard > n + 1) atomicAdd(&st->timeouts, 1ull);
+				}
 			}
 		}
 		R.x[tid] = x; R.y[tid] = y; R.z[tid] = z; R.key[tid] = key; R.lim[tid] = lim;
 		R.maxrank[tid] = maxrank;
 		R.local[tid] = local;
-		R.acc[tid] = 0;
 		R.nconf[tid] = 0;
+		R.state[tid] = valid ? 0 : 2;
+		{
+			uint8_t os = 0;
+			if (maxrank >= 0) {
+				if (MODE == 1) os = 1;
+				else if (maxrank >= cnt0 + tid - 10001) os = 1;       // conflicts whatever was accepted before it
+				else if (maxrank < cnt0 - 10001) os = 0;              // outside the window in any case
+				else os = 2;
+			}
+			R.old[tid] = os;
+		}
 		for (int s = tid; s < kRoundHash; s += kBigThreads) { R.hkey[s] = EMPTY_KEY; R.hhead[s] = -1; }
 		__syncthreads();
 		// ---- B: hash the round by cell, then collect earlier conflicting candidates
@@ -1030,7 +1094,6 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 				if (prev == EMPTY_KEY || prev == k) break;
 				s = (s + 1) & (kRoundHash - 1);
 			}
-			// lists are pushed with atomicExch on 16-bit heads via 32-bit CAS
 			int32_t* word = reinterpret_cast<int32_t*>(&R.hhead[s & ~1u]);
 			int shift = (s & 1u) ? 16 : 0;
 			while (true) {
@@ -1043,8 +1106,6 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 		}
 		__syncthreads();
 		if (valid) {
-			int o[3];
-			for (int a = 0; a < 3; a++) o[a] = fr[a] < 0.5 ? -1 : 1;
 			int nc = 0;
 			for (int q = 0; q < 8; q++) {
 				int qx = c[0] + ((q & 4) ? o[0] : 0), qy = c[1] + ((q & 2) ? o[1] : 0), qz = c[2] + ((q & 1) ? o[2] : 0);
@@ -1068,63 +1129,92 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 			R.nconf[tid] = (uint8_t)(nc < 255 ? nc : 255);
 		}
 		__syncthreads();
-		// ---- C: in-order decisions by warp 0
-		if (warp == 0) {
-			int32_t cnt = R.cnt;
+		// ---- C1: parallel passes
+		volatile uint8_t* vstate = R.state;
+		for (int pass = 0; pass < 64; pass++) {
+			bool changed = false;
+			if (valid && vstate[tid] == 0 && R.nconf[tid] <= kMaxLocal) {
+				const uint8_t os = R.old[tid];
+				uint8_t dec = 0;
+				if (os == 1) {
+					dec = 2;
+				} else {
+					bool any_acc = false, all_done = true;
+					for (int e = 0; e < R.nconf[tid]; e++) {
+						uint8_t sj = vstate[R.conf[tid][e]];
+						any_acc |= sj == 1;
+						all_done &= sj != 0;
+					}
+					if (any_acc) dec = 2;
+					else if (all_done && os == 0) dec = 1;
+				}
+				if (dec) { vstate[tid] = dec; changed = true; }
+			}
+			if (!__syncthreads_or(changed)) break;
+		}
+		const bool left = __syncthreads_or(valid && vstate[tid] == 0);
+		// ---- C2: warp 0 decides the rest in sorted order
+		if (left && warp == 0) {
+			int32_t cnt = cnt0;
+			const uint32_t ltm = lanemask_lt();
 			for (int cb = 0; cb < nr; cb += 32) {
 				const int i = cb + lane;
 				const bool v = i < nr;
-				bool prev_conflict = false;
-				uint32_t mask = 0;
-				if (v) {
-					int nc = R.nconf[i];
-					if (nc <= kMaxLocal) {
-						for (int e = 0; e < nc; e++) {
-							int j = R.conf[i][e];
-							if (j < cb) prev_conflict |= R.acc[j] != 0;
-							else mask |= 1u << (j - cb);
-						}
-					} else {  // list overflow: check every earlier candidate of the round
-						for (int j = 0; j < i; j++) {
-							if ((MODE == 1 || R.key[j] >= R.lim[i]) && sqdist(R.x[j], R.y[j], R.z[j], R.x[i], R.y[i], R.z[i]) < s2) {
-								if (j < cb) prev_conflict |= R.acc[j] != 0;
+				const uint8_t si = v ? vstate[i] : 2;
+				const bool undec = v && si == 0;
+				uint32_t accmask = __ballot_sync(FULL, v && si == 1);
+				if (__ballot_sync(FULL, undec) != 0) {
+					bool prev_conflict = false;
+					uint32_t mask = 0;
+					if (undec) {
+						const int nc = R.nconf[i];
+						if (nc <= kMaxLocal) {
+							for (int e = 0; e < nc; e++) {
+								int j = R.conf[i][e];
+								if (j < cb) prev_conflict |= vstate[j] == 1;
 								else mask |= 1u << (j - cb);
+							}
+						} else {  // list overflow: every earlier candidate of the round
+							for (int j = 0; j < i; j++) {
+								if ((MODE == 1 || R.key[j] >= R.lim[i]) && sqdist(R.x[j], R.y[j], R.z[j], R.x[i], R.y[i], R.z[i]) < s2) {
+									if (j < cb) prev_conflict |= vstate[j] == 1;
+									else mask |= 1u << (j - cb);
+								}
 							}
 						}
 					}
-				}
-				uint32_t accmask = 0;
-				const int mr = R.maxrank[v ? i : 0];
-				const int nvalid = nr - cb < 32 ? nr - cb : 32;
-				for (int b = 0; b < nvalid; b++) {
-					bool dec = false;
-					if (lane == b) {
-						int32_t m_i = cnt + __popc(accmask);
-						bool old_conflict = mr >= 0 && (MODE == 1 || mr >= m_i - 10001);
-						dec = !old_conflict && !prev_conflict && !(mask & accmask);
+					const int nvalid = nr - cb < 32 ? nr - cb : 32;
+					for (int b = 0; b < nvalid; b++) {
+						bool dec = false;
+						const bool ub = __shfl_sync(FULL, undec, b);
+						if (!ub) continue;
+						if (lane == b) {
+							int32_t m_i = cnt + __popc(accmask & ltm);
+							bool old_conflict = R.maxrank[i] >= 0 && (MODE == 1 || R.maxrank[i] >= m_i - 10001);
+							dec = !old_conflict && !prev_conflict && !(mask & accmask);
+							vstate[i] = dec ? 1 : 2;
+						}
+						dec = __shfl_sync(FULL, dec, b);
+						if (dec) accmask |= 1u << b;
 					}
-					dec = __shfl_sync(FULL, dec, b);
-					if (dec) accmask |= 1u << b;
 				}
-				if (v) R.acc[i] = (accmask >> lane) & 1u;
 				cnt += __popc(accmask);
 				__syncwarp();
 			}
 		}
 		__syncthreads();
 		// ---- D: publish
-		const bool acc = valid && R.acc[tid];
+		const bool acc = valid && vstate[tid] == 1;
 		unsigned long long total;
 		unsigned long long pre;
 		{
 			BlockScratch& bs = *reinterpret_cast<BlockScratch*>(R.warp_sums);
 			pre = block_scan_u64(acc ? 1ull : 0ull, total, bs);
 		}
-		const int32_t base = R.cnt;
 		if (valid) {
 			lb.accepted[co + local] = acc ? 1 : 0;
 			if (acc) {
-				int32_t rank = base + (int32_t)pre;
+				int32_t rank = cnt0 + (int32_t)pre;
 				lb.acc_rank[co + local] = rank;
 				const int64_t slot = co + rank;
 				ga.axyz[3 * slot] = x;
@@ -1132,13 +1222,19 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 				ga.axyz[3 * slot + 2] = z;
 				ga.akey[slot] = key;
 				ga.apos[slot] = (int32_t)t;
-				if (!hash_push(hk, hh, ga.anext + co, nd.hash_cap, cell_key(c[0], c[1], c[2]), rank)) atomicAdd(&st->timeouts, 1ull);
+				const int64_t ci = grid_index(c[0], c[1], c[2]);
+				const int32_t pos = atomicAdd(&cells[ci].count, 1);
+				if (pos < kCellSlots) cells[ci].slot[pos] = rank;
+				else arena.link[slot] = atomicExch(&ovf[ci], rank);
+				if (MODE == 1) {
+					// the colour pass walks the hash lists (linked through anext)
+					if (!hash_push(hk, hh, ga.anext + co, nd.hash_cap, cell_key(c[0], c[1], c[2]), rank)) atomicAdd(&st->timeouts, 1ull);
+				}
 			}
 		}
 		__syncthreads();
-		if (tid == 0) R.cnt = base + (int32_t)total;
+		if (tid == 0) R.cnt = cnt0 + (int32_t)total;
 		__syncthreads();
-		(void)lt;
 	}
 }
 
@@ -1206,14 +1302,25 @@ void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int3
 	const int big_end = num_big < node_end ? num_big : node_end;
 	if (big_end > node_begin) {
 		size_t smem = sizeof(RoundShared);
-		if (mode == 0) {
-			PCG_CUDA(cudaFuncSetAttribute(greedy_big_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_big_kernel<0><<<big_end - node_begin, kBigThreads, smem, s>>>(nodes, order, node_begin, X, Y, Z, pp, lb, ga, st);
-		} else {
-			PCG_CUDA(cudaFuncSetAttribute(greedy_big_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_big_kernel<1><<<big_end - node_begin, kBigThreads, smem, s>>>(nodes, order, node_begin, X, Y, Z, pp, lb, ga, st);
+		// one dense acceptance grid per resident CTA; large levels go in batches
+		const int batch = sm_count() * 2;
+		const int nbig = big_end - node_begin;
+		const int slots = nbig < batch ? nbig : batch;
+		GridArena arena;
+		arena.cells = mem.alloc<AccCell>((size_t)slots * kGridCells);
+		arena.ovf = mem.alloc<int32_t>((size_t)slots * kGridCells);
+		arena.link = mem.alloc<int32_t>((size_t)lb.M);
+		if (mode == 0) PCG_CUDA(cudaFuncSetAttribute(greedy_big_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		else PCG_CUDA(cudaFuncSetAttribute(greedy_big_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		for (int b0 = node_begin; b0 < big_end; b0 += slots) {
+			const int cnt = big_end - b0 < slots ? big_end - b0 : slots;
+			if (mode == 0) greedy_big_kernel<0><<<cnt, kBigThreads, smem, s>>>(nodes, order, b0, X, Y, Z, pp, lb, ga, arena, st);
+			else greedy_big_kernel<1><<<cnt, kBigThreads, smem, s>>>(nodes, order, b0, X, Y, Z, pp, lb, ga, arena, st);
+			PCG_LAUNCHED();
 		}
-		PCG_LAUNCHED();
+		mem.free(arena.cells);
+		mem.free(arena.ovf);
+		mem.free(arena.link);
 	}
 	const int small_begin = node_begin > num_big ? node_begin : num_big;
 	if (node_end > small_begin) {

@@ -56,7 +56,8 @@ void launch_keys(const LevelNode* nodes, const int32_t* X, const int32_t* Y, con
                  LevelBuffers& lb, DeviceMem& mem);
 // std::sort emulation per node; `order` lists node indices, largest first.
 // Nodes order[0..num_big) (the largest) get one CTA each, the rest one warp.
-constexpr int64_t kBigNodeCandidates = 16384;
+constexpr int64_t kBigNodeCandidates = 32768;
+constexpr int64_t kSmallLevelCtaCandidates = 2048;  // levels with fewer nodes than 2 x SMs
 void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, LevelBuffers& lb, SampleStats* st, DeviceMem& mem,
                       int node_begin = 0, int node_end = -1, int num_big = 0);
 // mode 0 = poisson (early exit + 10,001-check window), 1 = poisson_average (pure greedy)
