@@ -291,6 +291,8 @@ def main():
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "escalated_pairs": int(s["escalated_pairs"]),
+            "sampler": {k: int(s[k]) for k in ("sampled_nodes", "candidates", "replayed_nodes", "replayed_candidates",
+                                               "heapsort_fallbacks")},
         }
         print(json.dumps(line))
     ctx.close()

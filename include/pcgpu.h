@@ -101,6 +101,9 @@ typedef struct pcg_stats {
 	double ms_sort, ms_greedy;    /* device time of the sampler sort / acceptance kernels */
 	int64_t sampled_nodes;        /* inner nodes sampled                    */
 	int64_t candidates;           /* candidate points over all sampled nodes */
+	int64_t replayed_nodes;       /* nodes with equal keys, sorted by the
+	                                 element-for-element introsort replay   */
+	int64_t replayed_candidates;  /* their candidates                       */
 } pcg_stats;
 
 typedef struct pcg_result {

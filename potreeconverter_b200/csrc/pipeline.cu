@@ -677,7 +677,24 @@ struct Converter {
 				for (int k = 0; k < K; k++)
 					launch_greedy(mode, false, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, k, k + 1, num_big);
 			} else {
-				launch_node_sort(d_nodes, d_order, K, lb, d_st, mem, 0, -1, num_big);
+				// distinct keys: one exact radix sort of the level; equal keys:
+				// the introsort replay, for those nodes only
+				std::vector<uint8_t> tie;
+				sort_level_distinct(d_nodes, ln, lb, mem, tie);
+				std::vector<int32_t> tie_order;
+				int tie_big = 0;
+				for (int k = 0; k < K; k++) {
+					if (!tie[order[k]]) continue;
+					tie_order.push_back(order[k]);
+					if (ln[order[k]].count >= big_min) tie_big++;
+					res.stats.replayed_candidates += ln[order[k]].count;
+				}
+				res.stats.replayed_nodes += (int64_t)tie_order.size();
+				if (!tie_order.empty()) {
+					int32_t* d_tie_order = upload(tie_order, mem);
+					launch_node_sort(d_nodes, d_tie_order, (int)tie_order.size(), lb, d_st, mem, 0, -1, tie_big);
+					mem.free(d_tie_order);
+				}
 				PCG_CUDA(cudaEventRecord(ev[1], s));
 				launch_greedy(mode, guard, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, 0, -1, num_big);
 			}

@@ -60,6 +60,12 @@ constexpr int64_t kBigNodeCandidates = 32768;
 constexpr int64_t kSmallLevelCtaCandidates = 2048;  // levels with fewer nodes than 2 x SMs
 void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, LevelBuffers& lb, SampleStats* st, DeviceMem& mem,
                       int node_begin = 0, int node_end = -1, int num_big = 0);
+// Exact ascending sort of every node's keys (segmented LSD radix sort of the
+// key bits). Nodes whose keys are pairwise distinct end sorted in lb.keys,
+// lb.perm and lb.pos, which is std::sort's unique result for them; nodes with
+// equal keys are left as they were and flagged in tie[k] for the replay.
+void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, LevelBuffers& lb, DeviceMem& mem,
+                         std::vector<uint8_t>& tie);
 // mode 0 = poisson (early exit + 10,001-check window), 1 = poisson_average (pure greedy)
 void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int32_t* order, int K, const int32_t* X, const int32_t* Y,
                    const int32_t* Z, const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads,
