@@ -16,6 +16,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <climits>
+
 #include "devutil.cuh"
 #include "sampling.h"
 
@@ -135,7 +138,7 @@ __device__ int64_t warp_partition(double* key, int32_t* val, int64_t f, int64_t 
 
 constexpr int kStackDepth = 128;
 
-struct Seg { int64_t f, l; int32_t d; int32_t pad; };
+using Seg = SortSeg;
 
 __device__ __forceinline__ int introsort_depth(int64_t n) { return 2 * (63 - __clzll((long long)n)); }  // std::__lg(n) * 2
 
@@ -326,7 +329,8 @@ __device__ int64_t block_partition(double* key, int32_t* val, int64_t f, int64_t
 
 // std::sort on key/val[0..n) with one CTA: segments of at least
 // kBigSortMin elements are partitioned by the block, shorter ones by warps.
-__device__ void block_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL, int32_t* SR, int32_t* blk, SampleStats* st) {
+__device__ void block_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL, int32_t* SR, int32_t* blk, SampleStats* st,
+                               int d0 = -1) {
 	__shared__ Seg bstack[kStackDepth];
 	__shared__ Seg queue[kSmallQueue];
 	__shared__ Seg wstacks[kBigWarps][64];
@@ -345,7 +349,7 @@ __device__ void block_std_sort(double* key, int32_t* val, int64_t n, int32_t* SL
 	};
 	if (n > 1) {
 		int sp = 1;
-		if (tid == 0) bstack[0] = {0, n, introsort_depth(n), 0};
+		if (tid == 0) bstack[0] = {0, n, d0 < 0 ? introsort_depth(n) : d0, 0};
 		__syncthreads();
 		while (sp > 0) {
 			Seg s = bstack[sp - 1];
@@ -408,6 +412,270 @@ __global__ void __launch_bounds__(kBigThreads) sort_single_big_kernel(double* ke
 	block_std_sort(key, val, n, sc.SL, sc.SR, sc.blk, st);
 }
 
+
+// ------------------------------------------ segments replayed by the GPU
+// Segments longer than kWideMin (the top partitions of large nodes) are
+// partitioned level-synchronously across the whole GPU: every round
+// partitions all pending long segments of all nodes at once -- pivot move,
+// stop counts per 4096-element tile, one scan, stop lists, the pair search,
+// the swaps -- so the first partitions of a node with millions of
+// candidates no longer run on a single CTA. Both halves of a partition go on
+// with the decremented depth budget (std::__introsort_loop), so the order in
+// which disjoint segments are processed does not change the result.
+// Segments at most kWideMin long finish on one CTA (>= kBigSortMin elements)
+// or one warp each, with their remaining depth budget; <= 16-element
+// segments go to the final insertion pass.
+constexpr int64_t kWideMin = 32768;
+constexpr int kWideThreads = 256;
+constexpr int kWideWarps = kWideThreads / 32;
+constexpr int kWideSteps = 16;
+constexpr int kWideTile = kWideThreads * kWideSteps;  // 4096
+
+struct WideTile {
+	int64_t p0;          // first element of the tile (after the segment's pivot slot)
+	int32_t count;       // elements in the tile
+	int32_t seg;         // index in the round's segment list
+	int32_t first_tile;  // the segment's first tile
+	int32_t last_tile;   // the segment's last tile
+};
+
+struct WideLists {       // outputs of a round (device counters)
+	Seg* next; int* n_next;   // still longer than kWideMin
+	Seg* cta;  int* n_cta;    // CTA replay (>= kBigSortMin elements, or heapsort)
+	Seg* warp; int* n_warp;   // warp replay
+	int32_t* blk; int* n_blk; // <= 16 elements: final insertion pass (absolute f, l)
+	int64_t cap_seg, cap_blk;
+};
+
+__global__ void wide_pivot_kernel(const Seg* __restrict__ segs, int n, double* key, int32_t* val) {
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= n) return;
+	// std::__move_median_to_first(first, first + 1, mid, last - 1)
+	const int64_t f = segs[s].f, l = segs[s].l;
+	const int64_t a = f + 1, b = f + (l - f) / 2, c = l - 1;
+	const double ka = key[a], kb = key[b], kc = key[c];
+	int64_t m;
+	if (ka < kb) {
+		if (kb < kc) m = b;
+		else if (ka < kc) m = c;
+		else m = a;
+	} else if (ka < kc) m = a;
+	else if (kb < kc) m = c;
+	else m = b;
+	const double tk = key[f]; key[f] = key[m]; key[m] = tk;
+	const int32_t tv = val[f]; val[f] = val[m]; val[m] = tv;
+}
+
+// stop flags of one tile in warp-contiguous order: warp w covers tile
+// elements [512w, 512w + 512) in 16 lane-striped steps
+__device__ __forceinline__ void wide_flags(const WideTile& t, const double* key, double P, uint32_t& lbits, uint32_t& rbits) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	lbits = rbits = 0;
+#pragma unroll
+	for (int st = 0; st < kWideSteps; st++) {
+		const int li = warp * (kWideSteps * 32) + st * 32 + lane;
+		if (li < t.count) {
+			const double k = key[t.p0 + li];
+			if (!(k < P)) lbits |= 1u << st;
+			if (!(P < k)) rbits |= 1u << st;
+		}
+	}
+}
+
+__global__ void __launch_bounds__(kWideThreads) wide_count_kernel(const WideTile* __restrict__ tiles, const Seg* __restrict__ segs,
+                                                                const double* __restrict__ key, unsigned long long* __restrict__ counts) {
+	__shared__ unsigned long long wsum[kWideWarps];
+	const WideTile t = tiles[blockIdx.x];
+	const double P = key[segs[t.seg].f];
+	uint32_t lb, rb;
+	wide_flags(t, key, P, lb, rb);
+	unsigned long long v = ((unsigned long long)__popc(rb) << 32) | (unsigned long long)__popc(lb);
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+	if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = v;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		unsigned long long tot = 0;
+		for (int w = 0; w < kWideWarps; w++) tot += wsum[w];
+		counts[blockIdx.x] = tot;
+	}
+}
+
+__global__ void __launch_bounds__(kWideThreads) wide_write_kernel(const WideTile* __restrict__ tiles, const Seg* __restrict__ segs,
+                                                                const double* __restrict__ key, const unsigned long long* __restrict__ offs,
+                                                                int32_t* __restrict__ SL, int32_t* __restrict__ SR) {
+	__shared__ unsigned long long wsum[kWideWarps];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const WideTile t = tiles[blockIdx.x];
+	const int64_t f = segs[t.seg].f;
+	const double P = key[f];
+	uint32_t lb, rb;
+	wide_flags(t, key, P, lb, rb);
+	// per-warp totals, exclusive over the warps of the tile
+	unsigned long long v = ((unsigned long long)__popc(rb) << 32) | (unsigned long long)__popc(lb);
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+	if (lane == 0) wsum[warp] = v;
+	__syncthreads();
+	unsigned long long before = offs[blockIdx.x] - offs[t.first_tile];
+	for (int w = 0; w < warp; w++) before += wsum[w];
+	int64_t cl = (int64_t)(before & 0xffffffffull), cr = (int64_t)(before >> 32);
+	const uint32_t lt = lanemask_lt();
+	int32_t* sl = SL + f;
+	int32_t* sr = SR + f;
+#pragma unroll
+	for (int st = 0; st < kWideSteps; st++) {
+		const bool isL = (lb >> st) & 1u, isR = (rb >> st) & 1u;
+		const uint32_t bL = __ballot_sync(FULL, isL), bR = __ballot_sync(FULL, isR);
+		const int32_t rel = (int32_t)(t.p0 + warp * (kWideSteps * 32) + st * 32 + lane - f);
+		if (isL) sl[cl + __popc(bL & lt)] = rel;
+		if (isR) sr[cr + __popc(bR & lt)] = rel;
+		cl += __popc(bL);
+		cr += __popc(bR);
+	}
+}
+
+__device__ __forceinline__ void wide_push(Seg* list, int* n, int64_t cap, const Seg& s, SampleStats* st) {
+	const int i = atomicAdd(n, 1);
+	if (i < cap) list[i] = s;
+	else atomicAdd(&st->timeouts, 1ull);
+}
+
+__device__ void wide_classify(int64_t f, int64_t l, int d, const WideLists& L, SampleStats* st) {
+	const int64_t n = l - f;
+	if (n <= 16) {
+		if (n > 1) {
+			const int i = atomicAdd(L.n_blk, 1);
+			if (i < L.cap_blk) {
+				L.blk[2 * (int64_t)i] = (int32_t)f;
+				L.blk[2 * (int64_t)i + 1] = (int32_t)l;
+			} else {
+				atomicAdd(&st->timeouts, 1ull);
+			}
+		}
+	} else if (d == 0 || (n >= kBigSortMin && n <= kWideMin)) {
+		wide_push(L.cta, L.n_cta, L.cap_seg, {f, l, d, 0}, st);
+	} else if (n > kWideMin) {
+		wide_push(L.next, L.n_next, L.cap_seg, {f, l, d, 0}, st);
+	} else {
+		wide_push(L.warp, L.n_warp, L.cap_seg, {f, l, d, 0}, st);
+	}
+}
+
+// one warp per segment: Hoare's pair count K, the cut, the two halves
+__global__ void wide_split_kernel(const Seg* __restrict__ segs, int n, const WideTile* __restrict__ tiles, const int32_t* __restrict__ seg_tile,
+                                  const unsigned long long* __restrict__ counts, const unsigned long long* __restrict__ offs,
+                                  const int32_t* __restrict__ SL, const int32_t* __restrict__ SR, int64_t* __restrict__ segK,
+                                  int64_t* __restrict__ segCR, WideLists L, SampleStats* st) {
+	const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+	const int lane = threadIdx.x & 31;
+	if (s >= n) return;
+	const Seg g = segs[s];
+	const WideTile ft = tiles[seg_tile[s]];
+	const unsigned long long tot = offs[ft.last_tile] + counts[ft.last_tile] - offs[ft.first_tile];
+	const int64_t cL = (int64_t)(tot & 0xffffffffull), cR = (int64_t)(tot >> 32);
+	const int32_t* sl = SL + g.f;
+	const int32_t* sr = SR + g.f;
+	// first k in [0, m) with !(SL[k] < SR[cR-1-k]), m if none (monotone)
+	int64_t lo = 0, hi = cL < cR ? cL : cR;
+	while (hi - lo > 32) {
+		const int64_t step = (hi - lo + 31) / 32;
+		const int64_t k = lo + lane * step;
+		const bool p = k < hi && !(sl[k] < sr[cR - 1 - k]);
+		const uint32_t b = __ballot_sync(FULL, p);
+		if (b == 0) {
+			const int64_t jmax = (hi - 1 - lo) / step < 31 ? (hi - 1 - lo) / step : 31;
+			lo = lo + jmax * step + 1;
+		} else {
+			const int j = __ffs(b) - 1;
+			const int64_t nlo = j > 0 ? lo + (int64_t)(j - 1) * step + 1 : lo;
+			hi = lo + (int64_t)j * step;
+			lo = nlo;
+		}
+	}
+	{
+		const int64_t k = lo + lane;
+		const bool p = k < hi && !(sl[k] < sr[cR - 1 - k]);
+		const uint32_t b = __ballot_sync(FULL, p);
+		if (b) hi = lo + __ffs(b) - 1;
+	}
+	const int64_t K = hi;
+	if (lane != 0) return;
+	const int64_t c1 = K < cL ? (int64_t)sl[K] : INT64_MAX;
+	const int64_t c2 = K >= 1 ? (int64_t)sr[cR - K] : INT64_MAX;
+	const int64_t cut = g.f + (c1 < c2 ? c1 : c2);
+	segK[s] = K;
+	segCR[s] = cR;
+	if (cut <= g.f || cut >= g.l) {
+		atomicAdd(&st->timeouts, 1ull);
+		segK[s] = 0;
+		return;
+	}
+	const int d = g.d - 1;
+	wide_classify(cut, g.l, d, L, st);
+	wide_classify(g.f, cut, d, L, st);
+}
+
+__global__ void __launch_bounds__(kWideThreads) wide_swap_kernel(const WideTile* __restrict__ tiles, const Seg* __restrict__ segs,
+                                                               const int64_t* __restrict__ segK, const int64_t* __restrict__ segCR,
+                                                               const int32_t* __restrict__ SL, const int32_t* __restrict__ SR, double* key,
+                                                               int32_t* val) {
+	const WideTile t = tiles[blockIdx.x];
+	const int64_t f = segs[t.seg].f;
+	const int64_t K = segK[t.seg], cR = segCR[t.seg];
+	const int64_t k0 = t.p0 - (f + 1);  // the tile's elements double as its share of the pair indices
+	for (int j = threadIdx.x; j < t.count; j += kWideThreads) {
+		const int64_t k = k0 + j;
+		if (k >= K) break;
+		const int64_t a = f + SL[f + k], b = f + SR[f + cR - 1 - k];
+		const double tk = key[a]; key[a] = key[b]; key[b] = tk;
+		const int32_t tv = val[a]; val[a] = val[b]; val[b] = tv;
+	}
+}
+
+__global__ void __launch_bounds__(kBigThreads) seg_cta_kernel(const Seg* __restrict__ segs, double* key, int32_t* val, SortScratch sc,
+                                                             SampleStats* st) {
+	const Seg g = segs[blockIdx.x];
+	block_std_sort(key + g.f, val + g.f, g.l - g.f, sc.SL + g.f, sc.SR + g.f, sc.blk + 2 * g.f, st, g.d);
+}
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) seg_warp_kernel(const Seg* __restrict__ segs, int n, double* key, int32_t* val,
+                                                                      SortScratch sc, SampleStats* st, int* next_seg) {
+	__shared__ Seg stacks[kWarpsPerBlock][kStackDepth];
+	__shared__ int nblk[kWarpsPerBlock];
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	while (true) {
+		int idx = 0;
+		if (lane == 0) idx = atomicAdd(next_seg, 1);
+		idx = __shfl_sync(FULL, idx, 0);
+		if (idx >= n) break;
+		const Seg g = segs[idx];
+		const int64_t len = g.l - g.f;
+		if (lane == 0) nblk[warp] = 0;
+		__syncwarp();
+		warp_introsort(key + g.f, val + g.f, 0, len, g.d, sc.SL + g.f, sc.SR + g.f, sc.blk + 2 * g.f, &nblk[warp], stacks[warp], st);
+		__syncwarp();
+		insertion_blocks(key + g.f, val + g.f, sc.blk + 2 * g.f, nblk[warp], lane, 32);
+		__syncwarp();
+	}
+}
+
+__global__ void blk_insertion_kernel(const int32_t* __restrict__ blk, int n, double* key, int32_t* val) {
+	const int b = blockIdx.x * blockDim.x + threadIdx.x;
+	if (b < n) insertion_blocks(key, val, blk + 2 * (int64_t)b, 1, 0, 1);
+}
+
+__global__ void node_pos_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ list, LevelBuffers lb) {
+	const LevelNode nd = nodes[list[blockIdx.x]];
+	for (int64_t t = threadIdx.x; t < nd.count; t += blockDim.x) lb.pos[nd.cand_off + lb.perm[nd.cand_off + t]] = (int32_t)t;
+}
+
+int host_introsort_depth(int64_t n) {
+	int lg = 0;
+	while ((n >> (lg + 1)) != 0) lg++;
+	return 2 * lg;
+}
+
 }  // namespace
 
 void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, LevelBuffers& lb, SampleStats* st, DeviceMem& mem,
@@ -440,15 +708,153 @@ void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, Level
 	mem.free(sc.blk);
 }
 
+void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<SortSeg>& segs, SampleStats* st, DeviceMem& mem) {
+	if (segs.empty() || M == 0) return;
+	cudaStream_t s = mem.stream();
+	SortScratch sc;
+	sc.SL = mem.alloc<int32_t>(M);
+	sc.SR = mem.alloc<int32_t>(M);
+	sc.blk = mem.alloc<int32_t>(2 * M);
+	WideLists L;
+	L.cap_seg = M / 16 + 64;
+	L.cap_blk = M / 2 + 64;
+	Seg* ping[2] = {mem.alloc<Seg>(L.cap_seg), mem.alloc<Seg>(L.cap_seg)};
+	L.cta = mem.alloc<Seg>(L.cap_seg);
+	L.warp = mem.alloc<Seg>(L.cap_seg);
+	L.blk = mem.alloc<int32_t>(2 * L.cap_blk);
+	int* counters = mem.alloc<int>(5);  // next, cta, warp, blk, warp-kernel cursor
+	L.n_next = counters;
+	L.n_cta = counters + 1;
+	L.n_warp = counters + 2;
+	L.n_blk = counters + 3;
+	// the initial segments, classified like the halves of a partition
+	std::vector<Seg> cur, cta, warp;
+	std::vector<int32_t> blk;
+	for (const SortSeg& g : segs) {
+		const int64_t n = g.l - g.f;
+		if (n <= 16) {
+			if (n > 1) { blk.push_back((int32_t)g.f); blk.push_back((int32_t)g.l); }
+		} else if (g.d == 0 || (n >= kBigSortMin && n <= kWideMin)) {
+			cta.push_back(g);
+		} else if (n > kWideMin) {
+			cur.push_back(g);
+		} else {
+			warp.push_back(g);
+		}
+	}
+	int h_counts[5] = {0, (int)cta.size(), (int)warp.size(), (int)(blk.size() / 2), 0};
+	if (!cta.empty()) PCG_CUDA(cudaMemcpyAsync(L.cta, cta.data(), cta.size() * sizeof(Seg), cudaMemcpyHostToDevice, s));
+	if (!warp.empty()) PCG_CUDA(cudaMemcpyAsync(L.warp, warp.data(), warp.size() * sizeof(Seg), cudaMemcpyHostToDevice, s));
+	if (!blk.empty()) PCG_CUDA(cudaMemcpyAsync(L.blk, blk.data(), blk.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+	PCG_CUDA(cudaMemcpyAsync(counters, h_counts, sizeof(h_counts), cudaMemcpyHostToDevice, s));
+	int pp = 0;
+	int64_t* segK = nullptr;
+	int64_t* segCR = nullptr;
+	int64_t seg_cap = 0;
+	for (int round = 0; !cur.empty(); round++) {
+		if (round > 128) throw PcgError(4, "sort replay: partition rounds did not converge");
+		const int n = (int)cur.size();
+		std::vector<WideTile> tiles;
+		std::vector<int32_t> seg_tile(n);
+		for (int i = 0; i < n; i++) {
+			const int64_t f = cur[i].f, len = cur[i].l - cur[i].f - 1;  // elements after the pivot slot
+			const int first = (int)tiles.size();
+			const int nt = (int)ceil_div(len, kWideTile);
+			seg_tile[i] = first;
+			for (int j = 0; j < nt; j++) {
+				WideTile t;
+				t.p0 = f + 1 + (int64_t)j * kWideTile;
+				t.count = (int32_t)std::min<int64_t>(kWideTile, len - (int64_t)j * kWideTile);
+				t.seg = i;
+				t.first_tile = first;
+				t.last_tile = first + nt - 1;
+				tiles.push_back(t);
+			}
+		}
+		const int nt = (int)tiles.size();
+		Seg* d_cur = ping[pp];
+		L.next = ping[pp ^ 1];
+		PCG_CUDA(cudaMemcpyAsync(d_cur, cur.data(), n * sizeof(Seg), cudaMemcpyHostToDevice, s));
+		WideTile* d_tiles = mem.alloc<WideTile>(nt);
+		PCG_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), nt * sizeof(WideTile), cudaMemcpyHostToDevice, s));
+		int32_t* d_seg_tile = mem.alloc<int32_t>(n);
+		PCG_CUDA(cudaMemcpyAsync(d_seg_tile, seg_tile.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+		if (n > seg_cap) {
+			if (segK) { mem.free(segK); mem.free(segCR); }
+			seg_cap = 2 * (int64_t)n;
+			segK = mem.alloc<int64_t>(seg_cap);
+			segCR = mem.alloc<int64_t>(seg_cap);
+		}
+		unsigned long long* counts = mem.alloc<unsigned long long>(nt);
+		unsigned long long* offs = mem.alloc<unsigned long long>(nt);
+		PCG_CUDA(cudaMemsetAsync(L.n_next, 0, sizeof(int), s));
+		wide_pivot_kernel<<<(unsigned)ceil_div(n, 128), 128, 0, s>>>(d_cur, n, key, val);
+		PCG_LAUNCHED();
+		wide_count_kernel<<<nt, kWideThreads, 0, s>>>(d_tiles, d_cur, key, counts);
+		PCG_LAUNCHED();
+		exclusive_scan_i64(reinterpret_cast<const int64_t*>(counts), reinterpret_cast<int64_t*>(offs), nt, false, mem);
+		wide_write_kernel<<<nt, kWideThreads, 0, s>>>(d_tiles, d_cur, key, offs, sc.SL, sc.SR);
+		PCG_LAUNCHED();
+		wide_split_kernel<<<(unsigned)ceil_div((int64_t)n * 32, 128), 128, 0, s>>>(d_cur, n, d_tiles, d_seg_tile, counts, offs, sc.SL, sc.SR,
+		                                                                          segK, segCR, L, st);
+		PCG_LAUNCHED();
+		wide_swap_kernel<<<nt, kWideThreads, 0, s>>>(d_tiles, d_cur, segK, segCR, sc.SL, sc.SR, key, val);
+		PCG_LAUNCHED();
+		int n_next = 0;
+		PCG_CUDA(cudaMemcpyAsync(&n_next, L.n_next, sizeof(int), cudaMemcpyDeviceToHost, s));
+		PCG_CUDA(cudaStreamSynchronize(s));
+		if (n_next > L.cap_seg) throw PcgError(5, "sort replay: segment list overflow");
+		cur.resize(n_next);
+		if (n_next) PCG_CUDA(cudaMemcpyAsync(cur.data(), L.next, n_next * sizeof(Seg), cudaMemcpyDeviceToHost, s));
+		PCG_CUDA(cudaStreamSynchronize(s));
+		mem.free(counts);
+		mem.free(offs);
+		mem.free(d_tiles);
+		mem.free(d_seg_tile);
+		pp ^= 1;
+	}
+	PCG_CUDA(cudaMemcpyAsync(h_counts, counters, sizeof(h_counts), cudaMemcpyDeviceToHost, s));
+	PCG_CUDA(cudaStreamSynchronize(s));
+	if (h_counts[1] > L.cap_seg || h_counts[2] > L.cap_seg || h_counts[3] > L.cap_blk) throw PcgError(5, "sort replay: list overflow");
+	if (h_counts[1] > 0) {
+		seg_cta_kernel<<<h_counts[1], kBigThreads, 0, s>>>(L.cta, key, val, sc, st);
+		PCG_LAUNCHED();
+	}
+	if (h_counts[2] > 0) {
+		PCG_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(int), s));
+		int blocks = (int)ceil_div(h_counts[2], kWarpsPerBlock);
+		const int cap = sm_count() * 16;
+		if (blocks > cap) blocks = cap;
+		seg_warp_kernel<<<blocks, kWarpsPerBlock * 32, 0, s>>>(L.warp, h_counts[2], key, val, sc, st, counters + 4);
+		PCG_LAUNCHED();
+	}
+	if (h_counts[3] > 0) {
+		blk_insertion_kernel<<<(unsigned)ceil_div(h_counts[3], 128), 128, 0, s>>>(L.blk, h_counts[3], key, val);
+		PCG_LAUNCHED();
+	}
+	if (segK) { mem.free(segK); mem.free(segCR); }
+	mem.free(ping[0]);
+	mem.free(ping[1]);
+	mem.free(L.cta);
+	mem.free(L.warp);
+	mem.free(L.blk);
+	mem.free(counters);
+	mem.free(sc.SL);
+	mem.free(sc.SR);
+	mem.free(sc.blk);
+}
+
+void launch_node_pos(const LevelNode* nodes, const int32_t* node_list, int n, LevelBuffers& lb, DeviceMem& mem) {
+	if (n <= 0) return;
+	node_pos_kernel<<<n, 256, 0, mem.stream()>>>(nodes, node_list, lb);
+	PCG_LAUNCHED();
+}
+
+int sort_depth_budget(int64_t n) { return host_introsort_depth(n); }
+
 void launch_sort_keys_single(double* keys, int32_t* vals, int64_t n, DeviceMem& mem, SampleStats* st) {
 	if (n <= 0) return;
-	SortScratch sc;
-	sc.SL = mem.alloc<int32_t>(n);
-	sc.SR = mem.alloc<int32_t>(n);
-	sc.blk = mem.alloc<int32_t>(2 * n);
-	if (n >= kBigSortMin) sort_single_big_kernel<<<1, kBigThreads, 0, mem.stream()>>>(keys, vals, n, sc, st);
-	else sort_single_kernel<<<1, 32, 0, mem.stream()>>>(keys, vals, n, sc, st);
-	PCG_LAUNCHED();
+	replay_segments(keys, vals, n, {SortSeg{0, n, host_introsort_depth(n), 0}}, st, mem);
 }
 
 }  // namespace pcg

@@ -681,19 +681,20 @@ struct Converter {
 				// the introsort replay, for those nodes only
 				std::vector<uint8_t> tie;
 				sort_level_distinct(d_nodes, ln, lb, mem, tie);
-				std::vector<int32_t> tie_order;
-				int tie_big = 0;
+				std::vector<int32_t> tie_nodes;
+				std::vector<SortSeg> tie_segs;
 				for (int k = 0; k < K; k++) {
-					if (!tie[order[k]]) continue;
-					tie_order.push_back(order[k]);
-					if (ln[order[k]].count >= big_min) tie_big++;
-					res.stats.replayed_candidates += ln[order[k]].count;
+					if (!tie[k]) continue;
+					tie_nodes.push_back(k);
+					tie_segs.push_back({ln[k].cand_off, ln[k].cand_off + ln[k].count, sort_depth_budget(ln[k].count), 0});
+					res.stats.replayed_candidates += ln[k].count;
 				}
-				res.stats.replayed_nodes += (int64_t)tie_order.size();
-				if (!tie_order.empty()) {
-					int32_t* d_tie_order = upload(tie_order, mem);
-					launch_node_sort(d_nodes, d_tie_order, (int)tie_order.size(), lb, d_st, mem, 0, -1, tie_big);
-					mem.free(d_tie_order);
+				res.stats.replayed_nodes += (int64_t)tie_nodes.size();
+				if (!tie_nodes.empty()) {
+					replay_segments(lb.keys, lb.perm, M, tie_segs, d_st, mem);
+					int32_t* d_tie_nodes = upload(tie_nodes, mem);
+					launch_node_pos(d_nodes, d_tie_nodes, (int)tie_nodes.size(), lb, mem);
+					mem.free(d_tie_nodes);
 				}
 				PCG_CUDA(cudaEventRecord(ev[1], s));
 				launch_greedy(mode, guard, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, 0, -1, num_big);

@@ -40,6 +40,12 @@ struct LevelBuffers {
 	int32_t* acc_rank = nullptr;   // [M] acceptance rank for accepted candidates
 };
 
+struct SortSeg {            // a std::sort segment [f, l) with its depth budget
+	int64_t f, l;
+	int32_t d;
+	int32_t pad;
+};
+
 struct PosParamsS {
 	double scale[3], offset[3];
 };
@@ -66,6 +72,12 @@ void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, Level
 // equal keys are left as they were and flagged in tie[k] for the replay.
 void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, LevelBuffers& lb, DeviceMem& mem,
                          std::vector<uint8_t>& tie);
+// std::sort replayed on every segment [f, l) of key/val independently, each
+// with depth budget d (2 * floor(log2(l - f)) for a whole node).
+void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<SortSeg>& segs, SampleStats* st, DeviceMem& mem);
+int sort_depth_budget(int64_t n);
+// lb.pos of the listed nodes from their sorted lb.perm
+void launch_node_pos(const LevelNode* nodes, const int32_t* node_list, int n, LevelBuffers& lb, DeviceMem& mem);
 // mode 0 = poisson (early exit + 10,001-check window), 1 = poisson_average (pure greedy)
 void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int32_t* order, int K, const int32_t* X, const int32_t* Y,
                    const int32_t* Z, const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads,

@@ -7,7 +7,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n", [0, 1, 2, 15, 16, 17, 33, 100, 1000, 4097, 100_000])
+@pytest.mark.parametrize("n", [0, 1, 2, 15, 16, 17, 33, 100, 1000, 4097, 32769, 100_000, 1_000_000])
 @pytest.mark.parametrize("ties", ["none", "few", "many", "all"])
 def test_sort_matches_std_sort(gpu_ctx, oracle, n, ties):
     rng = np.random.default_rng(n * 7 + len(ties))
@@ -23,11 +23,21 @@ def test_sort_matches_std_sort(gpu_ctx, oracle, n, ties):
 
 
 @pytest.mark.parametrize("pattern", ["sorted", "reversed", "organ", "sawtooth"])
-def test_sort_adversarial_orders(gpu_ctx, oracle, pattern):
-    n = 50_000
+@pytest.mark.parametrize("n", [50_000, 400_000])
+def test_sort_adversarial_orders(gpu_ctx, oracle, pattern, n):
     i = np.arange(n, dtype=np.float64)
     keys = {"sorted": i, "reversed": i[::-1].copy(), "organ": np.minimum(i, n - i),
             "sawtooth": i % 97}[pattern]
+    assert (gpu_ctx.sort_keys(keys) == oracle.sort_perm(keys)).all()
+
+
+@pytest.mark.parametrize("n", [70_000, 2_000_000])
+def test_sort_quantized_distances(gpu_ctx, oracle, n):
+    # squared distances of millimetre-quantized points to a box centre: the
+    # key distribution of the samplers, with many exact ties
+    rng = np.random.default_rng(n)
+    q = rng.integers(-20_000, 20_000, (n, 3)).astype(np.float64) * 0.001
+    keys = (q * q).sum(axis=1)
     assert (gpu_ctx.sort_keys(keys) == oracle.sort_perm(keys)).all()
 
 
