@@ -1,0 +1,254 @@
+// Conflict lists for the poisson samplers, built for all nodes of a level at
+// once.
+//
+// The acceptance scan of sampler_poisson.h:133-245 (sampler_poisson_average.h
+// :184-281 without the early exit) compares candidate p, in sorted order,
+// with the points accepted before it: p is rejected by an accepted a when
+// they are closer than the spacing and a lies at or beyond the early-exit
+// bound, key(a) >= (sqrt(key(p)) - spacing)^2. Whether a given earlier
+// candidate q could reject p is therefore fixed before any decision is made;
+// only whether q gets accepted is not. This unit finds, for every candidate
+// p, the earlier candidates q of its node with that property -- a
+// fixed-radius neighbour search, fully parallel over the level -- so the
+// acceptance kernel only has to look at those candidates' decisions.
+//
+//  1. cell keys: cells of one spacing (x 1.000001) over the node box, so
+//     every point closer than the spacing lies in the 3 x 3 x 3 cells around
+//     a candidate's own;
+//  2. segmented radix sort of (cell, sorted position) per node;
+//  3. a hash table (node, cell) -> range of the cell-sorted records;
+//  4. one thread per candidate in cell order (a warp shares neighbourhoods)
+//     tests the 27 cells' records: an FP32 prefilter on exact integer deltas,
+//     then the reference's FP64 test, then the early-exit bound.
+// A candidate with more than kListCap such predecessors marks its node
+// dense; dense nodes keep the grid-based acceptance kernel.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "devutil.cuh"
+#include "sampling.h"
+
+namespace pcg {
+
+namespace {
+
+constexpr uint64_t kEmptyRun = ~0ull;
+constexpr int kCellsPerAxis = 128;  // node box = 128 spacings
+
+__device__ __forceinline__ uint64_t run_hash(uint64_t k, int64_t cap) {
+	return ((k * 0x9E3779B97F4A7C15ull) >> 20) & (uint64_t)(cap - 1);
+}
+
+__device__ __forceinline__ double qcoord(int32_t X, int a, const PosParamsS& pp) {
+	// (xyz[a] * scale) + offset, sampler_poisson.h:99-101
+	return ((double)X * pp.scale[a]) + pp.offset[a];
+}
+
+__device__ __forceinline__ int clamp_cell(double u) {
+	double f = floor(u);
+	f = f < 0.0 ? 0.0 : (f > (double)(kCellsPerAxis - 1) ? (double)(kCellsPerAxis - 1) : f);
+	return (int)f;
+}
+
+__global__ void conf_cell_keys_kernel(const LevelNode* __restrict__ nodes, PosParamsS pp, LevelBuffers lb, uint64_t* __restrict__ keys) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const LevelNode& nd = nodes[lb.node_of[j]];
+	const int4 r = lb.cq[j];
+	const double inv = 1.0 / (nd.spacing * 1.000001);
+	const int cx = clamp_cell((qcoord(r.x, 0, pp) - nd.min[0]) * inv);
+	const int cy = clamp_cell((qcoord(r.y, 1, pp) - nd.min[1]) * inv);
+	const int cz = clamp_cell((qcoord(r.z, 2, pp) - nd.min[2]) * inv);
+	keys[j] = ((uint64_t)cz * kCellsPerAxis + (uint64_t)cy) * kCellsPerAxis + (uint64_t)cx;
+}
+
+// cell-sorted records (X, Y, Z, sorted position)
+__global__ void conf_gather_kernel(const LevelNode* __restrict__ nodes, LevelBuffers lb, const uint32_t* __restrict__ cvals,
+                                   int4* __restrict__ crec) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const int64_t co = nodes[lb.node_of[j]].cand_off;
+	const uint32_t u = cvals[j];
+	int4 r = lb.cq[co + u];
+	r.w = (int32_t)u;
+	crec[j] = r;
+}
+
+__device__ __forceinline__ bool run_head(const LevelNode* nodes, const int32_t* node_of, const uint64_t* ck, int64_t j) {
+	return j == nodes[node_of[j]].cand_off || ck[j] != ck[j - 1];
+}
+
+__global__ void conf_count_runs_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ node_of, const uint64_t* __restrict__ ck,
+                                       int64_t M, unsigned long long* __restrict__ runs) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	const bool h = j < M && run_head(nodes, node_of, ck, j);
+	const unsigned b = __ballot_sync(FULL, h);
+	if ((threadIdx.x & 31) == 0 && b) atomicAdd(runs, (unsigned long long)__popc(b));
+}
+
+// run table: key (node << 32 | cell) -> (first record, count)
+__global__ void conf_insert_runs_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ node_of, const uint64_t* __restrict__ ck,
+                                        int64_t M, uint64_t* __restrict__ hkeys, int2* __restrict__ hvals, int64_t cap,
+                                        SampleStats* st) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= M || !run_head(nodes, node_of, ck, j)) return;
+	const int32_t node = node_of[j];
+	const int64_t end = nodes[node].cand_off + nodes[node].count;
+	int64_t e = j + 1;
+	while (e < end && ck[e] == ck[j]) e++;
+	const uint64_t key = ((uint64_t)(uint32_t)node << 32) | ck[j];
+	uint64_t s = run_hash(key, cap);
+	for (int64_t probe = 0; probe < cap; probe++) {
+		const unsigned long long prev = atomicCAS((unsigned long long*)&hkeys[s], (unsigned long long)kEmptyRun, (unsigned long long)key);
+		if (prev == kEmptyRun) {
+			hvals[s] = make_int2((int32_t)(j - nodes[node].cand_off), (int32_t)(e - j));
+			return;
+		}
+		s = (s + 1) & (uint64_t)(cap - 1);
+	}
+	atomicAdd(&st->timeouts, 1ull);
+}
+
+__device__ __forceinline__ int2 find_run(const uint64_t* hkeys, const int2* hvals, int64_t cap, uint64_t key) {
+	uint64_t s = run_hash(key, cap);
+	for (int64_t probe = 0; probe < cap; probe++) {
+		const uint64_t k = hkeys[s];
+		if (k == key) return hvals[s];
+		if (k == kEmptyRun) break;
+		s = (s + 1) & (uint64_t)(cap - 1);
+	}
+	return make_int2(0, 0);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, PosParamsS pp,
+                                                        LevelBuffers lb, const uint64_t* __restrict__ ck, const int4* __restrict__ crec,
+                                                        const uint64_t* __restrict__ hkeys, const int2* __restrict__ hvals, int64_t cap,
+                                                        ConflictLists cl) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const int32_t node = lb.node_of[j];
+	if (!use[node]) return;
+	const LevelNode& nd = nodes[node];
+	const int64_t co = nd.cand_off;
+	const int4 me = crec[j];
+	const int32_t t = me.w;
+	const double x = qcoord(me.x, 0, pp), y = qcoord(me.y, 1, pp), z = qcoord(me.z, 2, pp);
+	const double sp = nd.spacing, s2 = sp * sp;
+	double lim = 0.0;
+	if (MODE == 0) {
+		// the early-exit bound of the acceptance kernels, same expression
+		const double cd = sqrt(lb.keys[co + t]);
+		const double limit = cd - sp;
+		lim = limit * limit;
+	}
+	bool pre32 = s2 > 1e-30 && s2 < 1e30;
+	float sf[3];
+	for (int a = 0; a < 3; a++) {
+		sf[a] = (float)pp.scale[a];
+		pre32 = pre32 && pp.scale[a] > 0.0 && (nd.max[a] - nd.min[a]) / pp.scale[a] < 8.0e6;
+	}
+	const float s2hi = (float)(s2 * 1.001);
+	const uint64_t c = ck[j];
+	const int cx = (int)(c % kCellsPerAxis), cy = (int)((c / kCellsPerAxis) % kCellsPerAxis), cz = (int)(c / (kCellsPerAxis * kCellsPerAxis));
+	int32_t* out = cl.entries + (co + t) * (int64_t)kListCap;
+	int n = 0;
+	for (int dz = -1; dz <= 1; dz++) {
+		const int qz = cz + dz;
+		if (qz < 0 || qz >= kCellsPerAxis) continue;
+		for (int dy = -1; dy <= 1; dy++) {
+			const int qy = cy + dy;
+			if (qy < 0 || qy >= kCellsPerAxis) continue;
+			for (int dx = -1; dx <= 1; dx++) {
+				const int qx = cx + dx;
+				if (qx < 0 || qx >= kCellsPerAxis) continue;
+				const uint64_t cell = ((uint64_t)qz * kCellsPerAxis + (uint64_t)qy) * kCellsPerAxis + (uint64_t)qx;
+				const int2 run = find_run(hkeys, hvals, cap, ((uint64_t)(uint32_t)node << 32) | cell);
+				const int4* rp = crec + co + run.x;
+				for (int i = 0; i < run.y; i++) {
+					const int4 q = rp[i];
+					if (q.w >= t) continue;  // only earlier candidates
+					if (pre32) {
+						const float fx = (float)(q.x - me.x) * sf[0], fy = (float)(q.y - me.y) * sf[1], fz = (float)(q.z - me.z) * sf[2];
+						if (fx * fx + fy * fy + fz * fz >= s2hi) continue;
+					}
+					const double ax = qcoord(q.x, 0, pp), ay = qcoord(q.y, 1, pp), az = qcoord(q.z, 2, pp);
+					// squaredDistance(point, candidate), sampler_poisson.h:117-125
+					const double dx_ = ax - x, dy_ = ay - y, dz_ = az - z;
+					if (!(dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < s2)) continue;
+					if (MODE == 0 && !(lb.keys[co + q.w] >= lim)) continue;
+					if (n < kListCap) out[n] = q.w;
+					n++;
+				}
+			}
+		}
+	}
+	cl.count[co + t] = (uint8_t)(n <= kListCap ? n : kListDense);
+	if (n > kListCap) cl.node_dense[node] = 1;
+}
+
+}  // namespace
+
+void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<LevelNode>& ln, const std::vector<uint8_t>& use,
+                          const PosParamsS& pp, LevelBuffers& lb, ConflictLists& cl, std::vector<uint8_t>& dense, SampleStats* st,
+                          DeviceMem& mem) {
+	const int K = (int)ln.size();
+	const int64_t M = lb.M;
+	dense.assign(K, 0);
+	if (M == 0 || K == 0) return;
+	cudaStream_t s = mem.stream();
+	const unsigned blocks = (unsigned)ceil_div(M, 256);
+	uint64_t* keys = mem.alloc<uint64_t>(M);
+	conf_cell_keys_kernel<<<blocks, 256, 0, s>>>(d_nodes, pp, lb, keys);
+	PCG_LAUNCHED();
+	uint64_t* ck = mem.alloc<uint64_t>(M);
+	uint32_t* cv = mem.alloc<uint32_t>(M);
+	segmented_sort_pairs(ln, M, keys, nullptr, ck, cv, 21, mem);
+	mem.free(keys);
+	int4* crec = mem.alloc<int4>(M);
+	conf_gather_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb, cv, crec);
+	PCG_LAUNCHED();
+	mem.free(cv);
+	unsigned long long* d_runs = mem.alloc<unsigned long long>(1);
+	PCG_CUDA(cudaMemsetAsync(d_runs, 0, sizeof(unsigned long long), s));
+	conf_count_runs_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb.node_of, ck, M, d_runs);
+	PCG_LAUNCHED();
+	unsigned long long runs = 0;
+	PCG_CUDA(cudaMemcpyAsync(&runs, d_runs, sizeof(runs), cudaMemcpyDeviceToHost, s));
+	PCG_CUDA(cudaStreamSynchronize(s));
+	mem.free(d_runs);
+	int64_t cap = 64;
+	while (cap < 2 * (int64_t)runs) cap <<= 1;
+	uint64_t* hkeys = mem.alloc<uint64_t>(cap);
+	int2* hvals = mem.alloc<int2>(cap);
+	PCG_CUDA(cudaMemsetAsync(hkeys, 0xff, cap * sizeof(uint64_t), s));
+	conf_insert_runs_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb.node_of, ck, M, hkeys, hvals, cap, st);
+	PCG_LAUNCHED();
+	cl.entries = mem.alloc<int32_t>((size_t)M * kListCap);
+	cl.count = mem.alloc<uint8_t>(M);
+	cl.node_dense = mem.alloc<uint8_t>(K);
+	PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
+	uint8_t* d_use = mem.alloc<uint8_t>(K);
+	PCG_CUDA(cudaMemcpyAsync(d_use, use.data(), K, cudaMemcpyHostToDevice, s));
+	if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, hkeys, hvals, cap, cl);
+	else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, hkeys, hvals, cap, cl);
+	PCG_LAUNCHED();
+	PCG_CUDA(cudaMemcpyAsync(dense.data(), cl.node_dense, K, cudaMemcpyDeviceToHost, s));
+	PCG_CUDA(cudaStreamSynchronize(s));
+	mem.free(d_use);
+	mem.free(hkeys);
+	mem.free(hvals);
+	mem.free(crec);
+	mem.free(ck);
+}
+
+void free_conflict_lists(ConflictLists& cl, DeviceMem& mem) {
+	if (cl.entries) mem.free(cl.entries);
+	if (cl.count) mem.free(cl.count);
+	if (cl.node_dense) mem.free(cl.node_dense);
+	cl = ConflictLists{};
+}
+
+}  // namespace pcg

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <condition_variable>
 #include <deque>
 #include <fstream>
@@ -213,6 +214,15 @@ struct JobResult {
 	bool octree_on_device = false;
 	pcg_stats stats{};
 };
+
+// PCG_TRACE_LEVELS=1 prints one line per sampled octree level to stderr
+static bool trace_levels() {
+	static const bool on = [] {
+		const char* e = std::getenv("PCG_TRACE_LEVELS");
+		return e && e[0] == '1';
+	}();
+	return on;
+}
 
 struct Converter {
 	int device = 0;
@@ -422,6 +432,7 @@ struct Converter {
 		auto t_samp = Clock::now();
 		SampleStats* d_st = mem.alloc<SampleStats>(1);
 		PCG_CUDA(cudaMemsetAsync(d_st, 0, sizeof(SampleStats), stream));
+		GreedyArena grid_arena;
 		PosParamsS pps;
 		for (int a = 0; a < 3; a++) { pps.scale[a] = pp.scale[a]; pps.offset[a] = pp.offset[a]; }
 		const double base_spacing = (rmax - rmin).x / 128.0;  // indexer.cpp:1603
@@ -458,7 +469,7 @@ struct Converter {
 			for (int i = 0; i < (int)tree.nodes.size(); i++)
 				if (tree.nodes[i].depth == d && tree.nodes[i].has_children()) level_nodes.push_back(i);
 			if (level_nodes.empty()) continue;
-			sample_level(tree, level_nodes, method, base_spacing, pps, co, d_recs, p, d_st, mem, res);
+			sample_level(tree, level_nodes, method, base_spacing, pps, co, d_recs, p, d_st, grid_arena, mem, res);
 		}
 		// the root's final payload is its accepted buffer
 		TNode& root = tree.nodes[0];
@@ -590,8 +601,8 @@ struct Converter {
 	}
 
 	void sample_level(Tree& tree, const std::vector<int>& level_nodes, int method, double base_spacing, const PosParamsS& pps,
-	                  const ChunkingOut& co, const uint8_t* d_recs, const DecodeParams& p, SampleStats* d_st, DeviceMem& mem,
-	                  JobResult& res) {
+	                  const ChunkingOut& co, const uint8_t* d_recs, const DecodeParams& p, SampleStats* d_st, GreedyArena& grid_arena,
+	                  DeviceMem& mem, JobResult& res) {
 		int sms = 148;
 		PCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
 		(void)d_recs;
@@ -656,6 +667,7 @@ struct Converter {
 			lb.perm = mem.alloc<int32_t>(M);
 			lb.pos = mem.alloc<int32_t>(M);
 			lb.acc_rank = mem.alloc<int32_t>(M);
+			lb.cq = mem.alloc<int4>(M);
 			launch_keys(d_nodes, co.X, co.Y, co.Z, pps, lb, mem);
 			double* axyz = mem.alloc<double>(3 * M);
 			double* akey = mem.alloc<double>(M);
@@ -668,14 +680,17 @@ struct Converter {
 			int num_big = 0;
 			const int64_t big_min = K < 2 * sms ? kSmallLevelCtaCandidates : kBigNodeCandidates;
 			while (num_big < K && ln[order[num_big]].count >= big_min) num_big++;
+			int list_nodes = 0;
 			cudaEvent_t ev[3];
 			for (auto& e : ev) PCG_CUDA(cudaEventCreate(&e));
 			PCG_CUDA(cudaEventRecord(ev[0], s));
 			if (form == PCG_FORM_PLAIN) {
 				for (int k = 0; k < K; k++) launch_node_sort(d_nodes, d_order, K, lb, d_st, mem, k, k + 1, num_big);
+				launch_cand_records(d_nodes, co.X, co.Y, co.Z, lb, mem);
 				PCG_CUDA(cudaEventRecord(ev[1], s));
 				for (int k = 0; k < K; k++)
-					launch_greedy(mode, false, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, k, k + 1, num_big);
+					launch_greedy(mode, false, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, &grid_arena, k, k + 1,
+					              num_big);
 			} else {
 				// distinct keys: one exact radix sort of the level; equal keys:
 				// the introsort replay, for those nodes only
@@ -696,8 +711,28 @@ struct Converter {
 					launch_node_pos(d_nodes, d_tie_nodes, (int)tie_nodes.size(), lb, mem);
 					mem.free(d_tie_nodes);
 				}
+				launch_cand_records(d_nodes, co.X, co.Y, co.Z, lb, mem);
 				PCG_CUDA(cudaEventRecord(ev[1], s));
-				launch_greedy(mode, guard, d_nodes, d_order, K, co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey, anext, apos, d_st, mem, 0, -1, num_big);
+				// conflict lists for every node; a node where some candidate has
+				// too many close predecessors keeps the lookup kernels
+				ConflictLists cl;
+				std::vector<int32_t> cta_list, warp_list, order2;
+				{
+					std::vector<uint8_t> use(K, 1), dense;
+					build_conflict_lists(mode, d_nodes, ln, use, pps, lb, cl, dense, d_st, mem);
+					for (int i = 0; i < num_big; i++) (dense[order[i]] ? order2 : cta_list).push_back(order[i]);
+					const int num_grid = (int)order2.size();
+					for (int i = num_big; i < K; i++) (dense[order[i]] ? order2 : warp_list).push_back(order[i]);
+					list_nodes = (int)(cta_list.size() + warp_list.size());
+					launch_greedy_lists(mode, d_nodes, cta_list, warp_list, pps, lb, hkeys, hvals, axyz, akey, anext, apos, cl, d_st, mem);
+					if (!order2.empty()) {
+						int32_t* d_order2 = upload(order2, mem);
+						launch_greedy(mode, guard, d_nodes, d_order2, (int)order2.size(), co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey,
+						              anext, apos, d_st, mem, &grid_arena, 0, -1, num_grid);
+						mem.free(d_order2);
+					}
+				}
+				free_conflict_lists(cl, mem);
 			}
 			PCG_CUDA(cudaEventRecord(ev[2], s));
 			PCG_CUDA(cudaEventSynchronize(ev[2]));
@@ -706,6 +741,26 @@ struct Converter {
 			PCG_CUDA(cudaEventElapsedTime(&t_greedy, ev[1], ev[2]));
 			res.stats.ms_sort += t_sort;
 			res.stats.ms_greedy += t_greedy;
+			if (trace_levels()) {
+				int64_t mx = 0;
+				for (auto& l : ln) mx = std::max<int64_t>(mx, l.count);
+				static thread_local SampleStats prev{};
+				SampleStats now = download(d_st, 1, s)[0];
+				if (now.rounds < prev.rounds) prev = SampleStats{};
+				fprintf(stderr,
+				        "[pcg] level %d: nodes %d (cta %d, lists %d), candidates %lld, largest %lld, sort %.3f ms, greedy %.3f ms, "
+				        "cta rounds %llu, passes %llu, serial rounds %llu, kcycles/round A %.1f B %.1f C1 %.1f C2 %.1f D %.1f, "
+				        "cells>3 %llu, overflow points %llu\n",
+				        K ? ln[0].level : -1, K, num_big, list_nodes, (long long)M, (long long)mx, t_sort, t_greedy, now.rounds - prev.rounds,
+				        now.passes - prev.passes, now.serial - prev.serial,
+				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(0),
+				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(1),
+				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(2),
+				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(3),
+				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(4),
+				        now.cycles[5] - prev.cycles[5], now.cycles[6] - prev.cycles[6]);
+				prev = now;
+			}
 			for (auto& e : ev) cudaEventDestroy(e);
 			if (method == PCG_POISSON_AVERAGE) {
 				long long* sums = mem.alloc<long long>(4 * M);
@@ -713,7 +768,7 @@ struct Converter {
 				mem.free(sums);
 			}
 			mem.free(axyz); mem.free(akey); mem.free(anext); mem.free(apos);
-			mem.free(lb.keys); mem.free(lb.perm); mem.free(lb.pos); mem.free(lb.acc_rank);
+			mem.free(lb.keys); mem.free(lb.perm); mem.free(lb.pos); mem.free(lb.acc_rank); mem.free(lb.cq);
 		}
 		mem.free(hkeys);
 		mem.free(hvals);

@@ -59,6 +59,14 @@ __device__ __forceinline__ void point_xyz(const int32_t* X, const int32_t* Y, co
 	z = ((double)Z[id] * pp.scale[2]) + pp.offset[2];
 }
 
+// squared distance to the node centre, center = (min + max) * 0.5
+// (sampler_poisson.h:127, 183-203); the one expression every kernel uses
+__device__ __forceinline__ double center_key(const LevelNode& nd, double x, double y, double z) {
+	double cx = (nd.min[0] + nd.max[0]) * 0.5, cy = (nd.min[1] + nd.max[1]) * 0.5, cz = (nd.min[2] + nd.max[2]) * 0.5;
+	double ax = x - cx, ay = y - cy, az = z - cz;
+	return ax * ax + ay * ay + az * az;
+}
+
 __global__ void keys_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
                             const int32_t* __restrict__ Z, PosParamsS pp, LevelBuffers lb) {
 	int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -66,11 +74,19 @@ __global__ void keys_kernel(const LevelNode* __restrict__ nodes, const int32_t* 
 	const LevelNode& nd = nodes[lb.node_of[j]];
 	double x, y, z;
 	point_xyz(X, Y, Z, pp, lb.ids[j], x, y, z);
-	// center = (min + max) * 0.5 (sampler_poisson.h:127)
-	double cx = (nd.min[0] + nd.max[0]) * 0.5, cy = (nd.min[1] + nd.max[1]) * 0.5, cz = (nd.min[2] + nd.max[2]) * 0.5;
-	double ax = x - cx, ay = y - cy, az = z - cz;
-	lb.keys[j] = ax * ax + ay * ay + az * az;
+	lb.keys[j] = center_key(nd, x, y, z);
 	lb.perm[j] = (int32_t)(j - nd.cand_off);
+}
+
+// sorted candidate records: (X, Y, Z, local index) at each sorted position
+__global__ void cand_records_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
+                                    const int32_t* __restrict__ Z, LevelBuffers lb) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const int64_t off = nodes[lb.node_of[j]].cand_off;
+	const int32_t local = lb.perm[j];
+	const uint32_t id = lb.ids[off + local];
+	lb.cq[j] = make_int4(X[id], Y[id], Z[id], local);
 }
 
 // --------------------------------------------------------------- hashing
@@ -500,8 +516,12 @@ __global__ void shuffle_single_kernel(int64_t n, uint32_t seed, int32_t* perm) {
 // Greedy acceptance for a large node, one CTA, 512 candidates per round:
 //  A. each thread looks up its candidate's conflicts among the points
 //     accepted in earlier rounds. They live in a dense grid over the node
-//     box (64^3 cells of two spacings, 7 acceptance ranks inline per cell,
-//     overflow in a list), so a lookup is two dependent loads per cell;
+//     box: 64^3 cells of two spacings, each one 128-byte line holding the
+//     count and up to 7 accepted points inline as (X, Y, Z, rank) -- the
+//     quantized coordinates, from which the FP64 position and key are
+//     recomputed bit for bit -- with an overflow list beyond that. The
+//     eight cells around a candidate are fetched as independent 64-byte
+//     loads, so a lookup costs one memory latency, not a chain per point;
 //  B. conflicts among the round's own candidates are found through a shared
 //     memory hash of the round (earlier candidates within the spacing);
 //  C. decisions: parallel passes decide every candidate whose earlier
@@ -510,30 +530,36 @@ __global__ void shuffle_single_kernel(int64_t n, uint32_t seed, int32_t* perm) {
 //     order -- candidates whose old conflict sits at the edge of the
 //     10,001-check window, which depends on how many were accepted before;
 //  D. the round's accepted points get their ranks and enter the grid.
+// The grid starts empty; at the end of its node a CTA empties the cells it
+// filled, so the next node on the same slot finds it clean.
 constexpr int kRound = kBigThreads;
 constexpr int kRoundHash = 2 * kRound;
 constexpr int kMaxLocal = 12;
 constexpr int kGridDim = 64;  // node box = 128 spacings = 64 cells of 2 spacings
 constexpr int64_t kGridCells = (int64_t)kGridDim * kGridDim * kGridDim;
 constexpr int kCellSlots = 7;
+constexpr int32_t kEmptyCell = -1;
 
-struct alignas(32) AccCell {
+struct alignas(128) AccCell {
 	int32_t count;
-	int32_t slot[kCellSlots];
+	int32_t pad[3];
+	int4 slot[kCellSlots];  // (X, Y, Z, rank)
 };
+static_assert(sizeof(AccCell) == 128, "one cache line per cell");
 
 struct GridArena {
 	AccCell* cells;  // kGridCells per CTA slot
 	int32_t* ovf;    // overflow list heads, kGridCells per CTA slot
 	int32_t* link;   // overflow list links, one per candidate (cand_off + rank)
+	int4* accq;      // accepted points in rank order (cand_off + rank): X, Y, Z
 };
 
 struct RoundShared {
 	double x[kRound], y[kRound], z[kRound], key[kRound], lim[kRound];
 	int32_t maxrank[kRound];
 	int32_t local[kRound];
-	uint64_t hkey[kRoundHash];
-	int16_t hhead[kRoundHash];
+	int32_t hkey[kRoundHash];
+	int32_t hhead[kRoundHash];
 	int16_t hnext[kRound];
 	int16_t conf[kRound][kMaxLocal];
 	uint8_t nconf[kRound];
@@ -544,18 +570,52 @@ struct RoundShared {
 	unsigned long long warp_sums[kBigWarps];
 };
 
-__device__ __forceinline__ uint32_t round_slot(uint64_t k) { return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> 53) & (kRoundHash - 1); }
+__device__ __forceinline__ uint32_t round_slot(int32_t k) { return ((uint32_t)k * 0x9E3779B1u) >> (32 - 10); }
+static_assert(kRoundHash == 1024, "round_slot yields 10 bits");
+
+// 10 bits per axis: cells -512..511 (a node's points lie in cells 0..63)
+__device__ __forceinline__ int32_t round_cell_key(int cx, int cy, int cz) {
+	return ((cx + 512) << 20) | ((cy + 512) << 10) | (cz + 512);
+}
+__device__ __forceinline__ bool round_cell_ok(int cx, int cy, int cz) {
+	return cx >= -512 && cx < 512 && cy >= -512 && cy < 512 && cz >= -512 && cz < 512;
+}
 
 __device__ __forceinline__ int grid_clamp(int c) { return c < 0 ? 0 : (c >= kGridDim ? kGridDim - 1 : c); }
 __device__ __forceinline__ int64_t grid_index(int cx, int cy, int cz) {
 	return ((int64_t)grid_clamp(cz) * kGridDim + grid_clamp(cy)) * kGridDim + grid_clamp(cx);
 }
 
+// conflict test of candidate (x, y, z) against an accepted point stored as
+// quantized (X, Y, Z, rank): within the spacing and, for poisson, not behind
+// the early-exit bound lim (sampler_poisson.h:150-167)
+struct SlotTest {
+	float sf[3];   // scale as float, for the prefilter
+	float s2hi;    // s^2 (1 + 1e-3) as float
+	bool pre32;    // prefilter usable: small quantized extent, s^2 in float range
+};
+
+template <int MODE>
+__device__ __forceinline__ void test_slot(const int4& q, const int4& me, const SlotTest& T, const PosParamsS& pp, const LevelNode& nd, double x,
+                                          double y, double z, double s2, double lim, int32_t& maxrank) {
+	if (q.w <= maxrank) return;  // cannot raise the maximum
+	if (T.pre32) {
+		// FP32 distance from exact integer deltas: rules out every point
+		// farther than the spacing by a margin far above its rounding error
+		const float fx = (float)(q.x - me.x) * T.sf[0], fy = (float)(q.y - me.y) * T.sf[1], fz = (float)(q.z - me.z) * T.sf[2];
+		if (fx * fx + fy * fy + fz * fz >= T.s2hi) return;
+	}
+	const double ax = ((double)q.x * pp.scale[0]) + pp.offset[0];
+	const double ay = ((double)q.y * pp.scale[1]) + pp.offset[1];
+	const double az = ((double)q.z * pp.scale[2]) + pp.offset[2];
+	if (sqdist(ax, ay, az, x, y, z) < s2) {
+		if (MODE == 1 || center_key(nd, ax, ay, az) >= lim) maxrank = q.w;
+	}
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order, int node_begin,
-                                                                const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
-                                                                const int32_t* __restrict__ Z, PosParamsS pp, LevelBuffers lb, GreedyArgs ga,
-                                                                GridArena arena, SampleStats* st) {
+                                                                PosParamsS pp, LevelBuffers lb, GreedyArgs ga, GridArena arena, SampleStats* st) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	RoundShared& R = *reinterpret_cast<RoundShared*>(smem_raw);
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -563,12 +623,6 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 	const int64_t n = nd.count, co = nd.cand_off;
 	AccCell* cells = arena.cells + (int64_t)blockIdx.x * kGridCells;
 	int32_t* ovf = arena.ovf + (int64_t)blockIdx.x * kGridCells;
-	{
-		int4* c4 = reinterpret_cast<int4*>(cells);
-		const int64_t n4 = kGridCells * (int64_t)sizeof(AccCell) / 16;
-		for (int64_t i = tid; i < n4; i += kBigThreads) c4[i] = make_int4(0, 0, 0, 0);
-		for (int64_t i = tid; i < kGridCells; i += kBigThreads) ovf[i] = -1;
-	}
 	uint64_t* hk = ga.hkeys + nd.hash_off;
 	int32_t* hh = ga.hheads + nd.hash_off;
 	if (MODE == 1) {
@@ -581,18 +635,35 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 	CellGrid g;
 	g.min[0] = nd.min[0]; g.min[1] = nd.min[1]; g.min[2] = nd.min[2];
 	g.inv = 1.0 / (2.0 * sp * 1.000001);
+	SlotTest T;
+	{
+		bool ok = s2 > 1e-30 && s2 < 1e30;
+		for (int a = 0; a < 3; a++) {
+			T.sf[a] = (float)pp.scale[a];
+			// all points of the node lie in its box: integer deltas stay below 2^23
+			ok = ok && pp.scale[a] > 0.0 && (nd.max[a] - nd.min[a]) / pp.scale[a] < 8.0e6;
+		}
+		T.s2hi = (float)(s2 * 1.001);
+		T.pre32 = ok;
+	}
+	unsigned long long n_past3 = 0, n_ovf = 0;
 	for (int64_t r0 = 0; r0 < n; r0 += kRound) {
 		const int64_t t = r0 + tid;
 		const bool valid = t < n;
 		const int nr = (int)((n - r0) < kRound ? (n - r0) : kRound);
 		const int32_t cnt0 = R.cnt;
 		// ---- A
+		long long clk0 = clock64();
 		double x = 0, y = 0, z = 0, key = 0, lim = -CUDART_INF;
 		int32_t local = 0, maxrank = -1;
+		int4 me = make_int4(0, 0, 0, 0);
 		int c[3] = {0, 0, 0}, o[3] = {1, 1, 1};
 		if (valid) {
-			local = lb.perm[co + t];
-			point_xyz(X, Y, Z, pp, lb.ids[co + local], x, y, z);
+			me = lb.cq[co + t];
+			local = me.w;
+			x = ((double)me.x * pp.scale[0]) + pp.offset[0];
+			y = ((double)me.y * pp.scale[1]) + pp.offset[1];
+			z = ((double)me.z * pp.scale[2]) + pp.offset[2];
 			key = lb.keys[co + t];
 			if (MODE == 0) {
 				double cd = sqrt(key);
@@ -602,36 +673,48 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 			double fr[3];
 			cell_of(g, x, y, z, c, fr);
 			for (int a = 0; a < 3; a++) o[a] = fr[a] < 0.5 ? -1 : 1;
-			int64_t cidx[8];
-			int32_t ccount[8];
 #pragma unroll
-			for (int q = 0; q < 8; q++) {
-				cidx[q] = grid_index(c[0] + ((q & 4) ? o[0] : 0), c[1] + ((q & 2) ? o[1] : 0), c[2] + ((q & 1) ? o[2] : 0));
-				ccount[q] = cells[cidx[q]].count;
-			}
+			for (int h = 0; h < 2; h++) {
+				// four cells at a time: count and the first three points in one 64-byte read each
+				int64_t cidx[4];
+				int4 v[4][4];
 #pragma unroll
-			for (int q = 0; q < 8; q++) {
-				// a clamped neighbour may repeat a cell; scanning it twice is harmless
-				const AccCell& cell = cells[cidx[q]];
-				const int inl = ccount[q] < kCellSlots ? ccount[q] : kCellSlots;
-				for (int k = 0; k < inl; k++) {
-					const int32_t rr = cell.slot[k];
-					const int64_t slot = co + rr;
-					if (MODE == 1 || ga.akey[slot] >= lim) {
-						if (sqdist(ga.axyz[3 * slot], ga.axyz[3 * slot + 1], ga.axyz[3 * slot + 2], x, y, z) < s2 && rr > maxrank) maxrank = rr;
-					}
+				for (int q = 0; q < 4; q++) {
+					const int qq = 4 * h + q;
+					cidx[q] = grid_index(c[0] + ((qq & 4) ? o[0] : 0), c[1] + ((qq & 2) ? o[1] : 0), c[2] + ((qq & 1) ? o[2] : 0));
+					const int4* cp = reinterpret_cast<const int4*>(cells + cidx[q]);
+#pragma unroll
+					for (int w = 0; w < 4; w++) v[q][w] = cp[w];
 				}
-				if (ccount[q] > kCellSlots) {
-					int32_t rr = ovf[cidx[q]];
-					int64_t guard = 0;
-					while (rr >= 0 && guard++ <= n) {
-						const int64_t slot = co + rr;
-						if (MODE == 1 || ga.akey[slot] >= lim) {
-							if (sqdist(ga.axyz[3 * slot], ga.axyz[3 * slot + 1], ga.axyz[3 * slot + 2], x, y, z) < s2 && rr > maxrank) maxrank = rr;
-						}
-						rr = arena.link[slot];
+#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					// a clamped neighbour may repeat a cell; scanning it twice is harmless
+					const int cntq = v[q][0].x;
+#pragma unroll
+					for (int k = 0; k < 3; k++)
+						if (k < cntq) test_slot<MODE>(v[q][1 + k], me, T, pp, nd, x, y, z, s2, lim, maxrank);
+					if (cntq > 3) {
+						const int4* cp = reinterpret_cast<const int4*>(cells + cidx[q]);
+						int4 u[4];
+#pragma unroll
+						for (int w = 0; w < 4; w++) u[w] = cp[4 + w];
+#pragma unroll
+						for (int k = 0; k < 4; k++)
+							if (3 + k < cntq) test_slot<MODE>(u[k], me, T, pp, nd, x, y, z, s2, lim, maxrank);
 					}
-					if (guard > n + 1) atomicAdd(&st->timeouts, 1ull);
+					if (cntq > 3) n_past3++;
+					if (cntq > kCellSlots) {
+						n_ovf += cntq - kCellSlots;
+						int32_t rr = ovf[cidx[q]];
+						int64_t guard = 0;
+						while (rr >= 0 && guard++ <= n) {
+							int4 a = arena.accq[co + rr];
+							a.w = rr;
+							test_slot<MODE>(a, me, T, pp, nd, x, y, z, s2, lim, maxrank);
+							rr = arena.link[co + rr];
+						}
+						if (guard > n + 1) atomicAdd(&st->timeouts, 1ull);
+					}
 				}
 			}
 		}
@@ -650,44 +733,39 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 			}
 			R.old[tid] = os;
 		}
-		for (int s = tid; s < kRoundHash; s += kBigThreads) { R.hkey[s] = EMPTY_KEY; R.hhead[s] = -1; }
+		for (int s = tid; s < kRoundHash; s += kBigThreads) { R.hkey[s] = kEmptyCell; R.hhead[s] = -1; }
 		__syncthreads();
 		// ---- B: hash the round by cell, then collect earlier conflicting candidates
+		long long clk1 = clock64();
 		if (valid) {
-			uint64_t k = cell_key(c[0], c[1], c[2]);
+			if (!round_cell_ok(c[0], c[1], c[2])) atomicAdd(&st->timeouts, 1ull);
+			const int32_t k = round_cell_key(c[0], c[1], c[2]);
 			uint32_t s = round_slot(k);
 			for (int probe = 0; probe < kRoundHash; probe++) {
-				unsigned long long prev = atomicCAS((unsigned long long*)&R.hkey[s], (unsigned long long)EMPTY_KEY, (unsigned long long)k);
-				if (prev == EMPTY_KEY || prev == k) break;
+				const int32_t prev = atomicCAS(&R.hkey[s], kEmptyCell, k);
+				if (prev == kEmptyCell || prev == k) break;
 				s = (s + 1) & (kRoundHash - 1);
 			}
-			int32_t* word = reinterpret_cast<int32_t*>(&R.hhead[s & ~1u]);
-			int shift = (s & 1u) ? 16 : 0;
-			while (true) {
-				int32_t old = *word;
-				int16_t head = (int16_t)((old >> shift) & 0xffff);
-				int32_t neu = (old & ~(0xffff << shift)) | ((int32_t)(uint16_t)tid << shift);
-				R.hnext[tid] = head;
-				if (atomicCAS(word, old, neu) == old) break;
-			}
+			R.hnext[tid] = (int16_t)atomicExch(&R.hhead[s], tid);
 		}
 		__syncthreads();
 		if (valid) {
 			int nc = 0;
 			for (int q = 0; q < 8; q++) {
-				int qx = c[0] + ((q & 4) ? o[0] : 0), qy = c[1] + ((q & 2) ? o[1] : 0), qz = c[2] + ((q & 1) ? o[2] : 0);
-				uint64_t k = cell_key(qx, qy, qz);
+				const int qx = c[0] + ((q & 4) ? o[0] : 0), qy = c[1] + ((q & 2) ? o[1] : 0), qz = c[2] + ((q & 1) ? o[2] : 0);
+				if (!round_cell_ok(qx, qy, qz)) continue;
+				const int32_t k = round_cell_key(qx, qy, qz);
 				uint32_t s = round_slot(k);
-				int16_t j = -1;
+				int j = -1;
 				for (int probe = 0; probe < kRoundHash; probe++) {
-					uint64_t kk = R.hkey[s];
+					const int32_t kk = R.hkey[s];
 					if (kk == k) { j = R.hhead[s]; break; }
-					if (kk == EMPTY_KEY) break;
+					if (kk == kEmptyCell) break;
 					s = (s + 1) & (kRoundHash - 1);
 				}
 				while (j >= 0) {
 					if (j < tid && (MODE == 1 || R.key[j] >= lim) && sqdist(R.x[j], R.y[j], R.z[j], x, y, z) < s2) {
-						if (nc < kMaxLocal) R.conf[tid][nc] = j;
+						if (nc < kMaxLocal) R.conf[tid][nc] = (int16_t)j;
 						nc++;
 					}
 					j = R.hnext[j];
@@ -697,6 +775,7 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 		}
 		__syncthreads();
 		// ---- C1: parallel passes
+		long long clk2 = clock64();
 		volatile uint8_t* vstate = R.state;
 		for (int pass = 0; pass < 64; pass++) {
 			bool changed = false;
@@ -717,9 +796,17 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 				}
 				if (dec) { vstate[tid] = dec; changed = true; }
 			}
-			if (!__syncthreads_or(changed)) break;
+			if (!__syncthreads_or(changed)) {
+				if (tid == 0) atomicAdd(&st->passes, (unsigned long long)pass + 1);
+				break;
+			}
 		}
 		const bool left = __syncthreads_or(valid && vstate[tid] == 0);
+		if (tid == 0) {
+			atomicAdd(&st->rounds, 1ull);
+			if (left) atomicAdd(&st->serial, 1ull);
+		}
+		long long clk3 = clock64();
 		// ---- C2: warp 0 decides the rest in sorted order
 		if (left && warp == 0) {
 			int32_t cnt = cnt0;
@@ -771,6 +858,7 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 		}
 		__syncthreads();
 		// ---- D: publish
+		long long clk4 = clock64();
 		const bool acc = valid && vstate[tid] == 1;
 		unsigned long long total;
 		unsigned long long pre;
@@ -781,27 +869,380 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 		if (valid) {
 			lb.accepted[co + local] = acc ? 1 : 0;
 			if (acc) {
-				int32_t rank = cnt0 + (int32_t)pre;
+				const int32_t rank = cnt0 + (int32_t)pre;
 				lb.acc_rank[co + local] = rank;
 				const int64_t slot = co + rank;
-				ga.axyz[3 * slot] = x;
-				ga.axyz[3 * slot + 1] = y;
-				ga.axyz[3 * slot + 2] = z;
-				ga.akey[slot] = key;
-				ga.apos[slot] = (int32_t)t;
+				arena.accq[slot] = make_int4(me.x, me.y, me.z, 0);
 				const int64_t ci = grid_index(c[0], c[1], c[2]);
 				const int32_t pos = atomicAdd(&cells[ci].count, 1);
-				if (pos < kCellSlots) cells[ci].slot[pos] = rank;
+				if (pos < kCellSlots) cells[ci].slot[pos] = make_int4(me.x, me.y, me.z, rank);
 				else arena.link[slot] = atomicExch(&ovf[ci], rank);
 				if (MODE == 1) {
 					// the colour pass walks the hash lists (linked through anext)
+					ga.axyz[3 * slot] = x;
+					ga.axyz[3 * slot + 1] = y;
+					ga.axyz[3 * slot + 2] = z;
+					ga.akey[slot] = key;
+					ga.apos[slot] = (int32_t)t;
 					if (!hash_push(hk, hh, ga.anext + co, nd.hash_cap, cell_key(c[0], c[1], c[2]), rank)) atomicAdd(&st->timeouts, 1ull);
 				}
 			}
 		}
 		__syncthreads();
-		if (tid == 0) R.cnt = cnt0 + (int32_t)total;
+		if (tid == 0) {
+			R.cnt = cnt0 + (int32_t)total;
+			const long long clk5 = clock64();
+			atomicAdd(&st->cycles[0], (unsigned long long)(clk1 - clk0));
+			atomicAdd(&st->cycles[1], (unsigned long long)(clk2 - clk1));
+			atomicAdd(&st->cycles[2], (unsigned long long)(clk3 - clk2));
+			atomicAdd(&st->cycles[3], (unsigned long long)(clk4 - clk3));
+			atomicAdd(&st->cycles[4], (unsigned long long)(clk5 - clk4));
+		}
 		__syncthreads();
+	}
+	if (n_past3) atomicAdd(&st->cycles[5], n_past3);
+	if (n_ovf) atomicAdd(&st->cycles[6], n_ovf);
+	// empty the cells this node filled (count and overflow head)
+	const int32_t total = R.cnt;
+	for (int32_t r = tid; r < total; r += kBigThreads) {
+		const int4 q = arena.accq[co + r];
+		const double ax = ((double)q.x * pp.scale[0]) + pp.offset[0];
+		const double ay = ((double)q.y * pp.scale[1]) + pp.offset[1];
+		const double az = ((double)q.z * pp.scale[2]) + pp.offset[2];
+		int cc[3];
+		double fr[3];
+		cell_of(g, ax, ay, az, cc, fr);
+		const int64_t ci = grid_index(cc[0], cc[1], cc[2]);
+		cells[ci].count = 0;
+		ovf[ci] = -1;
+	}
+}
+
+
+// Greedy acceptance for a large node from its conflict lists (conflicts.cu),
+// one CTA, 512 candidates per round. A candidate's list names every earlier
+// candidate that would reject it if accepted, so the round needs no spatial
+// lookups: earlier rounds' decisions are read from srank (rank, or -1 for
+// rejected), this round's are resolved by the same parallel passes and
+// in-order warp as the grid kernel.
+struct ListRound {
+	int32_t maxrank[kRound];
+	int32_t local[kRound];
+	int16_t conf[kRound][kListCap];
+	uint8_t nconf[kRound];
+	uint8_t state[kRound];   // 0 undecided, 1 accepted, 2 rejected
+	uint8_t old[kRound];     // old-window status: 0 no conflict, 1 conflict, 2 depends on the count
+	int32_t cnt;             // accepted before this round
+	unsigned long long warp_sums[kBigWarps];
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(kBigThreads) greedy_list_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order,
+                                                                 int node_begin, PosParamsS pp, LevelBuffers lb, GreedyArgs ga,
+                                                                 ConflictLists cl, int32_t* __restrict__ srank, SampleStats* st) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	ListRound& R = *reinterpret_cast<ListRound*>(smem_raw);
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const LevelNode nd = nodes[order[node_begin + blockIdx.x]];
+	const int64_t n = nd.count, co = nd.cand_off;
+	uint64_t* hk = ga.hkeys + nd.hash_off;
+	int32_t* hh = ga.hheads + nd.hash_off;
+	if (MODE == 1) {
+		// poisson_average's colour pass finds accepted points through the hash
+		for (int64_t i = tid; i < nd.hash_cap; i += kBigThreads) { hk[i] = EMPTY_KEY; hh[i] = -1; }
+	}
+	if (tid == 0) R.cnt = 0;
+	__syncthreads();
+	CellGrid g;
+	g.min[0] = nd.min[0]; g.min[1] = nd.min[1]; g.min[2] = nd.min[2];
+	g.inv = 1.0 / (2.0 * nd.spacing * 1.000001);
+	for (int64_t r0 = 0; r0 < n; r0 += kRound) {
+		const int64_t t = r0 + tid;
+		const bool valid = t < n;
+		const int nr = (int)((n - r0) < kRound ? (n - r0) : kRound);
+		const int32_t cnt0 = R.cnt;
+		// ---- A: the candidate's list
+		long long clk0 = clock64();
+		int32_t maxrank = -1, local = 0;
+		int nc = 0;
+		int4 me = make_int4(0, 0, 0, 0);
+		if (valid) {
+			me = lb.cq[co + t];
+			local = me.w;
+			const int nl = cl.count[co + t];
+			const int4* lp = reinterpret_cast<const int4*>(cl.entries + (co + t) * (int64_t)kListCap);
+			int32_t ent[kListCap];
+#pragma unroll
+			for (int w = 0; w < kListCap / 4; w++) {
+				int4 v = make_int4(0, 0, 0, 0);
+				if (4 * w < nl) v = lp[w];
+				ent[4 * w] = v.x; ent[4 * w + 1] = v.y; ent[4 * w + 2] = v.z; ent[4 * w + 3] = v.w;
+			}
+			int32_t rk[kListCap];
+#pragma unroll
+			for (int e = 0; e < kListCap; e++) rk[e] = (e < nl && ent[e] < r0) ? srank[co + ent[e]] : -1;
+#pragma unroll
+			for (int e = 0; e < kListCap; e++) {
+				if (e < nl) {
+					if (ent[e] < r0) maxrank = rk[e] > maxrank ? rk[e] : maxrank;
+					else R.conf[tid][nc++] = (int16_t)(ent[e] - r0);
+				}
+			}
+		}
+		R.maxrank[tid] = maxrank;
+		R.local[tid] = local;
+		R.nconf[tid] = (uint8_t)nc;
+		R.state[tid] = valid ? 0 : 2;
+		{
+			uint8_t os = 0;
+			if (maxrank >= 0) {
+				if (MODE == 1) os = 1;
+				else if (maxrank >= cnt0 + tid - 10001) os = 1;       // conflicts whatever was accepted before it
+				else if (maxrank < cnt0 - 10001) os = 0;              // outside the window in any case
+				else os = 2;
+			}
+			R.old[tid] = os;
+		}
+		__syncthreads();
+		long long clk1 = clock64();
+		long long clk2 = clk1;
+		// ---- C1: parallel passes
+		volatile uint8_t* vstate = R.state;
+		for (int pass = 0; pass < 64; pass++) {
+			bool changed = false;
+			if (valid && vstate[tid] == 0) {
+				const uint8_t os = R.old[tid];
+				uint8_t dec = 0;
+				if (os == 1) {
+					dec = 2;
+				} else {
+					bool any_acc = false, all_done = true;
+					for (int e = 0; e < R.nconf[tid]; e++) {
+						uint8_t sj = vstate[R.conf[tid][e]];
+						any_acc |= sj == 1;
+						all_done &= sj != 0;
+					}
+					if (any_acc) dec = 2;
+					else if (all_done && os == 0) dec = 1;
+				}
+				if (dec) { vstate[tid] = dec; changed = true; }
+			}
+			if (!__syncthreads_or(changed)) {
+				if (tid == 0) atomicAdd(&st->passes, (unsigned long long)pass + 1);
+				break;
+			}
+		}
+		const bool left = __syncthreads_or(valid && vstate[tid] == 0);
+		if (tid == 0) {
+			atomicAdd(&st->rounds, 1ull);
+			if (left) atomicAdd(&st->serial, 1ull);
+		}
+		long long clk3 = clock64();
+		// ---- C2: warp 0 decides the rest in sorted order
+		if (left && warp == 0) {
+			int32_t cnt = cnt0;
+			const uint32_t ltm = lanemask_lt();
+			for (int cb = 0; cb < nr; cb += 32) {
+				const int i = cb + lane;
+				const bool v = i < nr;
+				const uint8_t si = v ? vstate[i] : 2;
+				const bool undec = v && si == 0;
+				uint32_t accmask = __ballot_sync(FULL, v && si == 1);
+				if (__ballot_sync(FULL, undec) != 0) {
+					bool prev_conflict = false;
+					uint32_t mask = 0;
+					if (undec) {
+						const int ncf = R.nconf[i];
+						for (int e = 0; e < ncf; e++) {
+							int j = R.conf[i][e];
+							if (j < cb) prev_conflict |= vstate[j] == 1;
+							else mask |= 1u << (j - cb);
+						}
+					}
+					const int nvalid = nr - cb < 32 ? nr - cb : 32;
+					for (int b = 0; b < nvalid; b++) {
+						bool dec = false;
+						const bool ub = __shfl_sync(FULL, undec, b);
+						if (!ub) continue;
+						if (lane == b) {
+							int32_t m_i = cnt + __popc(accmask & ltm);
+							bool old_conflict = R.maxrank[i] >= 0 && (MODE == 1 || R.maxrank[i] >= m_i - 10001);
+							dec = !old_conflict && !prev_conflict && !(mask & accmask);
+							vstate[i] = dec ? 1 : 2;
+						}
+						dec = __shfl_sync(FULL, dec, b);
+						if (dec) accmask |= 1u << b;
+					}
+				}
+				cnt += __popc(accmask);
+				__syncwarp();
+			}
+		}
+		__syncthreads();
+		// ---- D: publish
+		long long clk4 = clock64();
+		const bool acc = valid && vstate[tid] == 1;
+		unsigned long long total;
+		unsigned long long pre;
+		{
+			BlockScratch& bs = *reinterpret_cast<BlockScratch*>(R.warp_sums);
+			pre = block_scan_u64(acc ? 1ull : 0ull, total, bs);
+		}
+		if (valid) {
+			const int32_t rank = cnt0 + (int32_t)pre;
+			srank[co + t] = acc ? rank : -1;
+			lb.accepted[co + local] = acc ? 1 : 0;
+			if (acc) {
+				lb.acc_rank[co + local] = rank;
+				if (MODE == 1) {
+					// the colour pass walks the hash lists (linked through anext)
+					const int64_t slot = co + rank;
+					const double x = ((double)me.x * pp.scale[0]) + pp.offset[0];
+					const double y = ((double)me.y * pp.scale[1]) + pp.offset[1];
+					const double z = ((double)me.z * pp.scale[2]) + pp.offset[2];
+					ga.axyz[3 * slot] = x;
+					ga.axyz[3 * slot + 1] = y;
+					ga.axyz[3 * slot + 2] = z;
+					ga.akey[slot] = lb.keys[co + t];
+					ga.apos[slot] = (int32_t)t;
+					int c[3];
+					double fr[3];
+					cell_of(g, x, y, z, c, fr);
+					if (!hash_push(hk, hh, ga.anext + co, nd.hash_cap, cell_key(c[0], c[1], c[2]), rank)) atomicAdd(&st->timeouts, 1ull);
+				}
+			}
+		}
+		__syncthreads();
+		if (tid == 0) {
+			R.cnt = cnt0 + (int32_t)total;
+			const long long clk5 = clock64();
+			atomicAdd(&st->cycles[0], (unsigned long long)(clk1 - clk0));
+			atomicAdd(&st->cycles[1], (unsigned long long)(clk2 - clk1));
+			atomicAdd(&st->cycles[2], (unsigned long long)(clk3 - clk2));
+			atomicAdd(&st->cycles[3], (unsigned long long)(clk4 - clk3));
+			atomicAdd(&st->cycles[4], (unsigned long long)(clk5 - clk4));
+		}
+		__syncthreads();
+	}
+}
+
+
+// Greedy acceptance from conflict lists for the smaller nodes, one warp per
+// node, 32 candidates per step. Conflicts with earlier steps come from
+// srank; inside a step they are a lane mask, resolved by ballot passes (a
+// lane decides once its earlier conflicting lanes have) or, when a lane's
+// old conflict sits at the edge of the 10,001-check window, in lane order.
+template <int MODE>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) greedy_list_warp_kernel(const LevelNode* __restrict__ nodes,
+                                                                              const int32_t* __restrict__ order, int num, PosParamsS pp,
+                                                                              LevelBuffers lb, GreedyArgs ga, ConflictLists cl,
+                                                                              int32_t* __restrict__ srank, SampleStats* st,
+                                                                              int* next_node) {
+	const int lane = threadIdx.x & 31;
+	const uint32_t lt = lanemask_lt();
+	while (true) {
+		int idx = 0;
+		if (lane == 0) idx = atomicAdd(next_node, 1);
+		idx = __shfl_sync(FULL, idx, 0);
+		if (idx >= num) break;
+		const LevelNode nd = nodes[order[idx]];
+		const int64_t n = nd.count, co = nd.cand_off;
+		uint64_t* hk = ga.hkeys + nd.hash_off;
+		int32_t* hh = ga.hheads + nd.hash_off;
+		CellGrid g;
+		g.min[0] = nd.min[0]; g.min[1] = nd.min[1]; g.min[2] = nd.min[2];
+		g.inv = 1.0 / (2.0 * nd.spacing * 1.000001);
+		if (MODE == 1) {
+			for (int64_t s = lane; s < nd.hash_cap; s += 32) { hk[s] = EMPTY_KEY; hh[s] = -1; }
+			__syncwarp();
+		}
+		int32_t cnt = 0;  // accepted so far
+		for (int64_t b0 = 0; b0 < n; b0 += 32) {
+			const int64_t t = b0 + lane;
+			const bool valid = t < n;
+			int4 me = make_int4(0, 0, 0, 0);
+			int32_t maxrank = -1;
+			uint32_t mask = 0;  // earlier lanes of this step that conflict
+			if (valid) {
+				me = lb.cq[co + t];
+				const int nl = cl.count[co + t];
+				const int4* lp = reinterpret_cast<const int4*>(cl.entries + (co + t) * (int64_t)kListCap);
+				int32_t ent[kListCap];
+#pragma unroll
+				for (int w = 0; w < kListCap / 4; w++) {
+					int4 v = make_int4(0, 0, 0, 0);
+					if (4 * w < nl) v = lp[w];
+					ent[4 * w] = v.x; ent[4 * w + 1] = v.y; ent[4 * w + 2] = v.z; ent[4 * w + 3] = v.w;
+				}
+				int32_t rk[kListCap];
+#pragma unroll
+				for (int e = 0; e < kListCap; e++) rk[e] = (e < nl && ent[e] < b0) ? srank[co + ent[e]] : -1;
+#pragma unroll
+				for (int e = 0; e < kListCap; e++) {
+					if (e < nl) {
+						if (ent[e] < b0) maxrank = rk[e] > maxrank ? rk[e] : maxrank;
+						else mask |= 1u << (ent[e] - b0);
+					}
+				}
+			}
+			int os = 0;
+			if (maxrank >= 0) {
+				if (MODE == 1) os = 1;
+				else if (maxrank >= cnt + lane - 10001) os = 1;  // conflicts whatever was accepted before it
+				else if (maxrank < cnt - 10001) os = 0;          // outside the window in any case
+				else os = 2;
+			}
+			const uint32_t validmask = __ballot_sync(FULL, valid);
+			uint32_t accmask = 0;
+			if (__ballot_sync(FULL, valid && os == 2) == 0) {
+				uint32_t undec = validmask & ~__ballot_sync(FULL, valid && os == 1);
+				for (int it = 0; it < 33 && undec; it++) {
+					const bool mine = (undec >> lane) & 1u;
+					const bool ready = mine && (mask & undec) == 0;
+					const bool a = ready && (mask & accmask) == 0;
+					accmask |= __ballot_sync(FULL, a);
+					undec &= ~__ballot_sync(FULL, ready);
+				}
+			} else {
+				for (int b = 0; b < 32; b++) {
+					if (!((validmask >> b) & 1u)) continue;
+					bool dec = false;
+					if (lane == b && os != 1) {
+						const int32_t m_i = cnt + __popc(accmask & lt);
+						const bool old_conflict = maxrank >= 0 && (MODE == 1 || maxrank >= m_i - 10001);
+						dec = !old_conflict && !(mask & accmask);
+					}
+					dec = __shfl_sync(FULL, dec, b);
+					if (dec) accmask |= 1u << b;
+				}
+			}
+			const bool acc = (accmask >> lane) & 1u;
+			if (valid) {
+				const int32_t rank = cnt + __popc(accmask & lt);
+				const int32_t local = me.w;
+				srank[co + t] = acc ? rank : -1;
+				lb.accepted[co + local] = acc ? 1 : 0;
+				if (acc) {
+					lb.acc_rank[co + local] = rank;
+					if (MODE == 1) {
+						const int64_t slot = co + rank;
+						const double x = ((double)me.x * pp.scale[0]) + pp.offset[0];
+						const double y = ((double)me.y * pp.scale[1]) + pp.offset[1];
+						const double z = ((double)me.z * pp.scale[2]) + pp.offset[2];
+						ga.axyz[3 * slot] = x;
+						ga.axyz[3 * slot + 1] = y;
+						ga.axyz[3 * slot + 2] = z;
+						ga.akey[slot] = lb.keys[co + t];
+						ga.apos[slot] = (int32_t)t;
+						int c[3];
+						double fr[3];
+						cell_of(g, x, y, z, c, fr);
+						if (!hash_push(hk, hh, ga.anext + co, nd.hash_cap, cell_key(c[0], c[1], c[2]), rank)) atomicAdd(&st->timeouts, 1ull);
+					}
+				}
+			}
+			cnt += __popc(accmask);
+		}
 	}
 }
 
@@ -822,36 +1263,55 @@ void launch_keys(const LevelNode* nodes, const int32_t* X, const int32_t* Y, con
 }
 
 
+void launch_cand_records(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, LevelBuffers& lb, DeviceMem& mem) {
+	if (lb.M == 0) return;
+	cand_records_kernel<<<(unsigned)ceil_div(lb.M, 256), 256, 0, mem.stream()>>>(nodes, X, Y, Z, lb);
+	PCG_LAUNCHED();
+}
+
+void greedy_arena_reserve(GreedyArena& a, int slots, DeviceMem& mem) {
+	if (slots <= a.slots) return;
+	if (a.cells) { mem.free(a.cells); mem.free(a.ovf); }
+	a.cells = mem.alloc<AccCell>((size_t)slots * kGridCells);
+	a.ovf = mem.alloc<int32_t>((size_t)slots * kGridCells);
+	PCG_CUDA(cudaMemsetAsync(a.cells, 0, (size_t)slots * kGridCells * sizeof(AccCell), mem.stream()));
+	PCG_CUDA(cudaMemsetAsync(a.ovf, 0xff, (size_t)slots * kGridCells * sizeof(int32_t), mem.stream()));
+	a.slots = slots;
+}
+
 void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int32_t* order, int K, const int32_t* X, const int32_t* Y,
                    const int32_t* Z, const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads,
                    double* acc_xyz, double* acc_key, int32_t* acc_next, int32_t* acc_pos, SampleStats* st, DeviceMem& mem,
-                   int node_begin, int node_end, int num_big) {
+                   GreedyArena* grid, int node_begin, int node_end, int num_big) {
 	if (node_end < 0) node_end = K;
-	if (node_end <= node_begin || lb.M == 0) return;
+	if (lb.M == 0) return;
 	GreedyArgs ga{hash_keys, hash_heads, acc_xyz, acc_key, acc_next, acc_pos};
 	cudaStream_t s = mem.stream();
+	if (node_end <= node_begin) return;
 	const int big_end = num_big < node_end ? num_big : node_end;
 	if (big_end > node_begin) {
 		size_t smem = sizeof(RoundShared);
-		// one dense acceptance grid per resident CTA; large levels go in batches
+		// one dense acceptance grid per resident CTA (kept empty between
+		// nodes); large levels go in batches
 		const int batch = sm_count() * 2;
 		const int nbig = big_end - node_begin;
 		const int slots = nbig < batch ? nbig : batch;
+		greedy_arena_reserve(*grid, slots, mem);
 		GridArena arena;
-		arena.cells = mem.alloc<AccCell>((size_t)slots * kGridCells);
-		arena.ovf = mem.alloc<int32_t>((size_t)slots * kGridCells);
+		arena.cells = static_cast<AccCell*>(grid->cells);
+		arena.ovf = grid->ovf;
 		arena.link = mem.alloc<int32_t>((size_t)lb.M);
+		arena.accq = mem.alloc<int4>((size_t)lb.M);
 		if (mode == 0) PCG_CUDA(cudaFuncSetAttribute(greedy_big_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 		else PCG_CUDA(cudaFuncSetAttribute(greedy_big_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 		for (int b0 = node_begin; b0 < big_end; b0 += slots) {
 			const int cnt = big_end - b0 < slots ? big_end - b0 : slots;
-			if (mode == 0) greedy_big_kernel<0><<<cnt, kBigThreads, smem, s>>>(nodes, order, b0, X, Y, Z, pp, lb, ga, arena, st);
-			else greedy_big_kernel<1><<<cnt, kBigThreads, smem, s>>>(nodes, order, b0, X, Y, Z, pp, lb, ga, arena, st);
+			if (mode == 0) greedy_big_kernel<0><<<cnt, kBigThreads, smem, s>>>(nodes, order, b0, pp, lb, ga, arena, st);
+			else greedy_big_kernel<1><<<cnt, kBigThreads, smem, s>>>(nodes, order, b0, pp, lb, ga, arena, st);
 			PCG_LAUNCHED();
 		}
-		mem.free(arena.cells);
-		mem.free(arena.ovf);
 		mem.free(arena.link);
+		mem.free(arena.accq);
 	}
 	const int small_begin = node_begin > num_big ? node_begin : num_big;
 	if (node_end > small_begin) {
@@ -868,6 +1328,65 @@ void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int3
 		PCG_LAUNCHED();
 		mem.free(counter);
 	}
+}
+
+void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int32_t>& cta_nodes, const std::vector<int32_t>& warp_nodes,
+                         const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads, double* acc_xyz,
+                         double* acc_key, int32_t* acc_next, int32_t* acc_pos, const ConflictLists& cl, SampleStats* st, DeviceMem& mem) {
+	if (lb.M == 0 || (cta_nodes.empty() && warp_nodes.empty())) return;
+	GreedyArgs ga{hash_keys, hash_heads, acc_xyz, acc_key, acc_next, acc_pos};
+	cudaStream_t s = mem.stream();
+	int32_t* srank = mem.alloc<int32_t>((size_t)lb.M);
+	int32_t* d_cta = cta_nodes.empty() ? nullptr : mem.alloc<int32_t>(cta_nodes.size());
+	int32_t* d_warp = warp_nodes.empty() ? nullptr : mem.alloc<int32_t>(warp_nodes.size());
+	int* counter = mem.alloc<int>(1);
+	if (d_cta) PCG_CUDA(cudaMemcpyAsync(d_cta, cta_nodes.data(), cta_nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+	if (d_warp) PCG_CUDA(cudaMemcpyAsync(d_warp, warp_nodes.data(), warp_nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+	PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), s));
+	// the two node sets are independent: the warp kernel runs beside the
+	// CTA kernel on a forked stream
+	cudaStream_t side = nullptr;
+	cudaEvent_t fork = nullptr, join = nullptr;
+	if (d_cta && d_warp) {
+		PCG_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+		PCG_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+		PCG_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+		PCG_CUDA(cudaEventRecord(fork, s));
+		PCG_CUDA(cudaStreamWaitEvent(side, fork, 0));
+	}
+	if (d_cta) {
+		const size_t smem = sizeof(ListRound);
+		const int nc = (int)cta_nodes.size();
+		if (mode == 0) {
+			PCG_CUDA(cudaFuncSetAttribute(greedy_list_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			greedy_list_kernel<0><<<nc, kBigThreads, smem, s>>>(nodes, d_cta, 0, pp, lb, ga, cl, srank, st);
+		} else {
+			PCG_CUDA(cudaFuncSetAttribute(greedy_list_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			greedy_list_kernel<1><<<nc, kBigThreads, smem, s>>>(nodes, d_cta, 0, pp, lb, ga, cl, srank, st);
+		}
+		PCG_LAUNCHED();
+	}
+	if (d_warp) {
+		cudaStream_t ws = side ? side : s;
+		const int nw = (int)warp_nodes.size();
+		int blocks = (int)ceil_div(nw, kWarpsPerBlock);
+		const int cap = sm_count() * 16;
+		if (blocks > cap) blocks = cap;
+		if (mode == 0) greedy_list_warp_kernel<0><<<blocks, kWarpsPerBlock * 32, 0, ws>>>(nodes, d_warp, nw, pp, lb, ga, cl, srank, st, counter);
+		else greedy_list_warp_kernel<1><<<blocks, kWarpsPerBlock * 32, 0, ws>>>(nodes, d_warp, nw, pp, lb, ga, cl, srank, st, counter);
+		PCG_LAUNCHED();
+	}
+	if (side) {
+		PCG_CUDA(cudaEventRecord(join, side));
+		PCG_CUDA(cudaStreamWaitEvent(s, join, 0));
+		cudaEventDestroy(fork);
+		cudaEventDestroy(join);
+		cudaStreamDestroy(side);
+	}
+	mem.free(srank);
+	if (d_cta) mem.free(d_cta);
+	if (d_warp) mem.free(d_warp);
+	mem.free(counter);
 }
 
 void launch_average_colors(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,

@@ -38,6 +38,7 @@ struct LevelBuffers {
 	int32_t* pos = nullptr;        // [M] local candidate index -> sorted position
 	uint8_t* accepted = nullptr;   // [M]
 	int32_t* acc_rank = nullptr;   // [M] acceptance rank for accepted candidates
+	int4* cq = nullptr;            // [M] sorted position -> (X, Y, Z, local index)
 };
 
 struct SortSeg {            // a std::sort segment [f, l) with its depth budget
@@ -54,7 +55,10 @@ struct SampleStats {
 	unsigned long long escalated;  // FP32 decisions re-made in FP64
 	unsigned long long heapsorts;  // introsort depth-limit fallbacks
 	unsigned long long timeouts;   // bounded loops that gave up
-	unsigned long long pad;
+	unsigned long long rounds;     // CTA greedy rounds
+	unsigned long long passes;     // parallel decision passes over all rounds
+	unsigned long long serial;     // rounds that needed the in-order decision warp
+	unsigned long long cycles[7];  // CTA greedy: SM cycles of thread 0 in phases A, B, C1, C2, D; cells read past 3 and 7 points
 };
 
 void launch_gather(const GatherItem* items, int num_items, LevelBuffers& lb, DeviceMem& mem);
@@ -70,6 +74,12 @@ void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, Level
 // key bits). Nodes whose keys are pairwise distinct end sorted in lb.keys,
 // lb.perm and lb.pos, which is std::sort's unique result for them; nodes with
 // equal keys are left as they were and flagged in tie[k] for the replay.
+// Stable sort of every node's (key, value) pairs by key bits [0, bits) into
+// (keys_out, vals_out), each node within its own range [cand_off,
+// cand_off + count). vals_in == nullptr means value = index in the node.
+// keys_in must not alias keys_out.
+void segmented_sort_pairs(const std::vector<LevelNode>& ln, int64_t M, const uint64_t* keys_in, const uint32_t* vals_in,
+                          uint64_t* keys_out, uint32_t* vals_out, int bits, DeviceMem& mem);
 void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, LevelBuffers& lb, DeviceMem& mem,
                          std::vector<uint8_t>& tie);
 // std::sort replayed on every segment [f, l) of key/val independently, each
@@ -78,11 +88,41 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 int sort_depth_budget(int64_t n);
 // lb.pos of the listed nodes from their sorted lb.perm
 void launch_node_pos(const LevelNode* nodes, const int32_t* node_list, int n, LevelBuffers& lb, DeviceMem& mem);
+// Earlier candidates of the same node that would reject a candidate if
+// accepted (within the spacing and, for poisson, not before the early-exit
+// bound), by sorted position; built for the nodes flagged in `use`.
+constexpr int kListCap = 32;
+constexpr uint8_t kListDense = 255;
+struct ConflictLists {
+	int32_t* entries = nullptr;     // [M * kListCap] node-local sorted positions
+	uint8_t* count = nullptr;       // [M] by sorted position: entries, or kListDense past kListCap
+	uint8_t* node_dense = nullptr;  // [K] some candidate has more than kListCap
+};
+void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<LevelNode>& ln, const std::vector<uint8_t>& use,
+                          const PosParamsS& pp, LevelBuffers& lb, ConflictLists& cl, std::vector<uint8_t>& dense, SampleStats* st,
+                          DeviceMem& mem);
+void free_conflict_lists(ConflictLists& cl, DeviceMem& mem);
+// sorted candidate records lb.cq from lb.perm
+void launch_cand_records(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, LevelBuffers& lb, DeviceMem& mem);
+// Acceptance grids of the CTA-per-node greedy, one per resident CTA. They
+// are cleared once when allocated and left empty by every node, so a job
+// keeps one set for all of its levels.
+struct GreedyArena {
+	void* cells = nullptr;
+	int32_t* ovf = nullptr;
+	int slots = 0;
+};
+void greedy_arena_reserve(GreedyArena& a, int slots, DeviceMem& mem);
 // mode 0 = poisson (early exit + 10,001-check window), 1 = poisson_average (pure greedy)
 void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int32_t* order, int K, const int32_t* X, const int32_t* Y,
                    const int32_t* Z, const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads,
                    double* acc_xyz, double* acc_key, int32_t* acc_next, int32_t* acc_pos, SampleStats* st, DeviceMem& mem,
-                   int node_begin = 0, int node_end = -1, int num_big = 0);
+                   GreedyArena* grid, int node_begin = 0, int node_end = -1, int num_big = 0);
+// acceptance from conflict lists: cta_nodes get a CTA each (largest first),
+// warp_nodes a warp each
+void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int32_t>& cta_nodes, const std::vector<int32_t>& warp_nodes,
+                         const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads, double* acc_xyz,
+                         double* acc_key, int32_t* acc_next, int32_t* acc_pos, const ConflictLists& cl, SampleStats* st, DeviceMem& mem);
 // poisson_average colour sums: new packed colour per accepted candidate
 void launch_average_colors(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
                            LevelBuffers& lb, const uint64_t* hash_keys, const int32_t* hash_heads, const double* acc_xyz,

@@ -176,12 +176,10 @@ __global__ void seg_finish_kernel(const LevelNode* __restrict__ nodes, const uin
 
 }  // namespace
 
-void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, LevelBuffers& lb, DeviceMem& mem,
-                         std::vector<uint8_t>& tie) {
+void segmented_sort_pairs(const std::vector<LevelNode>& ln, int64_t M, const uint64_t* keys_in, const uint32_t* vals_in,
+                          uint64_t* keys_out, uint32_t* vals_out, int bits, DeviceMem& mem) {
 	const int K = (int)ln.size();
-	const int64_t M = lb.M;
-	tie.assign(K, 0);
-	if (M == 0 || K == 0) return;
+	if (M == 0 || K == 0 || bits <= 0) return;
 	cudaStream_t s = mem.stream();
 	std::vector<SegTile> tiles;
 	int64_t mat = 0, before = 0;
@@ -204,20 +202,23 @@ void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>&
 		before += n;
 	}
 	const int num_tiles = (int)tiles.size();
+	const int passes = (bits + 7) / 8;
 	SegTile* d_tiles = mem.alloc<SegTile>(tiles.size());
 	PCG_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(SegTile), cudaMemcpyHostToDevice, s));
-	uint64_t* kb[2] = {mem.alloc<uint64_t>(M), mem.alloc<uint64_t>(M)};
-	uint32_t* vb[2] = {mem.alloc<uint32_t>(M), mem.alloc<uint32_t>(M)};
+	// the last pass writes (keys_out, vals_out)
+	uint64_t* kb[2] = {keys_out, passes > 1 ? mem.alloc<uint64_t>(M) : nullptr};
+	uint32_t* vb[2] = {vals_out, passes > 1 ? mem.alloc<uint32_t>(M) : nullptr};
 	uint32_t* counts = mem.alloc<uint32_t>(mat);
 	uint32_t* offsets = mem.alloc<uint32_t>(mat);
 	static_assert(sizeof(SegShared) <= 227 * 1024, "tile does not fit shared memory");
 	PCG_CUDA(cudaFuncSetAttribute(seg_downsweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SegShared)));
-	const uint64_t* kin = reinterpret_cast<const uint64_t*>(lb.keys);
-	const uint32_t* vin = nullptr;
-	for (int pass = 0; pass < kKeyPasses; pass++) {
+	const uint64_t* kin = keys_in;
+	const uint32_t* vin = vals_in;
+	for (int pass = 0; pass < passes; pass++) {
 		const int shift = 8 * pass;
-		uint64_t* kout = kb[pass & 1];
-		uint32_t* vout = vb[pass & 1];
+		const int dst = (passes - 1 - pass) & 1;
+		uint64_t* kout = kb[dst];
+		uint32_t* vout = vb[dst];
 		seg_upsweep<<<num_tiles, kSegThreads, 0, s>>>(d_tiles, kin, shift, counts);
 		PCG_LAUNCHED();
 		exclusive_scan_u32(counts, offsets, mat, false, mem);
@@ -226,23 +227,35 @@ void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>&
 		kin = kout;
 		vin = vout;
 	}
+	mem.free(counts);
+	mem.free(offsets);
+	if (kb[1]) mem.free(kb[1]);
+	if (vb[1]) mem.free(vb[1]);
+	mem.free(d_tiles);
+}
+
+void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, LevelBuffers& lb, DeviceMem& mem,
+                         std::vector<uint8_t>& tie) {
+	const int K = (int)ln.size();
+	const int64_t M = lb.M;
+	tie.assign(K, 0);
+	if (M == 0 || K == 0) return;
+	cudaStream_t s = mem.stream();
+	uint64_t* sk = mem.alloc<uint64_t>(M);
+	uint32_t* sv = mem.alloc<uint32_t>(M);
+	segmented_sort_pairs(ln, M, reinterpret_cast<const uint64_t*>(lb.keys), nullptr, sk, sv, 64, mem);
 	uint8_t* d_tie = mem.alloc<uint8_t>(K);
 	PCG_CUDA(cudaMemsetAsync(d_tie, 0, K, s));
 	const unsigned blocks = (unsigned)ceil_div(M, 256);
-	seg_ties_kernel<<<blocks, 256, 0, s>>>(lb.node_of, kin, M, d_tie);
+	seg_ties_kernel<<<blocks, 256, 0, s>>>(lb.node_of, sk, M, d_tie);
 	PCG_LAUNCHED();
-	seg_finish_kernel<<<blocks, 256, 0, s>>>(d_nodes, d_tie, kin, vin, lb);
+	seg_finish_kernel<<<blocks, 256, 0, s>>>(d_nodes, d_tie, sk, sv, lb);
 	PCG_LAUNCHED();
 	PCG_CUDA(cudaMemcpyAsync(tie.data(), d_tie, K, cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));
 	mem.free(d_tie);
-	mem.free(counts);
-	mem.free(offsets);
-	mem.free(kb[0]);
-	mem.free(kb[1]);
-	mem.free(vb[0]);
-	mem.free(vb[1]);
-	mem.free(d_tiles);
+	mem.free(sk);
+	mem.free(sv);
 }
 
 }  // namespace pcg
