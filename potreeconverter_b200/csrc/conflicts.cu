@@ -37,6 +37,11 @@ namespace {
 constexpr uint64_t kEmptyRun = ~0ull;
 constexpr int kCellsPerAxis = 128;  // node box = 128 spacings
 
+struct alignas(16) RunSlot {  // run table entry, one 16-byte load per probe
+	uint64_t key;             // node << 32 | cell, kEmptyRun when free
+	int32_t start, count;     // first record in the node, records
+};
+
 __device__ __forceinline__ uint64_t run_hash(uint64_t k, int64_t cap) {
 	return ((k * 0x9E3779B97F4A7C15ull) >> 20) & (uint64_t)(cap - 1);
 }
@@ -76,6 +81,22 @@ __global__ void conf_gather_kernel(const LevelNode* __restrict__ nodes, LevelBuf
 	crec[j] = r;
 }
 
+// occupancy bitmap of a node's cells: 128 bits per (z, y) row, 4 words
+constexpr int kRowWords = kCellsPerAxis / 32;
+constexpr int64_t kBitmapWords = (int64_t)kCellsPerAxis * kCellsPerAxis * kRowWords;
+constexpr int64_t kBitmapMinCandidates = 2048;  // smaller nodes probe the hash for every cell
+
+__global__ void conf_bitmap_kernel(const int32_t* __restrict__ node_of, const uint64_t* __restrict__ ck, int64_t M,
+                                   const int64_t* __restrict__ bm_off, uint32_t* __restrict__ bm) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= M) return;
+	const int64_t off = bm_off[node_of[j]];
+	if (off < 0) return;
+	const uint64_t c = ck[j];
+	const int cx = (int)(c % kCellsPerAxis);
+	atomicOr(&bm[off + (int64_t)(c / kCellsPerAxis) * kRowWords + (cx >> 5)], 1u << (cx & 31));
+}
+
 __device__ __forceinline__ bool run_head(const LevelNode* nodes, const int32_t* node_of, const uint64_t* ck, int64_t j) {
 	return j == nodes[node_of[j]].cand_off || ck[j] != ck[j - 1];
 }
@@ -90,8 +111,7 @@ __global__ void conf_count_runs_kernel(const LevelNode* __restrict__ nodes, cons
 
 // run table: key (node << 32 | cell) -> (first record, count)
 __global__ void conf_insert_runs_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ node_of, const uint64_t* __restrict__ ck,
-                                        int64_t M, uint64_t* __restrict__ hkeys, int2* __restrict__ hvals, int64_t cap,
-                                        SampleStats* st) {
+                                        int64_t M, RunSlot* __restrict__ table, int64_t cap, SampleStats* st) {
 	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= M || !run_head(nodes, node_of, ck, j)) return;
 	const int32_t node = node_of[j];
@@ -101,9 +121,10 @@ __global__ void conf_insert_runs_kernel(const LevelNode* __restrict__ nodes, con
 	const uint64_t key = ((uint64_t)(uint32_t)node << 32) | ck[j];
 	uint64_t s = run_hash(key, cap);
 	for (int64_t probe = 0; probe < cap; probe++) {
-		const unsigned long long prev = atomicCAS((unsigned long long*)&hkeys[s], (unsigned long long)kEmptyRun, (unsigned long long)key);
+		const unsigned long long prev = atomicCAS((unsigned long long*)&table[s].key, (unsigned long long)kEmptyRun, (unsigned long long)key);
 		if (prev == kEmptyRun) {
-			hvals[s] = make_int2((int32_t)(j - nodes[node].cand_off), (int32_t)(e - j));
+			table[s].start = (int32_t)(j - nodes[node].cand_off);
+			table[s].count = (int32_t)(e - j);
 			return;
 		}
 		s = (s + 1) & (uint64_t)(cap - 1);
@@ -111,12 +132,12 @@ __global__ void conf_insert_runs_kernel(const LevelNode* __restrict__ nodes, con
 	atomicAdd(&st->timeouts, 1ull);
 }
 
-__device__ __forceinline__ int2 find_run(const uint64_t* hkeys, const int2* hvals, int64_t cap, uint64_t key) {
+__device__ __forceinline__ int2 find_run(const RunSlot* table, int64_t cap, uint64_t key) {
 	uint64_t s = run_hash(key, cap);
 	for (int64_t probe = 0; probe < cap; probe++) {
-		const uint64_t k = hkeys[s];
-		if (k == key) return hvals[s];
-		if (k == kEmptyRun) break;
+		const RunSlot r = table[s];
+		if (r.key == key) return make_int2(r.start, r.count);
+		if (r.key == kEmptyRun) break;
 		s = (s + 1) & (uint64_t)(cap - 1);
 	}
 	return make_int2(0, 0);
@@ -125,7 +146,7 @@ __device__ __forceinline__ int2 find_run(const uint64_t* hkeys, const int2* hval
 template <int MODE>
 __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, PosParamsS pp,
                                                         LevelBuffers lb, const uint64_t* __restrict__ ck, const int4* __restrict__ crec,
-                                                        const uint64_t* __restrict__ hkeys, const int2* __restrict__ hvals, int64_t cap,
+                                                        const RunSlot* __restrict__ table, int64_t cap, const int64_t* __restrict__ bm_off, const uint32_t* __restrict__ bm,
                                                         ConflictLists cl) {
 	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= lb.M) return;
@@ -155,17 +176,29 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 	const int cx = (int)(c % kCellsPerAxis), cy = (int)((c / kCellsPerAxis) % kCellsPerAxis), cz = (int)(c / (kCellsPerAxis * kCellsPerAxis));
 	int32_t* out = cl.entries + (co + t) * (int64_t)kListCap;
 	int n = 0;
+	const int64_t boff = bm_off[node];
 	for (int dz = -1; dz <= 1; dz++) {
 		const int qz = cz + dz;
 		if (qz < 0 || qz >= kCellsPerAxis) continue;
 		for (int dy = -1; dy <= 1; dy++) {
 			const int qy = cy + dy;
 			if (qy < 0 || qy >= kCellsPerAxis) continue;
+			// occupied cells among x = cx-1 .. cx+1 of this row
+			uint32_t occ = 7u;
+			if (boff >= 0) {
+				const uint32_t* row = bm + boff + ((int64_t)qz * kCellsPerAxis + qy) * kRowWords;
+				const int x0 = cx - 1;
+				occ = 0;
+				for (int b = 0; b < 3; b++) {
+					const int qx = x0 + b;
+					if (qx >= 0 && qx < kCellsPerAxis && ((row[qx >> 5] >> (qx & 31)) & 1u)) occ |= 1u << b;
+				}
+			}
 			for (int dx = -1; dx <= 1; dx++) {
 				const int qx = cx + dx;
-				if (qx < 0 || qx >= kCellsPerAxis) continue;
+				if (qx < 0 || qx >= kCellsPerAxis || !((occ >> (dx + 1)) & 1u)) continue;
 				const uint64_t cell = ((uint64_t)qz * kCellsPerAxis + (uint64_t)qy) * kCellsPerAxis + (uint64_t)qx;
-				const int2 run = find_run(hkeys, hvals, cap, ((uint64_t)(uint32_t)node << 32) | cell);
+				const int2 run = find_run(table, cap, ((uint64_t)(uint32_t)node << 32) | cell);
 				const int4* rp = crec + co + run.x;
 				for (int i = 0; i < run.y; i++) {
 					const int4 q = rp[i];
@@ -221,25 +254,38 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	mem.free(d_runs);
 	int64_t cap = 64;
 	while (cap < 2 * (int64_t)runs) cap <<= 1;
-	uint64_t* hkeys = mem.alloc<uint64_t>(cap);
-	int2* hvals = mem.alloc<int2>(cap);
-	PCG_CUDA(cudaMemsetAsync(hkeys, 0xff, cap * sizeof(uint64_t), s));
-	conf_insert_runs_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb.node_of, ck, M, hkeys, hvals, cap, st);
+	RunSlot* table = mem.alloc<RunSlot>(cap);
+	PCG_CUDA(cudaMemsetAsync(table, 0xff, cap * sizeof(RunSlot), s));
+	conf_insert_runs_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb.node_of, ck, M, table, cap, st);
 	PCG_LAUNCHED();
+	// occupancy bitmaps of the larger nodes
+	std::vector<int64_t> bm_off(K, -1);
+	int64_t bm_words = 0;
+	for (int k = 0; k < K; k++)
+		if (use[k] && ln[k].count >= kBitmapMinCandidates) { bm_off[k] = bm_words; bm_words += kBitmapWords; }
+	int64_t* d_bm_off = mem.alloc<int64_t>(K);
+	PCG_CUDA(cudaMemcpyAsync(d_bm_off, bm_off.data(), K * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+	uint32_t* bm = mem.alloc<uint32_t>(bm_words > 0 ? bm_words : 1);
+	if (bm_words > 0) {
+		PCG_CUDA(cudaMemsetAsync(bm, 0, bm_words * sizeof(uint32_t), s));
+		conf_bitmap_kernel<<<blocks, 256, 0, s>>>(lb.node_of, ck, M, d_bm_off, bm);
+		PCG_LAUNCHED();
+	}
 	cl.entries = mem.alloc<int32_t>((size_t)M * kListCap);
 	cl.count = mem.alloc<uint8_t>(M);
 	cl.node_dense = mem.alloc<uint8_t>(K);
 	PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
 	uint8_t* d_use = mem.alloc<uint8_t>(K);
 	PCG_CUDA(cudaMemcpyAsync(d_use, use.data(), K, cudaMemcpyHostToDevice, s));
-	if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, hkeys, hvals, cap, cl);
-	else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, hkeys, hvals, cap, cl);
+	if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, table, cap, d_bm_off, bm, cl);
+	else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, table, cap, d_bm_off, bm, cl);
 	PCG_LAUNCHED();
 	PCG_CUDA(cudaMemcpyAsync(dense.data(), cl.node_dense, K, cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));
 	mem.free(d_use);
-	mem.free(hkeys);
-	mem.free(hvals);
+	mem.free(d_bm_off);
+	mem.free(bm);
+	mem.free(table);
 	mem.free(crec);
 	mem.free(ck);
 }

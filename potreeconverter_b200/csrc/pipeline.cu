@@ -230,6 +230,7 @@ struct Converter {
 	uint32_t seed = 1592614637u;
 	int form = PCG_FORM_BATCHED;
 	PinnedPool* host_buffers = &g_pinned;
+	std::shared_ptr<DeviceArena> arena;  // device memory kept between jobs on `stream`
 
 	void run(const pcg_job& job, JobResult& res) {
 		auto t0 = Clock::now();
@@ -247,7 +248,7 @@ struct Converter {
 		if (s.total_points >= (int64_t(1) << 31)) throw PcgError(PCG_BAD_INPUT, "more than 2^31 points per job");
 		const int64_t N = s.total_points;
 		const int method = job.method;
-		DeviceMem mem(stream);
+		DeviceMem mem(stream, arena.get());
 		res.stats.num_points = N;
 
 		// ---------------------------------------------------------- input
@@ -603,6 +604,8 @@ struct Converter {
 	void sample_level(Tree& tree, const std::vector<int>& level_nodes, int method, double base_spacing, const PosParamsS& pps,
 	                  const ChunkingOut& co, const uint8_t* d_recs, const DecodeParams& p, SampleStats* d_st, GreedyArena& grid_arena,
 	                  DeviceMem& mem, JobResult& res) {
+		const auto t_level = Clock::now();
+		const double alloc0 = mem.alloc_ms();
 		int sms = 148;
 		PCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
 		(void)d_recs;
@@ -681,6 +684,8 @@ struct Converter {
 			const int64_t big_min = K < 2 * sms ? kSmallLevelCtaCandidates : kBigNodeCandidates;
 			while (num_big < K && ln[order[num_big]].count >= big_min) num_big++;
 			int list_nodes = 0;
+			cudaEvent_t ev_lists;
+			PCG_CUDA(cudaEventCreate(&ev_lists));
 			cudaEvent_t ev[3];
 			for (auto& e : ev) PCG_CUDA(cudaEventCreate(&e));
 			PCG_CUDA(cudaEventRecord(ev[0], s));
@@ -720,6 +725,7 @@ struct Converter {
 				{
 					std::vector<uint8_t> use(K, 1), dense;
 					build_conflict_lists(mode, d_nodes, ln, use, pps, lb, cl, dense, d_st, mem);
+					PCG_CUDA(cudaEventRecord(ev_lists, s));
 					for (int i = 0; i < num_big; i++) (dense[order[i]] ? order2 : cta_list).push_back(order[i]);
 					const int num_grid = (int)order2.size();
 					for (int i = num_big; i < K; i++) (dense[order[i]] ? order2 : warp_list).push_back(order[i]);
@@ -741,6 +747,9 @@ struct Converter {
 			PCG_CUDA(cudaEventElapsedTime(&t_greedy, ev[1], ev[2]));
 			res.stats.ms_sort += t_sort;
 			res.stats.ms_greedy += t_greedy;
+			float t_lists = 0;
+			if (form != PCG_FORM_PLAIN) PCG_CUDA(cudaEventElapsedTime(&t_lists, ev[1], ev_lists));
+			cudaEventDestroy(ev_lists);
 			if (trace_levels()) {
 				int64_t mx = 0;
 				for (auto& l : ln) mx = std::max<int64_t>(mx, l.count);
@@ -748,17 +757,14 @@ struct Converter {
 				SampleStats now = download(d_st, 1, s)[0];
 				if (now.rounds < prev.rounds) prev = SampleStats{};
 				fprintf(stderr,
-				        "[pcg] level %d: nodes %d (cta %d, lists %d), candidates %lld, largest %lld, sort %.3f ms, greedy %.3f ms, "
-				        "cta rounds %llu, passes %llu, serial rounds %llu, kcycles/round A %.1f B %.1f C1 %.1f C2 %.1f D %.1f, "
-				        "cells>3 %llu, overflow points %llu\n",
-				        K ? ln[0].level : -1, K, num_big, list_nodes, (long long)M, (long long)mx, t_sort, t_greedy, now.rounds - prev.rounds,
-				        now.passes - prev.passes, now.serial - prev.serial,
+				        "[pcg] level %d: nodes %d (cta %d, lists %d), candidates %lld, largest %lld, sort %.3f ms, greedy %.3f ms (lists %.3f), "
+				        "host %.3f ms (alloc %.3f), cta rounds %llu, passes %llu, serial rounds %llu, kcycles/round A %.1f C1 %.1f C2 %.1f D %.1f\n",
+				        K ? ln[0].level : -1, K, num_big, list_nodes, (long long)M, (long long)mx, t_sort, t_greedy, t_lists, ms_since(t_level), mem.alloc_ms() - alloc0,
+				        now.rounds - prev.rounds, now.passes - prev.passes, now.serial - prev.serial,
 				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(0),
-				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(1),
 				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(2),
 				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(3),
-				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(4),
-				        now.cycles[5] - prev.cycles[5], now.cycles[6] - prev.cycles[6]);
+				        [&](int i) { return (double)(now.cycles[i] - prev.cycles[i]) / 1e3 / std::max(1ull, now.rounds - prev.rounds); }(4));
 				prev = now;
 			}
 			for (auto& e : ev) cudaEventDestroy(e);
@@ -1009,6 +1015,9 @@ size_t estimate_footprint(const pcg_job& job) {
 void worker_main(pcg_ctx* ctx, int wi) {
 	pcg::Converter conv = ctx->conv;
 	conv.stream = ctx->worker_streams[wi];
+	// jobs of a worker share its arena; it is emptied after each job so the
+	// memory admission of the queue sees what the jobs hold
+	conv.arena = std::make_shared<pcg::DeviceArena>(conv.stream);
 	while (true) {
 		std::shared_ptr<pcg_ctx::Job> job;
 		{
@@ -1040,6 +1049,7 @@ void worker_main(pcg_ctx* ctx, int wi) {
 		} catch (const std::exception& e) {
 			st = PCG_INTERNAL; err = e.what();
 		}
+		conv.arena->release_all();
 		{
 			std::lock_guard<std::mutex> lk(ctx->qmtx);
 			job->status = st;
@@ -1094,6 +1104,7 @@ pcg_status pcg_create(pcg_ctx** out, const pcg_opts* opts) {
 		PCG_CUDA(cudaDeviceGetDefaultMemPool(&pool, ctx->conv.device));
 		uint64_t threshold = UINT64_MAX;
 		PCG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+		ctx->conv.arena = std::make_shared<pcg::DeviceArena>(ctx->conv.stream);
 	});
 	if (st != PCG_OK) {
 		fprintf(stderr, "pcg_create: %s\n", ctx->last_error.c_str());
@@ -1116,6 +1127,7 @@ void pcg_destroy(pcg_ctx* ctx) {
 		if (kv.second->result.octree && !pcg::g_pinned.give(kv.second->result.octree)) cudaFreeHost(kv.second->result.octree);
 	cudaSetDevice(ctx->conv.device);
 	for (auto s : ctx->worker_streams) cudaStreamDestroy(s);
+	ctx->conv.arena.reset();
 	if (ctx->conv.stream) {
 		cudaStreamSynchronize(ctx->conv.stream);
 		if (ctx->own_stream) cudaStreamDestroy(ctx->conv.stream);
@@ -1228,7 +1240,7 @@ pcg_status pcg_kernel_sort_keys(pcg_ctx* ctx, const double* keys, int64_t n, int
 	return guarded(ctx, [&] {
 		if (n == 0) return;
 		PCG_CUDA(cudaSetDevice(ctx->conv.device));
-		pcg::DeviceMem mem(ctx->conv.stream);
+		pcg::DeviceMem mem(ctx->conv.stream, ctx->conv.arena.get());
 		double* dk = mem.alloc<double>(n);
 		int32_t* dv = mem.alloc<int32_t>(n);
 		pcg::SampleStats* st = mem.alloc<pcg::SampleStats>(1);
@@ -1249,7 +1261,7 @@ pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* p
 	return guarded(ctx, [&] {
 		if (n == 0) return;
 		PCG_CUDA(cudaSetDevice(ctx->conv.device));
-		pcg::DeviceMem mem(ctx->conv.stream);
+		pcg::DeviceMem mem(ctx->conv.stream, ctx->conv.arena.get());
 		int32_t* dp = mem.alloc<int32_t>(n);
 		pcg::launch_shuffle_single(n, seed, dp, mem);
 		PCG_CUDA(cudaMemcpyAsync(perm_out, dp, n * sizeof(int32_t), cudaMemcpyDeviceToHost, mem.stream()));

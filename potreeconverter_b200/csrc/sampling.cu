@@ -919,6 +919,16 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 }
 
 
+// Pulls the list row, list length and record of sorted position u into L2
+// ahead of the round that reads them (they were written by an earlier kernel
+// and usually sit in DRAM).
+__device__ __forceinline__ void prefetch_list(const ConflictLists& cl, const LevelBuffers& lb, int64_t co, int64_t u) {
+	const int32_t* row = cl.entries + (co + u) * (int64_t)kListCap;
+	asm volatile("prefetch.global.L2 [%0];" ::"l"(row));
+	asm volatile("prefetch.global.L2 [%0];" ::"l"(cl.count + co + u));
+	asm volatile("prefetch.global.L2 [%0];" ::"l"(lb.cq + co + u));
+}
+
 // Greedy acceptance for a large node from its conflict lists (conflicts.cu),
 // one CTA, 512 candidates per round. A candidate's list names every earlier
 // candidate that would reject it if accepted, so the round needs no spatial
@@ -963,6 +973,7 @@ __global__ void __launch_bounds__(kBigThreads) greedy_list_kernel(const LevelNod
 		const int32_t cnt0 = R.cnt;
 		// ---- A: the candidate's list
 		long long clk0 = clock64();
+		if (t + kRound < n) prefetch_list(cl, lb, co, t + kRound);
 		int32_t maxrank = -1, local = 0;
 		int nc = 0;
 		int4 me = make_int4(0, 0, 0, 0);
@@ -1160,6 +1171,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) greedy_list_warp_kernel(c
 		for (int64_t b0 = 0; b0 < n; b0 += 32) {
 			const int64_t t = b0 + lane;
 			const bool valid = t < n;
+			if (t + 64 < n) prefetch_list(cl, lb, co, t + 64);
 			int4 me = make_int4(0, 0, 0, 0);
 			int32_t maxrank = -1;
 			uint32_t mask = 0;  // earlier lanes of this step that conflict
