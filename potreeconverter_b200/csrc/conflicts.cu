@@ -238,7 +238,7 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	PCG_LAUNCHED();
 	uint64_t* ck = mem.alloc<uint64_t>(M);
 	uint32_t* cv = mem.alloc<uint32_t>(M);
-	segmented_sort_pairs(ln, M, keys, nullptr, ck, cv, 21, mem);
+	segmented_sort_pairs(ln, M, keys, nullptr, ck, cv, 0, 21, mem);
 	mem.free(keys);
 	int4* crec = mem.alloc<int4>(M);
 	conf_gather_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb, cv, crec);

@@ -665,9 +665,13 @@ __global__ void blk_insertion_kernel(const int32_t* __restrict__ blk, int n, dou
 	if (b < n) insertion_blocks(key, val, blk + 2 * (int64_t)b, 1, 0, 1);
 }
 
-__global__ void node_pos_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ list, LevelBuffers lb) {
-	const LevelNode nd = nodes[list[blockIdx.x]];
-	for (int64_t t = threadIdx.x; t < nd.count; t += blockDim.x) lb.pos[nd.cand_off + lb.perm[nd.cand_off + t]] = (int32_t)t;
+__global__ void node_pos_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ pick, LevelBuffers lb) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const int32_t n = lb.node_of[j];
+	if (!pick[n]) return;
+	const int64_t co = nodes[n].cand_off;
+	lb.pos[co + lb.perm[j]] = (int32_t)(j - co);
 }
 
 int host_introsort_depth(int64_t n) {
@@ -844,10 +848,13 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 	mem.free(sc.blk);
 }
 
-void launch_node_pos(const LevelNode* nodes, const int32_t* node_list, int n, LevelBuffers& lb, DeviceMem& mem) {
-	if (n <= 0) return;
-	node_pos_kernel<<<n, 256, 0, mem.stream()>>>(nodes, node_list, lb);
+void launch_node_pos(const LevelNode* nodes, const std::vector<uint8_t>& pick, LevelBuffers& lb, DeviceMem& mem) {
+	if (lb.M == 0 || pick.empty()) return;
+	uint8_t* d_pick = mem.alloc<uint8_t>(pick.size());
+	PCG_CUDA(cudaMemcpyAsync(d_pick, pick.data(), pick.size(), cudaMemcpyHostToDevice, mem.stream()));
+	node_pos_kernel<<<(unsigned)ceil_div(lb.M, 256), 256, 0, mem.stream()>>>(nodes, d_pick, lb);
 	PCG_LAUNCHED();
+	mem.free(d_pick);
 }
 
 int sort_depth_budget(int64_t n) { return host_introsort_depth(n); }

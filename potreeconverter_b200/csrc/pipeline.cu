@@ -671,6 +671,7 @@ struct Converter {
 			lb.pos = mem.alloc<int32_t>(M);
 			lb.acc_rank = mem.alloc<int32_t>(M);
 			lb.cq = mem.alloc<int4>(M);
+			lb.rec = mem.alloc<int4>(M);
 			launch_keys(d_nodes, co.X, co.Y, co.Z, pps, lb, mem);
 			double* axyz = mem.alloc<double>(3 * M);
 			double* akey = mem.alloc<double>(M);
@@ -712,9 +713,7 @@ struct Converter {
 				res.stats.replayed_nodes += (int64_t)tie_nodes.size();
 				if (!tie_nodes.empty()) {
 					replay_segments(lb.keys, lb.perm, M, tie_segs, d_st, mem);
-					int32_t* d_tie_nodes = upload(tie_nodes, mem);
-					launch_node_pos(d_nodes, d_tie_nodes, (int)tie_nodes.size(), lb, mem);
-					mem.free(d_tie_nodes);
+					launch_node_pos(d_nodes, tie, lb, mem);
 				}
 				launch_cand_records(d_nodes, co.X, co.Y, co.Z, lb, mem);
 				PCG_CUDA(cudaEventRecord(ev[1], s));
@@ -774,7 +773,7 @@ struct Converter {
 				mem.free(sums);
 			}
 			mem.free(axyz); mem.free(akey); mem.free(anext); mem.free(apos);
-			mem.free(lb.keys); mem.free(lb.perm); mem.free(lb.pos); mem.free(lb.acc_rank); mem.free(lb.cq);
+			mem.free(lb.keys); mem.free(lb.perm); mem.free(lb.pos); mem.free(lb.acc_rank); mem.free(lb.cq); mem.free(lb.rec);
 		}
 		mem.free(hkeys);
 		mem.free(hvals);

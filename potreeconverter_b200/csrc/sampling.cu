@@ -72,10 +72,15 @@ __global__ void keys_kernel(const LevelNode* __restrict__ nodes, const int32_t* 
 	int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= lb.M) return;
 	const LevelNode& nd = nodes[lb.node_of[j]];
-	double x, y, z;
-	point_xyz(X, Y, Z, pp, lb.ids[j], x, y, z);
+	const uint32_t id = lb.ids[j];
+	const int4 r = make_int4(X[id], Y[id], Z[id], 0);
+	// (xyz * scale) + offset, sampler_poisson.h:99-101
+	const double x = ((double)r.x * pp.scale[0]) + pp.offset[0];
+	const double y = ((double)r.y * pp.scale[1]) + pp.offset[1];
+	const double z = ((double)r.z * pp.scale[2]) + pp.offset[2];
 	lb.keys[j] = center_key(nd, x, y, z);
 	lb.perm[j] = (int32_t)(j - nd.cand_off);
+	lb.rec[j] = r;
 }
 
 // sorted candidate records: (X, Y, Z, local index) at each sorted position
@@ -85,8 +90,9 @@ __global__ void cand_records_kernel(const LevelNode* __restrict__ nodes, const i
 	if (j >= lb.M) return;
 	const int64_t off = nodes[lb.node_of[j]].cand_off;
 	const int32_t local = lb.perm[j];
-	const uint32_t id = lb.ids[off + local];
-	lb.cq[j] = make_int4(X[id], Y[id], Z[id], local);
+	int4 r = lb.rec[off + local];
+	r.w = local;
+	lb.cq[j] = r;
 }
 
 // --------------------------------------------------------------- hashing

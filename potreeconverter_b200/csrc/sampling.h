@@ -39,6 +39,7 @@ struct LevelBuffers {
 	uint8_t* accepted = nullptr;   // [M]
 	int32_t* acc_rank = nullptr;   // [M] acceptance rank for accepted candidates
 	int4* cq = nullptr;            // [M] sorted position -> (X, Y, Z, local index)
+	int4* rec = nullptr;           // [M] candidate (gather order) -> (X, Y, Z, -)
 };
 
 struct SortSeg {            // a std::sort segment [f, l) with its depth budget
@@ -74,20 +75,20 @@ void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, Level
 // key bits). Nodes whose keys are pairwise distinct end sorted in lb.keys,
 // lb.perm and lb.pos, which is std::sort's unique result for them; nodes with
 // equal keys are left as they were and flagged in tie[k] for the replay.
-// Stable sort of every node's (key, value) pairs by key bits [0, bits) into
+// Stable sort of every node's (key, value) pairs by key bits [begin_bit, end_bit) into
 // (keys_out, vals_out), each node within its own range [cand_off,
 // cand_off + count). vals_in == nullptr means value = index in the node.
 // keys_in must not alias keys_out.
 void segmented_sort_pairs(const std::vector<LevelNode>& ln, int64_t M, const uint64_t* keys_in, const uint32_t* vals_in,
-                          uint64_t* keys_out, uint32_t* vals_out, int bits, DeviceMem& mem);
+                          uint64_t* keys_out, uint32_t* vals_out, int begin_bit, int end_bit, DeviceMem& mem);
 void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, LevelBuffers& lb, DeviceMem& mem,
                          std::vector<uint8_t>& tie);
 // std::sort replayed on every segment [f, l) of key/val independently, each
 // with depth budget d (2 * floor(log2(l - f)) for a whole node).
 void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<SortSeg>& segs, SampleStats* st, DeviceMem& mem);
 int sort_depth_budget(int64_t n);
-// lb.pos of the listed nodes from their sorted lb.perm
-void launch_node_pos(const LevelNode* nodes, const int32_t* node_list, int n, LevelBuffers& lb, DeviceMem& mem);
+// lb.pos of the nodes k with pick[k] != 0, from their sorted lb.perm
+void launch_node_pos(const LevelNode* nodes, const std::vector<uint8_t>& pick, LevelBuffers& lb, DeviceMem& mem);
 // Earlier candidates of the same node that would reject a candidate if
 // accepted (within the spacing and, for poisson, not before the early-exit
 // bound), by sorted position; built for the nodes flagged in `use`.

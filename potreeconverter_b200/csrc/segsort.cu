@@ -9,9 +9,11 @@
 // order among equal keys is an artefact of the partitions.
 //
 // This unit sorts every node of a level at once with a segmented LSD radix
-// sort of the key bits (keys are finite and >= +0, so their IEEE bit
-// patterns order like the values), then flags the nodes that hold two equal
-// adjacent keys. Segmentation comes from the tiling: tiles never straddle a
+// sort of the high 32 key bits (keys are finite and >= +0, so their IEEE bit
+// patterns order like the values), puts each short run of equal high words
+// in full-key order in place (a node with a run longer than 32 gets all 64
+// bits by radix instead), then flags the nodes that hold two equal adjacent
+// keys. Segmentation comes from the tiling: tiles never straddle a
 // node, and the per-tile digit counts are laid out node-major, digit-major,
 // tile-minor, so one flat exclusive scan of the count matrix yields, for
 // every (node, digit, tile), the output position inside the node's own range
@@ -40,7 +42,6 @@ constexpr int kSegWarps = kSegThreads / 32;
 constexpr int kSegSteps = 16;
 constexpr int kSegTile = kSegThreads * kSegSteps;  // 4096
 constexpr int kSegDigits = 256;
-constexpr int kKeyPasses = 8;                       // 64 key bits, 8 per pass
 static_assert(kSegThreads == kSegDigits, "one thread per digit");
 
 struct SegTile {
@@ -154,11 +155,46 @@ __global__ void __launch_bounds__(kSegThreads) seg_downsweep(const SegTile* __re
 	}
 }
 
+// After a sort on the high 32 key bits: every run of equal high words is
+// put in full-key order by its first element's thread (stable insertion
+// sort). Runs longer than kLowRunMax flag their node (bit 1) for a full sort.
+constexpr int kLowRunMax = 32;
+
+__global__ void seg_fix_low_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ node_of, uint64_t* __restrict__ sk,
+                                   uint32_t* __restrict__ sv, int64_t M, uint8_t* __restrict__ flags) {
+	const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= M) return;
+	const int32_t n = node_of[t];
+	const int64_t co = nodes[n].cand_off, end = co + nodes[n].count;
+	const uint64_t hi = sk[t] >> 32;
+	if (t > co && (sk[t - 1] >> 32) == hi) return;  // not the first of its run
+	int64_t e = t + 1;
+	while (e < end && (sk[e] >> 32) == hi) {
+		e++;
+		if (e - t > kLowRunMax) {
+			flags[n] |= 2;
+			return;
+		}
+	}
+	for (int64_t i = t + 1; i < e; i++) {
+		const uint64_t k = sk[i];
+		const uint32_t v = sv[i];
+		int64_t j = i;
+		while (j > t && k < sk[j - 1]) {
+			sk[j] = sk[j - 1];
+			sv[j] = sv[j - 1];
+			j--;
+		}
+		sk[j] = k;
+		sv[j] = v;
+	}
+}
+
 __global__ void seg_ties_kernel(const int32_t* __restrict__ node_of, const uint64_t* __restrict__ sk, int64_t M, uint8_t* __restrict__ tie) {
 	const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (t + 1 >= M) return;
 	const int32_t n = node_of[t];
-	if (node_of[t + 1] == n && sk[t] == sk[t + 1]) tie[n] = 1;
+	if (node_of[t + 1] == n && sk[t] == sk[t + 1]) tie[n] |= 1;
 }
 
 __global__ void seg_finish_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ tie, const uint64_t* __restrict__ sk,
@@ -177,9 +213,9 @@ __global__ void seg_finish_kernel(const LevelNode* __restrict__ nodes, const uin
 }  // namespace
 
 void segmented_sort_pairs(const std::vector<LevelNode>& ln, int64_t M, const uint64_t* keys_in, const uint32_t* vals_in,
-                          uint64_t* keys_out, uint32_t* vals_out, int bits, DeviceMem& mem) {
+                          uint64_t* keys_out, uint32_t* vals_out, int begin_bit, int end_bit, DeviceMem& mem) {
 	const int K = (int)ln.size();
-	if (M == 0 || K == 0 || bits <= 0) return;
+	if (M == 0 || K == 0 || end_bit <= begin_bit) return;
 	cudaStream_t s = mem.stream();
 	std::vector<SegTile> tiles;
 	int64_t mat = 0, before = 0;
@@ -202,7 +238,7 @@ void segmented_sort_pairs(const std::vector<LevelNode>& ln, int64_t M, const uin
 		before += n;
 	}
 	const int num_tiles = (int)tiles.size();
-	const int passes = (bits + 7) / 8;
+	const int passes = (end_bit - begin_bit + 7) / 8;
 	SegTile* d_tiles = mem.alloc<SegTile>(tiles.size());
 	PCG_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(SegTile), cudaMemcpyHostToDevice, s));
 	// the last pass writes (keys_out, vals_out)
@@ -215,7 +251,7 @@ void segmented_sort_pairs(const std::vector<LevelNode>& ln, int64_t M, const uin
 	const uint64_t* kin = keys_in;
 	const uint32_t* vin = vals_in;
 	for (int pass = 0; pass < passes; pass++) {
-		const int shift = 8 * pass;
+		const int shift = begin_bit + 8 * pass;
 		const int dst = (passes - 1 - pass) & 1;
 		uint64_t* kout = kb[dst];
 		uint32_t* vout = vb[dst];
@@ -243,17 +279,31 @@ void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>&
 	cudaStream_t s = mem.stream();
 	uint64_t* sk = mem.alloc<uint64_t>(M);
 	uint32_t* sv = mem.alloc<uint32_t>(M);
-	segmented_sort_pairs(ln, M, reinterpret_cast<const uint64_t*>(lb.keys), nullptr, sk, sv, 64, mem);
-	uint8_t* d_tie = mem.alloc<uint8_t>(K);
-	PCG_CUDA(cudaMemsetAsync(d_tie, 0, K, s));
+	const uint64_t* keys = reinterpret_cast<const uint64_t*>(lb.keys);
+	// the high words by radix (four passes), the low words inside the short
+	// runs of equal high words
+	segmented_sort_pairs(ln, M, keys, nullptr, sk, sv, 32, 64, mem);
+	uint8_t* d_flags = mem.alloc<uint8_t>(K);
+	PCG_CUDA(cudaMemsetAsync(d_flags, 0, K, s));
 	const unsigned blocks = (unsigned)ceil_div(M, 256);
-	seg_ties_kernel<<<blocks, 256, 0, s>>>(lb.node_of, sk, M, d_tie);
+	seg_fix_low_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb.node_of, sk, sv, M, d_flags);
 	PCG_LAUNCHED();
-	seg_finish_kernel<<<blocks, 256, 0, s>>>(d_nodes, d_tie, sk, sv, lb);
-	PCG_LAUNCHED();
-	PCG_CUDA(cudaMemcpyAsync(tie.data(), d_tie, K, cudaMemcpyDeviceToHost, s));
+	std::vector<uint8_t> flags(K);
+	PCG_CUDA(cudaMemcpyAsync(flags.data(), d_flags, K, cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));
-	mem.free(d_tie);
+	std::vector<LevelNode> redo;
+	for (int k = 0; k < K; k++)
+		if (flags[k] & 2) redo.push_back(ln[k]);
+	// nodes with a long run of equal high words: all 64 bits by radix
+	if (!redo.empty()) segmented_sort_pairs(redo, M, keys, nullptr, sk, sv, 0, 64, mem);
+	PCG_CUDA(cudaMemsetAsync(d_flags, 0, K, s));
+	seg_ties_kernel<<<blocks, 256, 0, s>>>(lb.node_of, sk, M, d_flags);
+	PCG_LAUNCHED();
+	seg_finish_kernel<<<blocks, 256, 0, s>>>(d_nodes, d_flags, sk, sv, lb);
+	PCG_LAUNCHED();
+	PCG_CUDA(cudaMemcpyAsync(tie.data(), d_flags, K, cudaMemcpyDeviceToHost, s));
+	PCG_CUDA(cudaStreamSynchronize(s));
+	mem.free(d_flags);
 	mem.free(sk);
 	mem.free(sv);
 }
