@@ -10,6 +10,7 @@
 
 #include <math_constants.h>
 
+#include "devutil.cuh"
 #include "kernels.h"
 
 namespace pcg {
@@ -72,15 +73,9 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(const uint
 	const double dG = (double)G;
 	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride) {
 		const uint8_t* r = recs + i * p.rec_len;
-		int32_t Xi = ld<int32_t>(r), Yi = ld<int32_t>(r + 4), Zi = ld<int32_t>(r + 8);
-		// laszip_get_coordinates (laszip_dll.cpp:1137-1139)
-		double x = p.in_scale[0] * (double)Xi + p.in_offset[0];
-		double y = p.in_scale[1] * (double)Yi + p.in_offset[1];
-		double z = p.in_scale[2] * (double)Zi + p.in_offset[2];
-		// quantize (chunker_countsort_laszip.cpp:228-230, 781-783)
-		int32_t X = (int32_t)((x - p.pos_offset[0]) / p.pos_scale[0]);
-		int32_t Y = (int32_t)((y - p.pos_offset[1]) / p.pos_scale[1]);
-		int32_t Z = (int32_t)((z - p.pos_offset[2]) / p.pos_scale[2]);
+		double x, y, z;
+		int32_t X, Y, Z;
+		quantize_record(p, r, x, y, z, X, Y, Z);
 		// unit cube coordinates and cell (:232-257)
 		double ux = ((double)X * p.pos_scale[0] + p.pos_offset[0] - p.cmin[0]) / p.csize;
 		double uy = ((double)Y * p.pos_scale[1] + p.pos_offset[1] - p.cmin[1]) / p.csize;

@@ -55,6 +55,24 @@ __device__ unsigned long long block_scan_u64(unsigned long long v, unsigned long
 	return before + x - v;
 }
 
+// The LAS record's coordinates requantized to the octree's integer grid:
+// laszip_get_coordinates (laszip_dll.cpp:1137-1139), then the chunker's
+// quantization (chunker_countsort_laszip.cpp:228-230, 781-783). Every kernel
+// that needs the integer coordinates of a record uses this one expression.
+__device__ __forceinline__ void quantize_record(const DecodeParams& p, const uint8_t* r, double& x, double& y, double& z, int32_t& X,
+                                                int32_t& Y, int32_t& Z) {
+	int32_t Xi, Yi, Zi;
+	memcpy(&Xi, r, 4);
+	memcpy(&Yi, r + 4, 4);
+	memcpy(&Zi, r + 8, 4);
+	x = p.in_scale[0] * (double)Xi + p.in_offset[0];
+	y = p.in_scale[1] * (double)Yi + p.in_offset[1];
+	z = p.in_scale[2] * (double)Zi + p.in_offset[2];
+	X = (int32_t)((x - p.pos_offset[0]) / p.pos_scale[0]);
+	Y = (int32_t)((y - p.pos_offset[1]) / p.pos_scale[1]);
+	Z = (int32_t)((z - p.pos_offset[2]) / p.pos_scale[2]);
+}
+
 // multiprocessors of the current device
 inline int sm_count() {
 	int dev = 0, sms = 0;

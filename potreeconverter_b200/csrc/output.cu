@@ -4,6 +4,7 @@
 // attribute handlers build it (chunker_countsort_laszip.cpp:380-658,
 // 770-803), so the sampling stages only move 4-byte point ids.
 
+#include "devutil.cuh"
 #include "output.h"
 
 namespace pcg {
@@ -12,13 +13,15 @@ namespace {
 
 template <class T> __device__ __forceinline__ void st(uint8_t* p, T v) { memcpy(p, &v, sizeof(T)); }
 
-// Output record of point `id`; cols != ~0 overrides rgb (poisson_average).
-__device__ void assemble_record(const uint8_t* __restrict__ recs, const DecodeParams& p, const int32_t* X, const int32_t* Y,
-                                const int32_t* Z, uint32_t id, uint64_t col, bool has_col, uint8_t* dst) {
-	const uint8_t* r = recs + (int64_t)id * p.rec_len;
-	st<int32_t>(dst + 0, X[id]);
-	st<int32_t>(dst + 4, Y[id]);
-	st<int32_t>(dst + 8, Z[id]);
+// Output record of point `id` from its LAS record r; has_col overrides rgb
+// with col (poisson_average).
+__device__ void assemble_record(const uint8_t* r, const DecodeParams& p, uint64_t col, bool has_col, uint8_t* dst) {
+	double x, y, z;
+	int32_t X, Y, Z;
+	quantize_record(p, r, x, y, z, X, Y, Z);
+	st<int32_t>(dst + 0, X);
+	st<int32_t>(dst + 4, Y);
+	st<int32_t>(dst + 8, Z);
 	if (p.off_intensity >= 0) { dst[p.off_intensity] = r[12]; dst[p.off_intensity + 1] = r[13]; }
 	if (p.off_retnum >= 0) dst[p.off_retnum] = r[14] & 7;
 	if (p.off_nret >= 0) dst[p.off_nret] = (r[14] >> 3) & 7;
@@ -45,28 +48,60 @@ __device__ void assemble_record(const uint8_t* __restrict__ recs, const DecodePa
 
 constexpr int kOutThreads = 256;
 
-// One CTA per payload; records are staged in shared memory so the global
-// writes of a CTA are one contiguous, coalesced span.
-__global__ void __launch_bounds__(kOutThreads) write_payloads_kernel(const uint8_t* __restrict__ recs, DecodeParams p, const int32_t* X,
-                                                                    const int32_t* Y, const int32_t* Z, const PayloadItem* __restrict__ items,
-                                                                    uint8_t* __restrict__ out) {
-	extern __shared__ uint8_t stage[];
-	const PayloadItem it = items[blockIdx.x];
-	const int bpp = p.bpp;
-	uint8_t* dst_base = out + it.out_offset * bpp;
-	for (int64_t t0 = 0; t0 < it.count; t0 += kOutThreads) {
-		int64_t t = t0 + threadIdx.x;
-		int64_t nthis = it.count - t0 < kOutThreads ? it.count - t0 : kOutThreads;
-		if (t < it.count) {
-			uint64_t col = it.cols ? it.cols[t] : 0ull;
-			assemble_record(recs, p, X, Y, Z, it.ids[t], col, it.cols != nullptr, stage + threadIdx.x * bpp);
+// words of shared scratch per thread for one LAS record (4-byte aligned
+// cover of rec_len bytes at any offset)
+__host__ __device__ __forceinline__ int rec_words(int rec_len) { return (rec_len + 3) / 4 + 1; }
+
+// 256 output points per CTA over the whole octree.bin image (payloads are
+// contiguous in completion order, so a CTA spans one or a few payloads).
+// Each thread copies its LAS record into shared memory with aligned 4-byte
+// loads (byte loads for the last records, whose cover would reach past the
+// buffer), assembles the output record there -- requantizing the record's
+// own coordinates -- and the CTA writes its span with 4-byte stores.
+__global__ void __launch_bounds__(kOutThreads) write_payloads_kernel(const uint8_t* __restrict__ recs, int64_t rec_bytes, DecodeParams p,
+                                                                    const PayloadItem* __restrict__ items, const int32_t* __restrict__ chunk_item,
+                                                                    int64_t total, uint8_t* __restrict__ out) {
+	extern __shared__ uint32_t smem_words[];
+	const int bpp = p.bpp, rl = p.rec_len, rw = rec_words(rl);
+	uint32_t* scratch = smem_words + threadIdx.x * rw;
+	uint8_t* stage = reinterpret_cast<uint8_t*>(smem_words + kOutThreads * rw);
+	const bool aligned = (reinterpret_cast<uintptr_t>(recs) & 3) == 0;
+	const int64_t q0 = (int64_t)blockIdx.x * kOutThreads, q = q0 + threadIdx.x;
+	const int64_t nthis = total - q0 < kOutThreads ? total - q0 : kOutThreads;
+	if (q < total) {
+		int k = chunk_item[blockIdx.x];
+		while (items[k].out_offset + items[k].count <= q) k++;
+		const PayloadItem& it = items[k];
+		const int64_t t = q - it.out_offset;
+		const uint32_t id = it.ids[t];
+		const int64_t start = (int64_t)id * rl;
+		const int64_t w0 = start >> 2, w1 = (start + rl + 3) >> 2;
+		const uint8_t* r;
+		if (aligned && w1 * 4 <= rec_bytes) {
+			const uint32_t* src = reinterpret_cast<const uint32_t*>(recs) + w0;
+			for (int w = 0; w < (int)(w1 - w0); w++) scratch[w] = src[w];
+			r = reinterpret_cast<const uint8_t*>(scratch) + (start & 3);
+		} else {
+			uint8_t* sb = reinterpret_cast<uint8_t*>(scratch);
+			for (int w = 0; w < rl; w++) sb[w] = recs[start + w];
+			r = sb;
 		}
-		__syncthreads();
-		int64_t bytes = nthis * bpp;
-		uint8_t* dst = dst_base + t0 * bpp;
-		for (int64_t b = threadIdx.x; b < bytes; b += kOutThreads) dst[b] = stage[b];
-		__syncthreads();
+		assemble_record(r, p, it.cols ? it.cols[t] : 0ull, it.cols != nullptr, stage + threadIdx.x * bpp);
 	}
+	__syncthreads();
+	const int64_t bytes = nthis * bpp;
+	uint8_t* dst = out + q0 * bpp;
+	// head bytes up to a 4-byte boundary, whole words, tail bytes
+	int64_t head = (int64_t)((4 - (reinterpret_cast<uintptr_t>(dst) & 3)) & 3);
+	if (head > bytes) head = bytes;
+	const int64_t words = (bytes - head) >> 2;
+	if (threadIdx.x < head) dst[threadIdx.x] = stage[threadIdx.x];
+	uint32_t* dw = reinterpret_cast<uint32_t*>(dst + head);
+	for (int64_t w = threadIdx.x; w < words; w += kOutThreads) {
+		const uint8_t* sp = stage + head + 4 * w;
+		dw[w] = (uint32_t)sp[0] | ((uint32_t)sp[1] << 8) | ((uint32_t)sp[2] << 16) | ((uint32_t)sp[3] << 24);
+	}
+	for (int64_t b = head + 4 * words + threadIdx.x; b < bytes; b += kOutThreads) dst[b] = stage[b];
 }
 
 __global__ void fill_colors_kernel(const uint8_t* __restrict__ recs, int rec_len, int src_rgb, const uint32_t* __restrict__ ids, int64_t n,
@@ -106,13 +141,28 @@ __global__ void split_kernel(const uint8_t* __restrict__ accepted, const uint32_
 
 }  // namespace
 
-void launch_write_payloads(const uint8_t* d_recs, const DecodeParams& p, const int32_t* X, const int32_t* Y, const int32_t* Z,
-                           const PayloadItem* items, int num_items, uint8_t* out, DeviceMem& mem) {
-	if (num_items == 0) return;
-	size_t smem = (size_t)kOutThreads * p.bpp;
+void launch_write_payloads(const uint8_t* d_recs, const DecodeParams& p, const std::vector<PayloadItem>& items, const PayloadItem* d_items,
+                           uint8_t* out, DeviceMem& mem) {
+	if (items.empty()) return;
+	const int64_t total = items.back().out_offset + items.back().count;
+	if (total == 0) return;
+	size_t smem = (size_t)kOutThreads * (rec_words(p.rec_len) * 4 + p.bpp);
+	if (smem > 200 * 1024) throw PcgError(1, "point records too long for the payload writer (record + output > 800 bytes)");
 	if (smem > 48 * 1024) PCG_CUDA(cudaFuncSetAttribute(write_payloads_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-	write_payloads_kernel<<<num_items, kOutThreads, smem, mem.stream()>>>(d_recs, p, X, Y, Z, items, out);
+	// the payload holding the first point of every 256-point chunk
+	const int64_t chunks = ceil_div(total, kOutThreads);
+	std::vector<int32_t> chunk_item(chunks);
+	size_t k = 0;
+	for (int64_t c = 0; c < chunks; c++) {
+		const int64_t q = c * kOutThreads;
+		while (items[k].out_offset + items[k].count <= q) k++;
+		chunk_item[c] = (int32_t)k;
+	}
+	int32_t* d_ci = mem.alloc<int32_t>(chunks);
+	PCG_CUDA(cudaMemcpyAsync(d_ci, chunk_item.data(), chunks * sizeof(int32_t), cudaMemcpyHostToDevice, mem.stream()));
+	write_payloads_kernel<<<(unsigned)chunks, kOutThreads, smem, mem.stream()>>>(d_recs, p.n * (int64_t)p.rec_len, p, d_items, d_ci, total, out);
 	PCG_LAUNCHED();
+	mem.free(d_ci);
 }
 
 void launch_fill_colors(const uint8_t* d_recs, int rec_len, int src_rgb, const uint32_t* ids, int64_t n, uint64_t* cols, DeviceMem& mem) {

@@ -514,7 +514,7 @@ struct Converter {
 			d_out = mem.alloc<uint8_t>(res.octree_size);
 		}
 		PayloadItem* d_items = upload(items, mem);
-		launch_write_payloads(d_recs, p, co.X, co.Y, co.Z, d_items, (int)items.size(), d_out, mem);
+		launch_write_payloads(d_recs, p, items, d_items, d_out, mem);
 		PCG_CUDA(cudaStreamSynchronize(stream));
 		res.stats.ms_output = ms_since(t_out);
 		auto t_d2h = Clock::now();
