@@ -43,6 +43,9 @@ WORKLOAD = {"workload": "hotspots-50M", "points": 50_000_000, "las": "1.4", "poi
             "extra_attributes": "1 x float32", "extent_m": [2000, 2000, 50], "hotspots": 20,
             "sampler": "poisson", "form": "batched", "l2": "inputs larger than L2 (1.9 GB records)"}
 REF_SAMPLE_POINTS = 2_000_000
+# DRAM bytes (read + write) per candidate of the acceptance kernel, from the
+# ncu capture summarised in profiles/accept_hotspots-5M_poisson.md
+ACCEPT_DRAM_BYTES_PER_CANDIDATE = None
 MEASURED_PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
 
 
@@ -101,13 +104,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def dist_init():
+def dist_init(backend: str = "nccl"):
+    """Process group for N > 1 ranks (one per GPU; gloo in the CPU tests)."""
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(minutes=10))
+        dist.init_process_group(backend, timeout=timedelta(minutes=10))
         return dist
     return None
+
+
+def replica_seed(rank: int) -> int:
+    """Each rank converts its own cloud: same generator, seed per rank."""
+    return 1001 + rank
 
 
 def max_over_ranks(dist, v: float, device) -> float:
@@ -121,9 +130,15 @@ def max_over_ranks(dist, v: float, device) -> float:
 
 def barrier(dist, device):
     import torch
-    torch.cuda.synchronize(device)
+    if getattr(device, "type", "cuda") == "cuda":
+        torch.cuda.synchronize(device)
     if dist is not None:
         dist.barrier()
+
+
+def aggregate_mpts(world: int, points_per_rank: int, ms_per_step: float) -> float:
+    """Whole-job Mpts/s: every rank's points over the max-over-ranks time."""
+    return world * points_per_rank / (ms_per_step * 1e3)
 
 
 def cpu_reference_step(las_path: str, outdir: str, threads: int | None = None) -> tuple[float, float]:
@@ -203,7 +218,7 @@ def main():
     device = torch.device("cuda", local)
 
     n = args.points
-    las = synth.hotspots(n, 1001 + rank)
+    las = synth.hotspots(n, replica_seed(rank))
     off = int.from_bytes(las[96:100], "little")
     header = las[:off]
     pinned = torch.empty(len(las), dtype=torch.uint8, pin_memory=True)
@@ -230,7 +245,7 @@ def main():
     barrier(dist, device)
     ms = start.elapsed_time(end) / args.steps
     ms = max_over_ranks(dist, ms, device)
-    value = world * n / (ms * 1e3)
+    value = aggregate_mpts(world, n, ms)
 
     # ---- e2e: through the C ABI from pinned host memory
     for _ in range(max(1, args.warmup // 2)):
@@ -248,19 +263,24 @@ def main():
     e_end.synchronize()
     barrier(dist, device)
     e_ms = max_over_ranks(dist, e_start.elapsed_time(e_end) / args.steps, device)
-    e2e = world * n / (e_ms * 1e3)
+    e2e = aggregate_mpts(world, n, e_ms)
 
     s = stats[-1]
     rec_len = int.from_bytes(header[105:107], "little")
     bpp = 39
     out_pts = s["output_points"]
-    # roofline: the greedy acceptance kernel dominates; algorithmic bytes per
-    # candidate = id + position + key + decision + permutation entries read
-    # and written once
-    greedy_bytes = s["candidates"] * 33 + out_pts * 0
-    greedy_ms = s["ms_greedy"]
+    # roofline: the dominant kernel of a step (ncu launch list) is the
+    # acceptance from conflict lists (greedy_list_kernel and its warp form),
+    # launched once per octree level. Algorithmic bytes: per candidate its
+    # record (16 B), list length (1 B) and its decision, rank and flag
+    # (9 B); per list entry the entry (4 B) and that candidate's decision
+    # (4 B). Duration: the acceptance device time of the step (ms_greedy
+    # minus the list builds), all levels.
+    accept_ms = s["ms_greedy"] - s["ms_lists"]
+    accept_bytes = s["candidates"] * 26 + s["list_entries"] * 8
     peak, peak_kind = peak_hbm()
-    achieved = greedy_bytes / (greedy_ms * 1e-3) / 1e9 if greedy_ms > 0 else 0.0
+    achieved = accept_bytes / (accept_ms * 1e-3) / 1e9 if accept_ms > 0 else 0.0
+    traffic = s["candidates"] * ACCEPT_DRAM_BYTES_PER_CANDIDATE if ACCEPT_DRAM_BYTES_PER_CANDIDATE else None
     whole_bytes = n * rec_len + out_pts * bpp  # B_alg: read every record once, write every output record once
     if rank == 0:
         cpu = None
@@ -281,10 +301,12 @@ def main():
             "e2e": {"value": e2e, "unit": "Mpts/s", "h2d_bytes_per_step": int(pinned.numel()),
                     "d2h_bytes_per_step": int(octree_bytes)},
             "gpu_launches": int(s["gpu_launches"]) * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "greedy (poisson acceptance)", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "roofline": {"bound": "hbm", "kernel": "greedy_list_kernel + greedy_list_warp_kernel (all levels of a step)",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "traffic_source": "DRAM bytes per candidate from ncu, profiles/accept_hotspots-5M_poisson.md",
+                         "algorithmic_bytes": accept_bytes, "kernel_ms": accept_ms,
                          "pipeline_achieved": whole_bytes / (ms * 1e-3) / 1e9, "pipeline_bytes_per_step": whole_bytes},
-            "stages_ms": {k: round(s[k], 3) for k in ("ms_chunking", "ms_octree", "ms_sampling", "ms_sort", "ms_greedy",
+            "stages_ms": {k: round(s[k], 3) for k in ("ms_chunking", "ms_octree", "ms_sampling", "ms_sort", "ms_greedy", "ms_lists",
                                                      "ms_output", "ms_host_writers")},
             "e2e_stages_ms": {k: round(e_stats[k], 3) for k in ("ms_total", "ms_h2d", "ms_sampling", "ms_output", "ms_d2h",
                                                                   "ms_host_writers")},
@@ -292,7 +314,7 @@ def main():
             "cpu_baseline": cpu,
             "escalated_pairs": int(s["escalated_pairs"]),
             "sampler": {k: int(s[k]) for k in ("sampled_nodes", "candidates", "replayed_nodes", "replayed_candidates",
-                                               "heapsort_fallbacks")},
+                                               "heapsort_fallbacks", "list_entries")},
         }
         print(json.dumps(line))
     ctx.close()

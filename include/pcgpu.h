@@ -104,6 +104,9 @@ typedef struct pcg_stats {
 	int64_t replayed_nodes;       /* nodes with equal keys, sorted by the
 	                                 element-for-element introsort replay   */
 	int64_t replayed_candidates;  /* their candidates                       */
+	double ms_lists;              /* device time of the conflict-list builds
+	                                 (part of ms_greedy)                     */
+	int64_t list_entries;         /* conflict-list entries over all levels  */
 } pcg_stats;
 
 typedef struct pcg_result {

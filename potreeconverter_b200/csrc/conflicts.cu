@@ -147,7 +147,7 @@ template <int MODE>
 __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, PosParamsS pp,
                                                         LevelBuffers lb, const uint64_t* __restrict__ ck, const int4* __restrict__ crec,
                                                         const RunSlot* __restrict__ table, int64_t cap, const int64_t* __restrict__ bm_off, const uint32_t* __restrict__ bm,
-                                                        ConflictLists cl) {
+                                                        ConflictLists cl, SampleStats* st) {
 	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= lb.M) return;
 	const int32_t node = lb.node_of[j];
@@ -220,6 +220,9 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 	}
 	cl.count[co + t] = (uint8_t)(n <= kListCap ? n : kListDense);
 	if (n > kListCap) cl.node_dense[node] = 1;
+	const unsigned active = __activemask();
+	const unsigned sum = __reduce_add_sync(active, (unsigned)(n <= kListCap ? n : kListCap));
+	if ((int)(threadIdx.x & 31) == __ffs(active) - 1) atomicAdd(&st->list_entries, (unsigned long long)sum);
 }
 
 }  // namespace
@@ -277,8 +280,8 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
 	uint8_t* d_use = mem.alloc<uint8_t>(K);
 	PCG_CUDA(cudaMemcpyAsync(d_use, use.data(), K, cudaMemcpyHostToDevice, s));
-	if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, table, cap, d_bm_off, bm, cl);
-	else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, table, cap, d_bm_off, bm, cl);
+	if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, table, cap, d_bm_off, bm, cl, st);
+	else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, table, cap, d_bm_off, bm, cl, st);
 	PCG_LAUNCHED();
 	PCG_CUDA(cudaMemcpyAsync(dense.data(), cl.node_dense, K, cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));

@@ -481,6 +481,7 @@ struct Converter {
 		if (hst.timeouts) throw PcgError(PCG_TIMEOUT, "a bounded device loop gave up");
 		res.stats.escalated_pairs = (int64_t)hst.escalated;
 		res.stats.heapsort_fallbacks = (int64_t)hst.heapsorts;
+		res.stats.list_entries = (int64_t)hst.list_entries;
 		res.stats.ms_sampling = ms_since(t_samp);
 
 		// ------------------------------------------------ completion order
@@ -748,6 +749,7 @@ struct Converter {
 			res.stats.ms_greedy += t_greedy;
 			float t_lists = 0;
 			if (form != PCG_FORM_PLAIN) PCG_CUDA(cudaEventElapsedTime(&t_lists, ev[1], ev_lists));
+			res.stats.ms_lists += t_lists;
 			cudaEventDestroy(ev_lists);
 			if (trace_levels()) {
 				int64_t mx = 0;

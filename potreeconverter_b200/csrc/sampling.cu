@@ -981,28 +981,30 @@ __global__ void __launch_bounds__(kBigThreads) greedy_list_kernel(const LevelNod
 		long long clk0 = clock64();
 		if (t + kRound < n) prefetch_list(cl, lb, co, t + kRound);
 		int32_t maxrank = -1, local = 0;
-		int nc = 0;
+		int nc = 0, nl = 0;
 		int4 me = make_int4(0, 0, 0, 0);
 		if (valid) {
 			me = lb.cq[co + t];
 			local = me.w;
-			const int nl = cl.count[co + t];
+			nl = cl.count[co + t];
+		}
+		{
+			// lists are short (about one entry on average): loop to the
+			// warp's longest list, four entries per 16-byte load
 			const int4* lp = reinterpret_cast<const int4*>(cl.entries + (co + t) * (int64_t)kListCap);
-			int32_t ent[kListCap];
+			const int wmax = (int)__reduce_max_sync(FULL, (unsigned)nl);
+			for (int w = 0; 4 * w < wmax; w++) {
+				const int4 v = 4 * w < nl ? lp[w] : make_int4(0, 0, 0, 0);
+				const int32_t u4[4] = {v.x, v.y, v.z, v.w};
+				int32_t rk4[4];
 #pragma unroll
-			for (int w = 0; w < kListCap / 4; w++) {
-				int4 v = make_int4(0, 0, 0, 0);
-				if (4 * w < nl) v = lp[w];
-				ent[4 * w] = v.x; ent[4 * w + 1] = v.y; ent[4 * w + 2] = v.z; ent[4 * w + 3] = v.w;
-			}
-			int32_t rk[kListCap];
+				for (int k = 0; k < 4; k++) rk4[k] = (4 * w + k < nl && u4[k] < r0) ? srank[co + u4[k]] : -1;
 #pragma unroll
-			for (int e = 0; e < kListCap; e++) rk[e] = (e < nl && ent[e] < r0) ? srank[co + ent[e]] : -1;
-#pragma unroll
-			for (int e = 0; e < kListCap; e++) {
-				if (e < nl) {
-					if (ent[e] < r0) maxrank = rk[e] > maxrank ? rk[e] : maxrank;
-					else R.conf[tid][nc++] = (int16_t)(ent[e] - r0);
+				for (int k = 0; k < 4; k++) {
+					if (4 * w + k < nl) {
+						if (u4[k] < r0) maxrank = rk4[k] > maxrank ? rk4[k] : maxrank;
+						else R.conf[tid][nc++] = (int16_t)(u4[k] - r0);
+					}
 				}
 			}
 		}
@@ -1181,25 +1183,26 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) greedy_list_warp_kernel(c
 			int4 me = make_int4(0, 0, 0, 0);
 			int32_t maxrank = -1;
 			uint32_t mask = 0;  // earlier lanes of this step that conflict
+			int nl = 0;
 			if (valid) {
 				me = lb.cq[co + t];
-				const int nl = cl.count[co + t];
+				nl = cl.count[co + t];
+			}
+			{
 				const int4* lp = reinterpret_cast<const int4*>(cl.entries + (co + t) * (int64_t)kListCap);
-				int32_t ent[kListCap];
+				const int wmax = (int)__reduce_max_sync(FULL, (unsigned)nl);
+				for (int w = 0; 4 * w < wmax; w++) {
+					const int4 v = 4 * w < nl ? lp[w] : make_int4(0, 0, 0, 0);
+					const int32_t u4[4] = {v.x, v.y, v.z, v.w};
+					int32_t rk4[4];
 #pragma unroll
-				for (int w = 0; w < kListCap / 4; w++) {
-					int4 v = make_int4(0, 0, 0, 0);
-					if (4 * w < nl) v = lp[w];
-					ent[4 * w] = v.x; ent[4 * w + 1] = v.y; ent[4 * w + 2] = v.z; ent[4 * w + 3] = v.w;
-				}
-				int32_t rk[kListCap];
+					for (int k = 0; k < 4; k++) rk4[k] = (4 * w + k < nl && u4[k] < b0) ? srank[co + u4[k]] : -1;
 #pragma unroll
-				for (int e = 0; e < kListCap; e++) rk[e] = (e < nl && ent[e] < b0) ? srank[co + ent[e]] : -1;
-#pragma unroll
-				for (int e = 0; e < kListCap; e++) {
-					if (e < nl) {
-						if (ent[e] < b0) maxrank = rk[e] > maxrank ? rk[e] : maxrank;
-						else mask |= 1u << (ent[e] - b0);
+					for (int k = 0; k < 4; k++) {
+						if (4 * w + k < nl) {
+							if (u4[k] < b0) maxrank = rk4[k] > maxrank ? rk4[k] : maxrank;
+							else mask |= 1u << (u4[k] - b0);
+						}
 					}
 				}
 			}

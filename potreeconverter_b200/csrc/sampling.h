@@ -59,6 +59,7 @@ struct SampleStats {
 	unsigned long long rounds;     // CTA greedy rounds
 	unsigned long long passes;     // parallel decision passes over all rounds
 	unsigned long long serial;     // rounds that needed the in-order decision warp
+	unsigned long long list_entries; // conflict-list entries written
 	unsigned long long cycles[7];  // CTA greedy: SM cycles of thread 0 in phases A, B, C1, C2, D; cells read past 3 and 7 points
 };
 
