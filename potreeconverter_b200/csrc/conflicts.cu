@@ -18,8 +18,10 @@
 //  2. segmented radix sort of (cell, sorted position) per node;
 //  3. a hash table (node, cell) -> range of the cell-sorted records;
 //  4. one thread per candidate in cell order (a warp shares neighbourhoods)
-//     tests the 27 cells' records: an FP32 prefilter on exact integer deltas,
-//     then the reference's FP64 test, then the early-exit bound.
+//     scans the occupied cells among its 27 up to its own sorted position:
+//     an FP32 prefilter on node-relative coordinates (margin 1e-3 of s^2,
+//     far above its rounding error), then the reference's FP64 test, then
+//     the early-exit bound.
 // A candidate with more than kListCap such predecessors marks its node
 // dense; dense nodes keep the grid-based acceptance kernel.
 
@@ -69,16 +71,21 @@ __global__ void conf_cell_keys_kernel(const LevelNode* __restrict__ nodes, PosPa
 	keys[j] = ((uint64_t)cz * kCellsPerAxis + (uint64_t)cy) * kCellsPerAxis + (uint64_t)cx;
 }
 
-// cell-sorted records (X, Y, Z, sorted position)
-__global__ void conf_gather_kernel(const LevelNode* __restrict__ nodes, LevelBuffers lb, const uint32_t* __restrict__ cvals,
-                                   int4* __restrict__ crec) {
+// cell-sorted records: (X, Y, Z, sorted position) and, for the prefilter,
+// the position relative to the node's minimum corner in FP32 (w = sorted
+// position). Within a cell, records are in sorted order (the cell sort is
+// stable).
+__global__ void conf_gather_kernel(const LevelNode* __restrict__ nodes, PosParamsS pp, LevelBuffers lb, const uint32_t* __restrict__ cvals,
+                                   int4* __restrict__ crec, float4* __restrict__ crf) {
 	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= lb.M) return;
-	const int64_t co = nodes[lb.node_of[j]].cand_off;
+	const LevelNode& nd = nodes[lb.node_of[j]];
 	const uint32_t u = cvals[j];
-	int4 r = lb.cq[co + u];
+	int4 r = lb.cq[nd.cand_off + u];
 	r.w = (int32_t)u;
 	crec[j] = r;
+	crf[j] = make_float4((float)(qcoord(r.x, 0, pp) - nd.min[0]), (float)(qcoord(r.y, 1, pp) - nd.min[1]),
+	                     (float)(qcoord(r.z, 2, pp) - nd.min[2]), __int_as_float((int)u));
 }
 
 // occupancy bitmap of a node's cells: 128 bits per (z, y) row, 4 words
@@ -146,7 +153,7 @@ __device__ __forceinline__ int2 find_run(const RunSlot* table, int64_t cap, uint
 template <int MODE>
 __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, PosParamsS pp,
                                                         LevelBuffers lb, const uint64_t* __restrict__ ck, const int4* __restrict__ crec,
-                                                        const RunSlot* __restrict__ table, int64_t cap, const int64_t* __restrict__ bm_off, const uint32_t* __restrict__ bm,
+                                                        const float4* __restrict__ crf, const RunSlot* __restrict__ table, int64_t cap, const int64_t* __restrict__ bm_off, const uint32_t* __restrict__ bm,
                                                         ConflictLists cl, SampleStats* st) {
 	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= lb.M) return;
@@ -155,6 +162,7 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 	const LevelNode& nd = nodes[node];
 	const int64_t co = nd.cand_off;
 	const int4 me = crec[j];
+	const float4 mf = crf[j];
 	const int32_t t = me.w;
 	const double x = qcoord(me.x, 0, pp), y = qcoord(me.y, 1, pp), z = qcoord(me.z, 2, pp);
 	const double sp = nd.spacing, s2 = sp * sp;
@@ -165,12 +173,8 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 		const double limit = cd - sp;
 		lim = limit * limit;
 	}
-	bool pre32 = s2 > 1e-30 && s2 < 1e30;
-	float sf[3];
-	for (int a = 0; a < 3; a++) {
-		sf[a] = (float)pp.scale[a];
-		pre32 = pre32 && pp.scale[a] > 0.0 && (nd.max[a] - nd.min[a]) / pp.scale[a] < 8.0e6;
-	}
+	// node-relative FP32 coordinates: error far below the 1e-3 margin on s^2
+	const bool pre32 = s2 > 1e-30 && s2 < 1e30;
 	const float s2hi = (float)(s2 * 1.001);
 	const uint64_t c = ck[j];
 	const int cx = (int)(c % kCellsPerAxis), cy = (int)((c / kCellsPerAxis) % kCellsPerAxis), cz = (int)(c / (kCellsPerAxis * kCellsPerAxis));
@@ -200,13 +204,16 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 				const uint64_t cell = ((uint64_t)qz * kCellsPerAxis + (uint64_t)qy) * kCellsPerAxis + (uint64_t)qx;
 				const int2 run = find_run(table, cap, ((uint64_t)(uint32_t)node << 32) | cell);
 				const int4* rp = crec + co + run.x;
+				const float4* rf = crf + co + run.x;
 				for (int i = 0; i < run.y; i++) {
-					const int4 q = rp[i];
-					if (q.w >= t) continue;  // only earlier candidates
+					const float4 qf = rf[i];
+					const int32_t u = __float_as_int(qf.w);
+					if (u >= t) break;  // a cell's records are in sorted order: only earlier candidates
 					if (pre32) {
-						const float fx = (float)(q.x - me.x) * sf[0], fy = (float)(q.y - me.y) * sf[1], fz = (float)(q.z - me.z) * sf[2];
+						const float fx = qf.x - mf.x, fy = qf.y - mf.y, fz = qf.z - mf.z;
 						if (fx * fx + fy * fy + fz * fz >= s2hi) continue;
 					}
+					const int4 q = rp[i];
 					const double ax = qcoord(q.x, 0, pp), ay = qcoord(q.y, 1, pp), az = qcoord(q.z, 2, pp);
 					// squaredDistance(point, candidate), sampler_poisson.h:117-125
 					const double dx_ = ax - x, dy_ = ay - y, dz_ = az - z;
@@ -244,7 +251,8 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	segmented_sort_pairs(ln, M, keys, nullptr, ck, cv, 0, 21, mem);
 	mem.free(keys);
 	int4* crec = mem.alloc<int4>(M);
-	conf_gather_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb, cv, crec);
+	float4* crf = mem.alloc<float4>(M);
+	conf_gather_kernel<<<blocks, 256, 0, s>>>(d_nodes, pp, lb, cv, crec, crf);
 	PCG_LAUNCHED();
 	mem.free(cv);
 	unsigned long long* d_runs = mem.alloc<unsigned long long>(1);
@@ -280,8 +288,8 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
 	uint8_t* d_use = mem.alloc<uint8_t>(K);
 	PCG_CUDA(cudaMemcpyAsync(d_use, use.data(), K, cudaMemcpyHostToDevice, s));
-	if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, table, cap, d_bm_off, bm, cl, st);
-	else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, table, cap, d_bm_off, bm, cl, st);
+	if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, st);
+	else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, st);
 	PCG_LAUNCHED();
 	PCG_CUDA(cudaMemcpyAsync(dense.data(), cl.node_dense, K, cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));
@@ -290,6 +298,7 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	mem.free(bm);
 	mem.free(table);
 	mem.free(crec);
+	mem.free(crf);
 	mem.free(ck);
 }
 
