@@ -57,7 +57,30 @@ class DeviceArena {
 public:
 	static constexpr size_t kArenaChunk = size_t(2) << 30;
 	explicit DeviceArena(cudaStream_t s) : stream_(s) {}
-	~DeviceArena() { release_all(); }
+	~DeviceArena() {
+		release_all();
+		if (side_) {
+			cudaStreamSynchronize(side_);
+			cudaStreamDestroy(side_);
+			cudaEventDestroy(fork_);
+			cudaEventDestroy(join_);
+		}
+	}
+
+	// A second stream for work that runs beside the arena's stream, with the
+	// events that fork it from and join it back to the arena's stream;
+	// created once (stream creation can stall the host).
+	cudaStream_t side_stream(cudaEvent_t& fork, cudaEvent_t& join) {
+		if (!side_) {
+			cudaError_t e = cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking);
+			if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming);
+			if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join_, cudaEventDisableTiming);
+			if (e != cudaSuccess) throw CudaError(e, std::string("side stream: ") + cudaGetErrorString(e));
+		}
+		fork = fork_;
+		join = join_;
+		return side_;
+	}
 	DeviceArena(const DeviceArena&) = delete;
 	DeviceArena& operator=(const DeviceArena&) = delete;
 
@@ -166,6 +189,8 @@ private:
 	}
 
 	cudaStream_t stream_;
+	cudaStream_t side_ = nullptr;
+	cudaEvent_t fork_ = nullptr, join_ = nullptr;
 	std::vector<Chunk> chunks_;
 	std::unordered_map<void*, std::pair<size_t, size_t>> live_;  // range -> (chunk, length)
 };
@@ -215,6 +240,7 @@ public:
 	size_t bytes() const { return bytes_; }
 	double alloc_ms() const { return alloc_ms_; }  // host time spent allocating
 	cudaStream_t stream() const { return stream_; }
+	DeviceArena* arena() const { return arena_; }
 
 private:
 	void give_back(void* p) {

@@ -935,25 +935,58 @@ __device__ __forceinline__ void prefetch_list(const ConflictLists& cl, const Lev
 	asm volatile("prefetch.global.L2 [%0];" ::"l"(lb.cq + co + u));
 }
 
+// Rounds of 1024 candidates, one per thread of a 1024-thread CTA.
+constexpr int kListThreads = 1024;
+constexpr int kListWarps = kListThreads / 32;
+constexpr int kListRound = kListThreads;
+
+// exclusive scan over the CTA of one count per thread
+__device__ __forceinline__ uint32_t list_block_scan(uint32_t v, uint32_t& total, uint32_t* warp_sums) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	uint32_t x = v;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const uint32_t y = __shfl_up_sync(FULL, x, o);
+		if (lane >= o) x += y;
+	}
+	if (lane == 31) warp_sums[warp] = x;
+	__syncthreads();
+	if (warp == 0) {
+		uint32_t w = warp_sums[lane];
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const uint32_t y = __shfl_up_sync(FULL, w, o);
+			if (lane >= o) w += y;
+		}
+		warp_sums[lane] = w;
+	}
+	__syncthreads();
+	const uint32_t before = warp > 0 ? warp_sums[warp - 1] : 0u;
+	total = warp_sums[kListWarps - 1];
+	__syncthreads();
+	return before + x - v;
+}
+static_assert(kListWarps == 32, "one warp-sum per lane of warp 0");
+
 // Greedy acceptance for a large node from its conflict lists (conflicts.cu),
-// one CTA, 512 candidates per round. A candidate's list names every earlier
+// one CTA, 1024 candidates per round. A candidate's list names every earlier
 // candidate that would reject it if accepted, so the round needs no spatial
 // lookups: earlier rounds' decisions are read from srank (rank, or -1 for
 // rejected), this round's are resolved by the same parallel passes and
 // in-order warp as the grid kernel.
 struct ListRound {
-	int32_t maxrank[kRound];
-	int32_t local[kRound];
-	int16_t conf[kRound][kListCap];
-	uint8_t nconf[kRound];
-	uint8_t state[kRound];   // 0 undecided, 1 accepted, 2 rejected
-	uint8_t old[kRound];     // old-window status: 0 no conflict, 1 conflict, 2 depends on the count
+	int32_t maxrank[kListRound];
+	int32_t local[kListRound];
+	int16_t conf[kListRound][kListCap];
+	uint8_t nconf[kListRound];
+	uint8_t state[kListRound];   // 0 undecided, 1 accepted, 2 rejected
+	uint8_t old[kListRound];     // old-window status: 0 no conflict, 1 conflict, 2 depends on the count
 	int32_t cnt;             // accepted before this round
-	unsigned long long warp_sums[kBigWarps];
+	uint32_t warp_sums[kListWarps];
 };
 
 template <int MODE>
-__global__ void __launch_bounds__(kBigThreads) greedy_list_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order,
+__global__ void __launch_bounds__(kListThreads) greedy_list_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order,
                                                                  int node_begin, PosParamsS pp, LevelBuffers lb, GreedyArgs ga,
                                                                  ConflictLists cl, int32_t* __restrict__ srank, SampleStats* st) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -965,21 +998,21 @@ __global__ void __launch_bounds__(kBigThreads) greedy_list_kernel(const LevelNod
 	int32_t* hh = ga.hheads + nd.hash_off;
 	if (MODE == 1) {
 		// poisson_average's colour pass finds accepted points through the hash
-		for (int64_t i = tid; i < nd.hash_cap; i += kBigThreads) { hk[i] = EMPTY_KEY; hh[i] = -1; }
+		for (int64_t i = tid; i < nd.hash_cap; i += kListThreads) { hk[i] = EMPTY_KEY; hh[i] = -1; }
 	}
 	if (tid == 0) R.cnt = 0;
 	__syncthreads();
 	CellGrid g;
 	g.min[0] = nd.min[0]; g.min[1] = nd.min[1]; g.min[2] = nd.min[2];
 	g.inv = 1.0 / (2.0 * nd.spacing * 1.000001);
-	for (int64_t r0 = 0; r0 < n; r0 += kRound) {
+	for (int64_t r0 = 0; r0 < n; r0 += kListRound) {
 		const int64_t t = r0 + tid;
 		const bool valid = t < n;
-		const int nr = (int)((n - r0) < kRound ? (n - r0) : kRound);
+		const int nr = (int)((n - r0) < kListRound ? (n - r0) : kListRound);
 		const int32_t cnt0 = R.cnt;
 		// ---- A: the candidate's list
 		long long clk0 = clock64();
-		if (t + kRound < n) prefetch_list(cl, lb, co, t + kRound);
+		if (t + kListRound < n) prefetch_list(cl, lb, co, t + kListRound);
 		int32_t maxrank = -1, local = 0;
 		int nc = 0, nl = 0;
 		int4 me = make_int4(0, 0, 0, 0);
@@ -1101,11 +1134,10 @@ __global__ void __launch_bounds__(kBigThreads) greedy_list_kernel(const LevelNod
 		// ---- D: publish
 		long long clk4 = clock64();
 		const bool acc = valid && vstate[tid] == 1;
-		unsigned long long total;
-		unsigned long long pre;
+		uint32_t total;
+		uint32_t pre;
 		{
-			BlockScratch& bs = *reinterpret_cast<BlockScratch*>(R.warp_sums);
-			pre = block_scan_u64(acc ? 1ull : 0ull, total, bs);
+			pre = list_block_scan(acc ? 1u : 0u, total, R.warp_sums);
 		}
 		if (valid) {
 			const int32_t rank = cnt0 + (int32_t)pre;
@@ -1368,10 +1400,8 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 	// CTA kernel on a forked stream
 	cudaStream_t side = nullptr;
 	cudaEvent_t fork = nullptr, join = nullptr;
-	if (d_cta && d_warp) {
-		PCG_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
-		PCG_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-		PCG_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+	if (d_cta && d_warp && mem.arena()) {
+		side = mem.arena()->side_stream(fork, join);
 		PCG_CUDA(cudaEventRecord(fork, s));
 		PCG_CUDA(cudaStreamWaitEvent(side, fork, 0));
 	}
@@ -1380,10 +1410,10 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 		const int nc = (int)cta_nodes.size();
 		if (mode == 0) {
 			PCG_CUDA(cudaFuncSetAttribute(greedy_list_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_list_kernel<0><<<nc, kBigThreads, smem, s>>>(nodes, d_cta, 0, pp, lb, ga, cl, srank, st);
+			greedy_list_kernel<0><<<nc, kListThreads, smem, s>>>(nodes, d_cta, 0, pp, lb, ga, cl, srank, st);
 		} else {
 			PCG_CUDA(cudaFuncSetAttribute(greedy_list_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_list_kernel<1><<<nc, kBigThreads, smem, s>>>(nodes, d_cta, 0, pp, lb, ga, cl, srank, st);
+			greedy_list_kernel<1><<<nc, kListThreads, smem, s>>>(nodes, d_cta, 0, pp, lb, ga, cl, srank, st);
 		}
 		PCG_LAUNCHED();
 	}
@@ -1400,9 +1430,6 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 	if (side) {
 		PCG_CUDA(cudaEventRecord(join, side));
 		PCG_CUDA(cudaStreamWaitEvent(s, join, 0));
-		cudaEventDestroy(fork);
-		cudaEventDestroy(join);
-		cudaStreamDestroy(side);
 	}
 	mem.free(srank);
 	if (d_cta) mem.free(d_cta);
