@@ -45,7 +45,7 @@ WORKLOAD = {"workload": "hotspots-50M", "points": 50_000_000, "las": "1.4", "poi
 REF_SAMPLE_POINTS = 2_000_000
 # DRAM bytes (read + write) per candidate of the acceptance kernel, from the
 # ncu capture summarised in profiles/accept_hotspots-5M_poisson.md
-ACCEPT_DRAM_BYTES_PER_CANDIDATE = None
+ACCEPT_DRAM_BYTES_PER_CANDIDATE = 225.6
 MEASURED_PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
 
 
