@@ -107,6 +107,7 @@ typedef struct pcg_stats {
 	double ms_lists;              /* device time of the conflict-list builds
 	                                 (part of ms_greedy)                     */
 	int64_t list_entries;         /* conflict-list entries over all levels  */
+	int64_t cluster_nodes;        /* nodes accepted by a cluster of CTAs    */
 } pcg_stats;
 
 typedef struct pcg_result {

@@ -56,7 +56,8 @@ class _Stats(ctypes.Structure):
                 ("ms_d2h", ctypes.c_double), ("ms_host_writers", ctypes.c_double), ("gpu_launches", ctypes.c_int64),
                 ("ms_sort", ctypes.c_double), ("ms_greedy", ctypes.c_double), ("sampled_nodes", ctypes.c_int64),
                 ("candidates", ctypes.c_int64), ("replayed_nodes", ctypes.c_int64),
-                ("replayed_candidates", ctypes.c_int64), ("ms_lists", ctypes.c_double), ("list_entries", ctypes.c_int64)]
+                ("replayed_candidates", ctypes.c_int64), ("ms_lists", ctypes.c_double), ("list_entries", ctypes.c_int64),
+                ("cluster_nodes", ctypes.c_int64)]
 
 
 class _Result(ctypes.Structure):

@@ -482,6 +482,7 @@ struct Converter {
 		res.stats.escalated_pairs = (int64_t)hst.escalated;
 		res.stats.heapsort_fallbacks = (int64_t)hst.heapsorts;
 		res.stats.list_entries = (int64_t)hst.list_entries;
+		res.stats.cluster_nodes = (int64_t)hst.cluster_nodes;
 		res.stats.ms_sampling = ms_since(t_samp);
 
 		// ------------------------------------------------ completion order
@@ -730,7 +731,7 @@ struct Converter {
 					const int num_grid = (int)order2.size();
 					for (int i = num_big; i < K; i++) (dense[order[i]] ? order2 : warp_list).push_back(order[i]);
 					list_nodes = (int)(cta_list.size() + warp_list.size());
-					launch_greedy_lists(mode, d_nodes, cta_list, warp_list, pps, lb, hkeys, hvals, axyz, akey, anext, apos, cl, d_st, mem);
+					launch_greedy_lists(mode, d_nodes, cta_list, warp_list, pps, lb, hkeys, hvals, axyz, akey, anext, apos, cl, d_st, mem, ln);
 					if (!order2.empty()) {
 						int32_t* d_order2 = upload(order2, mem);
 						launch_greedy(mode, guard, d_nodes, d_order2, (int)order2.size(), co.X, co.Y, co.Z, pps, lb, hkeys, hvals, axyz, akey,

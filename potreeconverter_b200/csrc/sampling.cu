@@ -26,6 +26,7 @@
 //  * shuffle_leaves     -- std::shuffle(..., std::default_random_engine(seed))
 //    of sampler_random.h:97-118, libstdc++'s two-draws-per-call variant.
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -1178,6 +1179,237 @@ __global__ void __launch_bounds__(kListThreads) greedy_list_kernel(const LevelNo
 }
 
 
+// Greedy acceptance for the largest nodes on a cluster of kClusterCtas CTAs
+// (4 x 1024 threads): a super-round decides 4096 candidates, CTA k holding
+// candidates [1024k, 1024k + 1024) of it. Each CTA keeps its candidates'
+// states in its own shared memory; a candidate's conflicts inside the
+// super-round (always with lower indices) are read from the owning CTA's
+// shared memory through the cluster's distributed shared memory. Passes,
+// the in-order warp (CTA 0, warp 0, reading and writing all four CTAs'
+// states) and the rank prefix are separated by cluster barriers, which
+// every CTA reaches the same number of times.
+constexpr int kClusterCtas = 4;
+constexpr int kSuper = kListRound * kClusterCtas;  // 4096
+constexpr int64_t kClusterMinCandidates = 65536;
+static_assert(kSuper <= 32767, "conflict indices are int16");
+
+struct ClusterRound {
+	int32_t maxrank[kListRound];
+	int32_t local[kListRound];
+	int16_t conf[kListRound][kListCap];  // indices inside the super-round
+	uint8_t nconf[kListRound];
+	uint8_t state[kListRound];   // 0 undecided, 1 accepted, 2 rejected
+	uint8_t old[kListRound];     // old-window status as in ListRound
+	uint32_t warp_sums[kListWarps];
+	int32_t changed[2];          // per pass parity: this CTA changed a state
+	int32_t left;                // this CTA has undecided candidates
+	int32_t total;               // accepted in this CTA's part of the super-round
+};
+
+template <int MODE>
+__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThreads, 1)
+    greedy_list_cluster_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order, PosParamsS pp, LevelBuffers lb,
+                               GreedyArgs ga, ConflictLists cl, int32_t* __restrict__ srank, SampleStats* st) {
+	namespace cgr = cooperative_groups;
+	cgr::cluster_group cluster = cgr::this_cluster();
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	ClusterRound& R = *reinterpret_cast<ClusterRound*>(smem_raw);
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int crank = (int)cluster.block_rank();
+	// another CTA's round state (distributed shared memory)
+	auto peer = [&](int r) { return cluster.map_shared_rank(&R, r); };
+	const LevelNode nd = nodes[order[blockIdx.x / kClusterCtas]];
+	const int64_t n = nd.count, co = nd.cand_off;
+	uint64_t* hk = ga.hkeys + nd.hash_off;
+	int32_t* hh = ga.hheads + nd.hash_off;
+	if (MODE == 1) {
+		for (int64_t i = crank * kListThreads + tid; i < nd.hash_cap; i += kSuper) { hk[i] = EMPTY_KEY; hh[i] = -1; }
+	}
+	CellGrid g;
+	g.min[0] = nd.min[0]; g.min[1] = nd.min[1]; g.min[2] = nd.min[2];
+	g.inv = 1.0 / (2.0 * nd.spacing * 1.000001);
+	int32_t cnt0 = 0;  // accepted before the super-round, the same in every CTA
+	if (crank == 0 && tid == 0) atomicAdd(&st->cluster_nodes, 1ull);
+	cluster.sync();
+	for (int64_t r0 = 0; r0 < n; r0 += kSuper) {
+		const int idx = crank * kListThreads + tid;  // index inside the super-round
+		const int64_t t = r0 + idx;
+		const bool valid = t < n;
+		const int nr = (int)((n - r0) < kSuper ? (n - r0) : kSuper);
+		// ---- A: the candidate's list
+		if (t + kSuper < n) prefetch_list(cl, lb, co, t + kSuper);
+		int32_t maxrank = -1, local = 0;
+		int nc = 0, nl = 0;
+		int4 me = make_int4(0, 0, 0, 0);
+		if (valid) {
+			me = lb.cq[co + t];
+			local = me.w;
+			nl = cl.count[co + t];
+		}
+		{
+			const int4* lp = reinterpret_cast<const int4*>(cl.entries + (co + t) * (int64_t)kListCap);
+			const int wmax = (int)__reduce_max_sync(FULL, (unsigned)nl);
+			for (int w = 0; 4 * w < wmax; w++) {
+				const int4 v = 4 * w < nl ? lp[w] : make_int4(0, 0, 0, 0);
+				const int32_t u4[4] = {v.x, v.y, v.z, v.w};
+				int32_t rk4[4];
+#pragma unroll
+				for (int k = 0; k < 4; k++) rk4[k] = (4 * w + k < nl && u4[k] < r0) ? srank[co + u4[k]] : -1;
+#pragma unroll
+				for (int k = 0; k < 4; k++) {
+					if (4 * w + k < nl) {
+						if (u4[k] < r0) maxrank = rk4[k] > maxrank ? rk4[k] : maxrank;
+						else R.conf[tid][nc++] = (int16_t)(u4[k] - r0);
+					}
+				}
+			}
+		}
+		R.maxrank[tid] = maxrank;
+		R.local[tid] = local;
+		R.nconf[tid] = (uint8_t)nc;
+		R.state[tid] = valid ? 0 : 2;
+		{
+			uint8_t os = 0;
+			if (maxrank >= 0) {
+				if (MODE == 1) os = 1;
+				else if (maxrank >= cnt0 + idx - 10001) os = 1;       // conflicts whatever was accepted before it
+				else if (maxrank < cnt0 - 10001) os = 0;              // outside the window in any case
+				else os = 2;
+			}
+			R.old[tid] = os;
+		}
+		cluster.sync();
+		// ---- C1: parallel passes over the cluster
+		for (int pass = 0; pass < 64; pass++) {
+			bool changed = false;
+			if (valid && R.state[tid] == 0) {
+				const uint8_t os = R.old[tid];
+				uint8_t dec = 0;
+				if (os == 1) {
+					dec = 2;
+				} else {
+					bool any_acc = false, all_done = true;
+					for (int e = 0; e < R.nconf[tid]; e++) {
+						const int j = R.conf[tid][e];
+						const uint8_t sj = *(volatile uint8_t*)&peer(j / kListRound)->state[j % kListRound];
+						any_acc |= sj == 1;
+						all_done &= sj != 0;
+					}
+					if (any_acc) dec = 2;
+					else if (all_done && os == 0) dec = 1;
+				}
+				if (dec) {
+					*(volatile uint8_t*)&R.state[tid] = dec;
+					changed = true;
+				}
+			}
+			const int any = __syncthreads_or(changed);
+			if (tid == 0) R.changed[pass & 1] = any;
+			cluster.sync();
+			int all = 0;
+#pragma unroll
+			for (int r = 0; r < kClusterCtas; r++) all |= *(volatile int32_t*)&peer(r)->changed[pass & 1];
+			if (!all) {
+				if (tid == 0 && crank == 0) atomicAdd(&st->passes, (unsigned long long)pass + 1);
+				break;
+			}
+		}
+		const int left_here = __syncthreads_or(valid && R.state[tid] == 0);
+		if (tid == 0) R.left = left_here;
+		cluster.sync();
+		int left = 0;
+#pragma unroll
+		for (int r = 0; r < kClusterCtas; r++) left |= *(volatile int32_t*)&peer(r)->left;
+		if (crank == 0 && tid == 0) {
+			atomicAdd(&st->rounds, 1ull);
+			if (left) atomicAdd(&st->serial, 1ull);
+		}
+		// ---- C2: one warp decides the rest in order
+		if (left && crank == 0 && warp == 0) {
+			int32_t cnt = cnt0;
+			const uint32_t ltm = lanemask_lt();
+			for (int cb = 0; cb < nr; cb += 32) {
+				const int i = cb + lane;
+				const bool v = i < nr;
+				ClusterRound* Ri = peer((v ? i : 0) / kListRound);
+				const int li = (v ? i : 0) % kListRound;
+				const uint8_t si = v ? *(volatile uint8_t*)&Ri->state[li] : 2;
+				const bool undec = v && si == 0;
+				uint32_t accmask = __ballot_sync(FULL, v && si == 1);
+				if (__ballot_sync(FULL, undec) != 0) {
+					bool prev_conflict = false;
+					uint32_t mask = 0;
+					if (undec) {
+						const int ncf = Ri->nconf[li];
+						for (int e = 0; e < ncf; e++) {
+							const int j = Ri->conf[li][e];
+							if (j < cb) prev_conflict |= *(volatile uint8_t*)&peer(j / kListRound)->state[j % kListRound] == 1;
+							else mask |= 1u << (j - cb);
+						}
+					}
+					const int nvalid = nr - cb < 32 ? nr - cb : 32;
+					for (int b = 0; b < nvalid; b++) {
+						bool dec = false;
+						const bool ub = __shfl_sync(FULL, undec, b);
+						if (!ub) continue;
+						if (lane == b) {
+							const int32_t m_i = cnt + __popc(accmask & ltm);
+							const int32_t mr = Ri->maxrank[li];
+							const bool old_conflict = mr >= 0 && (MODE == 1 || mr >= m_i - 10001);
+							dec = !old_conflict && !prev_conflict && !(mask & accmask);
+							*(volatile uint8_t*)&Ri->state[li] = dec ? 1 : 2;
+						}
+						dec = __shfl_sync(FULL, dec, b);
+						if (dec) accmask |= 1u << b;
+					}
+				}
+				cnt += __popc(accmask);
+				__syncwarp();
+			}
+		}
+		cluster.sync();
+		// ---- D: ranks across the cluster, publish
+		const bool acc = valid && R.state[tid] == 1;
+		uint32_t total;
+		const uint32_t pre = list_block_scan(acc ? 1u : 0u, total, R.warp_sums);
+		if (tid == 0) R.total = (int32_t)total;
+		cluster.sync();
+		int32_t before = 0, all_acc = 0;
+#pragma unroll
+		for (int r = 0; r < kClusterCtas; r++) {
+			const int32_t tr = *(volatile int32_t*)&peer(r)->total;
+			if (r < crank) before += tr;
+			all_acc += tr;
+		}
+		if (valid) {
+			const int32_t rank = cnt0 + before + (int32_t)pre;
+			srank[co + t] = acc ? rank : -1;
+			lb.accepted[co + local] = acc ? 1 : 0;
+			if (acc) {
+				lb.acc_rank[co + local] = rank;
+				if (MODE == 1) {
+					const int64_t slot = co + rank;
+					const double x = ((double)me.x * pp.scale[0]) + pp.offset[0];
+					const double y = ((double)me.y * pp.scale[1]) + pp.offset[1];
+					const double z = ((double)me.z * pp.scale[2]) + pp.offset[2];
+					ga.axyz[3 * slot] = x;
+					ga.axyz[3 * slot + 1] = y;
+					ga.axyz[3 * slot + 2] = z;
+					ga.akey[slot] = lb.keys[co + t];
+					ga.apos[slot] = (int32_t)t;
+					int c[3];
+					double fr[3];
+					cell_of(g, x, y, z, c, fr);
+					if (!hash_push(hk, hh, ga.anext + co, nd.hash_cap, cell_key(c[0], c[1], c[2]), rank)) atomicAdd(&st->timeouts, 1ull);
+				}
+			}
+		}
+		cnt0 += all_acc;
+		// the next super-round rewrites states, flags and totals other CTAs read
+		cluster.sync();
+	}
+}
+
 // Greedy acceptance from conflict lists for the smaller nodes, one warp per
 // node, 32 candidates per step. Conflicts with earlier steps come from
 // srank; inside a step they are a lane mask, resolved by ballot passes (a
@@ -1385,40 +1617,68 @@ void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int3
 
 void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int32_t>& cta_nodes, const std::vector<int32_t>& warp_nodes,
                          const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads, double* acc_xyz,
-                         double* acc_key, int32_t* acc_next, int32_t* acc_pos, const ConflictLists& cl, SampleStats* st, DeviceMem& mem) {
+                         double* acc_key, int32_t* acc_next, int32_t* acc_pos, const ConflictLists& cl, SampleStats* st, DeviceMem& mem,
+                         const std::vector<LevelNode>& ln) {
 	if (lb.M == 0 || (cta_nodes.empty() && warp_nodes.empty())) return;
 	GreedyArgs ga{hash_keys, hash_heads, acc_xyz, acc_key, acc_next, acc_pos};
 	cudaStream_t s = mem.stream();
+	// the largest nodes (cta_nodes is largest first) on a cluster each, the
+	// other CTA nodes on one CTA, the rest on a warp
+	std::vector<int32_t> clu, one;
+	for (int32_t k : cta_nodes) (ln[k].count >= kClusterMinCandidates ? clu : one).push_back(k);
 	int32_t* srank = mem.alloc<int32_t>((size_t)lb.M);
-	int32_t* d_cta = cta_nodes.empty() ? nullptr : mem.alloc<int32_t>(cta_nodes.size());
+	int32_t* d_clu = clu.empty() ? nullptr : mem.alloc<int32_t>(clu.size());
+	int32_t* d_one = one.empty() ? nullptr : mem.alloc<int32_t>(one.size());
 	int32_t* d_warp = warp_nodes.empty() ? nullptr : mem.alloc<int32_t>(warp_nodes.size());
 	int* counter = mem.alloc<int>(1);
-	if (d_cta) PCG_CUDA(cudaMemcpyAsync(d_cta, cta_nodes.data(), cta_nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+	if (d_clu) PCG_CUDA(cudaMemcpyAsync(d_clu, clu.data(), clu.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+	if (d_one) PCG_CUDA(cudaMemcpyAsync(d_one, one.data(), one.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 	if (d_warp) PCG_CUDA(cudaMemcpyAsync(d_warp, warp_nodes.data(), warp_nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 	PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), s));
-	// the two node sets are independent: the warp kernel runs beside the
-	// CTA kernel on a forked stream
+	// the node sets are independent: the smaller ones run beside the
+	// largest on a forked stream
 	cudaStream_t side = nullptr;
 	cudaEvent_t fork = nullptr, join = nullptr;
-	if (d_cta && d_warp && mem.arena()) {
+	const int sets = (d_clu ? 1 : 0) + (d_one ? 1 : 0) + (d_warp ? 1 : 0);
+	if (sets > 1 && mem.arena()) {
 		side = mem.arena()->side_stream(fork, join);
 		PCG_CUDA(cudaEventRecord(fork, s));
 		PCG_CUDA(cudaStreamWaitEvent(side, fork, 0));
 	}
-	if (d_cta) {
+	cudaStream_t next = s;  // the first set runs on s, the others on the side stream
+	auto stream_for_set = [&]() {
+		cudaStream_t r = next;
+		if (side) next = side;
+		return r;
+	};
+	if (d_clu) {
+		const size_t smem = sizeof(ClusterRound);
+		const unsigned grid = (unsigned)(clu.size() * kClusterCtas);
+		cudaStream_t cs = stream_for_set();
+		if (mode == 0) {
+			PCG_CUDA(cudaFuncSetAttribute(greedy_list_cluster_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			greedy_list_cluster_kernel<0><<<grid, kListThreads, smem, cs>>>(nodes, d_clu, pp, lb, ga, cl, srank, st);
+		} else {
+			PCG_CUDA(cudaFuncSetAttribute(greedy_list_cluster_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			greedy_list_cluster_kernel<1><<<grid, kListThreads, smem, cs>>>(nodes, d_clu, pp, lb, ga, cl, srank, st);
+		}
+		PCG_LAUNCHED();
+	}
+	if (d_one) {
 		const size_t smem = sizeof(ListRound);
-		const int nc = (int)cta_nodes.size();
+		const int nc = (int)one.size();
+		cudaStream_t cs = stream_for_set();
 		if (mode == 0) {
 			PCG_CUDA(cudaFuncSetAttribute(greedy_list_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_list_kernel<0><<<nc, kListThreads, smem, s>>>(nodes, d_cta, 0, pp, lb, ga, cl, srank, st);
+			greedy_list_kernel<0><<<nc, kListThreads, smem, cs>>>(nodes, d_one, 0, pp, lb, ga, cl, srank, st);
 		} else {
 			PCG_CUDA(cudaFuncSetAttribute(greedy_list_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_list_kernel<1><<<nc, kListThreads, smem, s>>>(nodes, d_cta, 0, pp, lb, ga, cl, srank, st);
+			greedy_list_kernel<1><<<nc, kListThreads, smem, cs>>>(nodes, d_one, 0, pp, lb, ga, cl, srank, st);
 		}
 		PCG_LAUNCHED();
 	}
 	if (d_warp) {
-		cudaStream_t ws = side ? side : s;
+		cudaStream_t ws = stream_for_set();
 		const int nw = (int)warp_nodes.size();
 		int blocks = (int)ceil_div(nw, kWarpsPerBlock);
 		const int cap = sm_count() * 16;
@@ -1432,7 +1692,8 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 		PCG_CUDA(cudaStreamWaitEvent(s, join, 0));
 	}
 	mem.free(srank);
-	if (d_cta) mem.free(d_cta);
+	if (d_clu) mem.free(d_clu);
+	if (d_one) mem.free(d_one);
 	if (d_warp) mem.free(d_warp);
 	mem.free(counter);
 }

@@ -60,6 +60,7 @@ struct SampleStats {
 	unsigned long long passes;     // parallel decision passes over all rounds
 	unsigned long long serial;     // rounds that needed the in-order decision warp
 	unsigned long long list_entries; // conflict-list entries written
+	unsigned long long cluster_nodes; // nodes accepted by a CTA cluster
 	unsigned long long cycles[7];  // CTA greedy: SM cycles of thread 0 in phases A, B, C1, C2, D; cells read past 3 and 7 points
 };
 
@@ -120,11 +121,13 @@ void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int3
                    const int32_t* Z, const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads,
                    double* acc_xyz, double* acc_key, int32_t* acc_next, int32_t* acc_pos, SampleStats* st, DeviceMem& mem,
                    GreedyArena* grid, int node_begin = 0, int node_end = -1, int num_big = 0);
-// acceptance from conflict lists: cta_nodes get a CTA each (largest first),
+// acceptance from conflict lists: cta_nodes (largest first) get a cluster of
+// CTAs each when they hold at least 65,536 candidates, else one CTA;
 // warp_nodes a warp each
 void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int32_t>& cta_nodes, const std::vector<int32_t>& warp_nodes,
                          const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads, double* acc_xyz,
-                         double* acc_key, int32_t* acc_next, int32_t* acc_pos, const ConflictLists& cl, SampleStats* st, DeviceMem& mem);
+                         double* acc_key, int32_t* acc_next, int32_t* acc_pos, const ConflictLists& cl, SampleStats* st, DeviceMem& mem,
+                         const std::vector<LevelNode>& ln);
 // poisson_average colour sums: new packed colour per accepted candidate
 void launch_average_colors(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
                            LevelBuffers& lb, const uint64_t* hash_keys, const int32_t* hash_heads, const double* acc_xyz,

@@ -294,3 +294,19 @@ def duplicates(n: int, seed: int, extent: float = 100.0, dup_fraction: float = 0
 
 
 GENERATORS["duplicates"] = duplicates
+
+
+def cube(n: int, seed: int, extent: float = 1000.0) -> bytes:
+    """Uniform points filling a cube, LAS 1.2 point format 2. Every octree
+    level stays volumetric, so the upper nodes gather hundreds of thousands
+    of candidates even for a cloud of a few hundred thousand points."""
+    rng = np.random.default_rng(seed)
+    xs = rng.uniform(0, extent, n)
+    ys = rng.uniform(0, extent, n)
+    zs = rng.uniform(0, extent, n)
+    X, Y, Z = _quantize(xs), _quantize(ys), _quantize(zs)
+    attrs = _common_attrs(rng, n, zs)
+    return write_las(X, Y, Z, attrs, pdrf=2, version_minor=2)
+
+
+GENERATORS["cube"] = cube

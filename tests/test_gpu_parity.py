@@ -50,6 +50,19 @@ def test_matches_oracle_on_fresh_inputs(gpu_ctx, oracle, kind, n, seed, method):
         assert _bytes(conv, f) == exp[f], f
 
 
+@pytest.mark.parametrize("method", ["poisson", "poisson_average"])
+def test_cluster_acceptance_matches_oracle(gpu_ctx, oracle, method):
+    # a volumetric cloud: its upper nodes hold enough candidates to be
+    # accepted by a cluster of CTAs (at least 65,536 candidates per node)
+    from potreeconverter_b200 import synth
+    las = synth.generate("cube", 400_000, 41)
+    exp = oracle.convert(las, method, name="cube")
+    conv = gpu_ctx.convert(las, method=method, name="cube")
+    assert conv.stats["cluster_nodes"] > 0
+    for f in FILES:
+        assert _bytes(conv, f) == exp[f], f
+
+
 def test_out_of_box_point_is_reported(gpu_ctx):
     from potreeconverter_b200 import synth
     import struct

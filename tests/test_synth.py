@@ -10,7 +10,7 @@ import pytest
 from potreeconverter_b200 import synth
 
 
-@pytest.mark.parametrize("kind", ["terrain", "hotspots", "lattice", "strips", "duplicates"])
+@pytest.mark.parametrize("kind", ["terrain", "hotspots", "lattice", "strips", "duplicates", "cube"])
 def test_header_box_is_exact(kind):
     las = synth.generate(kind, 20000, 11)
     assert las == synth.generate(kind, 20000, 11)
