@@ -1237,6 +1237,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 		const bool valid = t < n;
 		const int nr = (int)((n - r0) < kSuper ? (n - r0) : kSuper);
 		// ---- A: the candidate's list
+		const long long clk0 = clock64();
 		if (t + kSuper < n) prefetch_list(cl, lb, co, t + kSuper);
 		int32_t maxrank = -1, local = 0;
 		int nc = 0, nl = 0;
@@ -1279,41 +1280,50 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 			R.old[tid] = os;
 		}
 		cluster.sync();
-		// ---- C1: parallel passes over the cluster
-		for (int pass = 0; pass < 64; pass++) {
-			bool changed = false;
-			if (valid && R.state[tid] == 0) {
-				const uint8_t os = R.old[tid];
-				uint8_t dec = 0;
-				if (os == 1) {
-					dec = 2;
-				} else {
-					bool any_acc = false, all_done = true;
-					for (int e = 0; e < R.nconf[tid]; e++) {
-						const int j = R.conf[tid][e];
-						const uint8_t sj = *(volatile uint8_t*)&peer(j / kListRound)->state[j % kListRound];
-						any_acc |= sj == 1;
-						all_done &= sj != 0;
+		const long long clk1 = clock64();
+		// ---- C1: parallel passes. Decisions only go from undecided to final,
+		// so a stale read of another CTA's state only delays a decision:
+		// each CTA repeats local passes (block barriers) while it makes
+		// progress, then the cluster barrier publishes whether any CTA did;
+		// the fixpoint is a cluster round in which none did.
+		int passes = 0;
+		for (int gpass = 0; gpass < 64; gpass++) {
+			int progressed = 0;
+			for (int lp = 0; lp < 64; lp++) {
+				bool changed = false;
+				if (valid && R.state[tid] == 0) {
+					const uint8_t os = R.old[tid];
+					uint8_t dec = 0;
+					if (os == 1) {
+						dec = 2;
+					} else {
+						bool any_acc = false, all_done = true;
+						for (int e = 0; e < R.nconf[tid]; e++) {
+							const int j = R.conf[tid][e];
+							const uint8_t sj = *(volatile uint8_t*)&peer(j / kListRound)->state[j % kListRound];
+							any_acc |= sj == 1;
+							all_done &= sj != 0;
+						}
+						if (any_acc) dec = 2;
+						else if (all_done && os == 0) dec = 1;
 					}
-					if (any_acc) dec = 2;
-					else if (all_done && os == 0) dec = 1;
+					if (dec) {
+						*(volatile uint8_t*)&R.state[tid] = dec;
+						changed = true;
+					}
 				}
-				if (dec) {
-					*(volatile uint8_t*)&R.state[tid] = dec;
-					changed = true;
-				}
+				passes++;
+				if (!__syncthreads_or(changed)) break;
+				progressed = 1;
 			}
-			const int any = __syncthreads_or(changed);
-			if (tid == 0) R.changed[pass & 1] = any;
+			if (tid == 0) R.changed[gpass & 1] = progressed;
 			cluster.sync();
 			int all = 0;
 #pragma unroll
-			for (int r = 0; r < kClusterCtas; r++) all |= *(volatile int32_t*)&peer(r)->changed[pass & 1];
-			if (!all) {
-				if (tid == 0 && crank == 0) atomicAdd(&st->passes, (unsigned long long)pass + 1);
-				break;
-			}
+			for (int r = 0; r < kClusterCtas; r++) all |= *(volatile int32_t*)&peer(r)->changed[gpass & 1];
+			if (!all) break;
 		}
+		if (tid == 0 && crank == 0) atomicAdd(&st->passes, (unsigned long long)passes);
 		const int left_here = __syncthreads_or(valid && R.state[tid] == 0);
 		if (tid == 0) R.left = left_here;
 		cluster.sync();
@@ -1324,6 +1334,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 			atomicAdd(&st->rounds, 1ull);
 			if (left) atomicAdd(&st->serial, 1ull);
 		}
+		const long long clk2 = clock64();
 		// ---- C2: one warp decides the rest in order
 		if (left && crank == 0 && warp == 0) {
 			int32_t cnt = cnt0;
@@ -1368,6 +1379,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 			}
 		}
 		cluster.sync();
+		const long long clk3 = clock64();
 		// ---- D: ranks across the cluster, publish
 		const bool acc = valid && R.state[tid] == 1;
 		uint32_t total;
@@ -1407,6 +1419,13 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 		cnt0 += all_acc;
 		// the next super-round rewrites states, flags and totals other CTAs read
 		cluster.sync();
+		if (crank == 0 && tid == 0) {
+			const long long clk4 = clock64();
+			atomicAdd(&st->cycles[0], (unsigned long long)(clk1 - clk0));
+			atomicAdd(&st->cycles[2], (unsigned long long)(clk2 - clk1));
+			atomicAdd(&st->cycles[3], (unsigned long long)(clk3 - clk2));
+			atomicAdd(&st->cycles[4], (unsigned long long)(clk4 - clk3));
+		}
 	}
 }
 
