@@ -422,10 +422,13 @@ __global__ void __launch_bounds__(kBigThreads) sort_single_big_kernel(double* ke
 // candidates no longer run on a single CTA. Both halves of a partition go on
 // with the decremented depth budget (std::__introsort_loop), so the order in
 // which disjoint segments are processed does not change the result.
-// Segments at most kWideMin long finish on one CTA (>= kBigSortMin elements)
-// or one warp each, with their remaining depth budget; <= 16-element
-// segments go to the final insertion pass.
-constexpr int64_t kWideMin = 32768;
+// Segments at most kWideMin long finish on one warp each with their
+// remaining depth budget (a whole CTA for a segment of exactly kBigSortMin or
+// one whose budget is spent, which is heap-sorted); <= 16-element segments
+// go to the final insertion pass. kWideMin = 4096 measured fastest: the
+// rounds are HBM-efficient, a CTA replaying a segment in global memory is
+// not.
+constexpr int64_t kWideMin = 4096;
 constexpr int kWideThreads = 256;
 constexpr int kWideWarps = kWideThreads / 32;
 constexpr int kWideSteps = 16;
