@@ -126,14 +126,15 @@ __global__ void flags_to_u32_kernel(const uint8_t* __restrict__ f, int64_t n, ui
 }
 
 __global__ void split_kernel(const uint8_t* __restrict__ accepted, const uint32_t* __restrict__ pre, int64_t n, const uint32_t* __restrict__ ids,
-                             const uint64_t* __restrict__ cols, uint32_t* __restrict__ acc_ids, uint64_t* __restrict__ acc_cols,
-                             uint32_t* __restrict__ rej_ids) {
+                             const uint64_t* __restrict__ cols, const int4* __restrict__ rec, uint32_t* __restrict__ acc_ids,
+                             uint64_t* __restrict__ acc_cols, int4* __restrict__ acc_rec, uint32_t* __restrict__ rej_ids) {
 	int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= n) return;
 	uint32_t a = pre[j];
 	if (accepted[j]) {
 		acc_ids[a] = ids[j];
 		if (acc_cols) acc_cols[a] = cols[j];
+		if (acc_rec) acc_rec[a] = rec[j];
 	} else if (rej_ids) {
 		rej_ids[j - a] = ids[j];
 	}
@@ -177,15 +178,16 @@ void launch_gather_u32(const uint32_t* src, const int64_t* idx, int64_t n, uint3
 	PCG_LAUNCHED();
 }
 
-void launch_split(const uint8_t* accepted, int64_t n, const uint32_t* ids, const uint64_t* cols, uint32_t* pre, uint32_t* acc_ids,
-                  uint64_t* acc_cols, uint32_t* rej_ids, DeviceMem& mem) {
+void launch_split(const uint8_t* accepted, int64_t n, const uint32_t* ids, const uint64_t* cols, const int4* rec, uint32_t* pre,
+                  uint32_t* acc_ids, uint64_t* acc_cols, int4* acc_rec, uint32_t* rej_ids, DeviceMem& mem) {
 	if (n == 0) return;
 	uint32_t* f = mem.alloc<uint32_t>(n);
 	flags_to_u32_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(accepted, n, f);
 	PCG_LAUNCHED();
 	exclusive_scan_u32(f, pre, n, true, mem);
 	mem.free(f);
-	split_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(accepted, pre, n, ids, cols, acc_ids, acc_cols, rej_ids);
+	split_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(accepted, pre, n, ids, cols, rec, acc_ids, acc_cols, acc_rec,
+	                                                                 rej_ids);
 	PCG_LAUNCHED();
 }
 

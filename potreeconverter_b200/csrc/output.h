@@ -18,9 +18,10 @@ void launch_write_payloads(const uint8_t* d_recs, const DecodeParams& p, const s
 void launch_fill_colors(const uint8_t* d_recs, int rec_len, int src_rgb, const uint32_t* ids, int64_t n, uint64_t* cols, DeviceMem& mem);
 void launch_gather_u32(const uint32_t* src, const int64_t* idx, int64_t n, uint32_t* dst, DeviceMem& mem);
 // Stable split of candidates by accepted flag: pre = exclusive prefix of the
-// flags (n + 1 entries), accepted ids (and colours) compacted in order into
-// acc_ids, rejected ids into rej_ids (skipped when rej_ids is null).
-void launch_split(const uint8_t* accepted, int64_t n, const uint32_t* ids, const uint64_t* cols, uint32_t* pre, uint32_t* acc_ids,
-                  uint64_t* acc_cols, uint32_t* rej_ids, DeviceMem& mem);
+// flags (n + 1 entries), accepted ids (and colours, records) compacted in
+// order into acc_ids (acc_cols, acc_rec), rejected ids into rej_ids (skipped
+// when null).
+void launch_split(const uint8_t* accepted, int64_t n, const uint32_t* ids, const uint64_t* cols, const int4* rec, uint32_t* pre,
+                  uint32_t* acc_ids, uint64_t* acc_cols, int4* acc_rec, uint32_t* rej_ids, DeviceMem& mem);
 
 }  // namespace pcg

@@ -59,6 +59,7 @@ struct TNode {
 	// current buffer (what the parent's sampler sees)
 	const uint32_t* buf_ids = nullptr;
 	const uint64_t* buf_cols = nullptr;
+	const int4* buf_rec = nullptr;   // (X, Y, Z, -) per buffered id (poisson samplers)
 	int64_t buf_count = 0;
 	// state after the parent's sampling
 	const uint32_t* fin_ids = nullptr;
@@ -456,10 +457,17 @@ struct Converter {
 			leaf_cols = mem.alloc<uint64_t>(N);
 			launch_fill_colors(d_recs, info.record_length, p.src_rgb, ids, N, leaf_cols, mem);
 		}
+		int4* leaf_rec = nullptr;
+		if (method != PCG_RANDOM) {
+			// coordinates travel with the ids from here on
+			leaf_rec = mem.alloc<int4>(N);
+			launch_gather_records(leaf_ids, N, co.X, co.Y, co.Z, leaf_rec, mem);
+		}
 		for (auto& n : tree.nodes) {
 			if (!n.has_children()) {
 				n.buf_ids = leaf_ids + n.leaf_start;
 				n.buf_cols = leaf_cols ? leaf_cols + n.leaf_start : nullptr;
+				n.buf_rec = leaf_rec ? leaf_rec + n.leaf_start : nullptr;
 				n.buf_count = n.leaf_count;
 			}
 		}
@@ -519,15 +527,16 @@ struct Converter {
 		launch_write_payloads(d_recs, p, items, d_items, d_out, mem);
 		PCG_CUDA(cudaStreamSynchronize(stream));
 		res.stats.ms_output = ms_since(t_out);
+		// the attribute statistics first (small), then octree.bin, whose copy
+		// runs while the host writes hierarchy.bin and metadata.json
+		auto stats_dev = download(co.stats, MAX_ATTRS, stream);
+		auto hist = download(co.histogram, 256, stream);
 		auto t_d2h = Clock::now();
 		if (!keep_on_device) {
 			res.octree = host_buffers ? host_buffers->take(res.octree_size) : nullptr;
 			if (!res.octree) PCG_CUDA(cudaMallocHost((void**)&res.octree, res.octree_size ? res.octree_size : 1));
 			if (res.octree_size) PCG_CUDA(cudaMemcpyAsync(res.octree, d_out, res.octree_size, cudaMemcpyDeviceToHost, stream));
 		}
-		auto stats_dev = download(co.stats, MAX_ATTRS, stream);
-		auto hist = download(co.histogram, 256, stream);
-		res.stats.ms_d2h = ms_since(t_d2h);
 
 		// ---------------------------------------------------- host writers
 		auto t_w = Clock::now();
@@ -545,6 +554,8 @@ struct Converter {
 		res.metadata = build_metadata(job.name ? job.name : "", job.projection ? job.projection : "", N, first_chunk, octree_depth, s,
 		                              astats, base_spacing);
 		res.stats.ms_host_writers = ms_since(t_w);
+		PCG_CUDA(cudaStreamSynchronize(stream));
+		res.stats.ms_d2h = ms_since(t_d2h);  // the copy, overlapped with the host writers
 		res.stats.num_nodes = (int64_t)recs.size();
 		res.stats.output_points = out_points;
 		res.stats.gpu_launches = g_launch_count;
@@ -627,7 +638,7 @@ struct Converter {
 				int ci = n.child[c];
 				if (ci < 0) continue;
 				TNode& ch = tree.nodes[ci];
-				if (ch.buf_count > 0) items.push_back({ch.buf_ids, ch.buf_cols, M, ch.buf_count, c, k});
+				if (ch.buf_count > 0) items.push_back({ch.buf_ids, ch.buf_cols, ch.buf_rec, M, ch.buf_count, c, k});
 				child_slots.push_back({ci, M, ch.buf_count});
 				M += ch.buf_count;
 			}
@@ -655,6 +666,7 @@ struct Converter {
 		lb.node_of = mem.alloc<int32_t>(M);
 		lb.count_in_child = mem.alloc<int32_t>(M);
 		lb.accepted = mem.alloc<uint8_t>(M);
+		lb.rec = method == PCG_RANDOM ? nullptr : mem.alloc<int4>(M);
 		LevelNode* d_nodes = upload(ln, mem);
 		GatherItem* d_items = upload(items, mem);
 		launch_gather(d_items, (int)items.size(), lb, mem);
@@ -673,8 +685,7 @@ struct Converter {
 			lb.pos = mem.alloc<int32_t>(M);
 			lb.acc_rank = mem.alloc<int32_t>(M);
 			lb.cq = mem.alloc<int4>(M);
-			lb.rec = mem.alloc<int4>(M);
-			launch_keys(d_nodes, co.X, co.Y, co.Z, pps, lb, mem);
+			launch_keys(d_nodes, pps, lb, mem);
 			double* axyz = mem.alloc<double>(3 * M);
 			double* akey = mem.alloc<double>(M);
 			int32_t* anext = mem.alloc<int32_t>(M);
@@ -776,7 +787,7 @@ struct Converter {
 				mem.free(sums);
 			}
 			mem.free(axyz); mem.free(akey); mem.free(anext); mem.free(apos);
-			mem.free(lb.keys); mem.free(lb.perm); mem.free(lb.pos); mem.free(lb.acc_rank); mem.free(lb.cq); mem.free(lb.rec);
+			mem.free(lb.keys); mem.free(lb.perm); mem.free(lb.pos); mem.free(lb.acc_rank); mem.free(lb.cq);
 		}
 		mem.free(hkeys);
 		mem.free(hvals);
@@ -785,7 +796,8 @@ struct Converter {
 		uint32_t* acc_ids = mem.alloc<uint32_t>(M);
 		uint64_t* acc_cols = lb.cols ? mem.alloc<uint64_t>(M) : nullptr;
 		uint32_t* rej_ids = method == PCG_POISSON_AVERAGE ? nullptr : mem.alloc<uint32_t>(M);
-		launch_split(lb.accepted, M, lb.ids, lb.cols, pre, acc_ids, acc_cols, rej_ids, mem);
+		int4* acc_rec = lb.rec ? mem.alloc<int4>(M) : nullptr;
+		launch_split(lb.accepted, M, lb.ids, lb.cols, lb.rec, pre, acc_ids, acc_cols, acc_rec, rej_ids, mem);
 		// prefix values at node and child boundaries
 		std::vector<int64_t> bidx;
 		for (int k = 0; k < K; k++) { bidx.push_back(ln[k].cand_off); bidx.push_back(ln[k].cand_off + ln[k].count); }
@@ -800,6 +812,7 @@ struct Converter {
 			uint32_t a0 = bval[2 * k], a1 = bval[2 * k + 1];
 			n.buf_ids = acc_ids + a0;
 			n.buf_cols = acc_cols ? acc_cols + a0 : nullptr;
+			n.buf_rec = acc_rec ? acc_rec + a0 : nullptr;
 			n.buf_count = (int64_t)(a1 - a0);
 		}
 		// children (sampler_poisson.h:247-291, sampler_poisson_average.h:418-475, sampler_random.h:184-225)
@@ -841,6 +854,7 @@ struct Converter {
 		mem.free(lb.node_of);
 		mem.free(lb.count_in_child);
 		mem.free(lb.accepted);
+		if (lb.rec) mem.free(lb.rec);
 		if (method != PCG_POISSON_AVERAGE) mem.free(lb.ids);
 	}
 

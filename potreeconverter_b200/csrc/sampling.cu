@@ -46,6 +46,7 @@ __global__ void gather_kernel(const GatherItem* __restrict__ items, LevelBuffers
 		int64_t j = it.dst_off + t;
 		lb.ids[j] = it.src_ids[t];
 		if (lb.cols) lb.cols[j] = it.src_cols ? it.src_cols[t] : 0ull;
+		if (lb.rec) lb.rec[j] = it.src_rec[t];
 		lb.child[j] = (uint8_t)it.child;
 		lb.node_of[j] = it.node;
 		lb.count_in_child[j] = (int32_t)it.count;
@@ -68,20 +69,25 @@ __device__ __forceinline__ double center_key(const LevelNode& nd, double x, doub
 	return ax * ax + ay * ay + az * az;
 }
 
-__global__ void keys_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
-                            const int32_t* __restrict__ Z, PosParamsS pp, LevelBuffers lb) {
+__global__ void keys_kernel(const LevelNode* __restrict__ nodes, PosParamsS pp, LevelBuffers lb) {
 	int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= lb.M) return;
 	const LevelNode& nd = nodes[lb.node_of[j]];
-	const uint32_t id = lb.ids[j];
-	const int4 r = make_int4(X[id], Y[id], Z[id], 0);
+	const int4 r = lb.rec[j];
 	// (xyz * scale) + offset, sampler_poisson.h:99-101
 	const double x = ((double)r.x * pp.scale[0]) + pp.offset[0];
 	const double y = ((double)r.y * pp.scale[1]) + pp.offset[1];
 	const double z = ((double)r.z * pp.scale[2]) + pp.offset[2];
 	lb.keys[j] = center_key(nd, x, y, z);
 	lb.perm[j] = (int32_t)(j - nd.cand_off);
-	lb.rec[j] = r;
+}
+
+__global__ void gather_records_kernel(const uint32_t* __restrict__ ids, int64_t n, const int32_t* __restrict__ X,
+                                      const int32_t* __restrict__ Y, const int32_t* __restrict__ Z, int4* __restrict__ rec) {
+	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const uint32_t id = ids[i];
+	rec[i] = make_int4(X[id], Y[id], Z[id], 0);
 }
 
 // sorted candidate records: (X, Y, Z, local index) at each sorted position
@@ -1559,10 +1565,15 @@ void launch_gather(const GatherItem* items, int num_items, LevelBuffers& lb, Dev
 	PCG_LAUNCHED();
 }
 
-void launch_keys(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
-                 LevelBuffers& lb, DeviceMem& mem) {
+void launch_keys(const LevelNode* nodes, const PosParamsS& pp, LevelBuffers& lb, DeviceMem& mem) {
 	if (lb.M == 0) return;
-	keys_kernel<<<(unsigned)ceil_div(lb.M, 256), 256, 0, mem.stream()>>>(nodes, X, Y, Z, pp, lb);
+	keys_kernel<<<(unsigned)ceil_div(lb.M, 256), 256, 0, mem.stream()>>>(nodes, pp, lb);
+	PCG_LAUNCHED();
+}
+
+void launch_gather_records(const uint32_t* ids, int64_t n, const int32_t* X, const int32_t* Y, const int32_t* Z, int4* rec, DeviceMem& mem) {
+	if (n == 0) return;
+	gather_records_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(ids, n, X, Y, Z, rec);
 	PCG_LAUNCHED();
 }
 

@@ -16,9 +16,10 @@ struct LevelNode {          // one inner node sampled at this level
 	int32_t pad;
 };
 
-struct GatherItem {         // copy `count` ids (and colours) of one child buffer
+struct GatherItem {         // copy `count` ids (and colours, records) of one child buffer
 	const uint32_t* src_ids;
 	const uint64_t* src_cols; // packed r | g << 16 | b << 32, or null
+	const int4* src_rec;      // (X, Y, Z, -) per id, or null
 	int64_t dst_off;
 	int64_t count;
 	int32_t child;
@@ -39,7 +40,7 @@ struct LevelBuffers {
 	uint8_t* accepted = nullptr;   // [M]
 	int32_t* acc_rank = nullptr;   // [M] acceptance rank for accepted candidates
 	int4* cq = nullptr;            // [M] sorted position -> (X, Y, Z, local index)
-	int4* rec = nullptr;           // [M] candidate (gather order) -> (X, Y, Z, -)
+	int4* rec = nullptr;           // [M] candidate (gather order) -> (X, Y, Z, -), copied with the ids
 };
 
 struct SortSeg {            // a std::sort segment [f, l) with its depth budget
@@ -65,8 +66,10 @@ struct SampleStats {
 };
 
 void launch_gather(const GatherItem* items, int num_items, LevelBuffers& lb, DeviceMem& mem);
-void launch_keys(const LevelNode* nodes, const int32_t* X, const int32_t* Y, const int32_t* Z, const PosParamsS& pp,
-                 LevelBuffers& lb, DeviceMem& mem);
+// keys from the gathered records lb.rec
+void launch_keys(const LevelNode* nodes, const PosParamsS& pp, LevelBuffers& lb, DeviceMem& mem);
+// records (X, Y, Z, -) of ids[0..n)
+void launch_gather_records(const uint32_t* ids, int64_t n, const int32_t* X, const int32_t* Y, const int32_t* Z, int4* rec, DeviceMem& mem);
 // std::sort emulation per node; `order` lists node indices, largest first.
 // Nodes order[0..num_big) (the largest) get one CTA each, the rest one warp.
 constexpr int64_t kBigNodeCandidates = 32768;
