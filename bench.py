@@ -16,6 +16,10 @@ all sampler levels, octree.bin payloads, hierarchy.bin, metadata.json).
          octree.bin inside the timed region
   --impl reference   the reference converter (stock build in oracle/_ref)
          on the host cores, each step a bounded sample of the workload
+  plain_form  the plain form (one launch per node, every neighbour test in
+         FP64) on the same workload, one step, and the batched/plain ratio
+  serving  eight jobs of 0.5-4M points submitted together to the request
+         loop; p50/p99 latency from submit to completion, and the makespan
 
 Multi-GPU: the build path does not shard within one cloud (one GPU per cloud,
 replicas only); with N ranks every rank converts its own seeded cloud and
@@ -199,6 +203,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--points", type=int, default=WORKLOAD["points"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-form leg (one-launch-per-node form)")
+    ap.add_argument("--no-serving", action="store_true", help="skip the request-loop latency leg")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -282,6 +288,51 @@ def main():
     achieved = accept_bytes / (accept_ms * 1e-3) / 1e9 if accept_ms > 0 else 0.0
     traffic = s["candidates"] * ACCEPT_DRAM_BYTES_PER_CANDIDATE if ACCEPT_DRAM_BYTES_PER_CANDIDATE else None
     whole_bytes = n * rec_len + out_pts * bpp  # B_alg: read every record once, write every output record once
+    # ---- plain form on the same workload (one step, single GPU runs only):
+    # one launch per node, every neighbour test in FP64; the batched form
+    # above is measured against it
+    plain = None
+    if world == 1 and not args.no_plain:
+        pctx = pc.Context(device=local, stream=stream.cuda_stream, form="plain")
+        p_start = torch.cuda.Event(enable_timing=True)
+        p_end = torch.cuda.Event(enable_timing=True)
+        p_start.record(stream)
+        pctx.convert_resident(header, records.data_ptr(), method="poisson", name="bench")
+        p_end.record(stream)
+        p_end.synchronize()
+        p_ms = p_start.elapsed_time(p_end)
+        pctx.close()
+        plain = {"value": n / (p_ms * 1e3), "unit": "Mpts/s", "ms_per_step": p_ms, "steps": 1,
+                 "batched_over_plain": (n / (ms * 1e3)) / (n / (p_ms * 1e3))}
+
+    # ---- request loop: jobs of mixed sizes submitted together (from host
+    # memory, through pcg_submit), latency = submit to completion
+    serving = None
+    if world == 1 and not args.no_serving:
+        sizes = [500_000, 1_000_000, 2_000_000, 4_000_000] * 2
+        jobs = [synth.hotspots(m, 3000 + i) for i, m in enumerate(sizes)]
+        with pc.Context(device=local) as sctx:
+            sctx.wait(sctx.submit(jobs[0], method="poisson", name="warm"))
+            t_sub, t_done, ids = {}, {}, []
+            t0 = time.perf_counter()
+            for i, las in enumerate(jobs):
+                ids.append(sctx.submit(las, method="poisson", name=f"job{i}"))
+                t_sub[i] = time.perf_counter()
+            pending = set(range(len(ids)))
+            while pending:
+                for i in list(pending):
+                    if sctx.poll(ids[i]):
+                        t_done[i] = time.perf_counter()
+                        pending.discard(i)
+                time.sleep(0.0005)
+            makespan = max(t_done.values()) - t0
+            for j in ids:
+                sctx.wait(j)
+        lat = sorted(1e3 * (t_done[i] - t_sub[i]) for i in range(len(ids)))
+        serving = {"jobs": len(sizes), "points": sizes, "sampler": "poisson", "p50_ms": statistics.median(lat),
+                   "p99_ms": lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))], "makespan_ms": 1e3 * makespan,
+                   "mpts_per_s": sum(sizes) / (makespan * 1e6), "worker_streams": 4}
+
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and os.path.exists(os.path.join(REPO, "oracle", "_ref", "PotreeConverter")):
@@ -312,6 +363,8 @@ def main():
                                                                   "ms_host_writers")},
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "plain_form": plain,
+            "serving": serving,
             "escalated_pairs": int(s["escalated_pairs"]),
             "sampler": {k: int(s[k]) for k in ("sampled_nodes", "candidates", "replayed_nodes", "replayed_candidates",
                                                "heapsort_fallbacks", "list_entries")},
