@@ -120,9 +120,21 @@ class Conversion:
             f.write(self.metadata)
 
 
+def _copy_out(ptr, size: int) -> bytes:
+    """Bytes at a library buffer; ctypes.string_at takes a 32-bit size, so
+    images of 2 GiB and more are copied with memmove."""
+    if not size:
+        return b""
+    if size < (1 << 31):
+        return ctypes.string_at(ptr, size)
+    buf = bytearray(size)
+    ctypes.memmove((ctypes.c_char * size).from_buffer(buf), ptr, size)
+    return bytes(buf)
+
+
 def _take(lib, res: _Result) -> Conversion:
-    octree = ctypes.string_at(res.octree, res.octree_size) if res.octree_size else b""
-    hierarchy = ctypes.string_at(res.hierarchy, res.hierarchy_size) if res.hierarchy_size else b""
+    octree = _copy_out(res.octree, res.octree_size)
+    hierarchy = _copy_out(res.hierarchy, res.hierarchy_size)
     metadata = ctypes.string_at(res.metadata, res.metadata_size).decode() if res.metadata_size else ""
     stats = {name: getattr(res.stats, name) for name, _ in _Stats._fields_}
     lib.pcg_result_free(ctypes.byref(res))

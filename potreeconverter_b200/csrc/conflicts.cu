@@ -19,9 +19,10 @@
 //  3. a hash table (node, cell) -> range of the cell-sorted records;
 //  4. one thread per candidate in cell order (a warp shares neighbourhoods)
 //     scans the occupied cells among its 27 up to its own sorted position:
-//     an FP32 prefilter on node-relative coordinates (margin 1e-3 of s^2,
-//     far above its rounding error), then the reference's FP64 test, then
-//     the early-exit bound.
+//     the FP32 distance on node-relative coordinates decides every pair
+//     outside the band s^2 (1 -/+ 1e-3) (its rounding error is below 1e-4 of
+//     s^2); pairs inside the band are decided by the reference's FP64 test
+//     and counted as escalated; then the early-exit bound.
 // A candidate with more than kListCap such predecessors marks its node
 // dense; dense nodes keep the grid-based acceptance kernel.
 
@@ -175,7 +176,8 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 	}
 	// node-relative FP32 coordinates: error far below the 1e-3 margin on s^2
 	const bool pre32 = s2 > 1e-30 && s2 < 1e30;
-	const float s2hi = (float)(s2 * 1.001);
+	const float s2hi = (float)(s2 * 1.001), s2lo = (float)(s2 * 0.999);
+	unsigned escalated = 0;  // pairs inside the band, decided in FP64
 	const uint64_t c = ck[j];
 	const int cx = (int)(c % kCellsPerAxis), cy = (int)((c / kCellsPerAxis) % kCellsPerAxis), cz = (int)(c / (kCellsPerAxis * kCellsPerAxis));
 	int32_t* out = cl.entries + (co + t) * (int64_t)kListCap;
@@ -209,17 +211,25 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 					const float4 qf = rf[i];
 					const int32_t u = __float_as_int(qf.w);
 					if (u >= t) break;  // a cell's records are in sorted order: only earlier candidates
+					bool inside = false;
 					if (pre32) {
+						// FP32 decides outside the band s^2 (1 -/+ 1e-3), well clear
+						// of its rounding error; pairs in the band go to FP64
 						const float fx = qf.x - mf.x, fy = qf.y - mf.y, fz = qf.z - mf.z;
-						if (fx * fx + fy * fy + fz * fz >= s2hi) continue;
+						const float d2 = fx * fx + fy * fy + fz * fz;
+						if (d2 >= s2hi) continue;
+						inside = d2 < s2lo;
 					}
-					const int4 q = rp[i];
-					const double ax = qcoord(q.x, 0, pp), ay = qcoord(q.y, 1, pp), az = qcoord(q.z, 2, pp);
-					// squaredDistance(point, candidate), sampler_poisson.h:117-125
-					const double dx_ = ax - x, dy_ = ay - y, dz_ = az - z;
-					if (!(dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < s2)) continue;
-					if (MODE == 0 && !(lb.keys[co + q.w] >= lim)) continue;
-					if (n < kListCap) out[n] = q.w;
+					if (!inside) {
+						const int4 q = rp[i];
+						const double ax = qcoord(q.x, 0, pp), ay = qcoord(q.y, 1, pp), az = qcoord(q.z, 2, pp);
+						// squaredDistance(point, candidate), sampler_poisson.h:117-125
+						const double dx_ = ax - x, dy_ = ay - y, dz_ = az - z;
+						escalated++;
+						if (!(dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < s2)) continue;
+					}
+					if (MODE == 0 && !(lb.keys[co + u] >= lim)) continue;
+					if (n < kListCap) out[n] = u;
 					n++;
 				}
 			}
@@ -229,7 +239,11 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 	if (n > kListCap) cl.node_dense[node] = 1;
 	const unsigned active = __activemask();
 	const unsigned sum = __reduce_add_sync(active, (unsigned)(n <= kListCap ? n : kListCap));
-	if ((int)(threadIdx.x & 31) == __ffs(active) - 1) atomicAdd(&st->list_entries, (unsigned long long)sum);
+	const unsigned esc = __reduce_add_sync(active, escalated);
+	if ((int)(threadIdx.x & 31) == __ffs(active) - 1) {
+		atomicAdd(&st->list_entries, (unsigned long long)sum);
+		if (esc) atomicAdd(&st->escalated, (unsigned long long)esc);
+	}
 }
 
 }  // namespace
