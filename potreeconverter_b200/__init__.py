@@ -175,9 +175,12 @@ class Context:
 
     @staticmethod
     def _job(las, method, name, projection, keep, device_records=None, flags=0):
-        if isinstance(las, (bytes, bytearray, memoryview)):
-            buf = (ctypes.c_uint8 * len(las)).from_buffer_copy(las) if isinstance(las, bytes) else \
-                (ctypes.c_uint8 * len(las)).from_buffer(las)
+        if isinstance(las, bytes):
+            # the library only reads the image: pass the bytes object's own buffer
+            keep.append(las)
+            ptr, size = ctypes.cast(ctypes.c_char_p(las), ctypes.c_void_p).value, len(las)
+        elif isinstance(las, (bytearray, memoryview)):
+            buf = (ctypes.c_uint8 * len(las)).from_buffer(las)
             keep.append(buf)
             ptr, size = ctypes.addressof(buf), len(las)
         else:  # (pointer, size), e.g. pinned host memory

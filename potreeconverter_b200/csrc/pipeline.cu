@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <condition_variable>
 #include <deque>
 #include <fstream>
@@ -959,6 +960,11 @@ struct pcg_ctx {
 	// request loop
 	struct Job {
 		uint64_t id;
+		// the job's LAS image, copied at submit: into a pinned buffer of the
+		// pool when one can be had (the worker's host-to-device copy then
+		// runs at link speed), else into `las`
+		uint8_t* las_pinned = nullptr;
+		size_t las_size = 0;
 		std::vector<uint8_t> las;
 		std::string name, projection;
 		int32_t method;
@@ -1049,8 +1055,8 @@ void worker_main(pcg_ctx* ctx, int wi) {
 			ctx->in_use += job->footprint;
 		}
 		pcg_job pj{};
-		pj.las = job->las.data();
-		pj.las_size = job->las.size();
+		pj.las = job->las_pinned ? job->las_pinned : job->las.data();
+		pj.las_size = job->las_size;
 		pj.method = job->method;
 		pj.name = job->name.c_str();
 		pj.projection = job->projection.c_str();
@@ -1066,6 +1072,11 @@ void worker_main(pcg_ctx* ctx, int wi) {
 			st = PCG_INTERNAL; err = e.what();
 		}
 		conv.arena->release_all();
+		if (job->las_pinned) {
+			pcg::g_pinned.give(job->las_pinned);
+			job->las_pinned = nullptr;
+		}
+		std::vector<uint8_t>().swap(job->las);
 		{
 			std::lock_guard<std::mutex> lk(ctx->qmtx);
 			job->status = st;
@@ -1141,6 +1152,8 @@ void pcg_destroy(pcg_ctx* ctx) {
 	for (auto& t : ctx->workers) t.join();
 	for (auto& kv : ctx->jobs)
 		if (kv.second->result.octree && !pcg::g_pinned.give(kv.second->result.octree)) cudaFreeHost(kv.second->result.octree);
+	for (auto& kv : ctx->jobs)
+		if (kv.second->las_pinned) pcg::g_pinned.give(kv.second->las_pinned);
 	cudaSetDevice(ctx->conv.device);
 	for (auto s : ctx->worker_streams) cudaStreamDestroy(s);
 	ctx->conv.arena.reset();
@@ -1209,7 +1222,10 @@ pcg_status pcg_submit(pcg_ctx* ctx, const pcg_job* job, uint64_t* job_id) {
 		}
 		auto j = std::make_shared<pcg_ctx::Job>();
 		j->id = ctx->next_id++;
-		j->las.assign((const uint8_t*)job->las, (const uint8_t*)job->las + job->las_size);
+		j->las_size = job->las_size;
+		j->las_pinned = pcg::g_pinned.take(job->las_size);
+		if (j->las_pinned) std::memcpy(j->las_pinned, job->las, job->las_size);
+		else j->las.assign((const uint8_t*)job->las, (const uint8_t*)job->las + job->las_size);
 		j->name = job->name ? job->name : "";
 		j->projection = job->projection ? job->projection : "";
 		j->method = job->method;
