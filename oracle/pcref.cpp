@@ -214,11 +214,17 @@ static bool outputAttributesOf(const LasHeader& header, vector<Attribute>& list)
 }
 
 // ------------------------------------------------------------- the job
-struct Job {
+struct Source {  // one input file (main.cpp:146-200 Source)
 	const uint8_t* las = nullptr;
 	LasHeader header;
-	Attributes attributes;  // output attributes incl. scale/offset
-	Vec3 min, max;          // cubic box, main.cpp:237-239
+	vector<Attribute> list;  // its own attribute list, PotreeConverter.h:136-193
+};
+
+struct Job {
+	vector<Source> sources;     // in the order the reference takes them
+	vector<string> requested;   // --attributes (empty: all)
+	Attributes attributes;      // output attributes incl. scale/offset
+	Vec3 min, max;              // cubic box, main.cpp:237-239
 	int64_t totalPoints = 0;
 	string name;
 	string method;
@@ -227,25 +233,46 @@ struct Job {
 };
 
 static bool setup(Job& job) {
-	vector<Attribute> list;
-	if (!outputAttributesOf(job.header, list)) { job.err = "unsupported point format"; return false; }
-	// PotreeConverter.h:195-252 with one source
-	Vec3 scaleMin = job.header.scale;
-	Vec3 min = job.header.min, max = job.header.max;
+	// computeOutputAttributes(sources, requestedAttributes), PotreeConverter.h:195-276
+	Vec3 scaleMin(Inf, Inf, Inf), min(Inf, Inf, Inf), max(-Inf, -Inf, -Inf);
+	vector<Attribute> full;
+	for (auto& src : job.sources) {
+		if (!outputAttributesOf(src.header, src.list)) { job.err = "unsupported point format"; return false; }
+		for (auto& a : src.list) {
+			bool added = false;
+			for (auto& f : full) added = added || f.name == a.name;
+			if (!added) full.push_back(a);
+		}
+		const LasHeader& h = src.header;
+		scaleMin.x = std::min(scaleMin.x, h.scale.x); scaleMin.y = std::min(scaleMin.y, h.scale.y); scaleMin.z = std::min(scaleMin.z, h.scale.z);
+		min.x = std::min(min.x, h.min.x); min.y = std::min(min.y, h.min.y); min.z = std::min(min.z, h.min.z);
+		max.x = std::max(max.x, h.max.x); max.y = std::max(max.y, h.max.y); max.z = std::max(max.z, h.max.z);
+		job.totalPoints += h.numPoints;
+	}
 	// computeScaleOffset, PotreeConverter.h:29-76
 	Vec3 size = max - min;
 	double msx = size.x / pow(2.0, 30.0), msy = size.y / pow(2.0, 30.0), msz = size.z / pow(2.0, 30.0);
 	Vec3 scale(std::max(scaleMin.x, msx), std::max(scaleMin.y, msy), std::max(scaleMin.z, msz));
-	job.attributes = Attributes(list);
+	// the filter, PotreeConverter.h:252-275: position first, then the
+	// requested names found in the full list, in request order
+	vector<Attribute> filtered = full;
+	if (!job.requested.empty()) {
+		vector<string> should = job.requested;
+		should.insert(should.begin(), "position");
+		filtered.clear();
+		for (auto& nm : should)
+			for (auto& f : full)
+				if (f.name == nm) { filtered.push_back(f); break; }
+	}
+	job.attributes = Attributes(filtered);
 	job.attributes.posScale = scale;
 	job.attributes.posOffset = min;
-	// computeStats, main.cpp:215-284
+	// computeStats, main.cpp:215-284 (the same header boxes)
 	double cubeSize = (max - min).max();
 	Vec3 csize(cubeSize, cubeSize, cubeSize);
 	job.min = min;
 	job.max = min + cubeSize;
 	if (csize.x == 0.0 || csize.y == 0.0 || csize.z == 0) { job.err = "invalid bounding box"; return false; }
-	job.totalPoints = job.header.numPoints;
 	return true;
 }
 
@@ -269,10 +296,15 @@ static string toNodeID(int level, int gridSize, int64_t x, int64_t y, int64_t z)
 
 struct PointCoord { double x, y, z; };
 
-static inline PointCoord lasCoordinates(const Job& job, int64_t i) {  // laszip_dll.cpp:1137-1139
-	const uint8_t* r = job.las + job.header.offsetToPoints + (uint64_t)i * job.header.recordLength;
+static inline const uint8_t* lasRecord(const Source& src, int64_t i) {
+	return src.las + src.header.offsetToPoints + (uint64_t)i * src.header.recordLength;
+}
+
+static inline PointCoord lasCoordinates(const Source& src, int64_t i) {  // laszip_dll.cpp:1137-1139
+	const uint8_t* r = lasRecord(src, i);
+	const LasHeader& h = src.header;
 	int32_t X = rd<int32_t>(r), Y = rd<int32_t>(r + 4), Z = rd<int32_t>(r + 8);
-	return {job.header.scale.x * X + job.header.offset.x, job.header.scale.y * Y + job.header.offset.y, job.header.scale.z * Z + job.header.offset.z};
+	return {h.scale.x * X + h.offset.x, h.scale.y * Y + h.offset.y, h.scale.z * Z + h.offset.z};
 }
 
 struct Chunk { string id; Vec3 min, max; vector<uint8_t> data; };
@@ -293,8 +325,8 @@ static bool doChunking(Job& job, vector<Chunk>& chunksOut, Attributes& attrsOut,
 		double cubeSize = (max - min).max();
 		Vec3 size(cubeSize, cubeSize, cubeSize);
 		double dG = double(gridSize);
-		for (int64_t i = 0; i < total; i++) {
-			PointCoord c = lasCoordinates(job, i);
+		for (auto& src : job.sources) for (int64_t i = 0; i < src.header.numPoints; i++) {
+			PointCoord c = lasCoordinates(src, i);
 			int32_t X = int32_t((c.x - posOffset.x) / posScale.x);
 			int32_t Y = int32_t((c.y - posOffset.y) / posScale.y);
 			int32_t Z = int32_t((c.z - posOffset.z) / posScale.z);
@@ -356,25 +388,53 @@ static bool doChunking(Job& job, vector<Chunk>& chunksOut, Attributes& attrsOut,
 		}
 	}
 
-	// distributePoints, :660-1003 (handlers :380-658), one batch thread
+	// distributePoints, :660-1003 (handlers :380-658), one batch thread,
+	// sources in order
 	int bpp = out.bytes;
 	vector<vector<uint8_t>> buckets(nodes.size());
 	Attributes stats = out;  // global min/max/histogram accumulator
 	for (auto& a : stats.list) { a.min = {Inf, Inf, Inf}; a.max = {-Inf, -Inf, -Inf}; for (auto& h : a.histogram) h = 0; }
-	{
-		int fmt = job.header.pointDataFormat;
-		// input attribute list == output list (no --attributes filter)
-		vector<Attribute>& inList = out.list;
+	static const char* standard[] = {"rgb", "intensity", "return number", "number of returns", "classification", "scan angle rank",
+	                                 "scan angle", "user data", "point source id", "gps-time", "classification flags"};
+	for (auto& src : job.sources) {
+		int fmt = src.header.pointDataFormat;
+		// the handlers of createAttributeHandlers for this source's own
+		// attribute list (the input list, :952-983)
+		const vector<Attribute>& inList = src.list;
+		vector<string> handled;  // standard handlers, in input-list order (:531-545)
+		for (auto& ia : inList) {
+			if (ia.name == "position") continue;
+			bool mapped = false;
+			for (const char* sn : standard) mapped = mapped || ia.name == sn;
+			if (mapped && out.get(ia.name) != nullptr) handled.push_back(ia.name);
+		}
 		int firstExtraIndex = (fmt == 0) ? 8 : (fmt == 1 || fmt == 2) ? 9 : 10;  // :551-560 (formats 0-3)
+		int stdRecLen = (fmt == 0) ? 20 : (fmt == 1) ? 28 : (fmt == 2) ? 26 : 34;
+		struct ExtraHandler { int attributeOffset, sourceOffset, size; string name; };
+		vector<ExtraHandler> extraHandlers;  // :579-653: the target offset is counted over the input list
+		{
+			int attributeOffset = 0;
+			for (int k = 0; k < firstExtraIndex && k < (int)inList.size(); k++) attributeOffset += inList[k].size;
+			int sourceOffset = 0;
+			for (int k = firstExtraIndex; k < (int)inList.size(); k++) {
+				const Attribute* oa = out.get(inList[k].name);
+				if (oa) {
+					if (attributeOffset + inList[k].size > bpp) { job.err = "extra attribute written past the point record (undefined in the reference)"; return false; }
+					if (stdRecLen + sourceOffset + oa->numElements * oa->elementSize > src.header.recordLength) { job.err = "extra attribute read past the LAS record (undefined in the reference)"; return false; }
+					extraHandlers.push_back({attributeOffset, sourceOffset, inList[k].size, inList[k].name});
+					attributeOffset += oa->size;
+				}
+				sourceOffset += inList[k].size;
+			}
+		}
 		double cubeSize = (max - min).max();
 		Vec3 size(cubeSize, cubeSize, cubeSize);
 		double dG = double(gridSize);
 		vector<uint8_t> rec(bpp);
-		int stdRecLen = (fmt == 0) ? 20 : (fmt == 1) ? 28 : (fmt == 2) ? 26 : 34;
-		for (int64_t i = 0; i < total; i++) {
-			const uint8_t* r = job.las + job.header.offsetToPoints + (uint64_t)i * job.header.recordLength;
+		for (int64_t i = 0; i < src.header.numPoints; i++) {
+			const uint8_t* r = lasRecord(src, i);
 			std::fill(rec.begin(), rec.end(), 0);
-			PointCoord c = lasCoordinates(job, i);
+			PointCoord c = lasCoordinates(src, i);
 			int32_t X = int32_t((c.x - posOffset.x) / posScale.x);
 			int32_t Y = int32_t((c.y - posOffset.y) / posScale.y);
 			int32_t Z = int32_t((c.z - posOffset.z) / posScale.z);
@@ -382,13 +442,10 @@ static bool doChunking(Job& job, vector<Chunk>& chunksOut, Attributes& attrsOut,
 			Attribute* aPos = stats.get("position");
 			aPos->min.x = std::min(aPos->min.x, c.x); aPos->min.y = std::min(aPos->min.y, c.y); aPos->min.z = std::min(aPos->min.z, c.z);
 			aPos->max.x = std::max(aPos->max.x, c.x); aPos->max.y = std::max(aPos->max.y, c.y); aPos->max.z = std::max(aPos->max.z, c.z);
-			// standard attributes in input-list order
-			for (size_t k = 0; k < inList.size() && (int)k < firstExtraIndex; k++) {
-				const string& nm = inList[k].name;
+			for (const string& nm : handled) {
 				int off = out.getOffset(nm);
 				Attribute* a = stats.get(nm);
 				auto upd = [a](double v) { a->min.x = std::min(a->min.x, v); a->max.x = std::max(a->max.x, v); };
-				if (nm == "position") continue;
 				if (nm == "intensity") { uint16_t v = rd<uint16_t>(r + 12); memcpy(&rec[off], &v, 2); upd(double(v)); }
 				else if (nm == "return number") { uint8_t v = r[14] & 7; rec[off] = v; upd(double(v)); }
 				else if (nm == "number of returns") { uint8_t v = (r[14] >> 3) & 7; rec[off] = v; upd(double(v)); }
@@ -405,37 +462,29 @@ static bool doChunking(Job& job, vector<Chunk>& chunksOut, Attributes& attrsOut,
 					a->max.x = std::max(a->max.x, double(c3[0])); a->max.y = std::max(a->max.y, double(c3[1])); a->max.z = std::max(a->max.z, double(c3[2]));
 				}
 			}
-			// extra attributes, :547-653 (target offset counted over the input list)
-			{
-				int attributeOffset = 0;
-				for (int k = 0; k < firstExtraIndex && k < (int)inList.size(); k++) attributeOffset += inList[k].size;
-				int sourceOffset = 0;
-				const uint8_t* extra = r + stdRecLen;
-				for (int k = firstExtraIndex; k < (int)inList.size(); k++) {
-					Attribute* a = stats.get(inList[k].name);
-					int asz = inList[k].size;
-					memcpy(&rec[attributeOffset], extra + sourceOffset, asz);
-					auto f = [a](const uint8_t* p) -> double {
-						switch (a->type) {
-						case AType::INT8: return double(rd<int8_t>(p)); case AType::INT16: return double(rd<int16_t>(p));
-						case AType::INT32: return double(rd<int32_t>(p)); case AType::INT64: return double(rd<int64_t>(p));
-						case AType::UINT8: return double(rd<uint8_t>(p)); case AType::UINT16: return double(rd<uint16_t>(p));
-						case AType::UINT32: return double(rd<uint32_t>(p)); case AType::UINT64: return double(rd<uint64_t>(p));
-						case AType::FLOAT: return double(rd<float>(p)); case AType::DOUBLE: return rd<double>(p);
-						default: return 0.0;
-						}
-					};
-					if (a->numElements == 1) { double x = f(extra + sourceOffset); a->min.x = std::min(a->min.x, x); a->max.x = std::max(a->max.x, x); }
-					else if (a->numElements == 2) {
-						double x = f(extra + sourceOffset), y = f(extra + sourceOffset + a->elementSize);
-						a->min.x = std::min(a->min.x, x); a->min.y = std::min(a->min.y, y); a->max.x = std::max(a->max.x, x); a->max.y = std::max(a->max.y, y);
-					} else if (a->numElements == 3) {
-						double x = f(extra + sourceOffset), y = f(extra + sourceOffset + a->elementSize), z = f(extra + sourceOffset + 2 * a->elementSize);
-						a->min.x = std::min(a->min.x, x); a->min.y = std::min(a->min.y, y); a->min.z = std::min(a->min.z, z);
-						a->max.x = std::max(a->max.x, x); a->max.y = std::max(a->max.y, y); a->max.z = std::max(a->max.z, z);
+			const uint8_t* extra = r + stdRecLen;
+			for (auto& eh : extraHandlers) {
+				Attribute* a = stats.get(eh.name);
+				memcpy(&rec[eh.attributeOffset], extra + eh.sourceOffset, eh.size);
+				auto f = [a](const uint8_t* p) -> double {
+					switch (a->type) {
+					case AType::INT8: return double(rd<int8_t>(p)); case AType::INT16: return double(rd<int16_t>(p));
+					case AType::INT32: return double(rd<int32_t>(p)); case AType::INT64: return double(rd<int64_t>(p));
+					case AType::UINT8: return double(rd<uint8_t>(p)); case AType::UINT16: return double(rd<uint16_t>(p));
+					case AType::UINT32: return double(rd<uint32_t>(p)); case AType::UINT64: return double(rd<uint64_t>(p));
+					case AType::FLOAT: return double(rd<float>(p)); case AType::DOUBLE: return rd<double>(p);
+					default: return 0.0;
 					}
-					attributeOffset += a->size;
-					sourceOffset += asz;
+				};
+				const uint8_t* q = extra + eh.sourceOffset;
+				if (a->numElements == 1) { double x = f(q); a->min.x = std::min(a->min.x, x); a->max.x = std::max(a->max.x, x); }
+				else if (a->numElements == 2) {
+					double x = f(q), y = f(q + a->elementSize);
+					a->min.x = std::min(a->min.x, x); a->min.y = std::min(a->min.y, y); a->max.x = std::max(a->max.x, x); a->max.y = std::max(a->max.y, y);
+				} else if (a->numElements == 3) {
+					double x = f(q), y = f(q + a->elementSize), z = f(q + 2 * a->elementSize);
+					a->min.x = std::min(a->min.x, x); a->min.y = std::min(a->min.y, y); a->min.z = std::min(a->min.z, z);
+					a->max.x = std::max(a->max.x, x); a->max.y = std::max(a->max.y, y); a->max.z = std::max(a->max.z, z);
 				}
 			}
 			// bucket lookup, :817-904
@@ -1286,17 +1335,30 @@ static bool runIndexing(Job& job, vector<Chunk>& chunks, Attributes& attrs, Vec3
 	return true;
 }
 
-bool convert(const uint8_t* las, size_t size, const string& method, const string& name, uint32_t seed, Result& res, string& err) {
+bool convert(const vector<SourceImage>& sources, const vector<string>& attributes, const string& method, const string& name, uint32_t seed,
+             Result& res, string& err) {
 	Job job;
-	job.las = las; job.method = method; job.name = name; job.seed = seed;
+	job.method = method; job.name = name; job.seed = seed; job.requested = attributes;
 	if (method != "poisson" && method != "poisson_average" && method != "random") { err = "unknown method"; return false; }
-	if (!parseHeader(las, size, job.header, job.err) || !setup(job)) { err = job.err; return false; }
+	if (sources.empty()) { err = "no input"; return false; }
+	for (auto& si : sources) {
+		Source src;
+		src.las = si.las;
+		if (!parseHeader(si.las, si.size, src.header, job.err)) { err = job.err; return false; }
+		job.sources.push_back(std::move(src));
+	}
+	if (!setup(job)) { err = job.err; return false; }
+	if (method == "poisson_average" && job.attributes.getOffset("rgb") < 0) { err = "poisson_average needs rgb (undefined in the reference)"; return false; }
 	vector<Chunk> chunks; Attributes attrs; Vec3 min, max;
 	if (!doChunking(job, chunks, attrs, min, max)) { err = job.err; return false; }
 	res.chunkIds.clear(); res.chunkCounts.clear();
 	for (auto& c : chunks) { res.chunkIds.push_back(c.id); res.chunkCounts.push_back((int64_t)c.data.size() / attrs.bytes); }
 	if (!runIndexing(job, chunks, attrs, min, max, res)) { err = job.err; return false; }
 	return true;
+}
+
+bool convert(const uint8_t* las, size_t size, const string& method, const string& name, uint32_t seed, Result& res, string& err) {
+	return convert(vector<SourceImage>{{las, size}}, {}, method, name, seed, res, err);
 }
 
 }  // namespace pcref
@@ -1317,11 +1379,18 @@ struct pcref_output {
 	int64_t* node_info;      // per node: byte offset, byte size, point count
 };
 
-int pcref_convert(const void* las, uint64_t size, const char* method, const char* name, uint32_t seed, pcref_output* out) {
+// Several sources (the reference's input list, in order) and an optional
+// --attributes list (attrs may be NULL when nattrs is 0).
+int pcref_convert_sources(const void* const* las, const uint64_t* sizes, int32_t nsources, const char* const* attrs, int32_t nattrs,
+                          const char* method, const char* name, uint32_t seed, pcref_output* out) {
 	memset(out, 0, sizeof(*out));
+	std::vector<pcref::SourceImage> srcs;
+	for (int32_t i = 0; i < nsources; i++) srcs.push_back({(const uint8_t*)las[i], (size_t)sizes[i]});
+	std::vector<std::string> names;
+	for (int32_t i = 0; i < nattrs; i++) names.push_back(attrs[i]);
 	pcref::Result res;
 	std::string err;
-	if (!pcref::convert((const uint8_t*)las, size, method, name, seed, res, err)) {
+	if (!pcref::convert(srcs, names, method, name, seed, res, err)) {
 		snprintf(out->error, sizeof(out->error), "%s", err.c_str());
 		return 1;
 	}
@@ -1357,6 +1426,10 @@ int pcref_convert(const void* las, uint64_t size, const char* method, const char
 		out->node_info[3 * i + 2] = res.nodes[i].numPoints;
 	}
 	return 0;
+}
+
+int pcref_convert(const void* las, uint64_t size, const char* method, const char* name, uint32_t seed, pcref_output* out) {
+	return pcref_convert_sources(&las, &size, 1, nullptr, 0, method, name, seed, out);
 }
 
 void pcref_free(pcref_output* out) {

@@ -18,10 +18,21 @@ struct Result {
 	std::vector<NodeRecord> nodes;        // completion order
 };
 
+struct SourceImage {
+	const uint8_t* las;
+	size_t size;
+};
+
 // Converts one uncompressed LAS file image; method is "poisson",
 // "poisson_average" or "random"; name goes to metadata.json; seed is the
 // random sampler's pinned seed.
 bool convert(const uint8_t* las, size_t size, const std::string& method, const std::string& name,
              uint32_t seed, Result& res, std::string& err);
+
+// Converts several LAS file images as one point cloud (the reference's
+// source list, in order), keeping only the named attributes when
+// attributes is not empty (--attributes).
+bool convert(const std::vector<SourceImage>& sources, const std::vector<std::string>& attributes, const std::string& method,
+             const std::string& name, uint32_t seed, Result& res, std::string& err);
 
 }  // namespace pcref

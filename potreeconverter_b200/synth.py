@@ -42,52 +42,92 @@ _PDRF3 = np.dtype([
     ("user_data", "u1"), ("point_source_id", "<u2"), ("gps_time", "<f8"),
     ("red", "<u2"), ("green", "<u2"), ("blue", "<u2"),
 ])
-assert _PDRF2.itemsize == 26 and _PDRF3.itemsize == 34
+_PDRF0 = np.dtype([(n, _PDRF2.fields[n][0]) for n in _PDRF2.names[:9]])
+_PDRF1 = np.dtype([(n, _PDRF3.fields[n][0]) for n in _PDRF3.names[:10]])
+assert _PDRF0.itemsize == 20 and _PDRF1.itemsize == 28 and _PDRF2.itemsize == 26 and _PDRF3.itemsize == 34
+_PDRF = {0: _PDRF0, 1: _PDRF1, 2: _PDRF2, 3: _PDRF3}
+
+# LAS extra-bytes data types (type id of the descriptor) for scalar numpy types
+_EXTRA_TYPE_ID = {"u1": 1, "i1": 2, "<u2": 3, "<i2": 4, "<u4": 5, "<i4": 6, "<u8": 7, "<i8": 8, "<f4": 9, "<f8": 10}
 
 
-def _record_dtype(pdrf: int, extra_float: bool) -> np.dtype:
-    base = {2: _PDRF2, 3: _PDRF3}[pdrf]
-    if not extra_float:
-        return base
-    fields = [(n, base.fields[n][0]) for n in base.names] + [("extra", "<f4")]
+def _record_dtype(pdrf: int, extra_float: bool, extras=()) -> np.dtype:
+    base = _PDRF[pdrf]
+    fields = [(n, base.fields[n][0]) for n in base.names]
+    if extra_float:
+        fields.append(("extra", "<f4"))
+    for e in extras:
+        shape = e["values"].shape[1:]
+        fields.append((e["name"], e["dtype"], shape) if shape else (e["name"], e["dtype"]))
     return np.dtype(fields)
 
 
-def _extra_bytes_vlr(name: str = "extra", description: str = "N(0,1) float") -> bytes:
-    """One extra-bytes descriptor (record id 4, 192 bytes) for a float32."""
+def _extra_descriptor(name: str, type_id: int, description: str, scale=None, offset=None) -> bytes:
+    """One 192-byte extra-bytes descriptor (LAS 1.4 R15 table 24)."""
     rec = bytearray(192)
-    rec[2] = 9  # data type 9 = float
-    rec[3] = 0  # options: no scale/offset/min/max
+    rec[2] = type_id
+    options = (0b01000 if scale is not None else 0) | (0b10000 if offset is not None else 0)
+    rec[3] = options
     nb = name.encode()[:31]
     rec[4:4 + len(nb)] = nb
+    if scale is not None:
+        struct.pack_into("<3d", rec, 112, *scale)
+    if offset is not None:
+        struct.pack_into("<3d", rec, 136, *offset)
     db = description.encode()[:31]
     rec[160:160 + len(db)] = db
+    return bytes(rec)
+
+
+def _extra_bytes_vlr(name: str = "extra", description: str = "N(0,1) float", descriptors: bytes | None = None) -> bytes:
+    """The extra-bytes VLR (record id 4): by default one float32 descriptor."""
+    body = descriptors if descriptors is not None else _extra_descriptor(name, 9, description)
     hdr = bytearray(54)
     hdr[2:2 + 9] = b"LASF_Spec"
-    struct.pack_into("<HH", hdr, 18, 4, 192)
+    struct.pack_into("<HH", hdr, 18, 4, len(body))
     d = b"Extra bytes"
     hdr[22:22 + len(d)] = d
-    return bytes(hdr) + bytes(rec)
+    return bytes(hdr) + body
 
 
 def write_las(X, Y, Z, attrs: dict, *, pdrf: int, version_minor: int,
-              extra=None) -> bytes:
-    """Serialize quantized points into an uncompressed LAS file image."""
+              extra=None, scale=None, offset=None, extras=()) -> bytes:
+    """Serialize quantized points into an uncompressed LAS file image.
+
+    ``extra`` is the float32 attribute named "extra"; ``extras`` lists more
+    extra-bytes attributes as dicts with ``name``, ``dtype`` (a scalar numpy
+    type string of ``_EXTRA_TYPE_ID``), ``values`` of shape (n,) or (n, k)
+    for k = 2, 3 elements and an optional ``description``. ``scale`` and
+    ``offset`` default to 0.001 and 0."""
     n = int(X.shape[0])
-    dt = _record_dtype(pdrf, extra is not None)
+    sc = tuple(scale) if scale is not None else (SCALE, SCALE, SCALE)
+    of = tuple(offset) if offset is not None else (0.0, 0.0, 0.0)
+    dt = _record_dtype(pdrf, extra is not None, extras)
     recs = np.zeros(n, dtype=dt)
     recs["X"], recs["Y"], recs["Z"] = X, Y, Z
     for k, v in attrs.items():
-        recs[k] = v
+        if k in dt.names:
+            recs[k] = v
     if extra is not None:
         recs["extra"] = extra
+    for e in extras:
+        recs[e["name"]] = e["values"]
     header_size = 227 if version_minor <= 2 else 375
-    vlrs = _extra_bytes_vlr() if extra is not None else b""
+    if extras:
+        descs = b"" if extra is None else _extra_descriptor("extra", 9, "N(0,1) float")
+        for e in extras:
+            k = e["values"].shape[1] if e["values"].ndim > 1 else 1
+            tid = _EXTRA_TYPE_ID[e["dtype"]] + 10 * (k - 1)
+            descs += _extra_descriptor(e["name"], tid, e.get("description", ""))
+        vlrs = _extra_bytes_vlr(descriptors=descs)
+    else:
+        vlrs = _extra_bytes_vlr() if extra is not None else b""
     offset_to_points = header_size + len(vlrs)
 
-    xs = X.astype(np.float64) * SCALE
-    ys = Y.astype(np.float64) * SCALE
-    zs = Z.astype(np.float64) * SCALE
+    # LASzip's coordinate: scale * X + offset (the header box holds them all)
+    xs = X.astype(np.float64) * sc[0] + of[0]
+    ys = Y.astype(np.float64) * sc[1] + of[1]
+    zs = Z.astype(np.float64) * sc[2] + of[2]
     h = bytearray(header_size)
     h[0:4] = b"LASF"
     h[24], h[25] = 1, version_minor
@@ -96,15 +136,15 @@ def write_las(X, Y, Z, attrs: dict, *, pdrf: int, version_minor: int,
     struct.pack_into("<HH", h, 90, 1, 2024)
     struct.pack_into("<H", h, 94, header_size)
     struct.pack_into("<I", h, 96, offset_to_points)
-    struct.pack_into("<I", h, 100, 1 if extra is not None else 0)
+    struct.pack_into("<I", h, 100, 1 if (extra is not None or extras) else 0)
     struct.pack_into("<B", h, 104, pdrf)
     struct.pack_into("<H", h, 105, dt.itemsize)
     struct.pack_into("<I", h, 107, n if n < 2**32 else 0)
     ret = (recs["bits"] & 7).astype(np.int64)
     byret = np.bincount(np.clip(ret, 1, 5) - 1, minlength=5)[:5] if n else np.zeros(5, np.int64)
     struct.pack_into("<5I", h, 111, *[int(v) if n < 2**32 else 0 for v in byret])
-    struct.pack_into("<3d", h, 131, SCALE, SCALE, SCALE)
-    struct.pack_into("<3d", h, 155, 0.0, 0.0, 0.0)
+    struct.pack_into("<3d", h, 131, *sc)
+    struct.pack_into("<3d", h, 155, *of)
     if n:
         struct.pack_into("<6d", h, 179, xs.max(), xs.min(), ys.max(), ys.min(), zs.max(), zs.min())
     if version_minor >= 4:
@@ -310,3 +350,57 @@ def cube(n: int, seed: int, extent: float = 1000.0) -> bytes:
 
 
 GENERATORS["cube"] = cube
+
+
+# Tile layout of ``tiles``: point format, scale and extra bytes per tile,
+# tiles taken row by row over a 2 x 2 grid.
+TILE_FORMATS = (2, 0, 3, 1)
+TILE_SCALES = (0.001, 0.01, 0.002, 0.005)
+TILE_EXTRAS = ((), (), ("amplitude",), ("amplitude", "deviation"))
+
+
+def tiles(n: int, seed: int, extent: float = 400.0, origin=(652000.0, 5187000.0, 230.0),
+          formats=TILE_FORMATS, scales=TILE_SCALES, extras=TILE_EXTRAS) -> list:
+    """A multi-file input: one terrain with facades, cut into a 2 x 2 grid of
+    tiles, each written as its own LAS file with its own point format,
+    scale and offset (the tile's corner, in projected coordinates of a few
+    hundred kilometres) and extra-bytes attributes. Returns the file images
+    in tile order; tile k holds about n / 4 points.
+
+    Extra-bytes attributes: ``amplitude`` (float32, N(30, 5)) and
+    ``deviation`` (uint16 x 2)."""
+    rng = np.random.default_rng(seed)
+    amps = rng.uniform(2.0, 10.0, 3)
+    freqs = rng.uniform(0.5, 3.0, (3, 2)) * (2 * np.pi / extent)
+    phases = rng.uniform(0, 2 * np.pi, 3)
+    x = rng.uniform(0, extent, n)
+    y = rng.uniform(0, extent, n)
+    z = np.zeros(n)
+    for a, (fx, fy), p in zip(amps, freqs, phases):
+        z += a * np.sin(fx * x + fy * y + p)
+    z += rng.normal(0, 0.05, n)
+    wall = rng.uniform(0, 1, n) < 0.1
+    z[wall] += rng.uniform(0, 20.0, int(wall.sum()))
+    attrs_all = _common_attrs(rng, n, z)
+    attrs_all["gps_time"] = np.arange(n, dtype=np.float64) * 1e-4 + 2.0e5
+    amplitude = rng.normal(30.0, 5.0, n).astype(np.float32)
+    deviation = rng.integers(0, 4096, (n, 2)).astype(np.uint16)
+    half = extent / 2.0
+    tile = (x >= half).astype(np.int64) + 2 * (y >= half).astype(np.int64)
+    out = []
+    for k, (fmt, sc) in enumerate(zip(formats, scales)):
+        sel = np.flatnonzero(tile == k)
+        tx, ty = (k % 2) * half, (k // 2) * half
+        off = (origin[0] + tx, origin[1] + ty, origin[2])
+        X = np.round((x[sel] - tx) / sc).astype(np.int32)
+        Y = np.round((y[sel] - ty) / sc).astype(np.int32)
+        Z = np.round(z[sel] / sc).astype(np.int32)
+        attrs = {key: v[sel] for key, v in attrs_all.items()}
+        ex = []
+        if "amplitude" in extras[k]:
+            ex.append({"name": "amplitude", "dtype": "<f4", "values": amplitude[sel], "description": "echo amplitude"})
+        if "deviation" in extras[k]:
+            ex.append({"name": "deviation", "dtype": "<u2", "values": deviation[sel], "description": "pulse deviation"})
+        out.append(write_las(X, Y, Z, attrs, pdrf=fmt, version_minor=4 if fmt in (1, 3) else 2,
+                             scale=(sc, sc, sc), offset=off, extras=ex))
+    return out

@@ -3,7 +3,10 @@ the determinism-pinned reference converter (oracle/_ref/PotreeConverter_pinned,
 built from the reference sources by oracle/Makefile) writes for seeded
 synthetic inputs. Run in a container that has the reference sources:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [--multi-only]
+
+--multi-only keeps the single-source cases of the existing file and
+regenerates the multi-source / --attributes cases.
 """
 
 import hashlib
@@ -33,30 +36,94 @@ CASES = [
 ]
 
 
+# Inputs of several sources and --attributes lists:
+# (case name, generator, points, seed, generator kwargs, source order,
+#  --attributes, samplers). The "tiles" generator returns one file image per
+# tile; the others one image. Source k is written as <case>_<k>.las (or
+# <case>.las for one source) and the sources are passed in `order`; the
+# metadata name is the first source's stem (main.cpp:146-200).
+ALL = ["poisson", "poisson_average", "random"]
+MULTI_CASES = [
+    ("tiles_200k", "tiles", 200_000, 11, {}, [0, 1, 2, 3], [], ALL),
+    ("tiles_2m_reversed", "tiles", 2_000_000, 12, {}, [3, 2, 1, 0], [], ALL),
+    ("tiles_300k_attrs", "tiles", 300_000, 13, {}, [0, 1, 2, 3],
+     ["gps-time", "rgb", "return number", "no such attribute"], ALL),
+    ("terrain_200k_attrs", "terrain", 200_000, 1000, {}, [0], ["rgb", "classification", "intensity"], ALL),
+    ("hotspots_300k_reordered", "hotspots", 300_000, 1001, {}, [0],
+     ["extra", "intensity", "return number", "number of returns", "classification", "scan angle rank",
+      "user data", "point source id", "gps-time", "rgb"], ALL),
+]
+
+
+def multi_sources(kind, n, seed, kw, order):
+    """File images of a multi-source case, in the order they are passed."""
+    if kind == "tiles":
+        imgs = synth.tiles(n, seed, **kw)
+    else:
+        imgs = [synth.generate(kind, n, seed, **kw)]
+    return [imgs[k] for k in order]
+
+
+def source_names(case, kind, order):
+    return [f"{case}_{k}" if kind == "tiles" else case for k in order]
+
+
 def md5(path):
     with open(path, "rb") as f:
         return hashlib.md5(f.read()).hexdigest()
 
 
+def run_multi(tmp):
+    cases = []
+    for name, kind, n, seed, kw, order, attrs, methods in MULTI_CASES:
+        imgs = multi_sources(kind, n, seed, kw, order)
+        names = source_names(name, kind, order)
+        paths = []
+        for nm, img in zip(names, imgs):
+            paths.append(os.path.join(tmp, nm + ".las"))
+            with open(paths[-1], "wb") as f:
+                f.write(img)
+        entry = {"name": name, "kind": kind, "points": n, "seed": seed, "kwargs": kw, "order": order,
+                 "attributes": attrs, "meta_name": names[0],
+                 "las_md5": [hashlib.md5(img).hexdigest() for img in imgs], "outputs": {}}
+        for m in methods:
+            od = os.path.join(tmp, f"{name}_{m}")
+            cmd = [REF] + paths + ["-o", od, "-m", m]
+            if attrs:
+                cmd += ["--attributes"] + attrs
+            subprocess.run(cmd, check=True, capture_output=True)
+            entry["outputs"][m] = {f: {"md5": md5(os.path.join(od, f)), "size": os.path.getsize(os.path.join(od, f))}
+                                   for f in ("octree.bin", "hierarchy.bin", "metadata.json")}
+            print(name, m, entry["outputs"][m]["octree.bin"]["size"], flush=True)
+        cases.append(entry)
+    return cases
+
+
 def main():
+    multi_only = "--multi-only" in sys.argv
+    path = os.path.join(HERE, "golden.json")
     out = {"generator": "potreeconverter_b200.synth", "reference": "PotreeConverter 2.0, pinned (oracle/pin/pin.h)",
            "random_seed": 1592614637, "cases": []}
+    if multi_only:  # keep the single-source cases of the existing file
+        with open(path) as f:
+            out["cases"] = json.load(f)["cases"]
     with tempfile.TemporaryDirectory() as tmp:
-        for name, kind, n, seed, kw, methods in CASES:
+        for name, kind, n, seed, kw, methods in ([] if multi_only else CASES):
             las = synth.generate(kind, n, seed, **kw)
-            path = os.path.join(tmp, name + ".las")
-            with open(path, "wb") as f:
+            path_las = os.path.join(tmp, name + ".las")
+            with open(path_las, "wb") as f:
                 f.write(las)
             entry = {"name": name, "kind": kind, "points": n, "seed": seed, "kwargs": kw,
                      "las_md5": hashlib.md5(las).hexdigest(), "outputs": {}}
             for m in methods:
                 od = os.path.join(tmp, f"{name}_{m}")
-                subprocess.run([REF, path, "-o", od, "-m", m], check=True, capture_output=True)
+                subprocess.run([REF, path_las, "-o", od, "-m", m], check=True, capture_output=True)
                 entry["outputs"][m] = {f: {"md5": md5(os.path.join(od, f)), "size": os.path.getsize(os.path.join(od, f))}
                                        for f in ("octree.bin", "hierarchy.bin", "metadata.json")}
                 print(name, m, entry["outputs"][m]["octree.bin"]["size"], flush=True)
             out["cases"].append(entry)
-    with open(os.path.join(HERE, "golden.json"), "w") as f:
+        out["multi_cases"] = run_multi(tmp)
+    with open(path, "w") as f:
         json.dump(out, f, indent=1)
 
 

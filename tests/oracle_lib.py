@@ -41,16 +41,28 @@ class Oracle:
         lib = ctypes.CDLL(ORACLE_LIB)
         lib.pcref_convert.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_char_p,
                                       ctypes.c_uint32, ctypes.POINTER(_Out)]
+        lib.pcref_convert_sources.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                              ctypes.c_int32, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint32,
+                                              ctypes.POINTER(_Out)]
         lib.pcref_free.argtypes = [ctypes.POINTER(_Out)]
         lib.pcref_std_sort_perm.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
         lib.pcref_std_shuffle.argtypes = [ctypes.c_int64, ctypes.c_uint32, ctypes.c_void_p]
         self.lib = lib
 
     def convert(self, las: bytes, method: str, name: str = "cloud", seed: int = PINNED_SEED):
-        buf = (ctypes.c_uint8 * len(las)).from_buffer_copy(las)
+        return self.convert_sources([las], method, name=name, seed=seed)
+
+    def convert_sources(self, sources, method: str, name: str = "cloud", seed: int = PINNED_SEED, attributes=()):
+        """Several LAS images as one cloud, in order, keeping only
+        `attributes` when given (the reference's --attributes)."""
+        bufs = [(ctypes.c_uint8 * len(las)).from_buffer_copy(las) for las in sources]
+        ptrs = (ctypes.c_void_p * len(bufs))(*[ctypes.addressof(b) for b in bufs])
+        sizes = (ctypes.c_uint64 * len(bufs))(*[len(las) for las in sources])
+        names = [a.encode() for a in attributes]
+        arr = (ctypes.c_char_p * max(1, len(names)))(*names)
         out = _Out()
-        rc = self.lib.pcref_convert(ctypes.addressof(buf), len(las), method.encode(), name.encode(), seed,
-                                    ctypes.byref(out))
+        rc = self.lib.pcref_convert_sources(ptrs, sizes, len(bufs), arr, len(names), method.encode(), name.encode(),
+                                            seed, ctypes.byref(out))
         if rc != 0:
             raise RuntimeError(out.error.decode())
         res = {
@@ -107,3 +119,19 @@ def las_for(case: dict) -> bytes:
 
 def md5(b: bytes) -> str:
     return hashlib.md5(b).hexdigest()
+
+
+@functools.lru_cache(maxsize=8)
+def _case_sources(kind: str, n: int, seed: int, kwargs_json: str, order: tuple) -> tuple:
+    from potreeconverter_b200 import synth
+    kw = json.loads(kwargs_json)
+    imgs = synth.tiles(n, seed, **kw) if kind == "tiles" else [synth.generate(kind, n, seed, **kw)]
+    return tuple(imgs[k] for k in order)
+
+
+def sources_for(case: dict) -> list:
+    """File images of a multi-source golden case, in the order passed."""
+    imgs = _case_sources(case["kind"], case["points"], case["seed"], json.dumps(case["kwargs"], sort_keys=True),
+                         tuple(case["order"]))
+    assert [hashlib.md5(b).hexdigest() for b in imgs] == case["las_md5"], "synthetic generator output changed"
+    return list(imgs)

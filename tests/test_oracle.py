@@ -4,9 +4,10 @@ converter produced for the same seeded inputs (tests/golden/golden.json)."""
 
 import pytest
 
-from tests.oracle_lib import las_for, load_golden, md5
+from tests.oracle_lib import las_for, load_golden, md5, sources_for
 
 CASES = [(c, m) for c in load_golden()["cases"] for m in c["outputs"]]
+MULTI = [(c, m) for c in load_golden()["multi_cases"] for m in c["outputs"]]
 
 
 @pytest.mark.parametrize("case,method", CASES, ids=[f"{c['name']}-{m}" for c, m in CASES])
@@ -15,6 +16,28 @@ def test_oracle_matches_pinned_reference(oracle, case, method):
     for f in ("octree.bin", "hierarchy.bin", "metadata.json"):
         assert len(out[f]) == case["outputs"][method][f]["size"], f
         assert md5(out[f]) == case["outputs"][method][f]["md5"], f
+
+
+@pytest.mark.parametrize("case,method", MULTI, ids=[f"{c['name']}-{m}" for c, m in MULTI])
+def test_oracle_sources_and_attributes_match_pinned_reference(oracle, case, method):
+    # several LAS files (point formats 0-3, own scales and offsets, extra
+    # bytes) and --attributes lists, against the pinned reference
+    out = oracle.convert_sources(sources_for(case), method, name=case["meta_name"], attributes=case["attributes"])
+    for f in ("octree.bin", "hierarchy.bin", "metadata.json"):
+        assert len(out[f]) == case["outputs"][method][f]["size"], f
+        assert md5(out[f]) == case["outputs"][method][f]["md5"], f
+
+
+def test_oracle_rejects_what_the_reference_leaves_undefined(oracle):
+    from potreeconverter_b200 import synth
+    tiles = synth.tiles(20_000, 3)
+    # extra bytes kept while standard attributes before them are dropped:
+    # the reference writes them past the point record
+    with pytest.raises(RuntimeError, match="past the point record"):
+        oracle.convert_sources(tiles, "poisson", attributes=["amplitude"])
+    # poisson_average reads rgb at offset -1 when rgb is filtered out
+    with pytest.raises(RuntimeError, match="rgb"):
+        oracle.convert_sources(tiles[:2], "poisson_average", attributes=["intensity"])
 
 
 def test_oracle_std_sort_ties_are_deterministic(oracle):
