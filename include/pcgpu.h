@@ -73,6 +73,16 @@ enum {
 	                                 pcg_result.octree is then a device pointer */
 };
 
+/* One input file of a job with several sources (the reference's source
+   list after curateSources, main.cpp:146-200). */
+typedef struct pcg_source {
+	const void* las;       /* uncompressed LAS file image (host memory); with
+	                          device_records set, only its header and VLRs
+	                          are read                                        */
+	uint64_t las_size;
+	const void* device_records; /* its point records in device memory, or NULL */
+} pcg_source;
+
 typedef struct pcg_job {
 	const void* las;       /* uncompressed LAS file image (host memory); with
 	                          device_records set, only its header and VLRs
@@ -81,10 +91,21 @@ typedef struct pcg_job {
 	int32_t method;        /* pcg_method                                      */
 	int32_t flags;         /* PCG_JOB_* bits                                  */
 	const char* name;      /* metadata.json "name" (the reference uses the
-	                          input file's stem, main.cpp:171-173)            */
+	                          first input's stem, main.cpp:171-173)           */
 	const char* projection;/* metadata.json "projection" (may be NULL)       */
 	const void* device_records; /* point records already in device memory
 	                          (record_length * point count bytes), or NULL    */
+	/* Several input files converted as one point cloud
+	   (computeOutputAttributes(sources, ...), PotreeConverter.h:195-276, and
+	   doChunking(sources, ...), chunker_countsort_laszip.cpp:1206): with
+	   num_sources > 0, sources[0 .. num_sources) are the input, in this
+	   order, and las / las_size / device_records are ignored.             */
+	int32_t num_sources;
+	/* --attributes (main.cpp:108): keep "position" and these attributes, in
+	   this order (names not found are skipped); 0 keeps every attribute.  */
+	int32_t num_attributes;
+	const pcg_source* sources;
+	const char* const* attributes;
 } pcg_job;
 
 typedef struct pcg_stats {

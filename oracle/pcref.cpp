@@ -506,6 +506,18 @@ static bool doChunking(Job& job, vector<Chunk>& chunksOut, Attributes& attrsOut,
 	minOut = min; maxOut = max;
 	attrsOut = stats;
 	attrsOut.posScale = out.posScale; attrsOut.posOffset = out.posOffset;
+	// the statistics reach the indexer through the chunks' metadata.json
+	// (writeMetadata, :1005-1070; read back at indexer.cpp:72-130): a
+	// non-finite value is written as null and read back as +Infinity, for
+	// min and max alike (an attribute no point of any source carries)
+	for (auto& a : attrsOut.list) {
+		double* mn[3] = {&a.min.x, &a.min.y, &a.min.z};
+		double* mx[3] = {&a.max.x, &a.max.y, &a.max.z};
+		for (int c = 0; c < a.numElements && c < 3; c++) {
+			if (!std::isfinite(*mn[c])) *mn[c] = Inf;
+			if (!std::isfinite(*mx[c])) *mx[c] = Inf;
+		}
+	}
 
 	// getChunks, indexer.cpp:53-179 -- chunk order pinned to file-name order
 	vector<size_t> order(nodes.size());

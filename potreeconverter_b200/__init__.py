@@ -38,10 +38,16 @@ class _Opts(ctypes.Structure):
                 ("reserved", ctypes.c_int32), ("stream", ctypes.c_void_p)]
 
 
+class _Source(ctypes.Structure):
+    _fields_ = [("las", ctypes.c_void_p), ("las_size", ctypes.c_uint64), ("device_records", ctypes.c_void_p)]
+
+
 class _Job(ctypes.Structure):
     _fields_ = [("las", ctypes.c_void_p), ("las_size", ctypes.c_uint64), ("method", ctypes.c_int32),
                 ("flags", ctypes.c_int32), ("name", ctypes.c_char_p), ("projection", ctypes.c_char_p),
-                ("device_records", ctypes.c_void_p)]
+                ("device_records", ctypes.c_void_p), ("num_sources", ctypes.c_int32),
+                ("num_attributes", ctypes.c_int32), ("sources", ctypes.POINTER(_Source)),
+                ("attributes", ctypes.POINTER(ctypes.c_char_p))]
 
 
 OCTREE_ON_DEVICE = 1
@@ -174,37 +180,60 @@ class Context:
         return PcgError(st, self._lib.pcg_last_error(self._h).decode(errors="replace"))
 
     @staticmethod
-    def _job(las, method, name, projection, keep, device_records=None, flags=0):
+    def _image(las, keep):
+        """(pointer, size) of one LAS image: bytes, a writable buffer, or
+        (host pointer, size) already."""
         if isinstance(las, bytes):
             # the library only reads the image: pass the bytes object's own buffer
             keep.append(las)
-            ptr, size = ctypes.cast(ctypes.c_char_p(las), ctypes.c_void_p).value, len(las)
-        elif isinstance(las, (bytearray, memoryview)):
+            return ctypes.cast(ctypes.c_char_p(las), ctypes.c_void_p).value, len(las)
+        if isinstance(las, (bytearray, memoryview)):
             buf = (ctypes.c_uint8 * len(las)).from_buffer(las)
             keep.append(buf)
-            ptr, size = ctypes.addressof(buf), len(las)
-        else:  # (pointer, size), e.g. pinned host memory
-            ptr, size = las
+            return ctypes.addressof(buf), len(las)
+        return las  # (pointer, size), e.g. pinned host memory
+
+    @classmethod
+    def _job(cls, las, method, name, projection, keep, device_records=None, flags=0, attributes=None):
+        """las: one LAS image, or a list of images converted as one cloud in
+        that order (the reference's source list)."""
         nm = name.encode()
         pj = projection.encode()
         keep.extend([nm, pj])
-        return _Job(ptr, size, METHODS[method], flags, nm, pj, device_records)
+        if isinstance(las, list):
+            srcs = (_Source * len(las))(*[_Source(*cls._image(img, keep), None) for img in las])
+            keep.append(srcs)
+            job = _Job(None, 0, METHODS[method], flags, nm, pj, None)
+            job.num_sources = len(las)
+            job.sources = srcs
+        else:
+            ptr, size = cls._image(las, keep)
+            job = _Job(ptr, size, METHODS[method], flags, nm, pj, device_records)
+        if attributes:
+            names = (ctypes.c_char_p * len(attributes))(*[a.encode() for a in attributes])
+            keep.append(names)
+            job.num_attributes = len(attributes)
+            job.attributes = names
+        return job
 
-    def convert(self, las, method: str = "poisson", name: str = "cloud", projection: str = "") -> Conversion:
-        """Converts one LAS file image (bytes, or (host pointer, size))."""
+    def convert(self, las, method: str = "poisson", name: str = "cloud", projection: str = "",
+                attributes=None) -> Conversion:
+        """Converts one LAS file image (bytes, or (host pointer, size)), or a
+        list of images as one point cloud. attributes: the --attributes
+        list (None keeps every attribute)."""
         keep = []
-        job = self._job(las, method, name, projection, keep)
+        job = self._job(las, method, name, projection, keep, attributes=attributes)
         res = _Result()
         st = self._lib.pcg_convert(self._h, ctypes.byref(job), ctypes.byref(res))
         if st != 0:
             raise self._err(st)
         return _take(self._lib, res)
 
-    def convert_stats(self, las, method: str = "poisson", name: str = "cloud") -> dict:
+    def convert_stats(self, las, method: str = "poisson", name: str = "cloud", attributes=None) -> dict:
         """Converts like :meth:`convert` (octree.bin lands in pinned host
         memory) but returns only the statistics, releasing the outputs."""
         keep = []
-        job = self._job(las, method, name, "", keep)
+        job = self._job(las, method, name, "", keep, attributes=attributes)
         res = _Result()
         st = self._lib.pcg_convert(self._h, ctypes.byref(job), ctypes.byref(res))
         if st != 0:
@@ -228,9 +257,10 @@ class Context:
         self._lib.pcg_result_free(ctypes.byref(res))
         return stats
 
-    def submit(self, las, method: str = "poisson", name: str = "cloud", projection: str = "") -> int:
+    def submit(self, las, method: str = "poisson", name: str = "cloud", projection: str = "", attributes=None) -> int:
+        """Queues a conversion (the images are copied at once); returns its id."""
         keep = []
-        job = self._job(las, method, name, projection, keep)
+        job = self._job(las, method, name, projection, keep, attributes=attributes)
         jid = ctypes.c_uint64()
         st = self._lib.pcg_submit(self._h, ctypes.byref(job), ctypes.byref(jid))
         if st != 0:
@@ -272,7 +302,29 @@ class Context:
 
 
 def convert(las, method: str = "poisson", name: str = "cloud", form: str = "batched", seed: int = PINNED_SEED,
-            device: int = 0) -> Conversion:
-    """One-shot conversion: PotreeConverter <in.las> -m method."""
+            device: int = 0, attributes=None) -> Conversion:
+    """One-shot conversion: PotreeConverter <in.las> [<in.las> ...] -m method
+    [--attributes ...]; las is one image or a list of images."""
     with Context(device=device, seed=seed, form=form) as ctx:
-        return ctx.convert(las, method=method, name=name)
+        return ctx.convert(las, method=method, name=name, attributes=attributes)
+
+
+def curate_sources(paths) -> tuple:
+    """The reference's input list (curateSources, main.cpp:146-200): every
+    path that is a directory contributes its entries whose names end in
+    "las" or "laz" (case-insensitive), in name order (the pinned order);
+    files are taken when their names end so. Returns (name, paths), name
+    being the stem of the first path given."""
+    expanded = []
+    name = ""
+    for p in paths:
+        if os.path.isdir(p):
+            for e in sorted(os.listdir(p)):
+                full = os.path.join(p, e)
+                if e.lower().endswith(("las", "laz")):
+                    expanded.append(full)
+        elif os.path.isfile(p) and p.lower().endswith(("las", "laz")):
+            expanded.append(p)
+        if not name:
+            name = os.path.splitext(os.path.basename(p))[0]  # fs::path(p).stem()
+    return name, expanded

@@ -50,8 +50,8 @@ __device__ void flush_int(AttrStatsDev* st, int comp, const IntRange& r, unsigne
 // the count-grid cell, counts into the grid with warp-aggregated atomics and
 // reduces attribute min/max (in registers, then shared memory, then one
 // global atomic per block and statistic).
-__global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(const uint8_t* __restrict__ recs, DecodeParams p,
-                                                                    uint32_t* __restrict__ grid, ChunkingOut out) {
+template <bool kMulti>
+__global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodeParams p, uint32_t* __restrict__ grid, ChunkingOut out) {
 	// shared statistics: [attr][comp] ordered min / max
 	__shared__ unsigned long long s_mn[MAX_ATTRS][3];
 	__shared__ unsigned long long s_mx[MAX_ATTRS][3];
@@ -71,11 +71,11 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(const uint
 	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
 	const int G = p.grid;
 	const double dG = (double)G;
-	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride) {
-		const uint8_t* r = recs + i * p.rec_len;
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride) with_source<kMulti>(p, i, [&](const SourceDesc& sd) {
+		const uint8_t* r = sd.recs + (i - sd.first) * sd.rec_len;
 		double x, y, z;
 		int32_t X, Y, Z;
-		quantize_record(p, r, x, y, z, X, Y, Z);
+		quantize_record(p, sd, r, x, y, z, X, Y, Z);
 		// unit cube coordinates and cell (:232-257)
 		double ux = ((double)X * p.pos_scale[0] + p.pos_offset[0] - p.cmin[0]) / p.csize;
 		double uy = ((double)Y * p.pos_scale[1] + p.pos_offset[1] - p.cmin[1]) / p.csize;
@@ -117,18 +117,18 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(const uint
 		if (p.stat_sar >= 0) r_sar.add((int8_t)r[16]);
 		if (p.stat_user >= 0) r_user.add(r[17]);
 		if (p.stat_psid >= 0) r_psid.add(ld<uint16_t>(r + 18));
-		if (p.stat_gps >= 0) {
-			double g = ld<double>(r + p.src_gps);
+		if (p.stat_gps >= 0 && sd.src_gps >= 0) {
+			double g = ld<double>(r + sd.src_gps);
 			gmn = dmin(gmn, g);
 			gmx = dmax(gmx, g);
 		}
-		if (p.stat_rgb >= 0) {
-			r_r.add(ld<uint16_t>(r + p.src_rgb));
-			r_g.add(ld<uint16_t>(r + p.src_rgb + 2));
-			r_b.add(ld<uint16_t>(r + p.src_rgb + 4));
+		if (p.stat_rgb >= 0 && sd.src_rgb >= 0) {
+			r_r.add(ld<uint16_t>(r + sd.src_rgb));
+			r_g.add(ld<uint16_t>(r + sd.src_rgb + 2));
+			r_b.add(ld<uint16_t>(r + sd.src_rgb + 4));
 		}
-		for (int e = 0; e < p.n_extra; e++) {
-			const ExtraDesc& d = p.extra[e];
+		for (int e = 0; e < sd.n_extra; e++) {
+			const ExtraDesc& d = sd.extra[e];
 			for (int c = 0; c < d.num_elements && c < 3; c++) {
 				const uint8_t* q = r + d.src_off + c * d.element_size;
 				double v = 0.0;
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(const uint
 				atomicMax(&s_mx[d.stat_index][c], ordered(v));
 			}
 		}
-	}
+	});
 	// block reduction of the register accumulators
 	if (pmn[0] <= pmx[0]) {
 		for (int c = 0; c < 3; c++) {
@@ -253,7 +253,7 @@ __global__ void assign_kernel(const uint32_t* __restrict__ cell, const int32_t* 
 
 }  // namespace
 
-void launch_decode_count(const uint8_t* d_recs, const DecodeParams& p, uint32_t* grid, ChunkingOut& out, DeviceMem& mem) {
+void launch_decode_count(const DecodeParams& p, uint32_t* grid, ChunkingOut& out, DeviceMem& mem) {
 	if (p.n == 0) return;
 	int dev = 0;
 	PCG_CUDA(cudaGetDevice(&dev));
@@ -263,7 +263,8 @@ void launch_decode_count(const uint8_t* d_recs, const DecodeParams& p, uint32_t*
 	int64_t cap = (int64_t)sms * 8;
 	if (blocks > cap) blocks = cap;
 	if (blocks < 1) blocks = 1;
-	decode_count_kernel<<<(unsigned)blocks, kDecodeThreads, 0, mem.stream()>>>(d_recs, p, grid, out);
+	if (p.nsrc > 1) decode_count_kernel<true><<<(unsigned)blocks, kDecodeThreads, 0, mem.stream()>>>(p, grid, out);
+	else decode_count_kernel<false><<<(unsigned)blocks, kDecodeThreads, 0, mem.stream()>>>(p, grid, out);
 	PCG_LAUNCHED();
 }
 

@@ -1,15 +1,22 @@
 // PotreeConverter-compatible command line (flags of main.cpp:21-145):
 //
-//   PotreeConverter <input.las> -o <outdir> [-m poisson|poisson_average|random]
-//                   [--projection <string>] [--encoding DEFAULT]
-//                   [--plain] [--device N] [--seed N]
+//   PotreeConverter <source> [<source> ...] -o <outdir>
+//                   [-m poisson|poisson_average|random]
+//                   [--attributes <name> ...] [--projection <string>]
+//                   [--encoding DEFAULT] [--plain] [--device N] [--seed N]
 //
-// Writes octree.bin, hierarchy.bin and metadata.json through libpcgpu.
-// --plain selects the one-launch-per-node form; --seed sets the random
-// sampler's leaf-shuffle seed (the pinned reference uses 1592614637).
-// Flags of the reference that this build does not implement (BROTLI
-// encoding, --attributes filtering, page generation) are rejected.
+// Sources are LAS files or directories of them, taken like the reference's
+// curateSources (main.cpp:146-200; directory entries in name order); all
+// are converted as one point cloud named after the first source's stem.
+// --attributes keeps "position" and the named attributes, in that order
+// (PotreeConverter.h:252-275). Writes octree.bin, hierarchy.bin and
+// metadata.json through libpcgpu. --plain selects the one-launch-per-node
+// form; --seed sets the random sampler's leaf-shuffle seed (the pinned
+// reference uses 1592614637). Flags of the reference that this build does
+// not implement (BROTLI encoding, page generation) are rejected.
 
+#include <algorithm>
+#include <cctype>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -24,48 +31,92 @@
 namespace fs = std::filesystem;
 
 static int usage() {
-	fprintf(stderr, "PotreeConverter <source> -o <outdir> [-m poisson|poisson_average|random] [--projection P] [--plain]\n");
+	fprintf(stderr, "PotreeConverter <source> [<source> ...] -o <outdir> [-m poisson|poisson_average|random] [--attributes a ...] [--projection P] [--plain]\n");
 	return 1;
 }
 
+static bool ends_with_ci(const std::string& s, const char* suffix) {  // iEndsWith (unsuck.hpp)
+	const size_t n = std::strlen(suffix);
+	if (s.size() < n) return false;
+	for (size_t i = 0; i < n; i++)
+		if (std::tolower((unsigned char)s[s.size() - n + i]) != std::tolower((unsigned char)suffix[i])) return false;
+	return true;
+}
+
 int main(int argc, char** argv) {
-	std::string source, outdir, method = "poisson", encoding = "DEFAULT", projection;
+	std::vector<std::string> source, attributes;
+	std::string outdir, method = "poisson", encoding = "DEFAULT", projection;
 	pcg_opts opts{0, 1592614637u, PCG_FORM_BATCHED, 0};
+	bool in_attributes = false;
 	for (int i = 1; i < argc; i++) {
 		std::string a = argv[i];
 		auto val = [&]() -> std::string {
 			if (i + 1 >= argc) { fprintf(stderr, "missing value for %s\n", a.c_str()); exit(1); }
 			return argv[++i];
 		};
+		if (!a.empty() && a[0] == '-') in_attributes = false;
 		if (a == "-h" || a == "--help") return usage() ? 0 : 0;
-		else if (a == "-i" || a == "--source") source = val();
+		else if (a == "-i" || a == "--source") source.push_back(val());
 		else if (a == "-o" || a == "--outdir") outdir = val();
 		else if (a == "-m" || a == "--method") method = val();
 		else if (a == "--encoding") encoding = val();
 		else if (a == "--projection") projection = val();
+		else if (a == "--attributes") in_attributes = true;
 		else if (a == "--plain") opts.form = PCG_FORM_PLAIN;
 		else if (a == "--device") opts.device = atoi(val().c_str());
 		else if (a == "--seed") opts.random_seed = (uint32_t)strtoul(val().c_str(), nullptr, 10);
 		else if (a == "--chunkMethod") { if (val() != "LASZIP") { fprintf(stderr, "only --chunkMethod LASZIP is supported\n"); return 1; } }
-		else if (a == "--attributes" || a == "-p" || a == "--generate-page" || a == "--title") { fprintf(stderr, "%s is not supported by this build\n", a.c_str()); return 1; }
+		else if (a == "-p" || a == "--generate-page" || a == "--title") { fprintf(stderr, "%s is not supported by this build\n", a.c_str()); return 1; }
 		else if (a == "--keep-chunks" || a == "--no-chunking" || a == "--no-indexing") { fprintf(stderr, "%s is not supported (no chunk files are written)\n", a.c_str()); return 1; }
 		else if (!a.empty() && a[0] == '-') { fprintf(stderr, "unknown flag %s\n", a.c_str()); return 1; }
-		else source = a;
+		else if (in_attributes) attributes.push_back(a);
+		else source.push_back(a);
 	}
 	if (source.empty()) return usage();
 	if (encoding != "DEFAULT" && encoding != "UNCOMPRESSED") { fprintf(stderr, "encoding %s is not supported\n", encoding.c_str()); return 1; }
 	int m = method == "poisson" ? PCG_POISSON : method == "poisson_average" ? PCG_POISSON_AVERAGE : method == "random" ? PCG_RANDOM : -1;
 	if (m < 0) { fprintf(stderr, "unknown method %s\n", method.c_str()); return 1; }
-	if (!fs::exists(source)) { fprintf(stderr, "file does not exist: %s\n", source.c_str()); return 123; }
-	if (outdir.empty()) outdir = source + "/../" + fs::path(source).filename().string() + "_converted";  // main.cpp:64-101
-	std::ifstream f(source, std::ios::binary);
-	std::vector<uint8_t> las((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
-	std::string name = fs::path(source).stem().string();  // main.cpp:171-173
+	if (!fs::exists(source[0])) { fprintf(stderr, "file does not exist: %s\n", source[0].c_str()); return 123; }
+	if (outdir.empty()) outdir = source[0] + "/../" + fs::path(source[0]).filename().string() + "_converted";  // main.cpp:64-101
+	// curateSources, main.cpp:146-200
+	std::string name;
+	std::vector<std::string> paths;
+	for (auto& path : source) {
+		if (fs::is_directory(path)) {
+			std::vector<std::string> entries;
+			for (auto& e : fs::directory_iterator(path)) {
+				std::string str = e.path().string();
+				if (ends_with_ci(str, "las") || ends_with_ci(str, "laz")) entries.push_back(str);
+			}
+			std::sort(entries.begin(), entries.end());
+			paths.insert(paths.end(), entries.begin(), entries.end());
+		} else if (fs::is_regular_file(path)) {
+			if (ends_with_ci(path, "las") || ends_with_ci(path, "laz")) paths.push_back(path);
+		}
+		if (name.empty()) name = fs::path(path).stem().string();
+	}
+	if (paths.empty()) { fprintf(stderr, "no LAS input among the sources\n"); return 1; }
+	std::vector<std::vector<uint8_t>> images;
+	for (auto& path : paths) {
+		std::ifstream f(path, std::ios::binary);
+		images.emplace_back((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+	}
+	std::vector<pcg_source> srcs;
+	for (auto& img : images) srcs.push_back({img.data(), img.size(), nullptr});
+	std::vector<const char*> attr_names;
+	for (auto& a : attributes) attr_names.push_back(a.c_str());
 
 	pcg_ctx* ctx = nullptr;
 	pcg_status st = pcg_create(&ctx, &opts);
 	if (st != PCG_OK) { fprintf(stderr, "pcg_create failed: %s\n", pcg_status_string(st)); return 1; }
-	pcg_job job{las.data(), las.size(), m, 0, name.c_str(), projection.c_str()};
+	pcg_job job{};
+	job.method = m;
+	job.name = name.c_str();
+	job.projection = projection.c_str();
+	job.num_sources = (int32_t)srcs.size();
+	job.sources = srcs.data();
+	job.num_attributes = (int32_t)attr_names.size();
+	job.attributes = attr_names.empty() ? nullptr : attr_names.data();
 	pcg_result res{};
 	st = pcg_convert(ctx, &job, &res);
 	if (st != PCG_OK) {

@@ -19,7 +19,8 @@ struct ChunkingOut {
 	int64_t* error;                          // [0] = first failing point + 1 (out of box), [1] = lookup failure
 };
 
-void launch_decode_count(const uint8_t* d_recs, const DecodeParams& p, uint32_t* grid, ChunkingOut& out, DeviceMem& mem);
+// Decodes the records of every source (DecodeParams::src0 / srcs).
+void launch_decode_count(const DecodeParams& p, uint32_t* grid, ChunkingOut& out, DeviceMem& mem);
 // Pyramid merge of the count grid (createLUT, chunker_countsort_laszip.cpp:1074-1204).
 void launch_lut_merge(const uint32_t* grid, int grid_size, int64_t max_points_per_chunk, ChunkCell* chunks,
                       int32_t* num_chunks, int capacity, DeviceMem& mem);

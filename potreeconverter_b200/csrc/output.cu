@@ -13,12 +13,19 @@ namespace {
 
 template <class T> __device__ __forceinline__ void st(uint8_t* p, T v) { memcpy(p, &v, sizeof(T)); }
 
-// Output record of point `id` from its LAS record r; has_col overrides rgb
-// with col (poisson_average).
-__device__ void assemble_record(const uint8_t* r, const DecodeParams& p, uint64_t col, bool has_col, uint8_t* dst) {
+// Output record of a point from its LAS record r, as the chunker's handlers
+// build it: bytes no handler of the source writes stay zero (the batch
+// buffer is cleared, :729-732), the standard attributes go to their output
+// offsets, then the extra bytes to theirs (a kept extra can land on another
+// attribute's bytes, :565-653). has_col then overrides rgb with col, as
+// poisson_average rewrites the colour of the chunk records
+// (sampler_poisson_average.h:437-446).
+__device__ void assemble_record(const uint8_t* r, const DecodeParams& p, const SourceDesc& sd, uint64_t col, bool has_col, uint8_t* dst) {
+	if (sd.zero_fill)
+		for (int k = 12; k < p.bpp; k++) dst[k] = 0;
 	double x, y, z;
 	int32_t X, Y, Z;
-	quantize_record(p, r, x, y, z, X, Y, Z);
+	quantize_record(p, sd, r, x, y, z, X, Y, Z);
 	st<int32_t>(dst + 0, X);
 	st<int32_t>(dst + 4, Y);
 	st<int32_t>(dst + 8, Z);
@@ -29,21 +36,36 @@ __device__ void assemble_record(const uint8_t* r, const DecodeParams& p, uint64_
 	if (p.off_sar >= 0) dst[p.off_sar] = r[16];
 	if (p.off_user >= 0) dst[p.off_user] = r[17];
 	if (p.off_psid >= 0) { dst[p.off_psid] = r[18]; dst[p.off_psid + 1] = r[19]; }
-	if (p.off_gps >= 0)
-		for (int k = 0; k < 8; k++) dst[p.off_gps + k] = r[p.src_gps + k];
-	if (p.off_rgb >= 0) {
-		if (has_col) {
-			st<uint16_t>(dst + p.off_rgb, (uint16_t)(col & 0xffff));
-			st<uint16_t>(dst + p.off_rgb + 2, (uint16_t)((col >> 16) & 0xffff));
-			st<uint16_t>(dst + p.off_rgb + 4, (uint16_t)((col >> 32) & 0xffff));
-		} else {
-			for (int k = 0; k < 6; k++) dst[p.off_rgb + k] = r[p.src_rgb + k];
-		}
-	}
-	for (int e = 0; e < p.n_extra; e++) {
-		const ExtraDesc& d = p.extra[e];
+	if (p.off_gps >= 0 && sd.src_gps >= 0)
+		for (int k = 0; k < 8; k++) dst[p.off_gps + k] = r[sd.src_gps + k];
+	if (p.off_rgb >= 0 && sd.src_rgb >= 0)
+		for (int k = 0; k < 6; k++) dst[p.off_rgb + k] = r[sd.src_rgb + k];
+	for (int e = 0; e < sd.n_extra; e++) {
+		const ExtraDesc& d = sd.extra[e];
 		for (int k = 0; k < d.size; k++) dst[d.dst_off + k] = r[d.src_off + k];
 	}
+	if (has_col) {
+		st<uint16_t>(dst + p.off_rgb, (uint16_t)(col & 0xffff));
+		st<uint16_t>(dst + p.off_rgb + 2, (uint16_t)((col >> 16) & 0xffff));
+		st<uint16_t>(dst + p.off_rgb + 4, (uint16_t)((col >> 32) & 0xffff));
+	}
+}
+
+// The six rgb bytes of a point's output record (before any colour
+// averaging): the source's colour, or zeros, with the bytes of kept extras
+// that land on them.
+__device__ __forceinline__ uint64_t record_rgb(const uint8_t* r, const DecodeParams& p, const SourceDesc& sd) {
+	uint64_t c = 0;  // the six bytes, little endian: r | g << 16 | b << 32
+	if (sd.src_rgb >= 0)
+		for (int k = 0; k < 6; k++) c |= (uint64_t)r[sd.src_rgb + k] << (8 * k);
+	for (int e = 0; e < sd.n_extra; e++) {
+		const ExtraDesc& d = sd.extra[e];
+		for (int k = 0; k < d.size; k++) {
+			const int o = d.dst_off + k - p.off_rgb;
+			if (o >= 0 && o < 6) c = (c & ~(0xffull << (8 * o))) | ((uint64_t)r[d.src_off + k] << (8 * o));
+		}
+	}
+	return c;
 }
 
 constexpr int kOutThreads = 256;
@@ -56,16 +78,17 @@ __host__ __device__ __forceinline__ int rec_words(int rec_len) { return (rec_len
 // contiguous in completion order, so a CTA spans one or a few payloads).
 // Each thread copies its LAS record into shared memory with aligned 4-byte
 // loads (byte loads for the last records, whose cover would reach past the
-// buffer), assembles the output record there -- requantizing the record's
-// own coordinates -- and the CTA writes its span with 4-byte stores.
-__global__ void __launch_bounds__(kOutThreads) write_payloads_kernel(const uint8_t* __restrict__ recs, int64_t rec_bytes, DecodeParams p,
-                                                                    const PayloadItem* __restrict__ items, const int32_t* __restrict__ chunk_item,
-                                                                    int64_t total, uint8_t* __restrict__ out) {
+// source's records), assembles the output record there -- requantizing the
+// record's own coordinates -- and the CTA writes its span with 4-byte
+// stores.
+template <bool kMulti>
+__global__ void __launch_bounds__(kOutThreads) write_payloads_kernel(DecodeParams p, const PayloadItem* __restrict__ items,
+                                                                    const int32_t* __restrict__ chunk_item, int64_t total,
+                                                                    uint8_t* __restrict__ out) {
 	extern __shared__ uint32_t smem_words[];
-	const int bpp = p.bpp, rl = p.rec_len, rw = rec_words(rl);
+	const int bpp = p.bpp, rw = rec_words(p.max_rec_len);
 	uint32_t* scratch = smem_words + threadIdx.x * rw;
 	uint8_t* stage = reinterpret_cast<uint8_t*>(smem_words + kOutThreads * rw);
-	const bool aligned = (reinterpret_cast<uintptr_t>(recs) & 3) == 0;
 	const int64_t q0 = (int64_t)blockIdx.x * kOutThreads, q = q0 + threadIdx.x;
 	const int64_t nthis = total - q0 < kOutThreads ? total - q0 : kOutThreads;
 	if (q < total) {
@@ -74,19 +97,24 @@ __global__ void __launch_bounds__(kOutThreads) write_payloads_kernel(const uint8
 		const PayloadItem& it = items[k];
 		const int64_t t = q - it.out_offset;
 		const uint32_t id = it.ids[t];
-		const int64_t start = (int64_t)id * rl;
-		const int64_t w0 = start >> 2, w1 = (start + rl + 3) >> 2;
-		const uint8_t* r;
-		if (aligned && w1 * 4 <= rec_bytes) {
-			const uint32_t* src = reinterpret_cast<const uint32_t*>(recs) + w0;
-			for (int w = 0; w < (int)(w1 - w0); w++) scratch[w] = src[w];
-			r = reinterpret_cast<const uint8_t*>(scratch) + (start & 3);
-		} else {
-			uint8_t* sb = reinterpret_cast<uint8_t*>(scratch);
-			for (int w = 0; w < rl; w++) sb[w] = recs[start + w];
-			r = sb;
-		}
-		assemble_record(r, p, it.cols ? it.cols[t] : 0ull, it.cols != nullptr, stage + threadIdx.x * bpp);
+		with_source<kMulti>(p, id, [&](const SourceDesc& sd) {
+			const int rl = sd.rec_len;
+			const uint8_t* recs = sd.recs;
+			const int64_t start = ((int64_t)id - sd.first) * rl;
+			const int64_t w0 = start >> 2, w1 = (start + rl + 3) >> 2;
+			const bool aligned = (reinterpret_cast<uintptr_t>(recs) & 3) == 0;
+			const uint8_t* r;
+			if (aligned && w1 * 4 <= sd.count * rl) {
+				const uint32_t* src = reinterpret_cast<const uint32_t*>(recs) + w0;
+				for (int w = 0; w < (int)(w1 - w0); w++) scratch[w] = src[w];
+				r = reinterpret_cast<const uint8_t*>(scratch) + (start & 3);
+			} else {
+				uint8_t* sb = reinterpret_cast<uint8_t*>(scratch);
+				for (int w = 0; w < rl; w++) sb[w] = recs[start + w];
+				r = sb;
+			}
+			assemble_record(r, p, sd, it.cols ? it.cols[t] : 0ull, it.cols != nullptr, stage + threadIdx.x * bpp);
+		});
 	}
 	__syncthreads();
 	const int64_t bytes = nthis * bpp;
@@ -104,15 +132,12 @@ __global__ void __launch_bounds__(kOutThreads) write_payloads_kernel(const uint8
 	for (int64_t b = head + 4 * words + threadIdx.x; b < bytes; b += kOutThreads) dst[b] = stage[b];
 }
 
-__global__ void fill_colors_kernel(const uint8_t* __restrict__ recs, int rec_len, int src_rgb, const uint32_t* __restrict__ ids, int64_t n,
-                                   uint64_t* __restrict__ cols) {
+template <bool kMulti>
+__global__ void fill_colors_kernel(DecodeParams p, const uint32_t* __restrict__ ids, int64_t n, uint64_t* __restrict__ cols) {
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	const uint8_t* r = recs + (int64_t)ids[i] * rec_len + src_rgb;
-	uint64_t red = (uint64_t)r[0] | ((uint64_t)r[1] << 8);
-	uint64_t green = (uint64_t)r[2] | ((uint64_t)r[3] << 8);
-	uint64_t blue = (uint64_t)r[4] | ((uint64_t)r[5] << 8);
-	cols[i] = red | (green << 16) | (blue << 32);
+	const uint32_t id = ids[i];
+	with_source<kMulti>(p, id, [&](const SourceDesc& sd) { cols[i] = record_rgb(sd.recs + ((int64_t)id - sd.first) * sd.rec_len, p, sd); });
 }
 
 __global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const int64_t* __restrict__ idx, int64_t n, uint32_t* __restrict__ dst) {
@@ -142,14 +167,15 @@ __global__ void split_kernel(const uint8_t* __restrict__ accepted, const uint32_
 
 }  // namespace
 
-void launch_write_payloads(const uint8_t* d_recs, const DecodeParams& p, const std::vector<PayloadItem>& items, const PayloadItem* d_items,
-                           uint8_t* out, DeviceMem& mem) {
+void launch_write_payloads(const DecodeParams& p, const std::vector<PayloadItem>& items, const PayloadItem* d_items, uint8_t* out,
+                           DeviceMem& mem) {
 	if (items.empty()) return;
 	const int64_t total = items.back().out_offset + items.back().count;
 	if (total == 0) return;
-	size_t smem = (size_t)kOutThreads * (rec_words(p.rec_len) * 4 + p.bpp);
+	size_t smem = (size_t)kOutThreads * (rec_words(p.max_rec_len) * 4 + p.bpp);
 	if (smem > 200 * 1024) throw PcgError(1, "point records too long for the payload writer (record + output > 800 bytes)");
-	if (smem > 48 * 1024) PCG_CUDA(cudaFuncSetAttribute(write_payloads_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	auto kernel = p.nsrc > 1 ? write_payloads_kernel<true> : write_payloads_kernel<false>;
+	if (smem > 48 * 1024) PCG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 	// the payload holding the first point of every 256-point chunk
 	const int64_t chunks = ceil_div(total, kOutThreads);
 	std::vector<int32_t> chunk_item(chunks);
@@ -161,14 +187,15 @@ void launch_write_payloads(const uint8_t* d_recs, const DecodeParams& p, const s
 	}
 	int32_t* d_ci = mem.alloc<int32_t>(chunks);
 	PCG_CUDA(cudaMemcpyAsync(d_ci, chunk_item.data(), chunks * sizeof(int32_t), cudaMemcpyHostToDevice, mem.stream()));
-	write_payloads_kernel<<<(unsigned)chunks, kOutThreads, smem, mem.stream()>>>(d_recs, p.n * (int64_t)p.rec_len, p, d_items, d_ci, total, out);
+	kernel<<<(unsigned)chunks, kOutThreads, smem, mem.stream()>>>(p, d_items, d_ci, total, out);
 	PCG_LAUNCHED();
 	mem.free(d_ci);
 }
 
-void launch_fill_colors(const uint8_t* d_recs, int rec_len, int src_rgb, const uint32_t* ids, int64_t n, uint64_t* cols, DeviceMem& mem) {
+void launch_fill_colors(const DecodeParams& p, const uint32_t* ids, int64_t n, uint64_t* cols, DeviceMem& mem) {
 	if (n == 0) return;
-	fill_colors_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(d_recs, rec_len, src_rgb, ids, n, cols);
+	if (p.nsrc > 1) fill_colors_kernel<true><<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(p, ids, n, cols);
+	else fill_colors_kernel<false><<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(p, ids, n, cols);
 	PCG_LAUNCHED();
 }
 

@@ -13,9 +13,10 @@ struct PayloadItem {        // one completed node with points
 };
 
 // items: host copy of d_items (payloads in completion order, contiguous)
-void launch_write_payloads(const uint8_t* d_recs, const DecodeParams& p, const std::vector<PayloadItem>& items, const PayloadItem* d_items,
-                           uint8_t* out, DeviceMem& mem);
-void launch_fill_colors(const uint8_t* d_recs, int rec_len, int src_rgb, const uint32_t* ids, int64_t n, uint64_t* cols, DeviceMem& mem);
+void launch_write_payloads(const DecodeParams& p, const std::vector<PayloadItem>& items, const PayloadItem* d_items, uint8_t* out,
+                           DeviceMem& mem);
+// Packed colour (r | g << 16 | b << 32) of every point's output record.
+void launch_fill_colors(const DecodeParams& p, const uint32_t* ids, int64_t n, uint64_t* cols, DeviceMem& mem);
 void launch_gather_u32(const uint32_t* src, const int64_t* idx, int64_t n, uint32_t* dst, DeviceMem& mem);
 // Stable split of candidates by accepted flag: pre = exclusive prefix of the
 // flags (n + 1 entries), accepted ids (and colours, records) compacted in

@@ -71,13 +71,29 @@ struct LasInfo {
 	std::vector<Vlr> vlrs;
 };
 
-// All FP64 set-up the reference performs on the host before chunking:
-// attribute schema (PotreeConverter.h:136-193), scale/offset
+// One input file as the chunker's attribute handlers see it
+// (createAttributeHandlers, chunker_countsort_laszip.cpp:380-658, built per
+// source from its own attribute list, :952-983).
+struct SourceSetup {
+	LasInfo las;
+	std::vector<AttrDesc> attrs;    // the source's own attribute list (PotreeConverter.h:136-193)
+	int std_record_length = 0;      // LAS record bytes before extra bytes
+	// extra-bytes handlers (:579-653): `size` bytes from LAS record offset
+	// src_off to output offset dst_off; statistics go to output attribute
+	// out_index, read with that attribute's type and element layout
+	struct Extra { int src_off, dst_off, size, out_index; };
+	std::vector<Extra> extras;
+	bool zero_fill = false;         // some output bytes stay zero (memset, :729-732)
+};
+
+// All FP64 set-up the reference performs on the host before chunking, for
+// the sources in the order given: output attribute schema (union by name,
+// then the --attributes filter, PotreeConverter.h:195-276), scale/offset
 // (PotreeConverter.h:29-76), cubic box (main.cpp:215-284), chunk grid size
 // and chunk capacity (chunker_countsort_laszip.cpp:1210-1220).
 struct Setup {
-	LasInfo las;
-	std::vector<AttrDesc> attrs;
+	std::vector<SourceSetup> sources;
+	std::vector<AttrDesc> attrs;    // output attributes
 	int bpp = 0;
 	Vec3d pos_scale, pos_offset;
 	Vec3d cube_min, cube_max;       // max = min + cubeSize (main.cpp:237-239)
@@ -86,14 +102,15 @@ struct Setup {
 	int64_t total_points = 0;
 	int grid_size = 128;
 	int max_points_per_chunk = 0;   // min(total/20, 10M) as int
-	int std_record_length = 0;      // LAS record bytes before extra bytes
-	int first_extra_index = 0;
 };
 
 // points_elsewhere: the point records are not part of this buffer (they are
 // already in device memory), so only the header and VLRs must be present.
 bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& err, bool points_elsewhere = false);
-bool make_setup(const LasInfo& info, Setup& s, std::string& err);
+// requested: the --attributes names (empty: every attribute). Jobs whose
+// result the reference leaves undefined are refused with a message.
+bool make_setup(const std::vector<LasInfo>& sources, const std::vector<std::string>& requested, Setup& s, std::string& err);
+inline bool make_setup(const LasInfo& info, Setup& s, std::string& err) { return make_setup(std::vector<LasInfo>{info}, {}, s, err); }
 
 // ---------------------------------------------------------- device params
 struct ExtraDesc {
@@ -103,18 +120,34 @@ struct ExtraDesc {
 constexpr int MAX_EXTRA = 16;
 constexpr int MAX_ATTRS = 32;
 
-struct DecodeParams {
+// One input file on the device: where its records are, how its coordinates
+// decode, and which bytes its handlers move.
+struct SourceDesc {
 	double in_scale[3], in_offset[3];
+	const uint8_t* recs;  // device pointer to its first point record
+	int64_t first;        // job index of its first point
+	int64_t count;        // its points
+	int rec_len;
+	int src_gps, src_rgb; // record offsets of GPS time / RGB, -1 when absent
+	int zero_fill;        // output bytes not written by its handlers stay zero
+	int n_extra, pad;
+	ExtraDesc extra[MAX_EXTRA];
+};
+
+struct DecodeParams {
 	double pos_scale[3], pos_offset[3];
 	double cmin[3];
 	double csize;         // chunk_cube_size
-	int64_t n;
-	int rec_len, pdrf, bpp, grid;
+	int64_t n;            // points over all sources
+	int bpp, grid;
+	// output offsets of the standard attributes, -1 when not in the output
 	int off_intensity, off_retnum, off_nret, off_class, off_sar, off_user, off_psid, off_gps, off_rgb;
-	int src_rgb, src_gps;
 	int stat_intensity, stat_retnum, stat_nret, stat_class, stat_sar, stat_user, stat_psid, stat_gps, stat_rgb, stat_pos;
-	int n_extra;
-	ExtraDesc extra[MAX_EXTRA];
+	int nsrc;             // sources; kernels for one source read src0
+	int max_rec_len;
+	const SourceDesc* srcs;     // device table of the nsrc sources
+	const int64_t* src_first;   // device: first job index of every source
+	SourceDesc src0;
 };
 
 // Attribute statistics as order-preserving uint64 encodings of doubles.

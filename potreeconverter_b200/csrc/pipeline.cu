@@ -239,12 +239,32 @@ struct Converter {
 		g_launch_count = 0;
 		PCG_CUDA(cudaSetDevice(device));
 		std::string err;
-		LasInfo info;
-		const uint8_t* las = static_cast<const uint8_t*>(job.las);
-		if (!las || !parse_las(las, job.las_size, info, err, job.device_records != nullptr))
-			throw PcgError(PCG_BAD_INPUT, err.empty() ? "no input" : err);
+		// the job's sources, in order, and the --attributes list
+		std::vector<pcg_source> sources;
+		if (job.num_sources > 0) {
+			if (!job.sources) throw PcgError(PCG_BAD_INPUT, "num_sources is set but sources is NULL");
+			sources.assign(job.sources, job.sources + job.num_sources);
+		} else {
+			sources.push_back({job.las, job.las_size, job.device_records});
+		}
+		std::vector<std::string> requested;
+		if (job.num_attributes > 0) {
+			if (!job.attributes) throw PcgError(PCG_BAD_INPUT, "num_attributes is set but attributes is NULL");
+			for (int32_t i = 0; i < job.num_attributes; i++) {
+				if (!job.attributes[i]) throw PcgError(PCG_BAD_INPUT, "NULL attribute name");
+				requested.push_back(job.attributes[i]);
+			}
+		}
+		std::vector<LasInfo> infos(sources.size());
+		for (size_t k = 0; k < sources.size(); k++) {
+			const uint8_t* las = static_cast<const uint8_t*>(sources[k].las);
+			if (!las || !parse_las(las, sources[k].las_size, infos[k], err, sources[k].device_records != nullptr)) {
+				std::string what = err.empty() ? "no input" : err;
+				throw PcgError(PCG_BAD_INPUT, sources.size() > 1 ? "source " + std::to_string(k) + ": " + what : what);
+			}
+		}
 		Setup s;
-		if (!make_setup(info, s, err)) throw PcgError(PCG_BAD_INPUT, err);
+		if (!make_setup(infos, requested, s, err)) throw PcgError(PCG_BAD_INPUT, err);
 		if (job.method < 0 || job.method > 2) throw PcgError(PCG_BAD_INPUT, "unknown sampling method");
 		if (s.total_points < 2) throw PcgError(PCG_BAD_INPUT, "need at least two points");
 		if (s.total_points >= (int64_t(1) << 31)) throw PcgError(PCG_BAD_INPUT, "more than 2^31 points per job");
@@ -254,21 +274,43 @@ struct Converter {
 		res.stats.num_points = N;
 
 		// ---------------------------------------------------------- input
+		// host sources are copied back to back (16-byte aligned) into one
+		// device buffer, one copy each; device-resident ones stay in place
 		auto t_h2d = Clock::now();
-		const int64_t rec_bytes = N * (int64_t)info.record_length;
-		uint8_t* d_recs = nullptr;
-		if (job.device_records) {
-			d_recs = static_cast<uint8_t*>(const_cast<void*>(job.device_records));
-		} else {
-			d_recs = mem.alloc<uint8_t>(rec_bytes);
-			PCG_CUDA(cudaMemcpyAsync(d_recs, las + info.offset_to_points, rec_bytes, cudaMemcpyHostToDevice, stream));
+		std::vector<const uint8_t*> src_recs(sources.size(), nullptr);
+		std::vector<int64_t> src_base(sources.size(), -1);
+		int64_t host_bytes = 0;
+		for (size_t k = 0; k < sources.size(); k++) {
+			if (sources[k].device_records) {
+				src_recs[k] = static_cast<const uint8_t*>(sources[k].device_records);
+				continue;
+			}
+			src_base[k] = host_bytes;
+			host_bytes += (infos[k].num_points * (int64_t)infos[k].record_length + 15) & ~int64_t(15);
+		}
+		if (host_bytes > 0) {
+			uint8_t* d_host = mem.alloc<uint8_t>(host_bytes);
+			for (size_t k = 0; k < sources.size(); k++) {
+				if (src_base[k] < 0) continue;
+				const int64_t bytes = infos[k].num_points * (int64_t)infos[k].record_length;
+				src_recs[k] = d_host + src_base[k];
+				if (bytes > 0)
+					PCG_CUDA(cudaMemcpyAsync(d_host + src_base[k], static_cast<const uint8_t*>(sources[k].las) + infos[k].offset_to_points,
+					                         bytes, cudaMemcpyHostToDevice, stream));
+			}
 			PCG_CUDA(cudaStreamSynchronize(stream));
 		}
 		res.stats.ms_h2d = ms_since(t_h2d);
 
 		// ------------------------------------------------------- chunking
 		auto t_chunk = Clock::now();
-		DecodeParams p = decode_params(s);
+		std::vector<SourceDesc> descs;
+		std::vector<int64_t> firsts;
+		DecodeParams p = decode_params(s, src_recs, descs, firsts);
+		if (p.nsrc > 1) {
+			p.srcs = upload(descs, mem);
+			p.src_first = upload(firsts, mem);
+		}
 		const int G = s.grid_size;
 		const int64_t cells = (int64_t)G * G * G;
 		uint32_t* grid = mem.alloc<uint32_t>(cells);
@@ -285,7 +327,7 @@ struct Converter {
 		PCG_CUDA(cudaMemsetAsync(co.histogram, 0, 256 * 8, stream));
 		co.error = mem.alloc<int64_t>(2);
 		PCG_CUDA(cudaMemsetAsync(co.error, 0, 16, stream));
-		launch_decode_count(d_recs, p, grid, co, mem);
+		launch_decode_count(p, grid, co, mem);
 
 		const int chunk_cap = 1 << 20;
 		ChunkCell* d_chunks = mem.alloc<ChunkCell>(chunk_cap);
@@ -456,7 +498,7 @@ struct Converter {
 		if (method == PCG_POISSON_AVERAGE) {
 			if (p.off_rgb < 0) throw PcgError(PCG_BAD_INPUT, "poisson_average needs an rgb attribute");
 			leaf_cols = mem.alloc<uint64_t>(N);
-			launch_fill_colors(d_recs, info.record_length, p.src_rgb, ids, N, leaf_cols, mem);
+			launch_fill_colors(p, ids, N, leaf_cols, mem);
 		}
 		int4* leaf_rec = nullptr;
 		if (method != PCG_RANDOM) {
@@ -479,7 +521,7 @@ struct Converter {
 			for (int i = 0; i < (int)tree.nodes.size(); i++)
 				if (tree.nodes[i].depth == d && tree.nodes[i].has_children()) level_nodes.push_back(i);
 			if (level_nodes.empty()) continue;
-			sample_level(tree, level_nodes, method, base_spacing, pps, co, d_recs, p, d_st, grid_arena, mem, res);
+			sample_level(tree, level_nodes, method, base_spacing, pps, co, d_st, grid_arena, mem, res);
 		}
 		// the root's final payload is its accepted buffer
 		TNode& root = tree.nodes[0];
@@ -525,7 +567,7 @@ struct Converter {
 			d_out = mem.alloc<uint8_t>(res.octree_size);
 		}
 		PayloadItem* d_items = upload(items, mem);
-		launch_write_payloads(d_recs, p, items, d_items, d_out, mem);
+		launch_write_payloads(p, items, d_items, d_out, mem);
 		PCG_CUDA(cudaStreamSynchronize(stream));
 		res.stats.ms_output = ms_since(t_out);
 		// the attribute statistics first (small), then octree.bin, whose copy
@@ -548,6 +590,16 @@ struct Converter {
 			const auto& sd = stats_dev[i];
 			astats[i].min = {decode_ordered(sd.mn[0]), decode_ordered(sd.mn[1]), decode_ordered(sd.mn[2])};
 			astats[i].max = {decode_ordered(sd.mx[0]), decode_ordered(sd.mx[1]), decode_ordered(sd.mx[2])};
+			// the reference passes the statistics through the chunks'
+			// metadata.json, where a non-finite value (or none at all: an
+			// attribute no point carries) comes back as +Infinity
+			// (chunker_countsort_laszip.cpp:1005-1070, indexer.cpp:72-130)
+			for (int c = 0; c < s.attrs[i].numElements && c < 3; c++) {
+				double* mn = &astats[i].min.x + c;
+				double* mx = &astats[i].max.x + c;
+				if (!std::isfinite(*mn)) *mn = INFINITY;
+				if (!std::isfinite(*mx)) *mx = INFINITY;
+			}
 			astats[i].histogram.assign(256, 0);
 			if (s.attrs[i].kind == AK_CLASSIFICATION)
 				for (int k = 0; k < 256; k++) astats[i].histogram[k] = (int64_t)hist[k];
@@ -563,27 +615,25 @@ struct Converter {
 		res.stats.ms_total = ms_since(t0);
 	}
 
-	static DecodeParams decode_params(const Setup& s) {
+	// Kernel parameters of the decode: the output layout, and per source its
+	// records, coordinate transform and handler byte moves (src_recs: device
+	// pointer of each source's first record). descs / firsts receive the
+	// source table for jobs with several sources.
+	static DecodeParams decode_params(const Setup& s, const std::vector<const uint8_t*>& src_recs, std::vector<SourceDesc>& descs,
+	                                  std::vector<int64_t>& firsts) {
 		DecodeParams p{};
-		const LasInfo& L = s.las;
 		for (int a = 0; a < 3; a++) {
-			p.in_scale[a] = (&L.scale.x)[a];
-			p.in_offset[a] = (&L.offset.x)[a];
 			p.pos_scale[a] = (&s.pos_scale.x)[a];
 			p.pos_offset[a] = (&s.pos_offset.x)[a];
 			p.cmin[a] = (&s.cube_min.x)[a];
 		}
 		p.csize = s.chunk_cube_size;
 		p.n = s.total_points;
-		p.rec_len = L.record_length;
-		p.pdrf = L.pdrf;
 		p.bpp = s.bpp;
 		p.grid = s.grid_size;
 		p.off_intensity = p.off_retnum = p.off_nret = p.off_class = p.off_sar = p.off_user = p.off_psid = p.off_gps = p.off_rgb = -1;
 		p.stat_intensity = p.stat_retnum = p.stat_nret = p.stat_class = p.stat_sar = p.stat_user = p.stat_psid = p.stat_gps = p.stat_rgb = -1;
-		p.src_gps = 20;
-		p.src_rgb = (L.pdrf == 2) ? 20 : 28;
-		p.n_extra = 0;
+		if ((int)s.attrs.size() > MAX_ATTRS) throw PcgError(PCG_BAD_INPUT, "too many attributes");
 		for (int i = 0; i < (int)s.attrs.size(); i++) {
 			const AttrDesc& a = s.attrs[i];
 			switch (a.kind) {
@@ -597,33 +647,50 @@ struct Converter {
 			case AK_POINT_SOURCE_ID: p.off_psid = a.out_offset; p.stat_psid = i; break;
 			case AK_GPS_TIME: p.off_gps = a.out_offset; p.stat_gps = i; break;
 			case AK_RGB: p.off_rgb = a.out_offset; p.stat_rgb = i; break;
-			default: {
-				if (p.n_extra >= MAX_EXTRA) throw PcgError(PCG_BAD_INPUT, "too many extra attributes");
-				ExtraDesc& e = p.extra[p.n_extra++];
-				e.src_off = a.src_offset;
-				e.dst_off = a.out_offset;
-				e.size = a.size;
-				e.type = (int)a.type;
-				e.num_elements = a.numElements;
-				e.element_size = a.elementSize;
-				e.stat_index = i;
-				e.pad = 0;
-			}
+			default: break;  // extra bytes: per source below
 			}
 		}
-		if ((int)s.attrs.size() > MAX_ATTRS) throw PcgError(PCG_BAD_INPUT, "too many attributes");
+		descs.assign(s.sources.size(), SourceDesc{});
+		firsts.clear();
+		int64_t first = 0;
+		p.max_rec_len = 0;
+		for (size_t k = 0; k < s.sources.size(); k++) {
+			const SourceSetup& ss = s.sources[k];
+			const LasInfo& L = ss.las;
+			SourceDesc& d = descs[k];
+			for (int a = 0; a < 3; a++) {
+				d.in_scale[a] = (&L.scale.x)[a];
+				d.in_offset[a] = (&L.offset.x)[a];
+			}
+			d.recs = src_recs[k];
+			d.first = first;
+			d.count = L.num_points;
+			d.rec_len = L.record_length;
+			d.src_gps = (L.pdrf == 1 || L.pdrf == 3) ? 20 : -1;
+			d.src_rgb = L.pdrf == 2 ? 20 : (L.pdrf == 3 ? 28 : -1);
+			d.zero_fill = ss.zero_fill ? 1 : 0;
+			if ((int)ss.extras.size() > MAX_EXTRA) throw PcgError(PCG_BAD_INPUT, "too many extra attributes");
+			d.n_extra = (int)ss.extras.size();
+			for (int e = 0; e < d.n_extra; e++) {
+				const auto& x = ss.extras[e];
+				const AttrDesc& oa = s.attrs[x.out_index];
+				d.extra[e] = {x.src_off, x.dst_off, x.size, (int)oa.type, oa.numElements, oa.elementSize, x.out_index, 0};
+			}
+			firsts.push_back(first);
+			first += L.num_points;
+			p.max_rec_len = std::max(p.max_rec_len, L.record_length);
+		}
+		p.nsrc = (int)s.sources.size();
+		p.src0 = descs[0];
 		return p;
 	}
 
 	void sample_level(Tree& tree, const std::vector<int>& level_nodes, int method, double base_spacing, const PosParamsS& pps,
-	                  const ChunkingOut& co, const uint8_t* d_recs, const DecodeParams& p, SampleStats* d_st, GreedyArena& grid_arena,
-	                  DeviceMem& mem, JobResult& res) {
+	                  const ChunkingOut& co, SampleStats* d_st, GreedyArena& grid_arena, DeviceMem& mem, JobResult& res) {
 		const auto t_level = Clock::now();
 		const double alloc0 = mem.alloc_ms();
 		int sms = 148;
 		PCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-		(void)d_recs;
-		(void)p;
 		(void)res;
 		const int K = (int)level_nodes.size();
 		std::vector<LevelNode> ln(K);
@@ -960,12 +1027,15 @@ struct pcg_ctx {
 	// request loop
 	struct Job {
 		uint64_t id;
-		// the job's LAS image, copied at submit: into a pinned buffer of the
-		// pool when one can be had (the worker's host-to-device copy then
-		// runs at link speed), else into `las`
+		// the job's LAS images, copied back to back at submit: into a pinned
+		// buffer of the pool when one can be had (the worker's host-to-device
+		// copies then run at link speed), else into `las`
 		uint8_t* las_pinned = nullptr;
 		size_t las_size = 0;
 		std::vector<uint8_t> las;
+		std::vector<size_t> src_off, src_size;  // every source's image in it
+		bool multi = false;                     // given as a source list
+		std::vector<std::string> attributes;
 		std::string name, projection;
 		int32_t method;
 		bool done = false;
@@ -1029,9 +1099,9 @@ void move_result(pcg::JobResult& r, pcg_result* out, int device) {
 	out->stats = r.stats;
 }
 
-size_t estimate_footprint(const pcg_job& job) {
+size_t estimate_footprint(size_t las_bytes) {
 	// point records + positions/ids/keys per point, plus headroom
-	return (size_t)job.las_size * 3 + (size_t)(job.las_size / 20) * 64 + (size_t(64) << 20);
+	return las_bytes * 3 + (las_bytes / 20) * 64 + (size_t(64) << 20);
 }
 
 void worker_main(pcg_ctx* ctx, int wi) {
@@ -1055,8 +1125,20 @@ void worker_main(pcg_ctx* ctx, int wi) {
 			ctx->in_use += job->footprint;
 		}
 		pcg_job pj{};
-		pj.las = job->las_pinned ? job->las_pinned : job->las.data();
-		pj.las_size = job->las_size;
+		const uint8_t* image = job->las_pinned ? job->las_pinned : job->las.data();
+		std::vector<pcg_source> srcs;
+		for (size_t k = 0; k < job->src_off.size(); k++) srcs.push_back({image + job->src_off[k], job->src_size[k], nullptr});
+		std::vector<const char*> names;
+		for (auto& a : job->attributes) names.push_back(a.c_str());
+		if (job->multi) {
+			pj.num_sources = (int32_t)srcs.size();
+			pj.sources = srcs.data();
+		} else {
+			pj.las = image;
+			pj.las_size = job->las_size;
+		}
+		pj.num_attributes = (int32_t)names.size();
+		pj.attributes = names.empty() ? nullptr : names.data();
 		pj.method = job->method;
 		pj.name = job->name.c_str();
 		pj.projection = job->projection.c_str();
@@ -1204,7 +1286,20 @@ pcg_status pcg_write_files(const pcg_result* r, const char* dir) {
 }
 
 pcg_status pcg_submit(pcg_ctx* ctx, const pcg_job* job, uint64_t* job_id) {
-	if (!ctx || !job || !job_id || !job->las) return PCG_BAD_INPUT;
+	if (!ctx || !job || !job_id) return PCG_BAD_INPUT;
+	// the request loop takes host images only; they are copied here
+	std::vector<pcg_source> srcs;
+	if (job->num_sources > 0) {
+		if (!job->sources) return PCG_BAD_INPUT;
+		srcs.assign(job->sources, job->sources + job->num_sources);
+	} else {
+		srcs.push_back({job->las, job->las_size, job->device_records});
+	}
+	for (auto& src : srcs)
+		if (!src.las || src.device_records) return PCG_BAD_INPUT;
+	if (job->num_attributes > 0 && !job->attributes) return PCG_BAD_INPUT;
+	for (int32_t i = 0; i < job->num_attributes; i++)
+		if (!job->attributes[i]) return PCG_BAD_INPUT;
 	return guarded(ctx, [&] {
 		std::lock_guard<std::mutex> lk(ctx->qmtx);
 		if (ctx->workers.empty()) {
@@ -1222,14 +1317,27 @@ pcg_status pcg_submit(pcg_ctx* ctx, const pcg_job* job, uint64_t* job_id) {
 		}
 		auto j = std::make_shared<pcg_ctx::Job>();
 		j->id = ctx->next_id++;
-		j->las_size = job->las_size;
-		j->las_pinned = pcg::g_pinned.take(job->las_size);
-		if (j->las_pinned) std::memcpy(j->las_pinned, job->las, job->las_size);
-		else j->las.assign((const uint8_t*)job->las, (const uint8_t*)job->las + job->las_size);
+		size_t total = 0;
+		for (auto& src : srcs) {
+			j->src_off.push_back(total);
+			j->src_size.push_back(src.las_size);
+			total += (src.las_size + 15) & ~size_t(15);
+		}
+		j->multi = job->num_sources > 0;
+		j->las_size = total;
+		j->las_pinned = pcg::g_pinned.take(total ? total : 1);
+		uint8_t* image = j->las_pinned;
+		if (!image) {
+			j->las.resize(total);
+			image = j->las.data();
+		}
+		for (size_t k = 0; k < srcs.size(); k++) std::memcpy(image + j->src_off[k], srcs[k].las, srcs[k].las_size);
+		if (!j->multi) j->las_size = srcs[0].las_size;
+		for (int32_t i = 0; i < job->num_attributes; i++) j->attributes.push_back(job->attributes[i]);
 		j->name = job->name ? job->name : "";
 		j->projection = job->projection ? job->projection : "";
 		j->method = job->method;
-		j->footprint = estimate_footprint(*job);
+		j->footprint = estimate_footprint(total);
 		ctx->jobs[j->id] = j;
 		ctx->queue.push_back(j);
 		*job_id = j->id;

@@ -2,6 +2,7 @@
 // bounding box and chunk-grid parameters, evaluated with the same
 // expressions (and therefore the same rounding) as the reference.
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -85,8 +86,10 @@ static void las_type_info(int type_id, AttrType& type, int& num_elements) {  // 
 	num_elements = type_id <= 10 ? 1 : (type_id <= 20 ? 2 : 3);
 }
 
-bool make_setup(const LasInfo& info, Setup& s, std::string& err) {
-	s.las = info;
+// The source's own attribute list (PotreeConverter.h:136-193): the
+// standard attributes of its point format, then its extra bytes
+// (PotreeConverter.h:80-133) with their record offsets.
+static bool source_attributes(const LasInfo& info, SourceSetup& src, std::string& err) {
 	auto mk = [](const char* name, int size, int ne, int es, AttrType t, int kind) {
 		AttrDesc a; a.name = name; a.size = size; a.numElements = ne; a.elementSize = es; a.type = t; a.kind = kind; return a;
 	};
@@ -100,18 +103,17 @@ bool make_setup(const LasInfo& info, Setup& s, std::string& err) {
 	AttrDesc psid = mk("point source id", 2, 1, 2, AttrType::UINT16, AK_POINT_SOURCE_ID);
 	AttrDesc gps = mk("gps-time", 8, 1, 8, AttrType::DOUBLE, AK_GPS_TIME);
 	AttrDesc rgb = mk("rgb", 6, 3, 2, AttrType::UINT16, AK_RGB);
-	// attribute order per point format, PotreeConverter.h:160-181
+	src.las = info;
 	switch (info.pdrf) {
-	case 0: s.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid}; s.std_record_length = 20; break;
-	case 1: s.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid, gps}; s.std_record_length = 28; break;
-	case 2: s.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid, rgb}; s.std_record_length = 26; break;
-	case 3: s.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid, gps, rgb}; s.std_record_length = 34; break;
+	case 0: src.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid}; src.std_record_length = 20; break;
+	case 1: src.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid, gps}; src.std_record_length = 28; break;
+	case 2: src.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid, rgb}; src.std_record_length = 26; break;
+	case 3: src.attrs = {xyz, intensity, retnum, nret, cls, sar, user, psid, gps, rgb}; src.std_record_length = 34; break;
 	default: err = "unsupported LAS point data format " + std::to_string(info.pdrf) + " (0-3 are supported)"; return false;
 	}
-	s.first_extra_index = (int)s.attrs.size();  // chunker_countsort_laszip.cpp:551-560
-	if (info.record_length < s.std_record_length) { err = "point record length shorter than its format"; return false; }
-	// extra bytes, PotreeConverter.h:80-133
-	int src = s.std_record_length;
+	if (info.record_length < src.std_record_length) { err = "point record length shorter than its format"; return false; }
+	const size_t n_standard = src.attrs.size();
+	int off = src.std_record_length;
 	for (auto& vlr : info.vlrs) {
 		if (vlr.record_id != 4) continue;
 		int num = (int)vlr.data.size() / 192;
@@ -127,23 +129,111 @@ bool make_setup(const LasInfo& info, Setup& s, std::string& err) {
 			a.description = desc;
 			if (r[3] & 0b01000) std::memcpy(&a.scale, r + 112, 24);
 			if (r[3] & 0b10000) std::memcpy(&a.offset, r + 136, 24);
-			a.src_offset = src;
-			src += a.size;
-			s.attrs.push_back(a);
+			a.src_offset = off;
+			off += a.size;
+			// an extra named like a standard attribute would also receive
+			// that attribute's handler (:531-545); not supported
+			for (size_t k = 0; k < n_standard; k++)
+				if (src.attrs[k].name == a.name) { err = "extra-bytes attribute named like a standard attribute: " + a.name; return false; }
+			src.attrs.push_back(a);
 		}
 	}
-	if (src > info.record_length) { err = "extra bytes exceed the point record length"; return false; }
-	int off = 0;
-	for (auto& a : s.attrs) { a.out_offset = off; off += a.size; }
-	s.bpp = off;
+	if (off > info.record_length) { err = "extra bytes exceed the point record length"; return false; }
+	return true;
+}
 
-	// computeScaleOffset with a single source, PotreeConverter.h:29-76
-	Vec3d mn = info.min, mx = info.max;
+bool make_setup(const std::vector<LasInfo>& infos, const std::vector<std::string>& requested, Setup& s, std::string& err) {
+	if (infos.empty()) { err = "no input"; return false; }
+	// computeOutputAttributes(sources, requestedAttributes), PotreeConverter.h:195-276
+	const double inf = INFINITY;
+	Vec3d scale_min = {inf, inf, inf}, mn = {inf, inf, inf}, mx = {-inf, -inf, -inf};
+	std::vector<AttrDesc> full;
+	s.sources.assign(infos.size(), SourceSetup{});
+	s.total_points = 0;
+	for (size_t k = 0; k < infos.size(); k++) {
+		const LasInfo& info = infos[k];
+		SourceSetup& src = s.sources[k];
+		if (!source_attributes(info, src, err)) {
+			if (infos.size() > 1) err = "source " + std::to_string(k) + ": " + err;
+			return false;
+		}
+		for (auto& a : src.attrs) {  // union by name, first seen first
+			bool added = false;
+			for (auto& f : full) added = added || f.name == a.name;
+			if (!added) full.push_back(a);
+		}
+		scale_min.x = std::min(scale_min.x, info.scale.x); scale_min.y = std::min(scale_min.y, info.scale.y); scale_min.z = std::min(scale_min.z, info.scale.z);
+		mn.x = std::min(mn.x, info.min.x); mn.y = std::min(mn.y, info.min.y); mn.z = std::min(mn.z, info.min.z);
+		mx.x = std::max(mx.x, info.max.x); mx.y = std::max(mx.y, info.max.y); mx.z = std::max(mx.z, info.max.z);
+		s.total_points += info.num_points;
+	}
+	// the filter (:252-275): "position" first, then every requested name
+	// found in the full list, in request order
+	if (requested.empty()) {
+		s.attrs = full;
+	} else {
+		std::vector<std::string> should = requested;
+		should.insert(should.begin(), "position");
+		for (size_t i = 0; i < should.size(); i++)
+			for (size_t j = 0; j < i; j++)
+				if (should[i] == should[j]) { err = "attribute listed twice: " + should[i]; return false; }
+		s.attrs.clear();
+		for (auto& name : should)
+			for (auto& f : full)
+				if (f.name == name) { s.attrs.push_back(f); break; }
+	}
+	int out_off = 0;
+	for (auto& a : s.attrs) { a.out_offset = out_off; out_off += a.size; }
+	s.bpp = out_off;
+	auto out_index = [&](const std::string& name) {
+		for (size_t i = 0; i < s.attrs.size(); i++) if (s.attrs[i].name == name) return (int)i;
+		return -1;
+	};
+
+	// each source's handlers (:380-658): standard attributes go to their
+	// output offsets; extra bytes kept in the output go to the source's
+	// standard size plus the sizes of the kept extras before them (:565-653)
+	for (auto& src : s.sources) {
+		std::vector<bool> written(s.bpp, false);
+		for (int b = 0; b < 12; b++) written[b] = true;
+		int attribute_offset = 0;
+		size_t first_extra = 0;
+		for (auto& a : src.attrs) {
+			if (a.kind == AK_EXTRA) break;
+			attribute_offset += a.size;
+			first_extra++;
+		}
+		for (size_t k = 1; k < first_extra; k++) {
+			int oi = out_index(src.attrs[k].name);
+			if (oi < 0) continue;
+			for (int b = 0; b < s.attrs[oi].size; b++) written[s.attrs[oi].out_offset + b] = true;
+		}
+		for (size_t k = first_extra; k < src.attrs.size(); k++) {
+			const AttrDesc& ia = src.attrs[k];
+			int oi = out_index(ia.name);
+			if (oi < 0) continue;
+			const AttrDesc& oa = s.attrs[oi];
+			if (attribute_offset + ia.size > s.bpp) {
+				err = "attribute " + ia.name + " would be written past the point record (the reference's result is undefined)";
+				return false;
+			}
+			if (ia.src_offset + oa.numElements * oa.elementSize > src.las.record_length) {
+				err = "attribute " + ia.name + " would be read past the LAS record (the reference's result is undefined)";
+				return false;
+			}
+			src.extras.push_back({ia.src_offset, attribute_offset, ia.size, oi});
+			for (int b = 0; b < ia.size; b++) written[attribute_offset + b] = true;
+			attribute_offset += oa.size;
+		}
+		src.zero_fill = false;
+		for (bool w : written) src.zero_fill = src.zero_fill || !w;
+	}
+	// computeScaleOffset(min, max, scaleMin), PotreeConverter.h:29-76
 	Vec3d size = mx - mn;
 	double msx = size.x / std::pow(2.0, 30.0), msy = size.y / std::pow(2.0, 30.0), msz = size.z / std::pow(2.0, 30.0);
-	s.pos_scale = {info.scale.x < msx ? msx : info.scale.x, info.scale.y < msy ? msy : info.scale.y, info.scale.z < msz ? msz : info.scale.z};
+	s.pos_scale = {scale_min.x < msx ? msx : scale_min.x, scale_min.y < msy ? msy : scale_min.y, scale_min.z < msz ? msz : scale_min.z};
 	s.pos_offset = mn;
-	// computeStats, main.cpp:215-284
+	// computeStats, main.cpp:215-284, over the same header boxes
 	double cube = vmax3(mx - mn);
 	if (cube == 0.0) { err = "invalid bounding box: at least one axis has a size of zero"; return false; }
 	s.cube_min = mn;
@@ -152,7 +242,6 @@ bool make_setup(const LasInfo& info, Setup& s, std::string& err) {
 	// main.cpp:273-281 rejects a box with any zero-size cubic axis
 	s.chunk_cube_size = vmax3(s.cube_max - s.cube_min);  // chunker_countsort_laszip.cpp:205-207
 	s.root_max = s.cube_min + vmax3(s.cube_max - s.cube_min);  // :1252-1254
-	s.total_points = info.num_points;
 	int64_t t20 = s.total_points / 20;
 	s.max_points_per_chunk = (int)(t20 < 10'000'000 ? t20 : 10'000'000);
 	s.grid_size = s.total_points < 100'000'000 ? 128 : (s.total_points < 500'000'000 ? 256 : 512);

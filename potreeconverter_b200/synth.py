@@ -404,3 +404,24 @@ def tiles(n: int, seed: int, extent: float = 400.0, origin=(652000.0, 5187000.0,
         out.append(write_las(X, Y, Z, attrs, pdrf=fmt, version_minor=4 if fmt in (1, 3) else 2,
                              scale=(sc, sc, sc), offset=off, extras=ex))
     return out
+
+
+def without_points(las: bytes, pdrf: int = 2) -> bytes:
+    """A LAS file image in point format pdrf without points, whose scale,
+    offset and header bounding box are those of las."""
+    empty = bytearray(write_las(np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32), {}, pdrf=pdrf,
+                                version_minor=2))
+    empty[131:227] = las[131:227]
+    return bytes(empty)
+
+
+def sources(kind: str, n: int, seed: int, **kw) -> list:
+    """File images of a multi-source input: ``tiles``; ``tiles_empty`` (tiles
+    1 and 3 around a point-less format-2 file with tile 0's header box, so
+    rgb is an attribute no point carries); or one image of any generator."""
+    if kind == "tiles":
+        return tiles(n, seed, **kw)
+    if kind == "tiles_empty":
+        t = tiles(n, seed, **kw)
+        return [t[1], without_points(t[0]), t[3]]
+    return [generate(kind, n, seed, **kw)]

@@ -41,10 +41,12 @@ CASES = [
 #  --attributes, samplers). The "tiles" generator returns one file image per
 # tile; the others one image. Source k is written as <case>_<k>.las (or
 # <case>.las for one source) and the sources are passed in `order`; the
-# metadata name is the first source's stem (main.cpp:146-200).
+# metadata name is the first source's stem (main.cpp:146-200). Generators:
+# potreeconverter_b200.synth.sources.
 ALL = ["poisson", "poisson_average", "random"]
 MULTI_CASES = [
     ("tiles_200k", "tiles", 200_000, 11, {}, [0, 1, 2, 3], [], ALL),
+    ("tiles_empty_200k", "tiles_empty", 200_000, 14, {}, [0, 1, 2], [], ALL),
     ("tiles_2m_reversed", "tiles", 2_000_000, 12, {}, [3, 2, 1, 0], [], ALL),
     ("tiles_300k_attrs", "tiles", 300_000, 13, {}, [0, 1, 2, 3],
      ["gps-time", "rgb", "return number", "no such attribute"], ALL),
@@ -57,15 +59,12 @@ MULTI_CASES = [
 
 def multi_sources(kind, n, seed, kw, order):
     """File images of a multi-source case, in the order they are passed."""
-    if kind == "tiles":
-        imgs = synth.tiles(n, seed, **kw)
-    else:
-        imgs = [synth.generate(kind, n, seed, **kw)]
+    imgs = synth.sources(kind, n, seed, **kw)
     return [imgs[k] for k in order]
 
 
 def source_names(case, kind, order):
-    return [f"{case}_{k}" if kind == "tiles" else case for k in order]
+    return [f"{case}_{k}" if kind.startswith("tiles") else case for k in order]
 
 
 def md5(path):

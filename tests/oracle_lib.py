@@ -124,8 +124,7 @@ def md5(b: bytes) -> str:
 @functools.lru_cache(maxsize=8)
 def _case_sources(kind: str, n: int, seed: int, kwargs_json: str, order: tuple) -> tuple:
     from potreeconverter_b200 import synth
-    kw = json.loads(kwargs_json)
-    imgs = synth.tiles(n, seed, **kw) if kind == "tiles" else [synth.generate(kind, n, seed, **kw)]
+    imgs = synth.sources(kind, n, seed, **json.loads(kwargs_json))
     return tuple(imgs[k] for k in order)
 
 
