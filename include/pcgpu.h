@@ -1,7 +1,7 @@
 /*
  * pcgpu.h -- C ABI of the B200-native octree LOD builder (libpcgpu.so).
  *
- * The library converts an uncompressed LAS file image into the three files
+ * The library converts LAS or LAZ file images into the three files
  * PotreeConverter 2.0 writes (octree.bin, hierarchy.bin, metadata.json),
  * byte-identical to a determinism-pinned reference build, with every stage of
  * the build running as CUDA kernels for sm_100a on one GPU.
@@ -76,7 +76,7 @@ enum {
 /* One input file of a job with several sources (the reference's source
    list after curateSources, main.cpp:146-200). */
 typedef struct pcg_source {
-	const void* las;       /* uncompressed LAS file image (host memory); with
+	const void* las;       /* LAS or LAZ file image (host memory); with
 	                          device_records set, only its header and VLRs
 	                          are read                                        */
 	uint64_t las_size;
@@ -84,7 +84,7 @@ typedef struct pcg_source {
 } pcg_source;
 
 typedef struct pcg_job {
-	const void* las;       /* uncompressed LAS file image (host memory); with
+	const void* las;       /* LAS or LAZ file image (host memory); with
 	                          device_records set, only its header and VLRs
 	                          are read                                        */
 	uint64_t las_size;
@@ -129,6 +129,8 @@ typedef struct pcg_stats {
 	                                 (part of ms_greedy)                     */
 	int64_t list_entries;         /* conflict-list entries over all levels  */
 	int64_t cluster_nodes;        /* nodes accepted by a cluster of CTAs    */
+	double ms_decode;             /* LAZ decode of the job's .laz sources   */
+	int64_t laz_chunks;           /* LASzip chunks decoded                  */
 } pcg_stats;
 
 typedef struct pcg_result {
@@ -171,6 +173,13 @@ pcg_status pcg_kernel_sort_keys(pcg_ctx* ctx, const double* keys, int64_t n, int
 /* perm_out[i] = index that std::shuffle(0..n-1, std::default_random_engine(seed))
  * leaves at position i (sampler_random.h:97-104). */
 pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* perm_out);
+
+/* LASzip decode of every point of a LAZ file image (point formats 0-3,
+   LASzip's chunked point-wise coding: lasreadpoint.cpp:405-497 with the v2
+   item readers of lasreaditemcompressed_v2.cpp) into records_out
+   (point count x record length bytes), exactly the records the reference
+   reads through laszip_read_point. */
+pcg_status pcg_kernel_laz_decode(pcg_ctx* ctx, const void* laz_file, uint64_t size, void* records_out, uint64_t out_size);
 
 /* ---- the same sort for callers that cannot allocate ---------------------
  * No counterpart in the reference. pcg_kernel_sort_keys_noalloc is

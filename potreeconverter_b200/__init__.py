@@ -63,7 +63,7 @@ class _Stats(ctypes.Structure):
                 ("ms_sort", ctypes.c_double), ("ms_greedy", ctypes.c_double), ("sampled_nodes", ctypes.c_int64),
                 ("candidates", ctypes.c_int64), ("replayed_nodes", ctypes.c_int64),
                 ("replayed_candidates", ctypes.c_int64), ("ms_lists", ctypes.c_double), ("list_entries", ctypes.c_int64),
-                ("cluster_nodes", ctypes.c_int64)]
+                ("cluster_nodes", ctypes.c_int64), ("ms_decode", ctypes.c_double), ("laz_chunks", ctypes.c_int64)]
 
 
 class _Result(ctypes.Structure):
@@ -75,7 +75,7 @@ class _Result(ctypes.Structure):
 # every symbol include/pcgpu.h declares
 EXPORTS = ["pcg_create", "pcg_destroy", "pcg_last_error", "pcg_status_string", "pcg_convert", "pcg_result_free",
            "pcg_write_files", "pcg_submit", "pcg_poll", "pcg_wait", "pcg_kernel_sort_keys", "pcg_kernel_shuffle",
-           "pcg_kernel_sort_keys_noalloc"]
+           "pcg_kernel_sort_keys_noalloc", "pcg_kernel_laz_decode"]
 
 _lib = None
 
@@ -104,6 +104,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pcg_kernel_sort_keys.argtypes = [c.c_void_p, c.c_void_p, c.c_int64, c.c_void_p]
     lib.pcg_kernel_shuffle.argtypes = [c.c_void_p, c.c_int64, c.c_uint32, c.c_void_p]
     lib.pcg_kernel_sort_keys_noalloc.argtypes = [c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p]
+    lib.pcg_kernel_laz_decode.argtypes = [c.c_void_p, c.c_char_p, c.c_uint64, c.c_void_p, c.c_uint64]
     _lib = lib
     return lib
 
@@ -290,6 +291,20 @@ class Context:
         if st != 0:
             raise self._err(st)
         return perm
+
+    def laz_decode(self, laz: bytes) -> bytes:
+        """Point records of a LAZ file image, decoded on the device."""
+        import struct
+        hdr = struct.unpack_from("<H", laz, 94)[0]
+        n = struct.unpack_from("<I", laz, 107)[0]
+        if laz[25] >= 4 and hdr >= 375:
+            n = max(n, struct.unpack_from("<Q", laz, 247)[0])
+        size = n * struct.unpack_from("<H", laz, 105)[0]
+        out = ctypes.create_string_buffer(max(1, size))
+        st = self._lib.pcg_kernel_laz_decode(self._h, ctypes.c_char_p(laz), len(laz), out, size)
+        if st != 0:
+            raise self._err(st)
+        return out.raw[:size]
 
     def shuffle(self, n: int, seed: int = PINNED_SEED):
         """Index order std::shuffle(iota(n), default_random_engine(seed)) gives (device kernel)."""

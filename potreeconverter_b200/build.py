@@ -31,7 +31,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompil
                      "-Xcompiler", "-O2", f"-I{INCLUDE}", f"-I{CSRC}"]
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", f"-I{INCLUDE}", f"-I{CSRC}", f"-I{CUDA_HOME}/include"]
 
-CU_SOURCES = ["radix.cu", "chunking.cu", "octree.cu", "sampling.cu", "introsort.cu", "segsort.cu", "conflicts.cu", "output.cu", "pipeline.cu"]
+CU_SOURCES = ["radix.cu", "chunking.cu", "octree.cu", "sampling.cu", "introsort.cu", "segsort.cu", "conflicts.cu", "output.cu", "laz.cu", "pipeline.cu"]
 CPP_SOURCES = ["setup.cpp", "writers.cpp"]
 
 

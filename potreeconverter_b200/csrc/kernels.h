@@ -19,6 +19,13 @@ struct ChunkingOut {
 	int64_t* error;                          // [0] = first failing point + 1 (out of box), [1] = lookup failure
 };
 
+// ------------------------------------------------------------------ laz.cu
+// Decodes the LASzip chunks of one LAZ source into its point records
+// (chunks' byte offsets are file offsets; d_bytes holds the file from
+// `base` to the end of the last chunk). Throws on malformed data.
+void launch_laz_decode(const uint8_t* d_bytes, uint64_t base, const std::vector<laz::Chunk>& chunks, const laz::Layout& L, uint8_t* d_out,
+                       DeviceMem& mem);
+
 // Decodes the records of every source (DecodeParams::src0 / srcs).
 void launch_decode_count(const DecodeParams& p, uint32_t* grid, ChunkingOut& out, DeviceMem& mem);
 // Pyramid merge of the count grid (createLUT, chunker_countsort_laszip.cpp:1074-1204).

@@ -1,0 +1,58 @@
+// LAZ decode on the device: one LASzip chunk per block (its lane 0 runs the
+// chunk's arithmetic decoder, laz.cuh), all chunks of a source at once, each
+// with its own model arena; the decoded point records land where the LAS
+// path keeps a source's records, so the rest of the pipeline is unchanged.
+// The reference decodes the same chunks sequentially per file, twice
+// (countPointsInCells and distributePoints, chunker_countsort_laszip.cpp:
+// 194-203, 750-772).
+
+#include "kernels.h"
+#include "laz.cuh"
+
+namespace pcg {
+
+namespace {
+
+__global__ void __launch_bounds__(32) laz_decode_kernel(const uint8_t* __restrict__ bytes, uint64_t base, const laz::Chunk* __restrict__ chunks,
+                                                        int c0, int n, laz::Layout L, uint32_t* __restrict__ arena, uint32_t words,
+                                                        uint8_t* __restrict__ out, int* __restrict__ bad) {
+	if (threadIdx.x != 0 || (int)blockIdx.x >= n) return;
+	const int c = c0 + (int)blockIdx.x;
+	const laz::Chunk ch = chunks[c];
+	const bool ok = laz::decode_chunk(bytes + (ch.start - base), bytes + (ch.end - base), ch.count, L, arena + (size_t)blockIdx.x * words,
+	                                  words, out + ch.first * (int64_t)L.rec_len);
+	if (!ok) atomicCAS(bad, 0, c + 1);
+}
+
+}  // namespace
+
+void launch_laz_decode(const uint8_t* d_bytes, uint64_t base, const std::vector<laz::Chunk>& chunks, const laz::Layout& L, uint8_t* d_out,
+                       DeviceMem& mem) {
+	if (chunks.empty()) return;
+	const uint64_t end = chunks.back().end;
+	for (const auto& c : chunks)
+		if (c.start < base || c.end > end || c.start >= c.end) throw PcgError(1, "malformed LAZ chunk table");
+	laz::Chunk* d_chunks = mem.alloc<laz::Chunk>(chunks.size());
+	PCG_CUDA(cudaMemcpyAsync(d_chunks, chunks.data(), chunks.size() * sizeof(laz::Chunk), cudaMemcpyHostToDevice, mem.stream()));
+	const uint32_t words = laz::arena_words(L);
+	// chunks decoded at once: all, or as many as about 4 GiB of model arenas hold
+	const int64_t fit = std::max<int64_t>(1, (int64_t(4) << 30) / ((int64_t)words * 4));
+	const int wave = (int)std::min<int64_t>((int64_t)chunks.size(), fit);
+	uint32_t* arena = mem.alloc<uint32_t>((size_t)wave * words);
+	int* d_bad = mem.alloc<int>(1);
+	PCG_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), mem.stream()));
+	for (int c0 = 0; c0 < (int)chunks.size(); c0 += wave) {
+		const int n = std::min<int>(wave, (int)chunks.size() - c0);
+		laz_decode_kernel<<<(unsigned)n, 32, 0, mem.stream()>>>(d_bytes, base, d_chunks, c0, n, L, arena, words, d_out, d_bad);
+		PCG_LAUNCHED();
+	}
+	int bad = 0;
+	PCG_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, mem.stream()));
+	PCG_CUDA(cudaStreamSynchronize(mem.stream()));
+	mem.free(d_bad);
+	mem.free(arena);
+	mem.free(d_chunks);
+	if (bad) throw PcgError(1, "malformed LAZ data in chunk " + std::to_string(bad - 1));
+}
+
+}  // namespace pcg

@@ -7,6 +7,8 @@
 #include <string>
 #include <vector>
 
+#include "laz.cuh"
+
 namespace pcg {
 
 // ---------------------------------------------------------------- geometry
@@ -69,6 +71,10 @@ struct LasInfo {
 	Vec3d scale, offset, min, max;
 	struct Vlr { uint16_t record_id; std::vector<uint8_t> data; };
 	std::vector<Vlr> vlrs;
+	// LAZ (point format with a compression bit): record layout and chunks
+	bool compressed = false;
+	laz::Layout laz_layout{};
+	std::vector<laz::Chunk> laz_chunks;
 };
 
 // One input file as the chunker's attribute handlers see it

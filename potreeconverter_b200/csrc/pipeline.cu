@@ -288,19 +288,37 @@ struct Converter {
 			src_base[k] = host_bytes;
 			host_bytes += (infos[k].num_points * (int64_t)infos[k].record_length + 15) & ~int64_t(15);
 		}
+		double ms_decode = 0.0;
 		if (host_bytes > 0) {
 			uint8_t* d_host = mem.alloc<uint8_t>(host_bytes);
 			for (size_t k = 0; k < sources.size(); k++) {
-				if (src_base[k] < 0) continue;
+				if (src_base[k] < 0 || infos[k].compressed) continue;
 				const int64_t bytes = infos[k].num_points * (int64_t)infos[k].record_length;
 				src_recs[k] = d_host + src_base[k];
 				if (bytes > 0)
 					PCG_CUDA(cudaMemcpyAsync(d_host + src_base[k], static_cast<const uint8_t*>(sources[k].las) + infos[k].offset_to_points,
 					                         bytes, cudaMemcpyHostToDevice, stream));
 			}
+			// LAZ sources: the compressed chunks go to the device and are
+			// decoded there into the source's records
+			for (size_t k = 0; k < sources.size(); k++) {
+				if (src_base[k] < 0 || !infos[k].compressed) continue;
+				src_recs[k] = d_host + src_base[k];
+				const auto& chunks = infos[k].laz_chunks;
+				if (chunks.empty()) continue;
+				const uint64_t base = chunks.front().start, nbytes = chunks.back().end - base;
+				uint8_t* d_laz = mem.alloc<uint8_t>(nbytes);
+				PCG_CUDA(cudaMemcpyAsync(d_laz, static_cast<const uint8_t*>(sources[k].las) + base, nbytes, cudaMemcpyHostToDevice, stream));
+				const auto t_dec = Clock::now();
+				launch_laz_decode(d_laz, base, chunks, infos[k].laz_layout, d_host + src_base[k], mem);
+				ms_decode += ms_since(t_dec);
+				mem.free(d_laz);
+				res.stats.laz_chunks += (int64_t)chunks.size();
+			}
 			PCG_CUDA(cudaStreamSynchronize(stream));
 		}
-		res.stats.ms_h2d = ms_since(t_h2d);
+		res.stats.ms_h2d = ms_since(t_h2d) - ms_decode;
+		res.stats.ms_decode = ms_decode;
 
 		// ------------------------------------------------------- chunking
 		auto t_chunk = Clock::now();
@@ -1405,6 +1423,30 @@ pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* p
 		int32_t* dp = mem.alloc<int32_t>(n);
 		pcg::launch_shuffle_single(n, seed, dp, mem);
 		PCG_CUDA(cudaMemcpyAsync(perm_out, dp, n * sizeof(int32_t), cudaMemcpyDeviceToHost, mem.stream()));
+		PCG_CUDA(cudaStreamSynchronize(mem.stream()));
+	});
+}
+
+pcg_status pcg_kernel_laz_decode(pcg_ctx* ctx, const void* laz_file, uint64_t size, void* records_out, uint64_t out_size) {
+	if (!ctx || !laz_file) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->mtx);
+	return guarded(ctx, [&] {
+		pcg::LasInfo info;
+		std::string err;
+		if (!pcg::parse_las(static_cast<const uint8_t*>(laz_file), size, info, err)) throw pcg::PcgError(PCG_BAD_INPUT, err);
+		if (!info.compressed) throw pcg::PcgError(PCG_BAD_INPUT, "not a LAZ file");
+		const uint64_t bytes = (uint64_t)info.num_points * (uint64_t)info.record_length;
+		if (out_size < bytes || (bytes && !records_out)) throw pcg::PcgError(PCG_BAD_INPUT, "records_out is too small");
+		if (bytes == 0) return;
+		PCG_CUDA(cudaSetDevice(ctx->conv.device));
+		pcg::DeviceMem mem(ctx->conv.stream, ctx->conv.arena.get());
+		const auto& chunks = info.laz_chunks;
+		const uint64_t base = chunks.front().start, nbytes = chunks.back().end - base;
+		uint8_t* d_laz = mem.alloc<uint8_t>(nbytes);
+		uint8_t* d_out = mem.alloc<uint8_t>(bytes);
+		PCG_CUDA(cudaMemcpyAsync(d_laz, static_cast<const uint8_t*>(laz_file) + base, nbytes, cudaMemcpyHostToDevice, mem.stream()));
+		pcg::launch_laz_decode(d_laz, base, chunks, info.laz_layout, d_out, mem);
+		PCG_CUDA(cudaMemcpyAsync(records_out, d_out, bytes, cudaMemcpyDeviceToHost, mem.stream()));
 		PCG_CUDA(cudaStreamSynchronize(mem.stream()));
 	});
 }

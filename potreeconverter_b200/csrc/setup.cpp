@@ -48,7 +48,7 @@ bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& er
 	info.offset_to_points = get<uint32_t>(las + 96);
 	uint32_t num_vlrs = get<uint32_t>(las + 100);
 	uint8_t fmt = las[104];
-	if (fmt & 0xC0) { err = "compressed (LAZ) point data is not supported"; return false; }
+	info.compressed = (fmt & 0xC0) != 0;  // LASzip marks compressed formats with bit 7 (6 in old files)
 	info.pdrf = fmt & 0x3f;
 	info.record_length = get<uint16_t>(las + 105);
 	uint64_t legacy = get<uint32_t>(las + 107);
@@ -61,6 +61,8 @@ bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& er
 	if (info.version_minor >= 4 && header_size >= 375 && size >= 255) ext = get<uint64_t>(las + 247);
 	info.num_points = (int64_t)(ext > legacy ? ext : legacy);  // LasLoader.cpp:103
 	uint64_t pos = header_size;
+	const uint8_t* laszip_vlr = nullptr;
+	uint32_t laszip_len = 0;
 	for (uint32_t i = 0; i < num_vlrs; i++) {
 		if (pos + 54 > size) { err = "truncated variable length record"; return false; }
 		LasInfo::Vlr v;
@@ -68,8 +70,18 @@ bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& er
 		uint16_t len = get<uint16_t>(las + pos + 20);
 		if (pos + 54 + len > size) { err = "truncated variable length record"; return false; }
 		v.data.assign(las + pos + 54, las + pos + 54 + len);
+		if (v.record_id == 22204 && std::memcmp(las + pos + 2, "laszip encoded", 14) == 0) {
+			laszip_vlr = las + pos + 54;
+			laszip_len = len;
+		}
 		info.vlrs.push_back(std::move(v));
 		pos += 54 + len;
+	}
+	if (info.compressed) {
+		// the chunk table is read unless the records are already decoded
+		if (points_elsewhere) return true;
+		return laz::parse_table(las, size, info.offset_to_points, info.num_points, info.pdrf, info.record_length, laszip_vlr, laszip_len,
+		                        info.laz_layout, info.laz_chunks, err);
 	}
 	if (!points_elsewhere && info.offset_to_points + (uint64_t)info.num_points * (uint64_t)info.record_length > size) {
 		err = "truncated point data";

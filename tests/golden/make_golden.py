@@ -44,6 +44,15 @@ CASES = [
 # metadata name is the first source's stem (main.cpp:146-200). Generators:
 # potreeconverter_b200.synth.sources.
 ALL = ["poisson", "poisson_average", "random"]
+# LAZ variants: (case name, laz spec) where the spec lists the positions (in
+# the passed order) of sources given as .laz, made by oracle/_ref/laz_tool
+# with the vendored LASzip (chunk_size 0: LASzip's default)
+LAZ = {
+    "tiles_laz_200k": {"sources": [0, 1, 2, 3], "chunk_size": 0},
+    "tiles_mixed_200k": {"sources": [0, 2], "chunk_size": 7000},
+    "hotspots_laz_300k": {"sources": [0], "chunk_size": 9999},
+}
+LAZ_TOOL = os.path.join(REPO, "oracle", "_ref", "laz_tool")
 MULTI_CASES = [
     ("tiles_200k", "tiles", 200_000, 11, {}, [0, 1, 2, 3], [], ALL),
     ("tiles_empty_200k", "tiles_empty", 200_000, 14, {}, [0, 1, 2], [], ALL),
@@ -54,7 +63,20 @@ MULTI_CASES = [
     ("hotspots_300k_reordered", "hotspots", 300_000, 1001, {}, [0],
      ["extra", "intensity", "return number", "number of returns", "classification", "scan angle rank",
       "user data", "point source id", "gps-time", "rgb"], ALL),
+    ("tiles_laz_200k", "tiles", 200_000, 15, {}, [0, 1, 2, 3], [], ALL),
+    ("tiles_mixed_200k", "tiles", 200_000, 16, {}, [2, 0, 3, 1], ["rgb", "gps-time", "intensity"], ALL),
+    ("hotspots_laz_300k", "hotspots", 300_000, 17, {}, [0], [], ALL),
 ]
+
+
+def to_laz(las: bytes, chunk_size: int, tmp: str) -> bytes:
+    """The LAZ image LASzip writes for a LAS image."""
+    src, dst = os.path.join(tmp, "_in.las"), os.path.join(tmp, "_out.laz")
+    with open(src, "wb") as f:
+        f.write(las)
+    subprocess.run([LAZ_TOOL, "compress", src, dst] + ([str(chunk_size)] if chunk_size else []), check=True)
+    with open(dst, "rb") as f:
+        return f.read()
 
 
 def multi_sources(kind, n, seed, kw, order):
@@ -77,14 +99,23 @@ def run_multi(tmp):
     for name, kind, n, seed, kw, order, attrs, methods in MULTI_CASES:
         imgs = multi_sources(kind, n, seed, kw, order)
         names = source_names(name, kind, order)
+        laz = LAZ.get(name)
         paths = []
-        for nm, img in zip(names, imgs):
-            paths.append(os.path.join(tmp, nm + ".las"))
+        laz_md5 = []
+        for pos, (nm, img) in enumerate(zip(names, imgs)):
+            if laz and pos in laz["sources"]:
+                img = to_laz(img, laz["chunk_size"], tmp)
+                laz_md5.append(hashlib.md5(img).hexdigest())
+                paths.append(os.path.join(tmp, nm + ".laz"))
+            else:
+                paths.append(os.path.join(tmp, nm + ".las"))
             with open(paths[-1], "wb") as f:
                 f.write(img)
         entry = {"name": name, "kind": kind, "points": n, "seed": seed, "kwargs": kw, "order": order,
                  "attributes": attrs, "meta_name": names[0],
                  "las_md5": [hashlib.md5(img).hexdigest() for img in imgs], "outputs": {}}
+        if laz:
+            entry["laz"] = dict(laz, laz_md5=laz_md5)
         for m in methods:
             od = os.path.join(tmp, f"{name}_{m}")
             cmd = [REF] + paths + ["-o", od, "-m", m]

@@ -134,3 +134,48 @@ def sources_for(case: dict) -> list:
                          tuple(case["order"]))
     assert [hashlib.md5(b).hexdigest() for b in imgs] == case["las_md5"], "synthetic generator output changed"
     return list(imgs)
+
+
+LAZ_TOOL = os.path.join(ORACLE_DIR, "_ref", "laz_tool")
+
+
+def have_laz_tool() -> bool:
+    return os.path.exists(LAZ_TOOL)
+
+
+def to_laz(las: bytes, chunk_size: int = 0) -> bytes:
+    """The LAZ image the reference's vendored LASzip writes for a LAS image
+    (oracle/_ref/laz_tool; chunk_size 0 is LASzip's default)."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as tmp:
+        src, dst = os.path.join(tmp, "in.las"), os.path.join(tmp, "out.laz")
+        with open(src, "wb") as f:
+            f.write(las)
+        subprocess.run([LAZ_TOOL, "compress", src, dst] + ([str(chunk_size)] if chunk_size else []), check=True,
+                       capture_output=True)
+        with open(dst, "rb") as f:
+            return f.read()
+
+
+def laz_sources_for(case: dict) -> list:
+    """Sources of a golden case as the pinned reference was given them: the
+    positions the case's "laz" entry lists as LAZ images."""
+    imgs = sources_for(case)
+    spec = case.get("laz")
+    if not spec:
+        return imgs
+    out, k = [], 0
+    for pos, img in enumerate(imgs):
+        if pos in spec["sources"]:
+            z = to_laz(img, spec["chunk_size"])
+            assert hashlib.md5(z).hexdigest() == spec["laz_md5"][k], "LASzip output changed"
+            k += 1
+            out.append(z)
+        else:
+            out.append(img)
+    return out
+
+
+def las_records(las: bytes) -> bytes:
+    import struct
+    return las[struct.unpack_from("<I", las, 96)[0]:]
