@@ -1,7 +1,9 @@
 // LAZ decode on the device: one LASzip chunk per block (its lane 0 runs the
 // chunk's arithmetic decoder, laz.cuh), all chunks of a source at once, each
-// with its own model arena; the decoded point records land where the LAS
-// path keeps a source's records, so the rest of the pipeline is unchanged.
+// with its models in the block's shared memory as far as they fit and the
+// rest in its own slice of a global arena; the decoded point records land
+// where the LAS path keeps a source's records, so the rest of the pipeline
+// is unchanged.
 // The reference decodes the same chunks sequentially per file, twice
 // (countPointsInCells and distributePoints, chunker_countsort_laszip.cpp:
 // 194-203, 750-772).
@@ -13,14 +15,17 @@ namespace pcg {
 
 namespace {
 
+// models go to the block's shared memory first (fast_words of it), then to
+// the chunk's slice of the global arena
 __global__ void __launch_bounds__(32) laz_decode_kernel(const uint8_t* __restrict__ bytes, uint64_t base, const laz::Chunk* __restrict__ chunks,
-                                                        int c0, int n, laz::Layout L, uint32_t* __restrict__ arena, uint32_t words,
-                                                        uint8_t* __restrict__ out, int* __restrict__ bad) {
+                                                        int c0, int n, laz::Layout L, uint32_t fast_words, uint32_t* __restrict__ arena,
+                                                        uint32_t words, uint8_t* __restrict__ out, int* __restrict__ bad) {
+	extern __shared__ uint32_t fast[];
 	if (threadIdx.x != 0 || (int)blockIdx.x >= n) return;
 	const int c = c0 + (int)blockIdx.x;
 	const laz::Chunk ch = chunks[c];
-	const bool ok = laz::decode_chunk(bytes + (ch.start - base), bytes + (ch.end - base), ch.count, L, arena + (size_t)blockIdx.x * words,
-	                                  words, out + ch.first * (int64_t)L.rec_len);
+	const bool ok = laz::decode_chunk(bytes + (ch.start - base), bytes + (ch.end - base), ch.count, L, fast_words ? fast : nullptr, fast_words,
+	                                  arena + (size_t)blockIdx.x * words, words, out + ch.first * (int64_t)L.rec_len);
 	if (!ok) atomicCAS(bad, 0, c + 1);
 }
 
@@ -41,9 +46,21 @@ void launch_laz_decode(const uint8_t* d_bytes, uint64_t base, const std::vector<
 	uint32_t* arena = mem.alloc<uint32_t>((size_t)wave * words);
 	int* d_bad = mem.alloc<int>(1);
 	PCG_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), mem.stream()));
+	// shared memory per block: as much as keeps every block of a wave
+	// resident at once, within the per-block limit
+	int dev = 0, sms = 0, per_sm = 0, per_block = 0;
+	PCG_CUDA(cudaGetDevice(&dev));
+	PCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+	PCG_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+	PCG_CUDA(cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+	const int blocks_per_sm = std::max(1, (wave + sms - 1) / sms);
+	size_t fast_bytes = std::min<size_t>((size_t)per_block, (size_t)per_sm / blocks_per_sm);
+	fast_bytes = fast_bytes > 2048 ? ((fast_bytes - 1024) & ~size_t(15)) : 0;
+	if (fast_bytes > 48 * 1024) PCG_CUDA(cudaFuncSetAttribute(laz_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fast_bytes));
 	for (int c0 = 0; c0 < (int)chunks.size(); c0 += wave) {
 		const int n = std::min<int>(wave, (int)chunks.size() - c0);
-		laz_decode_kernel<<<(unsigned)n, 32, 0, mem.stream()>>>(d_bytes, base, d_chunks, c0, n, L, arena, words, d_out, d_bad);
+		laz_decode_kernel<<<(unsigned)n, 32, fast_bytes, mem.stream()>>>(d_bytes, base, d_chunks, c0, n, L, (uint32_t)(fast_bytes / 4), arena,
+		                                                                  words, d_out, d_bad);
 		PCG_LAUNCHED();
 	}
 	int bad = 0;

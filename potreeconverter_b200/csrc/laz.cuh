@@ -41,20 +41,41 @@ constexpr uint32_t kSymShift = 15;         // symbol model: probability bits
 constexpr uint32_t kSymMaxCount = 1u << 15;
 
 // ------------------------------------------------------------------ arena
+// Model storage of one chunk decoder: words are taken from a fast region
+// first (the block's shared memory on the device; none on the host), then
+// from a global region. A null global region only measures.
 struct Arena {
-	uint32_t* A;     // null: only measure
-	uint32_t top, cap;
+	uint32_t* fast;
+	uint32_t f_top, f_cap;
+	uint32_t* glob;
+	uint32_t g_top, g_cap;
 	bool overflow;
-	LAZ_HD uint32_t take(uint32_t words) {
-		const uint32_t o = top;
-		top += words;
-		if (top > cap) overflow = true;
-		return o;
+	LAZ_HD bool measuring() const { return glob == nullptr; }
+	LAZ_HD uint32_t* take(uint32_t words) {
+		if (fast && f_top + words <= f_cap) {
+			uint32_t* p = fast + f_top;
+			f_top += words;
+			return p;
+		}
+		return take_global(words);
+	}
+	LAZ_HD uint32_t* take_global(uint32_t words) {
+		uint32_t* p = glob ? glob + g_top : nullptr;
+		g_top += words;
+		if (g_top > g_cap) {
+			overflow = true;
+			return nullptr;
+		}
+		return p;
 	}
 };
 
-// symbol model at A[m]: header, cumulative distribution[n], counts[n], and a
-// decoder table of table_size + 2 entries when n > 16
+// A symbol model is a pointer h to: a header of M_HDR words, then 16-bit
+// arrays: cumulative distribution[n], counts[n] and, for n > 16, a decoder
+// table of table_size + 2 entries. Every value fits 16 bits: distribution
+// values are below 2^15, counts below 2^15 + 8 (n + 6) (they are halved
+// when their total passes 2^15 at an update, at most 8 (n + 6) symbols
+// apart), table entries below n <= 516.
 enum { M_N = 0, M_SHIFT, M_TSIZE, M_TOTAL, M_CYCLE, M_UNTIL, M_HDR };
 
 LAZ_HD uint32_t table_bits_for(uint32_t n) {
@@ -64,40 +85,47 @@ LAZ_HD uint32_t table_bits_for(uint32_t n) {
 }
 
 LAZ_HD uint32_t model_words(uint32_t n) {
-	return M_HDR + 2 * n + (n > 16 ? (1u << table_bits_for(n)) + 2 : 0);
+	const uint32_t halves = 2 * n + (n > 16 ? (1u << table_bits_for(n)) + 2 : 0);
+	return M_HDR + (halves + 1) / 2;
 }
+
+LAZ_HD uint16_t* model_dist(uint32_t* h) { return reinterpret_cast<uint16_t*>(h + M_HDR); }
 
 // counts halved at the limit, cumulative distribution, decoder table, next
 // update interval (5/4 of the last, at most 8 (n + 6))
-LAZ_HD void model_update(uint32_t* A, uint32_t m) {
-	uint32_t* h = A + m;
+LAZ_HD void model_update(uint32_t* h) {
 	const uint32_t n = h[M_N];
-	uint32_t* dist = h + M_HDR;
-	uint32_t* cnt = dist + n;
+	uint16_t* dist = model_dist(h);
+	uint16_t* cnt = dist + n;
 	if ((h[M_TOTAL] += h[M_CYCLE]) > kSymMaxCount) {
 		uint32_t t = 0;
-		for (uint32_t k = 0; k < n; k++) t += (cnt[k] = (cnt[k] + 1) >> 1);
+		for (uint32_t k = 0; k < n; k++) {
+			const uint32_t c = ((uint32_t)cnt[k] + 1) >> 1;
+			cnt[k] = (uint16_t)c;
+			t += c;
+		}
 		h[M_TOTAL] = t;
 	}
 	const uint32_t scale = 0x80000000u / h[M_TOTAL];
 	uint32_t sum = 0;
 	if (h[M_TSIZE] == 0) {
 		for (uint32_t k = 0; k < n; k++) {
-			dist[k] = (scale * sum) >> (31 - kSymShift);
+			dist[k] = (uint16_t)((scale * sum) >> (31 - kSymShift));
 			sum += cnt[k];
 		}
 	} else {
-		uint32_t* tab = cnt + n;
+		uint16_t* tab = cnt + n;
 		const uint32_t shift = h[M_SHIFT], tsize = h[M_TSIZE];
 		uint32_t s = 0;
 		for (uint32_t k = 0; k < n; k++) {
-			dist[k] = (scale * sum) >> (31 - kSymShift);
+			const uint32_t dk = (scale * sum) >> (31 - kSymShift);
+			dist[k] = (uint16_t)dk;
 			sum += cnt[k];
-			const uint32_t w = dist[k] >> shift;
-			while (s < w && s < tsize) tab[++s] = k - 1;
+			const uint32_t w = dk >> shift;
+			while (s < w && s < tsize) tab[++s] = (uint16_t)(k - 1);
 		}
 		tab[0] = 0;
-		while (s <= tsize) tab[++s] = n - 1;
+		while (s <= tsize) tab[++s] = (uint16_t)(n - 1);
 	}
 	uint32_t cycle = (5 * h[M_CYCLE]) >> 2;
 	const uint32_t max_cycle = (n + 6) << 3;
@@ -106,46 +134,44 @@ LAZ_HD void model_update(uint32_t* A, uint32_t m) {
 }
 
 // uniform counts, then the first update after (n + 6) / 2 symbols
-LAZ_HD void model_init(uint32_t* A, uint32_t m) {
-	uint32_t* h = A + m;
+LAZ_HD void model_init(uint32_t* h) {
 	const uint32_t n = h[M_N];
-	uint32_t* cnt = h + M_HDR + n;
+	uint16_t* cnt = model_dist(h) + n;
 	h[M_TOTAL] = 0;
 	h[M_CYCLE] = n;
 	for (uint32_t k = 0; k < n; k++) cnt[k] = 1;
-	model_update(A, m);
+	model_update(h);
 	h[M_CYCLE] = h[M_UNTIL] = (n + 6) >> 1;
 }
 
-LAZ_HD uint32_t model_new(Arena& ar, uint32_t n) {
-	const uint32_t m = ar.take(model_words(n));
-	if (ar.A && !ar.overflow) {
-		uint32_t* h = ar.A + m;
-		h[M_N] = n;
-		if (n > 16) {
-			const uint32_t tb = table_bits_for(n);
-			h[M_TSIZE] = 1u << tb;
-			h[M_SHIFT] = kSymShift - tb;
-		} else {
-			h[M_TSIZE] = h[M_SHIFT] = 0;
-		}
+LAZ_HD void model_header(uint32_t* h, uint32_t n) {
+	h[M_N] = n;
+	if (n > 16) {
+		const uint32_t tb = table_bits_for(n);
+		h[M_TSIZE] = 1u << tb;
+		h[M_SHIFT] = kSymShift - tb;
+	} else {
+		h[M_TSIZE] = h[M_SHIFT] = 0;
 	}
-	return m;
 }
 
-// bit model at A[b]: count of zeros, count, probability of zero, interval
+LAZ_HD uint32_t* model_new(Arena& ar, uint32_t n) {
+	uint32_t* h = ar.take(model_words(n));
+	if (h) model_header(h, n);
+	return h;
+}
+
+// bit model: count of zeros, count, probability of zero, interval
 enum { B_ZERO = 0, B_COUNT, B_PROB, B_CYCLE, B_UNTIL, B_WORDS };
 
-LAZ_HD void bit_init(uint32_t* A, uint32_t b) {
-	uint32_t* h = A + b;
+LAZ_HD void bit_init(uint32_t* h) {
 	h[B_ZERO] = 1;
 	h[B_COUNT] = 2;
 	h[B_PROB] = 1u << (kBitShift - 1);
 	h[B_CYCLE] = h[B_UNTIL] = 4;
 }
 
-LAZ_HD void bit_update(uint32_t* A, uint32_t b) {
-	uint32_t* h = A + b;
+LAZ_HD void bit_update(uint32_t* h) {
 	if ((h[B_COUNT] += h[B_CYCLE]) > kBitMaxCount) {
 		h[B_COUNT] = (h[B_COUNT] + 1) >> 1;
 		h[B_ZERO] = (h[B_ZERO] + 1) >> 1;
@@ -192,8 +218,7 @@ struct Decoder {
 			length = kMinLength;
 		}
 	}
-	LAZ_HD uint32_t bit(uint32_t* A, uint32_t b) {
-		uint32_t* h = A + b;
+	LAZ_HD uint32_t bit(uint32_t* h) {
 		const uint32_t x = h[B_PROB] * (length >> kBitShift);
 		const uint32_t sym = value >= x;
 		if (sym == 0) {
@@ -204,21 +229,20 @@ struct Decoder {
 			length -= x;
 		}
 		if (length < kMinLength) renorm();
-		if (--h[B_UNTIL] == 0) bit_update(A, b);
+		if (--h[B_UNTIL] == 0) bit_update(h);
 		return sym;
 	}
-	LAZ_HD uint32_t symbol(uint32_t* A, uint32_t m) {
-		uint32_t* h = A + m;
+	LAZ_HD uint32_t symbol(uint32_t* h) {
 		const uint32_t nsym = h[M_N];
-		const uint32_t* dist = h + M_HDR;
+		const uint16_t* dist = model_dist(h);
 		uint32_t n, sym, x, y = length;
 		if (h[M_TSIZE]) {
-			const uint32_t* tab = dist + 2 * nsym;
+			const uint16_t* tab = dist + 2 * nsym;
 			const uint32_t dv = value / (length >>= kSymShift);
 			uint32_t t = dv >> h[M_SHIFT];
 			if (t > h[M_TSIZE]) t = h[M_TSIZE];
 			sym = tab[t];
-			n = tab[t + 1] + 1;
+			n = (uint32_t)tab[t + 1] + 1;
 			if (n > nsym) n = nsym;
 			if (sym >= nsym) sym = nsym - 1;
 			while (n > sym + 1) {
@@ -247,9 +271,9 @@ struct Decoder {
 		value -= x;
 		length = y - x;
 		if (length < kMinLength) renorm();
-		uint32_t* cnt = h + M_HDR + nsym;
+		uint16_t* cnt = model_dist(h) + nsym;
 		++cnt[sym];
-		if (--h[M_UNTIL] == 0) model_update(A, m);
+		if (--h[M_UNTIL] == 0) model_update(h);
 		return sym;
 	}
 	// raw bits (readBits, readShort, readInt)
@@ -282,14 +306,13 @@ struct Decoder {
 struct IntCoder {
 	uint32_t bits_high, corr_bits, corr_range;
 	int32_t corr_min;
-	uint32_t contexts;
-	uint32_t mbits;  // first of `contexts` class models (consecutive)
-	uint32_t mbits_words;
-	uint32_t corr0;  // bit model for k = 0
-	uint32_t corr[33];  // symbol model per k = 1..corr_bits
+	uint32_t contexts, mbits_words;
+	uint32_t* mbits;    // `contexts` class models, back to back
+	uint32_t* corr0;    // bit model for k = 0
+	uint32_t* corr[33]; // symbol model per k = 1..corr_bits
 	uint32_t k;         // class of the last value
 
-	LAZ_HD void create(Arena& ar, uint32_t bits, uint32_t nctx, uint32_t high = 8) {
+	LAZ_HD void setup(uint32_t bits, uint32_t nctx, uint32_t high = 8) {
 		bits_high = high;
 		contexts = nctx;
 		if (bits && bits < 32) {
@@ -302,33 +325,39 @@ struct IntCoder {
 			corr_min = (int32_t)0x80000000u;
 		}
 		mbits_words = model_words(corr_bits + 1);
-		mbits = ar.take(0);
-		for (uint32_t i = 0; i < nctx; i++) model_new(ar, corr_bits + 1);
+		mbits = corr0 = nullptr;
+		for (int i = 0; i < 33; i++) corr[i] = nullptr;
+		k = 0;
+	}
+	LAZ_HD void alloc_classes(Arena& ar) {
+		mbits = ar.take(contexts * mbits_words);
+		if (mbits)
+			for (uint32_t i = 0; i < contexts; i++) model_header(mbits + i * mbits_words, corr_bits + 1);
 		corr0 = ar.take(B_WORDS);
-		corr[0] = 0;
-		for (uint32_t i = 1; i <= corr_bits; i++) corr[i] = model_new(ar, i <= bits_high ? (1u << i) : (1u << bits_high));
+	}
+	LAZ_HD void alloc_correctors(Arena& ar, uint32_t lo, uint32_t hi) {
+		for (uint32_t i = lo; i <= hi && i <= corr_bits; i++) corr[i] = model_new(ar, i <= bits_high ? (1u << i) : (1u << bits_high));
+	}
+	LAZ_HD void init() {
+		for (uint32_t i = 0; i < contexts; i++) model_init(mbits + i * mbits_words);
+		bit_init(corr0);
+		for (uint32_t i = 1; i <= corr_bits; i++) model_init(corr[i]);
 		k = 0;
 	}
-	LAZ_HD void init(uint32_t* A) {
-		for (uint32_t i = 0; i < contexts; i++) model_init(A, mbits + i * mbits_words);
-		bit_init(A, corr0);
-		for (uint32_t i = 1; i <= corr_bits; i++) model_init(A, corr[i]);
-		k = 0;
-	}
-	LAZ_HD int32_t corrector(Decoder& d, uint32_t* A, uint32_t ctx) {
+	LAZ_HD int32_t corrector(Decoder& d, uint32_t ctx) {
 		if (ctx >= contexts) {
 			d.bad = true;
 			ctx = 0;
 		}
-		k = d.symbol(A, mbits + ctx * mbits_words);
+		k = d.symbol(mbits + ctx * mbits_words);
 		uint32_t c;
 		if (k) {
 			if (k < 32) {
 				if (k <= bits_high) {
-					c = d.symbol(A, corr[k]);
+					c = d.symbol(corr[k]);
 				} else {
 					const uint32_t k1 = k - bits_high;
-					c = d.symbol(A, corr[k]);
+					c = d.symbol(corr[k]);
 					const uint32_t c1 = d.raw_bits(k1);
 					c = (c << k1) | c1;
 				}
@@ -339,12 +368,12 @@ struct IntCoder {
 				c = (uint32_t)corr_min;
 			}
 		} else {
-			c = d.bit(A, corr0);
+			c = d.bit(corr0);
 		}
 		return (int32_t)c;
 	}
-	LAZ_HD int32_t decode(Decoder& d, uint32_t* A, int32_t pred, uint32_t ctx = 0) {
-		int32_t real = (int32_t)((uint32_t)pred + (uint32_t)corrector(d, A, ctx));
+	LAZ_HD int32_t decode(Decoder& d, int32_t pred, uint32_t ctx = 0) {
+		int32_t real = (int32_t)((uint32_t)pred + (uint32_t)corrector(d, ctx));
 		if (real < 0) real = (int32_t)((uint32_t)real + corr_range);
 		else if ((uint32_t)real >= corr_range) real = (int32_t)((uint32_t)real - corr_range);
 		return real;
@@ -427,64 +456,85 @@ struct Layout {
 	int has_gps, has_rgb, n_extra, rec_len;
 };
 
-// Model offsets of one chunk decoder inside its arena (identical for all
-// chunks of a source; the three 256-entry lazy tables of POINT10 follow).
+// The models of one chunk decoder (identical for all chunks of a source),
+// placed in order of use so that the fast region holds the ones every point
+// needs: the classes of every integer coder, the per-point symbol models,
+// the correctors of classes up to 16, then the rest. The three 256-context
+// tables of POINT10 (bit byte, classification, user data) create their
+// models when a context first occurs.
 struct Models {
-	uint32_t changed, scan_angle[2];
-	IntCoder ic_intensity, ic_psid, ic_dx, ic_dy, ic_z;
-	uint32_t lazy;  // 3 x 256 words: model offset per context byte, 0 = none yet
-	uint32_t gps_multi, gps_0diff;
-	IntCoder ic_gps;
-	uint32_t rgb_used, rgb_diff[6];
-	uint32_t byte_model[kMaxExtraBytes];
-	uint32_t fixed_words;  // arena words before the lazily created models
+	uint32_t* changed;
+	uint32_t* scan_angle[2];
+	IntCoder ic_intensity, ic_psid, ic_dx, ic_dy, ic_z, ic_gps;
+	uint32_t* lazy;  // 3 x 256 handles: 0 none yet, else 1 + word offset | 2^31 when in the fast region
+	uint32_t* gps_multi;
+	uint32_t* gps_0diff;
+	uint32_t* rgb_used;
+	uint32_t* rgb_diff[6];
+	uint32_t* byte_model[kMaxExtraBytes];
 
 	LAZ_HD void create(Arena& ar, const Layout& L) {
+		ic_intensity.setup(16, 4);
+		ic_psid.setup(16, 1);
+		ic_dx.setup(32, 2);
+		ic_dy.setup(32, 22);
+		ic_z.setup(32, 20);
+		ic_gps.setup(32, 9);
 		changed = model_new(ar, 64);
-		ic_intensity.create(ar, 16, 4);
+		ic_dx.alloc_classes(ar);
+		ic_dy.alloc_classes(ar);
+		ic_z.alloc_classes(ar);
+		ic_intensity.alloc_classes(ar);
+		ic_psid.alloc_classes(ar);
+		if (L.has_gps) {
+			gps_0diff = model_new(ar, 6);
+			gps_multi = model_new(ar, 516);  // 500 multipliers, -10 .. -1, unchanged, full, 4 sequence switches
+			ic_gps.alloc_classes(ar);
+		}
 		scan_angle[0] = model_new(ar, 256);
 		scan_angle[1] = model_new(ar, 256);
-		ic_psid.create(ar, 16, 1);
-		ic_dx.create(ar, 32, 2);
-		ic_dy.create(ar, 32, 22);
-		ic_z.create(ar, 32, 20);
-		lazy = ar.take(3 * 256);
-		if (L.has_gps) {
-			gps_multi = model_new(ar, 516);  // 500 multipliers, -10 .. -1, unchanged, full, 4 sequence switches
-			gps_0diff = model_new(ar, 6);
-			ic_gps.create(ar, 32, 9);
-		}
 		if (L.has_rgb) {
 			rgb_used = model_new(ar, 128);
 			for (int i = 0; i < 6; i++) rgb_diff[i] = model_new(ar, 256);
 		}
 		for (int i = 0; i < L.n_extra && i < kMaxExtraBytes; i++) byte_model[i] = model_new(ar, 256);
-		fixed_words = ar.top;
+		ic_dx.alloc_correctors(ar, 1, 16);
+		ic_dy.alloc_correctors(ar, 1, 16);
+		ic_z.alloc_correctors(ar, 1, 16);
+		ic_intensity.alloc_correctors(ar, 1, 16);
+		ic_psid.alloc_correctors(ar, 1, 16);
+		if (L.has_gps) ic_gps.alloc_correctors(ar, 1, 16);
+		ic_dx.alloc_correctors(ar, 17, 32);
+		ic_dy.alloc_correctors(ar, 17, 32);
+		ic_z.alloc_correctors(ar, 17, 32);
+		if (L.has_gps) ic_gps.alloc_correctors(ar, 17, 32);
+		lazy = ar.take_global(3 * 256);
 	}
 };
 
-// Arena words one chunk decoder may need: the fixed models plus one
-// 256-symbol model for each of the 3 x 256 lazily created contexts.
+// Global words one chunk decoder may need with no fast region: the models
+// plus one 256-symbol model for each of the 3 x 256 lazily created contexts.
 inline uint32_t arena_words(const Layout& L) {
-	Arena ar{nullptr, 0, 0xFFFFFFFFu, false};
+	Arena ar{nullptr, 0, 0, nullptr, 0, 0xFFFFFFFFu, false};
 	Models M;
 	M.create(ar, L);
-	return ar.top + 3 * 256 * model_words(256);
+	return ar.g_top + 3 * 256 * model_words(256);
 }
 
 // Decodes one LASzip chunk of `count` points from bytes [p, end) into
-// `count` consecutive records of L.rec_len bytes at out. A is the chunk's
-// arena of `cap` words (at least arena_words(L)). Returns false on malformed
+// `count` consecutive records of L.rec_len bytes at out. Models go to the
+// fast region (fast, f_words; may be null) first, then to the global
+// region (glob, g_words >= arena_words(L)). Returns false on malformed
 // input. Follows LASreadPoint::read (lasreadpoint.cpp:405-497): the first
 // point is stored raw, the arithmetic decoder starts after it.
-LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, const Layout& L, uint32_t* A, uint32_t cap,
-                         uint8_t* out) {
+LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, const Layout& L, uint32_t* fast, uint32_t f_words,
+                         uint32_t* glob, uint32_t g_words, uint8_t* out) {
 	if (count <= 0) return true;
 	const int rl = L.rec_len;
 	const int std_len = 20 + (L.has_gps ? 8 : 0) + (L.has_rgb ? 6 : 0);
 	if (L.n_extra < 0 || L.n_extra > kMaxExtraBytes || std_len + L.n_extra != rl) return false;
 	if (end - p < rl) return false;
-	Arena ar{A, 0, cap, false};
+	Arena ar{fast, 0, fast ? f_words : 0u, glob, 0, g_words, false};
 	Models M;
 	M.create(ar, L);
 	if (ar.overflow) return false;
@@ -504,104 +554,102 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 		last_intensity[i] = 0;
 	}
 	for (int i = 0; i < 8; i++) last_height[i] = 0;
-	model_init(A, M.changed);
-	M.ic_intensity.init(A);
-	model_init(A, M.scan_angle[0]);
-	model_init(A, M.scan_angle[1]);
-	M.ic_psid.init(A);
-	M.ic_dx.init(A);
-	M.ic_dy.init(A);
-	M.ic_z.init(A);
-	uint32_t* lazy = A + M.lazy;
+	model_init(M.changed);
+	M.ic_intensity.init();
+	model_init(M.scan_angle[0]);
+	model_init(M.scan_angle[1]);
+	M.ic_psid.init();
+	M.ic_dx.init();
+	M.ic_dy.init();
+	M.ic_z.init();
+	uint32_t* lazy = M.lazy;
 	for (int i = 0; i < 3 * 256; i++) lazy[i] = 0;
-	uint32_t lazy_top = M.fixed_words;
 	// GPSTIME11 state
 	int64_t gps[4] = {0, 0, 0, 0};
 	int32_t gps_diff[4] = {0, 0, 0, 0};
 	int32_t gps_extreme[4] = {0, 0, 0, 0};
 	uint32_t gps_last = 0, gps_next = 0;
 	if (L.has_gps) {
-		model_init(A, M.gps_multi);
-		model_init(A, M.gps_0diff);
-		M.ic_gps.init(A);
+		model_init(M.gps_multi);
+		model_init(M.gps_0diff);
+		M.ic_gps.init();
 		gps[0] = rd<int64_t>(out + 20);
 	}
 	// RGB12 state
 	uint16_t last_rgb[3] = {0, 0, 0};
 	const int rgb_off = 20 + (L.has_gps ? 8 : 0);
 	if (L.has_rgb) {
-		model_init(A, M.rgb_used);
-		for (int i = 0; i < 6; i++) model_init(A, M.rgb_diff[i]);
+		model_init(M.rgb_used);
+		for (int i = 0; i < 6; i++) model_init(M.rgb_diff[i]);
 		for (int i = 0; i < 3; i++) last_rgb[i] = rd<uint16_t>(out + rgb_off + 2 * i);
 	}
 	// BYTE state
 	uint8_t last_extra[kMaxExtraBytes];
 	for (int i = 0; i < L.n_extra; i++) {
-		model_init(A, M.byte_model[i]);
+		model_init(M.byte_model[i]);
 		last_extra[i] = out[std_len + i];
 	}
 	Decoder d;
 	d.start(p, end);
 	// lazily created 256-symbol model of table t (0 bit byte, 1 class, 2 user data) for context c
-	auto lazy_model = [&](int t, uint32_t c) -> uint32_t {
+	auto lazy_model = [&](int t, uint32_t c) -> uint32_t* {
 		uint32_t& slot = lazy[t * 256 + (c & 255)];
 		if (slot == 0) {
-			Arena la{A, lazy_top, cap, false};
-			const uint32_t m = model_new(la, 256);
-			if (la.overflow) {
+			uint32_t* m = model_new(ar, 256);
+			if (!m) {
 				d.bad = true;
 				return M.scan_angle[0];
 			}
-			lazy_top = la.top;
-			model_init(A, m);
-			slot = m;
+			model_init(m);
+			slot = (fast && m >= fast && m < fast + f_words) ? (0x80000000u | (uint32_t)(m - fast)) : (uint32_t)(m - glob) + 1;
+			return m;
 		}
-		return slot;
+		return (slot & 0x80000000u) ? fast + (slot & 0x7FFFFFFFu) : glob + (slot - 1);
 	};
 
 	for (int64_t i = 1; i < count && !d.bad; i++) {
 		uint8_t* rec = out + i * rl;
 		// ---- POINT10 v2 (lasreaditemcompressed_v2.cpp, POINT10 read)
-		const uint32_t changed = d.symbol(A, M.changed);
+		const uint32_t changed = d.symbol(M.changed);
 		uint32_t r, n;
 		if (changed) {
-			if (changed & 32) last[14] = (uint8_t)d.symbol(A, lazy_model(0, last[14]));
+			if (changed & 32) last[14] = (uint8_t)d.symbol(lazy_model(0, last[14]));
 			r = last[14] & 7;
 			n = (last[14] >> 3) & 7;
 			const uint32_t m = return_map(n, r);
 			if (changed & 16) {
-				const uint16_t v = (uint16_t)M.ic_intensity.decode(d, A, last_intensity[m], m < 3 ? m : 3);
+				const uint16_t v = (uint16_t)M.ic_intensity.decode(d, last_intensity[m], m < 3 ? m : 3);
 				wr<uint16_t>(last + 12, v);
 				last_intensity[m] = v;
 			} else {
 				wr<uint16_t>(last + 12, last_intensity[m]);
 			}
-			if (changed & 8) last[15] = (uint8_t)d.symbol(A, lazy_model(1, last[15]));
+			if (changed & 8) last[15] = (uint8_t)d.symbol(lazy_model(1, last[15]));
 			if (changed & 4) {
-				const int32_t v = (int32_t)d.symbol(A, M.scan_angle[(last[14] >> 6) & 1]);
+				const int32_t v = (int32_t)d.symbol(M.scan_angle[(last[14] >> 6) & 1]);
 				last[16] = (uint8_t)fold8(v + last[16]);
 			}
-			if (changed & 2) last[17] = (uint8_t)d.symbol(A, lazy_model(2, last[17]));
-			if (changed & 1) wr<uint16_t>(last + 18, (uint16_t)M.ic_psid.decode(d, A, rd<uint16_t>(last + 18)));
+			if (changed & 2) last[17] = (uint8_t)d.symbol(lazy_model(2, last[17]));
+			if (changed & 1) wr<uint16_t>(last + 18, (uint16_t)M.ic_psid.decode(d, rd<uint16_t>(last + 18)));
 		} else {
 			r = last[14] & 7;
 			n = (last[14] >> 3) & 7;
 		}
 		const uint32_t m = return_map(n, r), l = return_level(n, r);
 		{
-			const int32_t diff = M.ic_dx.decode(d, A, mx[m].get(), n == 1);
+			const int32_t diff = M.ic_dx.decode(d, mx[m].get(), n == 1);
 			wr<int32_t>(last + 0, (int32_t)((uint32_t)rd<int32_t>(last + 0) + (uint32_t)diff));
 			mx[m].add(diff);
 		}
 		{
 			const uint32_t kb = M.ic_dx.k;
-			const int32_t diff = M.ic_dy.decode(d, A, my[m].get(), (n == 1) + (kb < 20 ? (kb & ~1u) : 20));
+			const int32_t diff = M.ic_dy.decode(d, my[m].get(), (n == 1) + (kb < 20 ? (kb & ~1u) : 20));
 			wr<int32_t>(last + 4, (int32_t)((uint32_t)rd<int32_t>(last + 4) + (uint32_t)diff));
 			my[m].add(diff);
 		}
 		{
 			const uint32_t kb = (M.ic_dx.k + M.ic_dy.k) / 2;
-			const int32_t z = M.ic_z.decode(d, A, last_height[l], (n == 1) + (kb < 18 ? (kb & ~1u) : 18));
+			const int32_t z = M.ic_z.decode(d, last_height[l], (n == 1) + (kb < 18 ? (kb & ~1u) : 18));
 			wr<int32_t>(last + 8, z);
 			last_height[l] = z;
 		}
@@ -615,14 +663,14 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 				}
 				bool again = false;
 				if (gps_diff[gps_last] == 0) {
-					const uint32_t multi = d.symbol(A, M.gps_0diff);
+					const uint32_t multi = d.symbol(M.gps_0diff);
 					if (multi == 1) {
-						gps_diff[gps_last] = M.ic_gps.decode(d, A, 0, 0);
+						gps_diff[gps_last] = M.ic_gps.decode(d, 0, 0);
 						gps[gps_last] = add_wrap(gps[gps_last], gps_diff[gps_last]);
 						gps_extreme[gps_last] = 0;
 					} else if (multi == 2) {
 						gps_next = (gps_next + 1) & 3;
-						const uint32_t hi = (uint32_t)M.ic_gps.decode(d, A, (int32_t)(uint32_t)((uint64_t)gps[gps_last] >> 32), 8);
+						const uint32_t hi = (uint32_t)M.ic_gps.decode(d, (int32_t)(uint32_t)((uint64_t)gps[gps_last] >> 32), 8);
 						const uint32_t lo = d.raw_int();
 						gps[gps_next] = (int64_t)(((uint64_t)hi << 32) | lo);
 						gps_last = gps_next;
@@ -633,24 +681,24 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 						again = true;
 					}
 				} else {
-					const int32_t multi = (int32_t)d.symbol(A, M.gps_multi);
+					const int32_t multi = (int32_t)d.symbol(M.gps_multi);
 					const int32_t ld = gps_diff[gps_last];
 					auto times = [](int32_t a, int32_t b) { return (int32_t)((uint32_t)a * (uint32_t)b); };
 					if (multi == 1) {
-						gps[gps_last] = add_wrap(gps[gps_last], M.ic_gps.decode(d, A, ld, 1));
+						gps[gps_last] = add_wrap(gps[gps_last], M.ic_gps.decode(d, ld, 1));
 						gps_extreme[gps_last] = 0;
 					} else if (multi < 511) {
 						int32_t gd;
 						if (multi == 0) {
-							gd = M.ic_gps.decode(d, A, 0, 7);
+							gd = M.ic_gps.decode(d, 0, 7);
 							if (++gps_extreme[gps_last] > 3) {
 								gps_diff[gps_last] = gd;
 								gps_extreme[gps_last] = 0;
 							}
 						} else if (multi < 500) {
-							gd = M.ic_gps.decode(d, A, times(multi, ld), multi < 10 ? 2 : 3);
+							gd = M.ic_gps.decode(d, times(multi, ld), multi < 10 ? 2 : 3);
 						} else if (multi == 500) {
-							gd = M.ic_gps.decode(d, A, times(500, ld), 4);
+							gd = M.ic_gps.decode(d, times(500, ld), 4);
 							if (++gps_extreme[gps_last] > 3) {
 								gps_diff[gps_last] = gd;
 								gps_extreme[gps_last] = 0;
@@ -658,9 +706,9 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 						} else {
 							const int32_t mm = 500 - multi;  // -1 .. -10
 							if (mm > -10) {
-								gd = M.ic_gps.decode(d, A, times(mm, ld), 5);
+								gd = M.ic_gps.decode(d, times(mm, ld), 5);
 							} else {
-								gd = M.ic_gps.decode(d, A, times(-10, ld), 6);
+								gd = M.ic_gps.decode(d, times(-10, ld), 6);
 								if (++gps_extreme[gps_last] > 3) {
 									gps_diff[gps_last] = gd;
 									gps_extreme[gps_last] = 0;
@@ -670,7 +718,7 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 						gps[gps_last] = add_wrap(gps[gps_last], gd);
 					} else if (multi == 512) {
 						gps_next = (gps_next + 1) & 3;
-						const uint32_t hi = (uint32_t)M.ic_gps.decode(d, A, (int32_t)(uint32_t)((uint64_t)gps[gps_last] >> 32), 8);
+						const uint32_t hi = (uint32_t)M.ic_gps.decode(d, (int32_t)(uint32_t)((uint64_t)gps[gps_last] >> 32), 8);
 						const uint32_t lo = d.raw_int();
 						gps[gps_next] = (int64_t)(((uint64_t)hi << 32) | lo);
 						gps_last = gps_next;
@@ -688,17 +736,17 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 		// ---- RGB12 v2
 		if (L.has_rgb) {
 			uint16_t c[3];
-			const uint32_t sym = d.symbol(A, M.rgb_used);
-			if (sym & 1) c[0] = (uint16_t)fold8((int32_t)(uint8_t)d.symbol(A, M.rgb_diff[0]) + (last_rgb[0] & 255));
+			const uint32_t sym = d.symbol(M.rgb_used);
+			if (sym & 1) c[0] = (uint16_t)fold8((int32_t)(uint8_t)d.symbol(M.rgb_diff[0]) + (last_rgb[0] & 255));
 			else c[0] = last_rgb[0] & 0xFF;
-			if (sym & 2) c[0] |= (uint16_t)(fold8((int32_t)(uint8_t)d.symbol(A, M.rgb_diff[1]) + (last_rgb[0] >> 8)) << 8);
+			if (sym & 2) c[0] |= (uint16_t)(fold8((int32_t)(uint8_t)d.symbol(M.rgb_diff[1]) + (last_rgb[0] >> 8)) << 8);
 			else c[0] |= last_rgb[0] & 0xFF00;
 			if (sym & 64) {
 				int32_t diff = (int32_t)(c[0] & 0xFF) - (int32_t)(last_rgb[0] & 0xFF);
-				if (sym & 4) c[1] = (uint16_t)fold8((int32_t)(uint8_t)d.symbol(A, M.rgb_diff[2]) + clamp8(diff + (last_rgb[1] & 255)));
+				if (sym & 4) c[1] = (uint16_t)fold8((int32_t)(uint8_t)d.symbol(M.rgb_diff[2]) + clamp8(diff + (last_rgb[1] & 255)));
 				else c[1] = last_rgb[1] & 0xFF;
 				if (sym & 16) {
-					const int32_t corr = (int32_t)(uint8_t)d.symbol(A, M.rgb_diff[4]);
+					const int32_t corr = (int32_t)(uint8_t)d.symbol(M.rgb_diff[4]);
 					diff = (diff + ((int32_t)(c[1] & 0xFF) - (int32_t)(last_rgb[1] & 0xFF))) / 2;
 					c[2] = (uint16_t)fold8(corr + clamp8(diff + (last_rgb[2] & 255)));
 				} else {
@@ -706,11 +754,11 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 				}
 				diff = (int32_t)(c[0] >> 8) - (int32_t)(last_rgb[0] >> 8);
 				if (sym & 8)
-					c[1] |= (uint16_t)(fold8((int32_t)(uint8_t)d.symbol(A, M.rgb_diff[3]) + clamp8(diff + (last_rgb[1] >> 8))) << 8);
+					c[1] |= (uint16_t)(fold8((int32_t)(uint8_t)d.symbol(M.rgb_diff[3]) + clamp8(diff + (last_rgb[1] >> 8))) << 8);
 				else
 					c[1] |= last_rgb[1] & 0xFF00;
 				if (sym & 32) {
-					const int32_t corr = (int32_t)(uint8_t)d.symbol(A, M.rgb_diff[5]);
+					const int32_t corr = (int32_t)(uint8_t)d.symbol(M.rgb_diff[5]);
 					diff = (diff + ((int32_t)(c[1] >> 8) - (int32_t)(last_rgb[1] >> 8))) / 2;
 					c[2] |= (uint16_t)(fold8(corr + clamp8(diff + (last_rgb[2] >> 8))) << 8);
 				} else {
@@ -727,7 +775,7 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 		}
 		// ---- BYTE v2
 		for (int e = 0; e < L.n_extra; e++) {
-			last_extra[e] = (uint8_t)fold8((int32_t)last_extra[e] + (int32_t)d.symbol(A, M.byte_model[e]));
+			last_extra[e] = (uint8_t)fold8((int32_t)last_extra[e] + (int32_t)d.symbol(M.byte_model[e]));
 			rec[std_len + e] = last_extra[e];
 		}
 	}
@@ -801,20 +849,23 @@ inline bool parse_table(const uint8_t* file, uint64_t size, uint64_t offset_to_p
 	if (n == 0 || n > (1u << 26)) { err = "LAZ chunk table without chunks"; return false; }
 	// entries: IntCoder(32 bits, 2 contexts) over the previous entry
 	const bool variable = chunk_size == 0xFFFFFFFFu;
-	std::vector<uint32_t> A;
-	Arena measure{nullptr, 0, 0xFFFFFFFFu, false};
 	IntCoder ic;
-	ic.create(measure, 32, 2);
-	A.assign(measure.top, 0);
-	Arena ar{A.data(), 0, (uint32_t)A.size(), false};
-	ic.create(ar, 32, 2);
-	ic.init(A.data());
+	ic.setup(32, 2);
+	Arena measure{nullptr, 0, 0, nullptr, 0, 0xFFFFFFFFu, false};
+	ic.alloc_classes(measure);
+	ic.alloc_correctors(measure, 1, 32);
+	std::vector<uint32_t> A(measure.g_top);
+	Arena ar{nullptr, 0, 0, A.data(), 0, (uint32_t)A.size(), false};
+	ic.setup(32, 2);
+	ic.alloc_classes(ar);
+	ic.alloc_correctors(ar, 1, 32);
+	ic.init();
 	Decoder d;
 	d.start(file + table + 8, file + size);
 	std::vector<uint32_t> totals(n + 1, 0), sizes(n + 1, 0);
 	for (uint32_t i = 1; i <= n; i++) {
-		if (variable) totals[i] = (uint32_t)ic.decode(d, A.data(), (int32_t)(i > 1 ? totals[i - 1] : 0), 0);
-		sizes[i] = (uint32_t)ic.decode(d, A.data(), (int32_t)(i > 1 ? sizes[i - 1] : 0), 1);
+		if (variable) totals[i] = (uint32_t)ic.decode(d, (int32_t)(i > 1 ? totals[i - 1] : 0), 0);
+		sizes[i] = (uint32_t)ic.decode(d, (int32_t)(i > 1 ? sizes[i - 1] : 0), 1);
 	}
 	if (d.bad) { err = "malformed LAZ chunk table"; return false; }
 	uint64_t start = chunks_start;
