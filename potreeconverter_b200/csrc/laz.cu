@@ -15,16 +15,22 @@ namespace pcg {
 
 namespace {
 
-// models go to the block's shared memory first (fast_words of it), then to
-// the chunk's slice of the global arena
+// words of shared memory the decoder state takes (16-byte multiple)
+constexpr uint32_t kStateWords = (uint32_t)((sizeof(laz::ChunkState) + 15) / 16 * 4);
+
+// models go to the block's shared memory first (fast_words of it, after the
+// decoder state), then to the chunk's slice of the global arena
 __global__ void __launch_bounds__(32) laz_decode_kernel(const uint8_t* __restrict__ bytes, uint64_t base, const laz::Chunk* __restrict__ chunks,
                                                         int c0, int n, laz::Layout L, uint32_t fast_words, uint32_t* __restrict__ arena,
                                                         uint32_t words, uint8_t* __restrict__ out, int* __restrict__ bad) {
-	extern __shared__ uint32_t fast[];
+	// the decoder's state first, then its fast model region
+	extern __shared__ __align__(16) uint32_t smem[];
 	if (threadIdx.x != 0 || (int)blockIdx.x >= n) return;
+	laz::ChunkState& S = *reinterpret_cast<laz::ChunkState*>(smem);
+	uint32_t* fast = smem + kStateWords;
 	const int c = c0 + (int)blockIdx.x;
 	const laz::Chunk ch = chunks[c];
-	const bool ok = laz::decode_chunk(bytes + (ch.start - base), bytes + (ch.end - base), ch.count, L, fast_words ? fast : nullptr, fast_words,
+	const bool ok = laz::decode_chunk(bytes + (ch.start - base), bytes + (ch.end - base), ch.count, L, S, fast_words ? fast : nullptr, fast_words,
 	                                  arena + (size_t)blockIdx.x * words, words, out + ch.first * (int64_t)L.rec_len);
 	if (!ok) atomicCAS(bad, 0, c + 1);
 }
@@ -54,13 +60,16 @@ void launch_laz_decode(const uint8_t* d_bytes, uint64_t base, const std::vector<
 	PCG_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
 	PCG_CUDA(cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
 	const int blocks_per_sm = std::max(1, (wave + sms - 1) / sms);
-	size_t fast_bytes = std::min<size_t>((size_t)per_block, (size_t)per_sm / blocks_per_sm);
-	fast_bytes = fast_bytes > 2048 ? ((fast_bytes - 1024) & ~size_t(15)) : 0;
-	if (fast_bytes > 48 * 1024) PCG_CUDA(cudaFuncSetAttribute(laz_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fast_bytes));
+	size_t smem_bytes = std::min<size_t>((size_t)per_block, (size_t)per_sm / blocks_per_sm);
+	smem_bytes = smem_bytes > 1024 ? ((smem_bytes - 1024) & ~size_t(15)) : 0;
+	const size_t state_bytes = (size_t)kStateWords * 4;
+	if (smem_bytes < state_bytes) smem_bytes = state_bytes;
+	const uint32_t fast_words = (uint32_t)((smem_bytes - state_bytes) / 4);
+	if (smem_bytes > 48 * 1024) PCG_CUDA(cudaFuncSetAttribute(laz_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes));
 	for (int c0 = 0; c0 < (int)chunks.size(); c0 += wave) {
 		const int n = std::min<int>(wave, (int)chunks.size() - c0);
-		laz_decode_kernel<<<(unsigned)n, 32, fast_bytes, mem.stream()>>>(d_bytes, base, d_chunks, c0, n, L, (uint32_t)(fast_bytes / 4), arena,
-		                                                                  words, d_out, d_bad);
+		laz_decode_kernel<<<(unsigned)n, 32, smem_bytes, mem.stream()>>>(d_bytes, base, d_chunks, c0, n, L, fast_words, arena, words, d_out,
+		                                                                  d_bad);
 		PCG_LAUNCHED();
 	}
 	int bad = 0;

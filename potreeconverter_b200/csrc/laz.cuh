@@ -309,7 +309,9 @@ struct IntCoder {
 	uint32_t contexts, mbits_words;
 	uint32_t* mbits;    // `contexts` class models, back to back
 	uint32_t* corr0;    // bit model for k = 0
-	uint32_t* corr[33]; // symbol model per k = 1..corr_bits
+	uint32_t* corr[33]; // symbol model per k = 1..corr_bits; for k > bits_high
+	                    // created when the class first occurs
+	Arena* arena;       // where those come from
 	uint32_t k;         // class of the last value
 
 	LAZ_HD void setup(uint32_t bits, uint32_t nctx, uint32_t high = 8) {
@@ -327,9 +329,11 @@ struct IntCoder {
 		mbits_words = model_words(corr_bits + 1);
 		mbits = corr0 = nullptr;
 		for (int i = 0; i < 33; i++) corr[i] = nullptr;
+		arena = nullptr;
 		k = 0;
 	}
 	LAZ_HD void alloc_classes(Arena& ar) {
+		arena = &ar;
 		mbits = ar.take(contexts * mbits_words);
 		if (mbits)
 			for (uint32_t i = 0; i < contexts; i++) model_header(mbits + i * mbits_words, corr_bits + 1);
@@ -341,8 +345,24 @@ struct IntCoder {
 	LAZ_HD void init() {
 		for (uint32_t i = 0; i < contexts; i++) model_init(mbits + i * mbits_words);
 		bit_init(corr0);
-		for (uint32_t i = 1; i <= corr_bits; i++) model_init(corr[i]);
+		for (uint32_t i = 1; i <= corr_bits; i++)
+			if (corr[i]) model_init(corr[i]);
 		k = 0;
+	}
+	// the corrector model of class kk, created (fresh, as the reference's
+	// model initialised at the chunk start) when kk first occurs
+	LAZ_HD uint32_t* corr_model(Decoder& d, uint32_t kk) {
+		uint32_t* m = corr[kk];
+		if (!m) {
+			m = model_new(*arena, 1u << bits_high);
+			if (!m) {
+				d.bad = true;
+				return mbits;
+			}
+			model_init(m);
+			corr[kk] = m;
+		}
+		return m;
 	}
 	LAZ_HD int32_t corrector(Decoder& d, uint32_t ctx) {
 		if (ctx >= contexts) {
@@ -357,7 +377,7 @@ struct IntCoder {
 					c = d.symbol(corr[k]);
 				} else {
 					const uint32_t k1 = k - bits_high;
-					c = d.symbol(corr[k]);
+					c = d.symbol(corr_model(d, k));
 					const uint32_t c1 = d.raw_bits(k1);
 					c = (c << k1) | c1;
 				}
@@ -456,12 +476,13 @@ struct Layout {
 	int has_gps, has_rgb, n_extra, rec_len;
 };
 
-// The models of one chunk decoder (identical for all chunks of a source),
-// placed in order of use so that the fast region holds the ones every point
-// needs: the classes of every integer coder, the per-point symbol models,
-// the correctors of classes up to 16, then the rest. The three 256-context
-// tables of POINT10 (bit byte, classification, user data) create their
-// models when a context first occurs.
+// The models of one chunk decoder, placed so that the fast region holds
+// what the data uses: first the models every point needs (the classes of
+// every integer coder, the per-point symbol models, correctors of classes
+// up to 8), then, in order of first use, the 256-symbol correctors of larger
+// classes and the models of the three 256-context tables of POINT10 (bit
+// byte, classification, user data). A model created at first use starts as
+// the reference's model initialised at the chunk start.
 struct Models {
 	uint32_t* changed;
 	uint32_t* scan_angle[2];
@@ -498,18 +519,32 @@ struct Models {
 			for (int i = 0; i < 6; i++) rgb_diff[i] = model_new(ar, 256);
 		}
 		for (int i = 0; i < L.n_extra && i < kMaxExtraBytes; i++) byte_model[i] = model_new(ar, 256);
-		ic_dx.alloc_correctors(ar, 1, 16);
-		ic_dy.alloc_correctors(ar, 1, 16);
-		ic_z.alloc_correctors(ar, 1, 16);
-		ic_intensity.alloc_correctors(ar, 1, 16);
-		ic_psid.alloc_correctors(ar, 1, 16);
-		if (L.has_gps) ic_gps.alloc_correctors(ar, 1, 16);
-		ic_dx.alloc_correctors(ar, 17, 32);
-		ic_dy.alloc_correctors(ar, 17, 32);
-		ic_z.alloc_correctors(ar, 17, 32);
-		if (L.has_gps) ic_gps.alloc_correctors(ar, 17, 32);
+		// correctors of classes up to 8 now; the larger ones (256 symbols
+		// each) when their class first occurs, so the fast region holds what
+		// the data uses (a measuring arena counts them all)
+		const uint32_t upto = ar.measuring() ? 32 : 8;
+		ic_dx.alloc_correctors(ar, 1, upto);
+		ic_dy.alloc_correctors(ar, 1, upto);
+		ic_z.alloc_correctors(ar, 1, upto);
+		ic_intensity.alloc_correctors(ar, 1, upto);
+		ic_psid.alloc_correctors(ar, 1, upto);
+		if (L.has_gps) ic_gps.alloc_correctors(ar, 1, upto);
 		lazy = ar.take_global(3 * 256);
 	}
+};
+
+// Everything a chunk decoder indexes at run time besides the models: the
+// arena, the model handles and the predictor state. The device keeps it in
+// the block's shared memory, the host on its stack.
+struct ChunkState {
+	Arena ar;
+	Models M;
+	Median5 mx[16], my[16];
+	uint16_t last_intensity[16];
+	int32_t last_height[8];
+	int64_t gps[4];
+	int32_t gps_diff[4], gps_extreme[4];
+	uint8_t last_extra[kMaxExtraBytes];
 };
 
 // Global words one chunk decoder may need with no fast region: the models
@@ -527,15 +562,16 @@ inline uint32_t arena_words(const Layout& L) {
 // region (glob, g_words >= arena_words(L)). Returns false on malformed
 // input. Follows LASreadPoint::read (lasreadpoint.cpp:405-497): the first
 // point is stored raw, the arithmetic decoder starts after it.
-LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, const Layout& L, uint32_t* fast, uint32_t f_words,
-                         uint32_t* glob, uint32_t g_words, uint8_t* out) {
+LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, const Layout& L, ChunkState& S, uint32_t* fast,
+                         uint32_t f_words, uint32_t* glob, uint32_t g_words, uint8_t* out) {
 	if (count <= 0) return true;
 	const int rl = L.rec_len;
 	const int std_len = 20 + (L.has_gps ? 8 : 0) + (L.has_rgb ? 6 : 0);
 	if (L.n_extra < 0 || L.n_extra > kMaxExtraBytes || std_len + L.n_extra != rl) return false;
 	if (end - p < rl) return false;
-	Arena ar{fast, 0, fast ? f_words : 0u, glob, 0, g_words, false};
-	Models M;
+	S.ar = Arena{fast, 0, fast ? f_words : 0u, glob, 0, g_words, false};
+	Arena& ar = S.ar;
+	Models& M = S.M;
 	M.create(ar, L);
 	if (ar.overflow) return false;
 	// first point: raw item bytes, which initialise the item predictors
@@ -545,9 +581,10 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 	uint8_t last[20];
 	for (int b = 0; b < 20; b++) last[b] = out[b];
 	last[12] = last[13] = 0;
-	Median5 mx[16], my[16];
-	uint16_t last_intensity[16];
-	int32_t last_height[8];
+	Median5* mx = S.mx;
+	Median5* my = S.my;
+	uint16_t* last_intensity = S.last_intensity;
+	int32_t* last_height = S.last_height;
 	for (int i = 0; i < 16; i++) {
 		mx[i].init();
 		my[i].init();
@@ -565,9 +602,10 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 	uint32_t* lazy = M.lazy;
 	for (int i = 0; i < 3 * 256; i++) lazy[i] = 0;
 	// GPSTIME11 state
-	int64_t gps[4] = {0, 0, 0, 0};
-	int32_t gps_diff[4] = {0, 0, 0, 0};
-	int32_t gps_extreme[4] = {0, 0, 0, 0};
+	int64_t* gps = S.gps;
+	int32_t* gps_diff = S.gps_diff;
+	int32_t* gps_extreme = S.gps_extreme;
+	for (int i = 0; i < 4; i++) gps[i] = gps_diff[i] = gps_extreme[i] = 0;
 	uint32_t gps_last = 0, gps_next = 0;
 	if (L.has_gps) {
 		model_init(M.gps_multi);
@@ -584,7 +622,7 @@ LAZ_HD bool decode_chunk(const uint8_t* p, const uint8_t* end, int64_t count, co
 		for (int i = 0; i < 3; i++) last_rgb[i] = rd<uint16_t>(out + rgb_off + 2 * i);
 	}
 	// BYTE state
-	uint8_t last_extra[kMaxExtraBytes];
+	uint8_t* last_extra = S.last_extra;
 	for (int i = 0; i < L.n_extra; i++) {
 		model_init(M.byte_model[i]);
 		last_extra[i] = out[std_len + i];

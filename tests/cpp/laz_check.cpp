@@ -42,7 +42,8 @@ int main(int argc, char** argv) {
 	std::vector<uint8_t> out(n * (uint64_t)rec_len);
 	for (size_t c = 0; c < chunks.size(); c++) {
 		const auto& ch = chunks[c];
-		if (!pcg::laz::decode_chunk(las.data() + ch.start, las.data() + ch.end, ch.count, L, nullptr, 0, arena.data(), words,
+		pcg::laz::ChunkState state;
+		if (!pcg::laz::decode_chunk(las.data() + ch.start, las.data() + ch.end, ch.count, L, state, nullptr, 0, arena.data(), words,
 		                            out.data() + ch.first * rec_len)) {
 			fprintf(stderr, "chunk %zu malformed\n", c);
 			return 1;
