@@ -186,54 +186,19 @@ LAZ_HD void bit_update(uint32_t* h) {
 
 // ---------------------------------------------------------------- decoder
 struct Decoder {
-	const uint8_t* p;     // next byte not yet in buf
+	const uint8_t* p;
 	const uint8_t* end;
-	uint64_t buf;         // up to 8 fetched bytes, next one lowest
-	uint32_t nbuf;
 	uint32_t value, length;
 	bool bad;
 
-	// the stream is fetched a word at a time: the aligned 8-byte word holding
-	// p when it lies wholly before `end` (buffers start 8-byte aligned), else
-	// the bytes up to `end` one by one
-	LAZ_HD void refill() {
-		if (p >= end) return;
-		const uint8_t* a = reinterpret_cast<const uint8_t*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(7));
-		const uint32_t off = (uint32_t)(p - a);
-		uint32_t n = 8 - off;
-		if ((uint64_t)(end - p) < n) n = (uint32_t)(end - p);
-		uint64_t v = 0;
-		if (a + 8 <= end) {
-#ifdef __CUDA_ARCH__
-			v = *reinterpret_cast<const uint64_t*>(a) >> (8 * off);
-#else
-			for (uint32_t i = 0; i < n; i++) v |= (uint64_t)p[i] << (8 * i);
-#endif
-		} else {
-			for (uint32_t i = 0; i < n; i++) v |= (uint64_t)p[i] << (8 * i);
-		}
-		buf = v;
-		nbuf = n;
-		p += n;
-	}
 	LAZ_HD uint32_t next_byte() {
-		if (nbuf == 0) {
-			refill();
-			if (nbuf == 0) {
-				bad = true;  // the reference stops with an end-of-chunk error
-				return 0;
-			}
-		}
-		const uint32_t b = (uint32_t)(buf & 0xFF);
-		buf >>= 8;
-		--nbuf;
-		return b;
+		if (p < end) return *p++;
+		bad = true;  // the reference stops with an end-of-chunk error
+		return 0;
 	}
 	LAZ_HD void start(const uint8_t* from, const uint8_t* to) {
 		p = from;
 		end = to;
-		buf = 0;
-		nbuf = 0;
 		bad = false;
 		length = 0xFFFFFFFFu;
 		value = next_byte() << 24;
