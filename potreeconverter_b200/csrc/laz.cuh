@@ -884,7 +884,8 @@ inline bool parse_table(const uint8_t* file, uint64_t size, uint64_t offset_to_p
 	if (table < (int64_t)chunks_start || (uint64_t)table + 8 > size) { err = "LAZ file without a chunk table"; return false; }
 	if (u32(file + table) != 0) { err = "unsupported LAZ chunk table version"; return false; }
 	const uint32_t n = u32(file + table + 4);
-	if (n == 0 || n > (1u << 26)) { err = "LAZ chunk table without chunks"; return false; }
+	// every chunk holds at least one point
+	if (n == 0 || (int64_t)n > num_points) { err = "malformed LAZ chunk table"; return false; }
 	// entries: IntCoder(32 bits, 2 contexts) over the previous entry
 	const bool variable = chunk_size == 0xFFFFFFFFu;
 	IntCoder ic;

@@ -59,7 +59,9 @@ bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& er
 	info.max.z = get<double>(las + 211); info.min.z = get<double>(las + 219);
 	uint64_t ext = 0;
 	if (info.version_minor >= 4 && header_size >= 375 && size >= 255) ext = get<uint64_t>(las + 247);
-	info.num_points = (int64_t)(ext > legacy ? ext : legacy);  // LasLoader.cpp:103
+	const uint64_t count = ext > legacy ? ext : legacy;  // LasLoader.cpp:103
+	if (count > (uint64_t(1) << 40)) { err = "implausible point count in the LAS header"; return false; }
+	info.num_points = (int64_t)count;
 	uint64_t pos = header_size;
 	const uint8_t* laszip_vlr = nullptr;
 	uint32_t laszip_len = 0;
@@ -83,7 +85,10 @@ bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& er
 		return laz::parse_table(las, size, info.offset_to_points, info.num_points, info.pdrf, info.record_length, laszip_vlr, laszip_len,
 		                        info.laz_layout, info.laz_chunks, err);
 	}
-	if (!points_elsewhere && info.offset_to_points + (uint64_t)info.num_points * (uint64_t)info.record_length > size) {
+	// offset + count x record length <= size, without overflow
+	if (!points_elsewhere && info.num_points > 0 &&
+	    (info.offset_to_points > size || info.record_length == 0 ||
+	     (uint64_t)info.num_points > (size - info.offset_to_points) / (uint64_t)info.record_length)) {
 		err = "truncated point data";
 		return false;
 	}
