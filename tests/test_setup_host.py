@@ -106,3 +106,27 @@ def test_undefined_lists_are_refused(setup_check, tmp_path):
     for attrs, msg in ((["amplitude"], "past the point record"), (["rgb", "rgb"], "twice"), (["position"], "twice")):
         got = _run(setup_check, tmp_path, t, attrs)
         assert msg in got.get("error", ""), attrs
+
+
+def test_malformed_headers_are_refused(setup_check, tmp_path):
+    # counts that overflow the size arithmetic, truncated records, and a LAZ
+    # chunk table that claims more chunks than points are errors, not crashes
+    import struct
+    from potreeconverter_b200 import synth
+    las = bytearray(synth.generate("hotspots", 5_000, 2))  # LAS 1.4: 64-bit point count at 247
+    cases = []
+    big = bytearray(las)
+    struct.pack_into("<Q", big, 247, (1 << 63) + 5)
+    cases.append((bytes(big), "implausible point count"))
+    wrap = bytearray(las)
+    struct.pack_into("<Q", wrap, 247, (1 << 64) // struct.unpack_from("<H", las, 105)[0] + 1)
+    cases.append((bytes(wrap), "point count"))
+    cases.append((bytes(las[: len(las) - 100]), "truncated point data"))
+    if have_laz_tool():
+        laz = bytearray(to_laz(bytes(las), 1000))
+        table = struct.unpack_from("<q", laz, struct.unpack_from("<I", laz, 96)[0])[0]
+        struct.pack_into("<I", laz, table + 4, 10_000)  # 10,000 chunks for 5,000 points
+        cases.append((bytes(laz), "chunk table"))
+    for img, msg in cases:
+        got = _run(setup_check, tmp_path, [img])
+        assert msg in got.get("error", ""), (msg, got)
