@@ -43,3 +43,31 @@ def test_missing_library_fails_loudly(tmp_path):
             pc.load_library(str(tmp_path / "missing.so"))
     finally:
         pc._lib = saved
+
+
+def test_binding_structs_match_the_header(tmp_path):
+    # every field of the ctypes mirrors sits at the offset the C compiler
+    # gives it in include/pcgpu.h, and the structs have the same size
+    import ctypes
+    import subprocess
+    structs = {"pcg_opts": pc._Opts, "pcg_source": pc._Source, "pcg_job": pc._Job, "pcg_stats": pc._Stats,
+               "pcg_result": pc._Result}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pcgpu.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I" + os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    seen = 0
+    for line in filter(None, out):
+        cname, what, value = line.split()
+        py = structs[cname]
+        got = ctypes.sizeof(py) if what == "size" else getattr(py, what).offset
+        assert got == int(value), (cname, what)
+        seen += 1
+    assert seen == sum(len(p._fields_) + 1 for p in structs.values())
