@@ -133,12 +133,25 @@ typedef struct pcg_stats {
 	int64_t laz_chunks;           /* LASzip chunks decoded                  */
 } pcg_stats;
 
+/* One completed node: what the reference's hierarchy flusher records for it
+   (indexer.h:146-162, Writer::writeAndUnload indexer.cpp:1453-1516). */
+typedef struct pcg_node {
+	const char* name;      /* "r" + child digits, NUL terminated (owned by the result) */
+	int64_t num_points;
+	uint64_t byte_offset;  /* of its payload in octree.bin; 0 without points */
+	uint64_t byte_size;
+} pcg_node;
+
 typedef struct pcg_result {
 	uint8_t* octree;       uint64_t octree_size;     /* host memory unless the
 	                                                    job asked for device */
 	uint8_t* hierarchy;    uint64_t hierarchy_size;
 	char* metadata;        uint64_t metadata_size;   /* NUL terminated */
 	pcg_stats stats;
+	pcg_node* nodes;       /* every node in completion order (the order of
+	                          the payloads in octree.bin); NULL if the host had
+	                          no memory for the list */
+	uint64_t num_nodes;
 } pcg_result;
 
 typedef struct pcg_ctx pcg_ctx;

@@ -66,10 +66,16 @@ class _Stats(ctypes.Structure):
                 ("cluster_nodes", ctypes.c_int64), ("ms_decode", ctypes.c_double), ("laz_chunks", ctypes.c_int64)]
 
 
+class _Node(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("num_points", ctypes.c_int64), ("byte_offset", ctypes.c_uint64),
+                ("byte_size", ctypes.c_uint64)]
+
+
 class _Result(ctypes.Structure):
     _fields_ = [("octree", ctypes.POINTER(ctypes.c_uint8)), ("octree_size", ctypes.c_uint64),
                 ("hierarchy", ctypes.POINTER(ctypes.c_uint8)), ("hierarchy_size", ctypes.c_uint64),
-                ("metadata", ctypes.c_char_p), ("metadata_size", ctypes.c_uint64), ("stats", _Stats)]
+                ("metadata", ctypes.c_char_p), ("metadata_size", ctypes.c_uint64), ("stats", _Stats),
+                ("nodes", ctypes.POINTER(_Node)), ("num_nodes", ctypes.c_uint64)]
 
 
 # every symbol include/pcgpu.h declares
@@ -111,11 +117,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 @dataclass
 class Conversion:
-    """The three PotreeConverter outputs plus run statistics."""
+    """The three PotreeConverter outputs plus run statistics and the nodes
+    in completion order as (name, byte offset, byte size, points)."""
     octree: bytes
     hierarchy: bytes
     metadata: str
     stats: dict
+    nodes: list
 
     def write(self, outdir: str) -> None:
         os.makedirs(outdir, exist_ok=True)
@@ -144,8 +152,10 @@ def _take(lib, res: _Result) -> Conversion:
     hierarchy = _copy_out(res.hierarchy, res.hierarchy_size)
     metadata = ctypes.string_at(res.metadata, res.metadata_size).decode() if res.metadata_size else ""
     stats = {name: getattr(res.stats, name) for name, _ in _Stats._fields_}
+    nodes = [(res.nodes[i].name.decode(), res.nodes[i].byte_offset, res.nodes[i].byte_size, res.nodes[i].num_points)
+             for i in range(res.num_nodes)] if res.nodes else []
     lib.pcg_result_free(ctypes.byref(res))
-    return Conversion(octree, hierarchy, metadata, stats)
+    return Conversion(octree, hierarchy, metadata, stats, nodes)
 
 
 class Context:

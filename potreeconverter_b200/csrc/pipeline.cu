@@ -215,6 +215,7 @@ struct JobResult {
 	uint64_t octree_size = 0;
 	bool octree_on_device = false;
 	pcg_stats stats{};
+	std::vector<HierRecord> nodes;  // completion order
 };
 
 // PCG_TRACE_LEVELS=1 prints one line per sampled octree level to stderr
@@ -628,6 +629,7 @@ struct Converter {
 		PCG_CUDA(cudaStreamSynchronize(stream));
 		res.stats.ms_d2h = ms_since(t_d2h);  // the copy, overlapped with the host writers
 		res.stats.num_nodes = (int64_t)recs.size();
+		res.nodes = std::move(recs);
 		res.stats.output_points = out_points;
 		res.stats.gpu_launches = g_launch_count;
 		res.stats.ms_total = ms_since(t0);
@@ -1115,6 +1117,22 @@ void move_result(pcg::JobResult& r, pcg_result* out, int device) {
 	out->metadata[r.metadata.size()] = 0;
 	out->metadata_size = r.metadata.size();
 	out->stats = r.stats;
+	// node list: the records, then their names, in one block
+	size_t chars = 0;
+	for (auto& n : r.nodes) chars += n.name.size() + 1;
+	char* block = (char*)malloc(sizeof(pcg_node) * r.nodes.size() + chars + 1);
+	if (block) {
+		pcg_node* nodes = reinterpret_cast<pcg_node*>(block);
+		char* name = block + sizeof(pcg_node) * r.nodes.size();
+		for (size_t i = 0; i < r.nodes.size(); i++) {
+			const auto& n = r.nodes[i];
+			memcpy(name, n.name.c_str(), n.name.size() + 1);
+			nodes[i] = pcg_node{name, n.num_points, (uint64_t)n.byte_offset, (uint64_t)n.byte_size};
+			name += n.name.size() + 1;
+		}
+		out->nodes = nodes;
+		out->num_nodes = r.nodes.size();
+	}
 }
 
 size_t estimate_footprint(size_t las_bytes) {
@@ -1286,6 +1304,7 @@ void pcg_result_free(pcg_result* r) {
 	pcg::release_octree(r->octree);
 	free(r->hierarchy);
 	free(r->metadata);
+	free(r->nodes);
 	memset(r, 0, sizeof(*r));
 }
 

@@ -51,7 +51,7 @@ def test_binding_structs_match_the_header(tmp_path):
     import ctypes
     import subprocess
     structs = {"pcg_opts": pc._Opts, "pcg_source": pc._Source, "pcg_job": pc._Job, "pcg_stats": pc._Stats,
-               "pcg_result": pc._Result}
+               "pcg_node": pc._Node, "pcg_result": pc._Result}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pcgpu.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')

@@ -81,3 +81,16 @@ def test_bad_input_is_rejected(gpu_ctx):
     with pytest.raises(pc.PcgError) as e:
         gpu_ctx.convert(b"not a las file at all" * 20)
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("method", ["poisson", "poisson_average", "random"])
+def test_node_records_match_oracle(gpu_ctx, oracle, method):
+    # pcg_result.nodes: every node in completion order with its payload's
+    # place in octree.bin, as the reference's hierarchy flusher records them
+    from potreeconverter_b200 import synth
+    las = synth.generate("terrain", 300_000, 21)
+    exp = oracle.convert(las, method, name="n")["nodes"]
+    conv = gpu_ctx.convert(las, method=method, name="n")
+    assert conv.nodes == exp
+    assert len(conv.nodes) == conv.stats["num_nodes"]
+    assert sum(n[2] for n in conv.nodes) == len(conv.octree)
