@@ -48,3 +48,20 @@ def test_oracle_matches_reference_on_random_jobs(oracle, tmp_path, seed):
     exp = oracle.convert_sources(srcs, method, name=f"t{order[0]}", attributes=attrs)
     for f in ("octree.bin", "hierarchy.bin", "metadata.json"):
         assert (out / f).read_bytes() == exp[f], (f, order, method, attrs)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_oracle_matches_reference_on_random_clouds(oracle, tmp_path, seed):
+    from potreeconverter_b200 import synth
+    rng = np.random.default_rng(700 + seed)
+    kind = ["terrain", "hotspots", "lattice", "strips", "duplicates", "cube"][seed % 6]
+    n = int(rng.integers(5_000, 80_000))
+    las = synth.generate(kind, n, 800 + seed)
+    method = ["poisson", "poisson_average", "random"][int(rng.integers(0, 3))]
+    path = tmp_path / "cloud.las"
+    path.write_bytes(las)
+    out = tmp_path / "out"
+    subprocess.run([REF, str(path), "-o", str(out), "-m", method], check=True, capture_output=True)
+    exp = oracle.convert(las, method, name="cloud")
+    for f in ("octree.bin", "hierarchy.bin", "metadata.json"):
+        assert (out / f).read_bytes() == exp[f], (f, kind, n, method)
