@@ -1135,9 +1135,31 @@ void move_result(pcg::JobResult& r, pcg_result* out, int device) {
 	}
 }
 
-size_t estimate_footprint(size_t las_bytes) {
+// Bytes of point records a source image stands for: its header's point
+// count x record length (a LAZ image is several times smaller than the
+// records it decodes to), at least the image size.
+size_t record_bytes(const void* image, size_t size) {
+	const uint8_t* h = static_cast<const uint8_t*>(image);
+	if (size < 227 || std::memcmp(h, "LASF", 4) != 0) return size;
+	uint16_t header_size, rec_len;
+	uint32_t legacy;
+	std::memcpy(&header_size, h + 94, 2);
+	std::memcpy(&rec_len, h + 105, 2);
+	std::memcpy(&legacy, h + 107, 4);
+	uint64_t count = legacy;
+	if (h[25] >= 4 && header_size >= 375 && size >= 255) {
+		uint64_t ext;
+		std::memcpy(&ext, h + 247, 8);
+		if (ext > count) count = ext;
+	}
+	if (count > (uint64_t(1) << 32)) return size;  // implausible; parsing will refuse it
+	const uint64_t bytes = count * rec_len;
+	return bytes > size ? (size_t)bytes : size;
+}
+
+size_t estimate_footprint(size_t record_bytes) {
 	// point records + positions/ids/keys per point, plus headroom
-	return las_bytes * 3 + (las_bytes / 20) * 64 + (size_t(64) << 20);
+	return record_bytes * 3 + (record_bytes / 20) * 64 + (size_t(64) << 20);
 }
 
 void worker_main(pcg_ctx* ctx, int wi) {
@@ -1374,7 +1396,9 @@ pcg_status pcg_submit(pcg_ctx* ctx, const pcg_job* job, uint64_t* job_id) {
 		j->name = job->name ? job->name : "";
 		j->projection = job->projection ? job->projection : "";
 		j->method = job->method;
-		j->footprint = estimate_footprint(total);
+		size_t records = 0;
+		for (auto& src : srcs) records += record_bytes(src.las, src.las_size);
+		j->footprint = estimate_footprint(records);
 		ctx->jobs[j->id] = j;
 		ctx->queue.push_back(j);
 		*job_id = j->id;
