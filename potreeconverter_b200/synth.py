@@ -425,3 +425,51 @@ def sources(kind: str, n: int, seed: int, **kw) -> list:
         t = tiles(n, seed, **kw)
         return [t[1], without_points(t[0]), t[3]]
     return [generate(kind, n, seed, **kw)]
+
+
+def exact(n: int, seed: int) -> bytes:
+    """Exact-arithmetic stress: scale 2^-8, a 256 x 256 x 16 slab whose cube
+    is 256 wide, so the root spacing is exactly 2 and every coordinate,
+    distance and spacing is exact in FP64. Random sites of the pitch-2
+    lattice (pairs exactly one spacing apart; every child-box plane is a
+    lattice plane), each with a seeded partner one quantization unit nearer
+    or farther along a random axis, or at the same position."""
+    rng = np.random.default_rng(seed)
+    sc = 2.0 ** -8
+    m = n // 2
+    ix = rng.integers(0, 129, m)
+    iy = rng.integers(0, 129, m)
+    iz = rng.integers(0, 9, m)
+    base = np.stack([ix * 512, iy * 512, iz * 512], 1).astype(np.int64)  # 2 world units = 512 quanta
+    axis = rng.integers(0, 3, m)
+    step = rng.choice([-1, 0, 1], m)
+    partner = base.copy()
+    partner[np.arange(m), axis] += step * 1
+    partner = np.clip(partner, 0, [65536, 65536, 4096])
+    pts = np.concatenate([base, partner, [[0, 0, 0], [65536, 65536, 0]]])[:max(n, 2)]
+    perm = rng.permutation(len(pts))
+    pts = pts[perm]
+    X, Y, Z = (pts[:, k].astype(np.int32) for k in range(3))
+    attrs = _common_attrs(rng, len(pts), Z.astype(np.float64) * sc)
+    return write_las(X, Y, Z, attrs, pdrf=2, version_minor=2, scale=(sc, sc, sc), offset=(0.0, 0.0, 0.0))
+
+
+def shell(n: int, seed: int, extent: float = 1000.0, radius: float = 0.45) -> bytes:
+    """Points on a sphere of radius `radius` x extent around the centre of
+    an `extent` cube (two corner points fix the cube): the candidates of the
+    upper nodes lie at almost the same distance from the node centre, so the
+    poisson sampler's early exit rarely fires and its scans reach the
+    10,001-check cap (30,921 candidates do at 400,000 points, seed 3)."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(0, 1, (n - 2, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    c = extent / 2.0
+    pts = np.concatenate([c + v * radius * extent, [[0, 0, 0], [extent, extent, extent]]])
+    pts = pts[rng.permutation(n)]
+    X, Y, Z = _quantize(pts[:, 0]), _quantize(pts[:, 1]), _quantize(pts[:, 2])
+    attrs = _common_attrs(rng, n, pts[:, 2])
+    return write_las(X, Y, Z, attrs, pdrf=2, version_minor=2)
+
+
+GENERATORS["exact"] = exact
+GENERATORS["shell"] = shell

@@ -33,6 +33,8 @@ CASES = [
     ("duplicates_300k", "duplicates", 300_000, 7, {}, ["poisson", "poisson_average", "random"]),
     ("terrain_3000", "terrain", 3_000, 4, {}, ["poisson", "poisson_average", "random"]),
     ("terrain_50", "terrain", 50, 3, {}, ["poisson", "poisson_average", "random"]),
+    ("exact_200k", "exact", 200_000, 3, {}, ["poisson", "poisson_average", "random"]),
+    ("shell_400k", "shell", 400_000, 3, {}, ["poisson", "poisson_average", "random"]),
 ]
 
 
