@@ -473,3 +473,33 @@ def shell(n: int, seed: int, extent: float = 1000.0, radius: float = 0.45) -> by
 
 GENERATORS["exact"] = exact
 GENERATORS["shell"] = shell
+
+
+def centres(n: int, seed: int, extent: float = 1024.0, levels: int = 6) -> bytes:
+    """Small balls at node centres: a uniform background plus, for levels
+    0 .. levels-1, clusters of points within half a node spacing
+    (extent / 128 / 2^level) of the centres of that level's nodes. Their
+    candidates lie within one spacing of their node's centre, where the
+    poisson sampler's early-exit bound (distance - spacing)^2 accepts them
+    past conflicting points (sampler_poisson.h:127-180)."""
+    rng = np.random.default_rng(seed)
+    pts = [rng.uniform(0, extent, (n // 2, 3))]
+    per_level = (n - n // 2) // levels
+    for lvl in range(levels):
+        cells = 2 ** lvl
+        s = extent / 128.0 / cells
+        idx = rng.integers(0, cells, (per_level, 3))
+        centre = (idx + 0.5) * (extent / cells)
+        d = rng.normal(0, 1, (per_level, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        r = rng.uniform(0, 0.5 * s, (per_level, 1))
+        pts.append(centre + d * r)
+    pts.append(np.array([[0.0, 0.0, 0.0], [extent, extent, extent]]))
+    pts = np.concatenate(pts)
+    pts = pts[rng.permutation(len(pts))]
+    X, Y, Z = _quantize(pts[:, 0]), _quantize(pts[:, 1]), _quantize(pts[:, 2])
+    attrs = _common_attrs(rng, len(pts), pts[:, 2])
+    return write_las(X, Y, Z, attrs, pdrf=2, version_minor=2)
+
+
+GENERATORS["centres"] = centres

@@ -35,6 +35,7 @@ CASES = [
     ("terrain_50", "terrain", 50, 3, {}, ["poisson", "poisson_average", "random"]),
     ("exact_200k", "exact", 200_000, 3, {}, ["poisson", "poisson_average", "random"]),
     ("shell_400k", "shell", 400_000, 3, {}, ["poisson", "poisson_average", "random"]),
+    ("centres_300k", "centres", 300_000, 3, {}, ["poisson", "poisson_average", "random"]),
 ]
 
 
