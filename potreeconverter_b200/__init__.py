@@ -2,8 +2,10 @@
 
 The conversion runs as CUDA kernels for sm_100a inside ``libpcgpu.so``; this
 package is a thin ctypes layer over its C ABI (``include/pcgpu.h``), mirroring
-the reference's conversion entry (``PotreeConverter <in.las> -o <dir> -m
-poisson|poisson_average|random``, main.cpp:497-569) as :func:`convert`.
+the reference's conversion entry (``PotreeConverter <source> ... -o <dir> -m
+poisson|poisson_average|random [--attributes ...]``, main.cpp:497-569) as
+:func:`convert`: LAS or LAZ file images, one or several converted as one
+cloud (:func:`curate_sources` expands paths like the reference).
 
 There is no CPU fallback: importing works without a GPU, but every call that
 converts or launches a kernel raises if the CUDA library or a device is
@@ -229,7 +231,7 @@ class Context:
 
     def convert(self, las, method: str = "poisson", name: str = "cloud", projection: str = "",
                 attributes=None) -> Conversion:
-        """Converts one LAS file image (bytes, or (host pointer, size)), or a
+        """Converts one LAS or LAZ file image (bytes, or (host pointer, size)), or a
         list of images as one point cloud. attributes: the --attributes
         list (None keeps every attribute)."""
         keep = []

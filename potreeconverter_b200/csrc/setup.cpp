@@ -39,8 +39,9 @@ int attr_type_size(AttrType t) {  // Attributes.h:33-49
 
 template <class T> static T get(const uint8_t* p) { T v; std::memcpy(&v, p, sizeof(T)); return v; }
 
-// Header fields as LASzip reports them for an uncompressed file
-// (LasLoader.cpp:72-128).
+// Header fields as LASzip reports them (LasLoader.cpp:72-128); for a LAZ
+// file (point format with a compression bit) also the laszip record and
+// the chunk table.
 bool parse_las(const uint8_t* las, uint64_t size, LasInfo& info, std::string& err, bool points_elsewhere) {
 	if (size < 227 || std::memcmp(las, "LASF", 4) != 0) { err = "input is not a LAS file"; return false; }
 	info.version_minor = las[25];
