@@ -55,6 +55,16 @@ class _Job(ctypes.Structure):
 OCTREE_ON_DEVICE = 1
 
 
+@dataclass
+class Resident:
+    """A source whose point records are already in device memory: `header`
+    holds the file's header and VLRs (a LAS or LAZ image, points not
+    needed), `device_records` the device address of its decoded records
+    (point count x record length bytes)."""
+    header: bytes
+    device_records: int
+
+
 class _Stats(ctypes.Structure):
     _fields_ = [("num_points", ctypes.c_int64), ("num_chunks", ctypes.c_int64), ("num_nodes", ctypes.c_int64),
                 ("output_points", ctypes.c_int64), ("octree_depth", ctypes.c_int64),
@@ -214,7 +224,11 @@ class Context:
         pj = projection.encode()
         keep.extend([nm, pj])
         if isinstance(las, list):
-            srcs = (_Source * len(las))(*[_Source(*cls._image(img, keep), None) for img in las])
+            def source(img):
+                if isinstance(img, Resident):
+                    return _Source(*cls._image(img.header, keep), img.device_records)
+                return _Source(*cls._image(img, keep), None)
+            srcs = (_Source * len(las))(*[source(img) for img in las])
             keep.append(srcs)
             job = _Job(None, 0, METHODS[method], flags, nm, pj, None)
             job.num_sources = len(las)

@@ -152,3 +152,31 @@ def test_cli_converts_a_directory_of_tiles(tmp_path, oracle):
     exp = oracle.convert_sources(tiles, "poisson", name="tiles", attributes=["rgb", "gps-time", "intensity"])
     for f in FILES:
         assert (out / f).read_bytes() == exp[f], f
+
+
+def test_sources_with_records_on_the_device(gpu_ctx):
+    # pcg_source.device_records: headers on the host, decoded records already
+    # in device memory (a LAZ header too), mixed with host images
+    import struct
+    import torch
+    from potreeconverter_b200 import synth
+    from tests.oracle_lib import have_laz_tool, to_laz
+    tiles = synth.tiles(200_000, 51)
+    exp = gpu_ctx.convert(tiles, method="poisson", name="d")
+    keep, srcs = [], []
+    for k, img in enumerate(tiles):
+        if k == 1:
+            srcs.append(img)  # a host image among them
+            continue
+        off = struct.unpack_from("<I", img, 96)[0]
+        rec = torch.frombuffer(bytearray(img[off:]), dtype=torch.uint8).cuda()
+        keep.append(rec)
+        header = img[:off]
+        if k == 2 and have_laz_tool():
+            laz = to_laz(img)
+            header = laz[:struct.unpack_from("<I", laz, 96)[0]]
+        srcs.append(pc.Resident(header, rec.data_ptr()))
+    torch.cuda.synchronize()
+    got = gpu_ctx.convert(srcs, method="poisson", name="d")
+    for f in FILES:
+        assert _bytes(got, f) == _bytes(exp, f), f
