@@ -187,6 +187,15 @@ pcg_status pcg_kernel_sort_keys(pcg_ctx* ctx, const double* keys, int64_t n, int
  * leaves at position i (sampler_random.h:97-104). */
 pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* perm_out);
 
+/* The counting pass of one LAS or LAZ file image (countPointsInCells,
+   chunker_countsort_laszip.cpp:131-361, with the decode and quantization of
+   :749-803): every point's quantized X, Y, Z and count-grid cell
+   (ix + iy G + iz G^2; X, Y, Z, cell hold the point count), and the grid of
+   G^3 counts, G (128, 256 or 512 by point count, chunker :1214-1220)
+   returned in *grid_size. Points outside the header box: PCG_OUT_OF_BOX. */
+pcg_status pcg_kernel_decode_count(pcg_ctx* ctx, const void* las, uint64_t size, int32_t* X, int32_t* Y, int32_t* Z, uint32_t* cell,
+                                   uint32_t* grid, int64_t grid_capacity, int32_t* grid_size);
+
 /* LASzip decode of every point of a LAZ file image (point formats 0-3,
    LASzip's chunked point-wise coding: lasreadpoint.cpp:405-497 with the v2
    item readers of lasreaditemcompressed_v2.cpp) into records_out

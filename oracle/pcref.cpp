@@ -1373,6 +1373,46 @@ bool convert(const uint8_t* las, size_t size, const string& method, const string
 	return convert(vector<SourceImage>{{las, size}}, {}, method, name, seed, res, err);
 }
 
+// The counting pass alone for one LAS image (countPointsInCells,
+// chunker_countsort_laszip.cpp:131-361): every point's quantized X, Y, Z and
+// count-grid cell, and the grid of counts. X/Y/Z/cell hold the point count,
+// grid gridSize^3 entries.
+bool decodeCount(const uint8_t* las, size_t size, int32_t* X, int32_t* Y, int32_t* Z, uint32_t* cell, vector<int64_t>& grid,
+                 int64_t& gridSize, string& err) {
+	Job job;
+	Source src;
+	src.las = las;
+	if (!parseHeader(las, size, src.header, job.err)) { err = job.err; return false; }
+	job.sources.push_back(std::move(src));
+	if (!setup(job)) { err = job.err; return false; }
+	const int64_t total = job.totalPoints;
+	gridSize = total < 100'000'000 ? 128 : (total < 500'000'000 ? 256 : 512);  // :1214-1220
+	grid.assign(gridSize * gridSize * gridSize, 0);
+	const Attributes& out = job.attributes;
+	const Vec3 posScale = out.posScale, posOffset = out.posOffset, min = job.min, max = job.max;
+	const double cubeSize = (max - min).max();
+	const Vec3 csize(cubeSize, cubeSize, cubeSize);
+	const double dG = double(gridSize);
+	int64_t k = 0;
+	for (auto& s : job.sources) for (int64_t i = 0; i < s.header.numPoints; i++, k++) {
+		PointCoord c = lasCoordinates(s, i);
+		X[k] = int32_t((c.x - posOffset.x) / posScale.x);
+		Y[k] = int32_t((c.y - posOffset.y) / posScale.y);
+		Z[k] = int32_t((c.z - posOffset.z) / posScale.z);
+		double ux = (double(X[k]) * posScale.x + posOffset.x - min.x) / csize.x;
+		double uy = (double(Y[k]) * posScale.y + posOffset.y - min.y) / csize.y;
+		double uz = (double(Z[k]) * posScale.z + posOffset.z - min.z) / csize.z;
+		if (!(ux >= 0.0 && uy >= 0.0 && uz >= 0.0 && ux <= 1.0 && uy <= 1.0 && uz <= 1.0)) { err = "point outside bounding box"; return false; }
+		int64_t ix = int64_t(std::min(dG * ux, dG - 1.0));
+		int64_t iy = int64_t(std::min(dG * uy, dG - 1.0));
+		int64_t iz = int64_t(std::min(dG * uz, dG - 1.0));
+		const int64_t index = ix + iy * gridSize + iz * gridSize * gridSize;
+		cell[k] = (uint32_t)index;
+		grid[index]++;
+	}
+	return true;
+}
+
 }  // namespace pcref
 
 // ----------------------------------------------------------------- C API
@@ -1437,6 +1477,20 @@ int pcref_convert_sources(const void* const* las, const uint64_t* sizes, int32_t
 		out->node_info[3 * i + 1] = res.nodes[i].byteSize;
 		out->node_info[3 * i + 2] = res.nodes[i].numPoints;
 	}
+	return 0;
+}
+
+// decodeCount: X/Y/Z/cell hold the point count, grid 512^3 at most (the
+// grid size used is returned); returns 0 or 1 with the message in err.
+int pcref_decode_count(const void* las, uint64_t size, int32_t* X, int32_t* Y, int32_t* Z, uint32_t* cell, int64_t* grid,
+                       int64_t grid_capacity, int64_t* grid_size, char* err) {
+	std::vector<int64_t> g;
+	std::string e;
+	int64_t gs = 0;
+	if (!pcref::decodeCount((const uint8_t*)las, size, X, Y, Z, cell, g, gs, e)) { snprintf(err, 256, "%s", e.c_str()); return 1; }
+	if ((int64_t)g.size() > grid_capacity) { snprintf(err, 256, "grid capacity too small"); return 1; }
+	memcpy(grid, g.data(), g.size() * sizeof(int64_t));
+	*grid_size = gs;
 	return 0;
 }
 

@@ -29,6 +29,11 @@ struct SourceImage {
 bool convert(const uint8_t* las, size_t size, const std::string& method, const std::string& name,
              uint32_t seed, Result& res, std::string& err);
 
+// The counting pass alone for one LAS image: quantized X, Y, Z and the
+// count-grid cell of every point, and the grid of counts (gridSize^3).
+bool decodeCount(const uint8_t* las, size_t size, int32_t* X, int32_t* Y, int32_t* Z, uint32_t* cell, std::vector<int64_t>& grid,
+                 int64_t& gridSize, std::string& err);
+
 // Converts several LAS file images as one point cloud (the reference's
 // source list, in order), keeping only the named attributes when
 // attributes is not empty (--attributes).

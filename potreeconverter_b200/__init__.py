@@ -93,7 +93,7 @@ class _Result(ctypes.Structure):
 # every symbol include/pcgpu.h declares
 EXPORTS = ["pcg_create", "pcg_destroy", "pcg_last_error", "pcg_status_string", "pcg_convert", "pcg_result_free",
            "pcg_write_files", "pcg_submit", "pcg_poll", "pcg_wait", "pcg_kernel_sort_keys", "pcg_kernel_shuffle",
-           "pcg_kernel_sort_keys_noalloc", "pcg_kernel_laz_decode"]
+           "pcg_kernel_sort_keys_noalloc", "pcg_kernel_laz_decode", "pcg_kernel_decode_count"]
 
 _lib = None
 
@@ -123,6 +123,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pcg_kernel_shuffle.argtypes = [c.c_void_p, c.c_int64, c.c_uint32, c.c_void_p]
     lib.pcg_kernel_sort_keys_noalloc.argtypes = [c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p]
     lib.pcg_kernel_laz_decode.argtypes = [c.c_void_p, c.c_char_p, c.c_uint64, c.c_void_p, c.c_uint64]
+    lib.pcg_kernel_decode_count.argtypes = [c.c_void_p, c.c_char_p, c.c_uint64, c.c_void_p, c.c_void_p, c.c_void_p,
+                                            c.c_void_p, c.c_void_p, c.c_int64, c.POINTER(c.c_int32)]
     _lib = lib
     return lib
 
@@ -317,6 +319,26 @@ class Context:
         if st != 0:
             raise self._err(st)
         return perm
+
+    def decode_count(self, las: bytes):
+        """The counting pass on the device: (X, Y, Z, cell, grid) as numpy
+        arrays (the grid flattened, G^3 counts)."""
+        import struct
+        import numpy as np
+        hdr = struct.unpack_from("<H", las, 94)[0]
+        n = struct.unpack_from("<I", las, 107)[0]
+        if las[25] >= 4 and hdr >= 375:
+            n = max(n, struct.unpack_from("<Q", las, 247)[0])
+        g = 128 if n < 100_000_000 else (256 if n < 500_000_000 else 512)
+        X, Y, Z = (np.empty(max(n, 1), np.int32) for _ in range(3))
+        cell = np.empty(max(n, 1), np.uint32)
+        grid = np.empty(g ** 3, np.uint32)
+        gs = ctypes.c_int32()
+        st = self._lib.pcg_kernel_decode_count(self._h, ctypes.c_char_p(las), len(las), X.ctypes.data, Y.ctypes.data,
+                                               Z.ctypes.data, cell.ctypes.data, grid.ctypes.data, grid.size, ctypes.byref(gs))
+        if st != 0:
+            raise self._err(st)
+        return X[:n], Y[:n], Z[:n], cell[:n], grid[: gs.value ** 3]
 
     def laz_decode(self, laz: bytes) -> bytes:
         """Point records of a LAZ file image, decoded on the device."""

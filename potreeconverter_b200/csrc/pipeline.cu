@@ -1470,6 +1470,70 @@ pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* p
 	});
 }
 
+pcg_status pcg_kernel_decode_count(pcg_ctx* ctx, const void* las, uint64_t size, int32_t* X, int32_t* Y, int32_t* Z, uint32_t* cell,
+                                   uint32_t* grid, int64_t grid_capacity, int32_t* grid_size) {
+	if (!ctx || !las || !grid_size) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->mtx);
+	return guarded(ctx, [&] {
+		pcg::LasInfo info;
+		std::string err;
+		if (!pcg::parse_las(static_cast<const uint8_t*>(las), size, info, err)) throw pcg::PcgError(PCG_BAD_INPUT, err);
+		pcg::Setup s;
+		if (!pcg::make_setup(info, s, err)) throw pcg::PcgError(PCG_BAD_INPUT, err);
+		const int64_t N = s.total_points;
+		const int64_t G = s.grid_size, cells = G * G * G;
+		if (N >= (int64_t(1) << 31)) throw pcg::PcgError(PCG_BAD_INPUT, "more than 2^31 points");
+		if (!grid || grid_capacity < cells) throw pcg::PcgError(PCG_BAD_INPUT, "grid is smaller than grid_size^3");
+		if (N > 0 && (!X || !Y || !Z || !cell)) throw pcg::PcgError(PCG_BAD_INPUT, "NULL output");
+		*grid_size = (int32_t)G;
+		PCG_CUDA(cudaSetDevice(ctx->conv.device));
+		cudaStream_t stream = ctx->conv.stream;
+		pcg::DeviceMem mem(stream, ctx->conv.arena.get());
+		// the records on the device, as the conversion puts them there
+		uint8_t* d_recs = mem.alloc<uint8_t>(std::max<int64_t>(1, N * (int64_t)info.record_length));
+		if (info.compressed) {
+			const auto& chunks = info.laz_chunks;
+			if (!chunks.empty()) {
+				const uint64_t base = chunks.front().start, nbytes = chunks.back().end - base;
+				uint8_t* d_laz = mem.alloc<uint8_t>(nbytes);
+				PCG_CUDA(cudaMemcpyAsync(d_laz, static_cast<const uint8_t*>(las) + base, nbytes, cudaMemcpyHostToDevice, stream));
+				pcg::launch_laz_decode(d_laz, base, chunks, info.laz_layout, d_recs, mem);
+			}
+		} else if (N > 0) {
+			PCG_CUDA(cudaMemcpyAsync(d_recs, static_cast<const uint8_t*>(las) + info.offset_to_points, N * (int64_t)info.record_length,
+			                         cudaMemcpyHostToDevice, stream));
+		}
+		std::vector<pcg::SourceDesc> descs;
+		std::vector<int64_t> firsts;
+		pcg::DecodeParams p = pcg::Converter::decode_params(s, {d_recs}, descs, firsts);
+		uint32_t* d_grid = mem.alloc<uint32_t>(cells);
+		PCG_CUDA(cudaMemsetAsync(d_grid, 0, cells * sizeof(uint32_t), stream));
+		pcg::ChunkingOut co;
+		co.X = mem.alloc<int32_t>(std::max<int64_t>(1, N));
+		co.Y = mem.alloc<int32_t>(std::max<int64_t>(1, N));
+		co.Z = mem.alloc<int32_t>(std::max<int64_t>(1, N));
+		co.cell = mem.alloc<uint32_t>(std::max<int64_t>(1, N));
+		std::vector<pcg::AttrStatsDev> st_init(pcg::MAX_ATTRS);
+		for (auto& a : st_init) for (int c = 0; c < 3; c++) { a.mn[c] = ~0ull; a.mx[c] = 0ull; }
+		co.stats = pcg::upload(st_init, mem);
+		co.histogram = mem.alloc<unsigned long long>(256);
+		PCG_CUDA(cudaMemsetAsync(co.histogram, 0, 256 * 8, stream));
+		co.error = mem.alloc<int64_t>(2);
+		PCG_CUDA(cudaMemsetAsync(co.error, 0, 16, stream));
+		pcg::launch_decode_count(p, d_grid, co, mem);
+		const auto errs = pcg::download(co.error, 2, stream);
+		if (errs[0]) throw pcg::PcgError(PCG_OUT_OF_BOX, "point " + std::to_string(errs[0] - 1) + " lies outside the header bounding box");
+		if (N > 0) {
+			PCG_CUDA(cudaMemcpyAsync(X, co.X, N * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+			PCG_CUDA(cudaMemcpyAsync(Y, co.Y, N * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+			PCG_CUDA(cudaMemcpyAsync(Z, co.Z, N * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+			PCG_CUDA(cudaMemcpyAsync(cell, co.cell, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+		}
+		PCG_CUDA(cudaMemcpyAsync(grid, d_grid, cells * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+		PCG_CUDA(cudaStreamSynchronize(stream));
+	});
+}
+
 pcg_status pcg_kernel_laz_decode(pcg_ctx* ctx, const void* laz_file, uint64_t size, void* records_out, uint64_t out_size) {
 	if (!ctx || !laz_file) return PCG_BAD_INPUT;
 	std::lock_guard<std::mutex> lk(ctx->mtx);

@@ -45,6 +45,8 @@ class Oracle:
                                               ctypes.c_int32, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint32,
                                               ctypes.POINTER(_Out)]
         lib.pcref_free.argtypes = [ctypes.POINTER(_Out)]
+        lib.pcref_decode_count.argtypes = [ctypes.c_void_p, ctypes.c_uint64] + [ctypes.c_void_p] * 5 + [
+            ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_char_p]
         lib.pcref_std_sort_perm.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
         lib.pcref_std_shuffle.argtypes = [ctypes.c_int64, ctypes.c_uint32, ctypes.c_void_p]
         self.lib = lib
@@ -87,6 +89,25 @@ class Oracle:
         res["nodes"] = nodes  # completion order: (name, byte offset, byte size, points)
         self.lib.pcref_free(ctypes.byref(out))
         return res
+
+    def decode_count(self, las: bytes):
+        """The counting pass (countPointsInCells): X, Y, Z, cell, grid."""
+        import struct
+        hdr = struct.unpack_from("<H", las, 94)[0]
+        n = struct.unpack_from("<I", las, 107)[0]
+        if las[25] >= 4 and hdr >= 375:
+            n = max(n, struct.unpack_from("<Q", las, 247)[0])
+        buf = (ctypes.c_uint8 * len(las)).from_buffer_copy(las)
+        X, Y, Z = (np.empty(max(n, 1), np.int32) for _ in range(3))
+        cell = np.empty(max(n, 1), np.uint32)
+        grid = np.empty(512 ** 3 if n >= 100_000_000 else 128 ** 3, np.int64)
+        gs = ctypes.c_int64()
+        err = ctypes.create_string_buffer(256)
+        rc = self.lib.pcref_decode_count(ctypes.addressof(buf), len(las), X.ctypes.data, Y.ctypes.data, Z.ctypes.data,
+                                         cell.ctypes.data, grid.ctypes.data, grid.size, ctypes.byref(gs), err)
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        return X[:n], Y[:n], Z[:n], cell[:n], grid[: gs.value ** 3]
 
     def sort_perm(self, keys):
         k = np.ascontiguousarray(keys, dtype=np.float64)

@@ -56,3 +56,39 @@ def test_oracle_shuffle_is_a_permutation(oracle):
     for n in (0, 1, 2, 3, 10, 9999, 10000):
         p = oracle.shuffle(n)
         assert sorted(p.tolist()) == list(range(n))
+
+
+@pytest.mark.parametrize("kind,n,seed", [("terrain", 60_000, 3), ("hotspots", 50_000, 4), ("tiles", 40_000, 5)])
+def test_oracle_counting_pass_matches_numpy(oracle, kind, n, seed):
+    # the oracle's counting-pass hook against the same FP64 expressions in
+    # numpy (chunker_countsort_laszip.cpp:213-257): x = scale X + offset,
+    # X' = int32((x - offset') / scale'), cell = ix + iy G + iz G^2
+    import struct
+    import numpy as np
+    from potreeconverter_b200 import synth
+    las = synth.generate(kind, n, seed) if kind != "tiles" else synth.tiles(n, seed)[3]
+    X, Y, Z, cell, grid = oracle.decode_count(las)
+    off = struct.unpack_from("<I", las, 96)[0]
+    rl = struct.unpack_from("<H", las, 105)[0]
+    cnt = struct.unpack_from("<I", las, 107)[0]
+    raw = np.frombuffer(las, dtype=np.dtype({"names": ["X", "Y", "Z"], "formats": ["<i4"] * 3, "offsets": [0, 4, 8],
+                                             "itemsize": rl}), count=cnt, offset=off)
+    sc = struct.unpack_from("<3d", las, 131)
+    of = struct.unpack_from("<3d", las, 155)
+    mx = struct.unpack_from("<6d", las, 179)
+    hmin = np.array([mx[1], mx[3], mx[5]])
+    hmax = np.array([mx[0], mx[2], mx[4]])
+    size = hmax - hmin
+    pscale = np.maximum(np.array(sc), size / 2.0 ** 30)
+    cube = max(size)
+    g = 128
+    cells = np.zeros(cnt, np.int64)
+    for a, (name, q) in enumerate(zip("XYZ", (X, Y, Z))):
+        x = sc[a] * raw[name].astype(np.float64) + of[a]
+        qq = ((x - hmin[a]) / pscale[a]).astype(np.int32)
+        assert (qq == q).all(), name
+        u = (qq.astype(np.float64) * pscale[a] + hmin[a] - hmin[a]) / cube
+        i = np.minimum(g * u, g - 1.0).astype(np.int64)
+        cells += i * g ** a
+    assert (cells == cell).all()
+    assert (np.bincount(cells, minlength=g ** 3) == grid).all()
