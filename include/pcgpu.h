@@ -192,9 +192,12 @@ pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* p
    :749-803): every point's quantized X, Y, Z and count-grid cell
    (ix + iy G + iz G^2; X, Y, Z, cell hold the point count), and the grid of
    G^3 counts, G (128, 256 or 512 by point count, chunker :1214-1220)
-   returned in *grid_size. Points outside the header box: PCG_OUT_OF_BOX. */
+   returned in *grid_size. X, Y, Z and cell hold point_capacity elements; a
+   file with more points (by its header) is refused with PCG_BAD_INPUT
+   before anything is written. Points outside the header box:
+   PCG_OUT_OF_BOX. */
 pcg_status pcg_kernel_decode_count(pcg_ctx* ctx, const void* las, uint64_t size, int32_t* X, int32_t* Y, int32_t* Z, uint32_t* cell,
-                                   uint32_t* grid, int64_t grid_capacity, int32_t* grid_size);
+                                   int64_t point_capacity, uint32_t* grid, int64_t grid_capacity, int32_t* grid_size);
 
 /* LASzip decode of every point of a LAZ file image (point formats 0-3,
    LASzip's chunked point-wise coding: lasreadpoint.cpp:405-497 with the v2
@@ -206,17 +209,23 @@ pcg_status pcg_kernel_laz_decode(pcg_ctx* ctx, const void* laz_file, uint64_t si
 /* ---- the same sort for callers that cannot allocate ---------------------
  * No counterpart in the reference. pcg_kernel_sort_keys_noalloc is
  * pcg_kernel_sort_keys for code that must not allocate device memory, e.g. a
- * plugin whose host framework owns every device allocation, or code
- * enqueuing work while a stream is captured (cudaMalloc is not allowed
- * there). Keys (n doubles) and the output permutation (n int32) are device
- * buffers the caller provides; all scratch lives in a static device array of
- * 28 * PCG_NOALLOC_SORT_MAX + 256 bytes that every GPU loading the library
- * holds until the process exits. No cudaMalloc/cudaFree is called.
+ * plugin inside a host framework that owns every device allocation and
+ * hands its plugins only the buffers it made (a cudaMalloc of the plugin's
+ * own would bypass that framework's memory accounting and can fail once the
+ * framework has reserved the device). Keys (n doubles) and the output
+ * permutation (n int32) are device buffers the caller provides; all scratch
+ * lives in a static device array of 28 * PCG_NOALLOC_SORT_MAX + 256 bytes
+ * that every GPU loading the library holds until the process exits. No
+ * cudaMalloc/cudaFree is called.
  *  - n > PCG_NOALLOC_SORT_MAX returns PCG_BAD_INPUT and does nothing;
  *  - the first call on a device looks up the array's device address (set-up
- *    per device); make that first call before any stream capture;
+ *    per device); make that first call before any stream capture. The
+ *    address is kept for the life of the process: do not call this entry
+ *    point again on a device after cudaDeviceReset;
  *  - work runs on `stream` (a cudaStream_t, NULL = legacy default) and the
- *    call waits for it to finish;
+ *    call waits for it to finish (it reads back a small error word);
+ *  - a CUDA error left pending by earlier work is reported as PCG_CUDA
+ *    before anything is launched, and left pending for the caller;
  *  - all calls share the one array: calls that overlap on the GPU (other
  *    streams or host threads) race and must be serialized by the caller. */
 #define PCG_NOALLOC_SORT_MAX 262144

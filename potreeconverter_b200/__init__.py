@@ -124,7 +124,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pcg_kernel_sort_keys_noalloc.argtypes = [c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p]
     lib.pcg_kernel_laz_decode.argtypes = [c.c_void_p, c.c_char_p, c.c_uint64, c.c_void_p, c.c_uint64]
     lib.pcg_kernel_decode_count.argtypes = [c.c_void_p, c.c_char_p, c.c_uint64, c.c_void_p, c.c_void_p, c.c_void_p,
-                                            c.c_void_p, c.c_void_p, c.c_int64, c.POINTER(c.c_int32)]
+                                            c.c_void_p, c.c_int64, c.c_void_p, c.c_int64, c.POINTER(c.c_int32)]
     _lib = lib
     return lib
 
@@ -335,7 +335,8 @@ class Context:
         grid = np.empty(g ** 3, np.uint32)
         gs = ctypes.c_int32()
         st = self._lib.pcg_kernel_decode_count(self._h, ctypes.c_char_p(las), len(las), X.ctypes.data, Y.ctypes.data,
-                                               Z.ctypes.data, cell.ctypes.data, grid.ctypes.data, grid.size, ctypes.byref(gs))
+                                               Z.ctypes.data, cell.ctypes.data, X.size, grid.ctypes.data, grid.size,
+                                               ctypes.byref(gs))
         if st != 0:
             raise self._err(st)
         return X[:n], Y[:n], Z[:n], cell[:n], grid[: gs.value ** 3]

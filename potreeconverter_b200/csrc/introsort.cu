@@ -898,7 +898,9 @@ constexpr int kMaxDevices = 128;
 void* g_noalloc_base[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device, looked up once
-// per device (the array's name is only a host-side handle).
+// per device (the array's name is only a host-side handle). The address is
+// kept for the process's lifetime; a cudaDeviceReset would make it stale,
+// which the header tells callers.
 cudaError_t noalloc_scratch(int dev, void** out) {
 	std::lock_guard<std::mutex> lk(g_noalloc_mtx);
 	if (!g_noalloc_base[dev]) {
@@ -936,6 +938,9 @@ extern "C" pcg_status pcg_kernel_sort_keys_noalloc(const double* d_keys, int64_t
 		cudaGetLastError();
 		return PCG_CUDA;
 	}
+	// an error somebody else left pending is theirs: report it without
+	// consuming it, and launch nothing
+	if (cudaPeekAtLastError() != cudaSuccess) return PCG_CUDA;
 	void* base = nullptr;
 	if (noalloc_scratch(dev, &base) != cudaSuccess) {
 		cudaGetLastError();
@@ -954,13 +959,16 @@ extern "C" pcg_status pcg_kernel_sort_keys_noalloc(const double* d_keys, int64_t
 	// must start at zero, every other byte is written before it is read
 	if (cudaMemsetAsync(st, 0, sizeof(SampleStats), s) != cudaSuccess) { cudaGetLastError(); return PCG_CUDA; }
 	const unsigned blocks = (unsigned)ceil_div(n, 256);
+	// each launch is checked at once, so a failure is this call's own
 	noalloc_prepare_kernel<<<blocks, 256, 0, s>>>(d_keys, n, key, val);
+	if (cudaGetLastError() != cudaSuccess) return PCG_CUDA;
 	if (n >= kBigSortMin) sort_single_big_kernel<<<1, kBigThreads, 0, s>>>(key, val, n, sc, st);
 	else sort_single_kernel<<<1, 32, 0, s>>>(key, val, n, sc, st);
+	if (cudaGetLastError() != cudaSuccess) return PCG_CUDA;
 	noalloc_finish_kernel<<<blocks, 256, 0, s>>>(val, n, d_perm);
+	if (cudaGetLastError() != cudaSuccess) return PCG_CUDA;
 	SampleStats h{};
-	if (cudaGetLastError() != cudaSuccess || cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-	    cudaStreamSynchronize(s) != cudaSuccess) {
+	if (cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
 		cudaGetLastError();
 		return PCG_CUDA;
 	}

@@ -1471,7 +1471,7 @@ pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* p
 }
 
 pcg_status pcg_kernel_decode_count(pcg_ctx* ctx, const void* las, uint64_t size, int32_t* X, int32_t* Y, int32_t* Z, uint32_t* cell,
-                                   uint32_t* grid, int64_t grid_capacity, int32_t* grid_size) {
+                                   int64_t point_capacity, uint32_t* grid, int64_t grid_capacity, int32_t* grid_size) {
 	if (!ctx || !las || !grid_size) return PCG_BAD_INPUT;
 	std::lock_guard<std::mutex> lk(ctx->mtx);
 	return guarded(ctx, [&] {
@@ -1484,6 +1484,7 @@ pcg_status pcg_kernel_decode_count(pcg_ctx* ctx, const void* las, uint64_t size,
 		const int64_t G = s.grid_size, cells = G * G * G;
 		if (N >= (int64_t(1) << 31)) throw pcg::PcgError(PCG_BAD_INPUT, "more than 2^31 points");
 		if (!grid || grid_capacity < cells) throw pcg::PcgError(PCG_BAD_INPUT, "grid is smaller than grid_size^3");
+		if (N > point_capacity) throw pcg::PcgError(PCG_BAD_INPUT, "the file holds more points than the X/Y/Z/cell buffers");
 		if (N > 0 && (!X || !Y || !Z || !cell)) throw pcg::PcgError(PCG_BAD_INPUT, "NULL output");
 		*grid_size = (int32_t)G;
 		PCG_CUDA(cudaSetDevice(ctx->conv.device));

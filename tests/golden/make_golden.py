@@ -3,10 +3,13 @@ the determinism-pinned reference converter (oracle/_ref/PotreeConverter_pinned,
 built from the reference sources by oracle/Makefile) writes for seeded
 synthetic inputs. Run in a container that has the reference sources:
 
-    make -C oracle ref && python tests/golden/make_golden.py [--multi-only]
+    make -C oracle ref REF=<reference tree> && python tests/golden/make_golden.py [--multi-only | --large-only]
 
 --multi-only keeps the single-source cases of the existing file and
-regenerates the multi-source / --attributes cases.
+regenerates the multi-source / --attributes cases. --large-only keeps every
+other case and regenerates `large_cases`: the full-size workloads (the
+benchmarked 50M hot-spot cloud, the 100M precision lattice, a scaled strip
+cloud), whose pinned runs take tens of minutes each and run in parallel.
 """
 
 import hashlib
@@ -15,6 +18,7 @@ import os
 import subprocess
 import sys
 import tempfile
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
@@ -37,6 +41,21 @@ CASES = [
     ("shell_400k", "shell", 400_000, 3, {}, ["poisson", "poisson_average", "random"]),
     ("centres_300k", "centres", 300_000, 3, {}, ["poisson", "poisson_average", "random"]),
 ]
+
+
+# Full-size workloads: (case name, generator, points, seed, generator kwargs,
+# samplers). hotspots_50m is the benchmarked cloud (50M points, LAS 1.4 point
+# format 3 + float extra, 20 hot-spots, seed 1001); lattice_100m the
+# precision-stress lattice (100M points, pitch = level-3 spacing, +-1-3
+# quantization units of jitter, seed 1002); strips_20m a scaled instance of
+# the aerial-strip cloud (seed 1003).
+LARGE_CASES = [
+    ("hotspots_10m", "hotspots", 10_000_000, 1001, {}, ["poisson", "poisson_average", "random"]),
+    ("hotspots_50m", "hotspots", 50_000_000, 1001, {}, ["poisson", "poisson_average", "random"]),
+    ("lattice_100m", "lattice", 100_000_000, 1002, {}, ["poisson"]),
+    ("strips_20m", "strips", 20_000_000, 1003, {}, ["poisson", "poisson_average", "random"]),
+]
+LARGE_JOBS = 4  # pinned reference runs at a time (each is single-threaded)
 
 
 # Inputs of several sources and --attributes lists:
@@ -132,14 +151,54 @@ def run_multi(tmp):
     return cases
 
 
+def run_large(tmp):
+    """Digests of the full-size workloads; the inputs are written one at a
+    time, the reference runs LARGE_JOBS at a time."""
+    cases, jobs = [], []
+    for name, kind, n, seed, kw, methods in LARGE_CASES:
+        las = synth.generate(kind, n, seed, **kw)
+        path_las = os.path.join(tmp, name + ".las")
+        with open(path_las, "wb") as f:
+            f.write(las)
+        entry = {"name": name, "kind": kind, "points": n, "seed": seed, "kwargs": kw,
+                 "las_md5": hashlib.md5(las).hexdigest(), "outputs": {}}
+        del las
+        cases.append(entry)
+        jobs += [(entry, path_las, m) for m in methods]
+
+    def one(job):
+        entry, path_las, m = job
+        od = os.path.join(tmp, f"{entry['name']}_{m}")
+        subprocess.run([REF, path_las, "-o", od, "-m", m], check=True, capture_output=True)
+        out = {f: {"md5": md5(os.path.join(od, f)), "size": os.path.getsize(os.path.join(od, f))}
+               for f in ("octree.bin", "hierarchy.bin", "metadata.json")}
+        subprocess.run(["rm", "-rf", od], check=True)
+        print(entry["name"], m, out["octree.bin"]["size"], flush=True)
+        return entry, m, out
+
+    with ThreadPoolExecutor(LARGE_JOBS) as pool:
+        for entry, m, out in pool.map(one, jobs):
+            entry["outputs"][m] = out
+    return cases
+
+
 def main():
     multi_only = "--multi-only" in sys.argv
+    large_only = "--large-only" in sys.argv
     path = os.path.join(HERE, "golden.json")
     out = {"generator": "potreeconverter_b200.synth", "reference": "PotreeConverter 2.0, pinned (oracle/pin/pin.h)",
            "random_seed": 1592614637, "cases": []}
     if multi_only:  # keep the single-source cases of the existing file
         with open(path) as f:
             out["cases"] = json.load(f)["cases"]
+    if large_only:  # keep everything but the full-size cases
+        with open(path) as f:
+            out = json.load(f)
+        with tempfile.TemporaryDirectory(dir=os.environ.get("GOLDEN_TMP")) as tmp:
+            out["large_cases"] = run_large(tmp)
+        with open(path, "w") as f:
+            json.dump(out, f, indent=1)
+        return
     with tempfile.TemporaryDirectory() as tmp:
         for name, kind, n, seed, kw, methods in ([] if multi_only else CASES):
             las = synth.generate(kind, n, seed, **kw)

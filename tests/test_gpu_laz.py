@@ -15,7 +15,7 @@ import potreeconverter_b200 as pc
 from tests.oracle_lib import have_laz_tool, las_records, laz_sources_for, load_golden, md5, to_laz
 
 pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(not have_laz_tool(), reason="oracle/_ref/laz_tool not built (make -C oracle ref)")]
+              pytest.mark.skipif(not have_laz_tool(), reason="oracle/_ref/laz_tool not built (make -C oracle ref REF=<reference tree>)")]
 
 LAZ_CASES = [(c, m) for c in load_golden()["multi_cases"] if c.get("laz") for m in c["outputs"]]
 FILES = {"octree.bin": "octree", "hierarchy.bin": "hierarchy", "metadata.json": "metadata"}

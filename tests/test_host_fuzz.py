@@ -33,7 +33,7 @@ def _inputs(tmp):
     return files
 
 
-@pytest.mark.skipif(not have_laz_tool(), reason="oracle/_ref/laz_tool not built (make -C oracle ref)")
+@pytest.mark.skipif(not have_laz_tool(), reason="oracle/_ref/laz_tool not built (make -C oracle ref REF=<reference tree>)")
 def test_laz_decoder_under_sanitizers(tmp_path):
     exe = _build(tmp_path, "laz_fuzz")
     for k, las in enumerate(_inputs(tmp_path)):

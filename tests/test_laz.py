@@ -14,7 +14,7 @@ import pytest
 from tests.oracle_lib import have_laz_tool, las_records, to_laz
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-pytestmark = pytest.mark.skipif(not have_laz_tool(), reason="oracle/_ref/laz_tool not built (make -C oracle ref)")
+pytestmark = pytest.mark.skipif(not have_laz_tool(), reason="oracle/_ref/laz_tool not built (make -C oracle ref REF=<reference tree>)")
 
 
 @pytest.fixture(scope="module")

@@ -16,7 +16,7 @@ REF = os.path.join(ORACLE_DIR, "_ref", "PotreeConverter_pinned")
 STANDARD = ["intensity", "return number", "number of returns", "classification", "scan angle rank", "user data",
             "point source id", "gps-time", "rgb"]
 
-pytestmark = pytest.mark.skipif(not os.path.exists(REF), reason="pinned reference not built (make -C oracle ref)")
+pytestmark = pytest.mark.skipif(not os.path.exists(REF), reason="pinned reference not built (make -C oracle ref REF=<reference tree>)")
 
 
 @pytest.mark.parametrize("seed", range(16))

@@ -87,7 +87,7 @@ def test_extra_bytes_follow_the_reference_rule(setup_check, tmp_path):
         assert src["extras"] == expect, fmt
 
 
-@pytest.mark.skipif(not have_laz_tool(), reason="oracle/_ref/laz_tool not built (make -C oracle ref)")
+@pytest.mark.skipif(not have_laz_tool(), reason="oracle/_ref/laz_tool not built (make -C oracle ref REF=<reference tree>)")
 def test_laz_sources_are_read(setup_check, tmp_path):
     from potreeconverter_b200 import synth
     t = synth.tiles(40_000, 9)
