@@ -199,6 +199,80 @@ pcg_status pcg_kernel_shuffle(pcg_ctx* ctx, int64_t n, uint32_t seed, int32_t* p
 pcg_status pcg_kernel_decode_count(pcg_ctx* ctx, const void* las, uint64_t size, int32_t* X, int32_t* Y, int32_t* Z, uint32_t* cell,
                                    int64_t point_capacity, uint32_t* grid, int64_t grid_capacity, int32_t* grid_size);
 
+/* One chunk of the chunker's LUT (createLUT, chunker_countsort_laszip.cpp:
+   1074-1204): its file name without ".bin" (toNodeID, :82-115: "r" + one
+   octant digit per level), its cell at its own level and its point count. */
+typedef struct pcg_chunk {
+	char id[16];
+	int32_t level, x, y, z;
+	int64_t count;
+} pcg_chunk;
+
+/* The LUT merge (createLUT, chunker_countsort_laszip.cpp:1074-1204) of a
+   count grid of G^3 cells (G a power of two up to 512, cell index ix + iy G +
+   iz G^2): 2x2x2 blocks merge bottom-up while no child is split and the sum
+   stays <= max_points_per_chunk. chunks_out receives the chunks in chunk
+   file-name order (the order the indexer visits them, indexer.cpp:149 with
+   sorted directory iteration), lut_out (G^3 entries) every cell's index in
+   that list, -1 for cells no chunk covers. More chunks than chunk_capacity:
+   PCG_BAD_INPUT, with *num_chunks set to the count needed. */
+pcg_status pcg_kernel_lut(pcg_ctx* ctx, const uint32_t* grid, int32_t grid_size, int64_t max_points_per_chunk, int32_t* lut_out,
+                          pcg_chunk* chunks_out, int64_t chunk_capacity, int32_t* num_chunks);
+
+/* The distribution of points to chunks (distributePoints,
+   chunker_countsort_laszip.cpp:837-904, with one chunker thread): ids_out
+   lists the point indices 0..n-1 grouped by chunk (chunk 0 first), input
+   order inside each chunk, and chunk_start[k] (num_chunks + 1 entries) is
+   where chunk k starts in ids_out. cell: every point's count-grid cell
+   (pcg_kernel_decode_count), lut: G^3 entries (pcg_kernel_lut). A cell no
+   chunk covers: PCG_INTERNAL. */
+pcg_status pcg_kernel_scatter(pcg_ctx* ctx, const uint32_t* cell, int64_t n, const int32_t* lut, int32_t grid_size, int32_t num_chunks,
+                              uint32_t* ids_out, int64_t* chunk_start);
+
+/* One node of a chunk's octree (buildHierarchy, indexer.cpp:823-1109). */
+typedef struct pcg_octree_node {
+	char name[32];         /* root_name + octant digits                       */
+	int64_t start;         /* its points: order_out[start .. start + count)    */
+	int64_t count;         /* 0 for inner nodes                                */
+	int32_t is_leaf;
+	int32_t pad;
+} pcg_octree_node;
+
+/* The per-chunk octree of one chunk (buildHierarchy, indexer.cpp:823-1109:
+   32^3 counting sort in Morton order, sum pyramid, createNodes :732-817 with
+   the 10,000-point split threshold, recursion into over-full nodes and the
+   duplicate rule of :1002-1099). X, Y, Z: the chunk's quantized points (n,
+   in chunk order); scale / offset: the output position transform
+   (x = X * scale + offset); box_min / box_max: the chunk's cube;
+   root_name: the chunk's id. order_out (n entries) receives the points'
+   indices in the order the reference leaves them, nodes_out every node of
+   the chunk's subtree below and including the root, sorted by name;
+   *octree_depth the deepest level created (the reference's octreeDepth).
+   More nodes than node_capacity: PCG_BAD_INPUT, *num_nodes = count needed. */
+pcg_status pcg_kernel_octree(pcg_ctx* ctx, const int32_t* X, const int32_t* Y, const int32_t* Z, int64_t n, const double* scale,
+                             const double* offset, const double* box_min, const double* box_max, const char* root_name,
+                             uint32_t* order_out, pcg_octree_node* nodes_out, int64_t node_capacity, int64_t* num_nodes,
+                             int64_t* octree_depth);
+
+/* The sampler's decision for one inner node (method = pcg_method):
+   SamplerPoisson (sampler_poisson.h:127-203: std::sort by squared distance
+   to the node centre, greedy acceptance with the early-exit bound and the
+   10,001-check cap), SamplerPoissonAverage (sampler_poisson_average.h:
+   184-445: pure greedy in a 16^3 grid window, order-dependent colour sums)
+   or SamplerRandom (sampler_random.h:123-182: children under 100 points, or
+   the first point of a 128^3 cell within 0.7 sqrt(3) of its centre; a fresh
+   cell grid, as for the first node a thread samples). The candidates are the
+   children's points in gather order: child[] (n entries) is non-decreasing
+   in 0..7, X, Y, Z are quantized positions, rgb (3 x uint16 per point) the
+   colours (poisson_average only, else may be NULL). box_min / box_max: the
+   node's cube, spacing: the node's spacing (baseSpacing / 2^level).
+   accepted_out[i] = 1 when candidate i moves to the parent; for
+   poisson_average rgb_out (3 x n, may be NULL otherwise) receives the
+   averaged colour written into every candidate (:440-445). */
+pcg_status pcg_kernel_accept(pcg_ctx* ctx, int32_t method, const int32_t* X, const int32_t* Y, const int32_t* Z, const uint8_t* child,
+                             const uint16_t* rgb, int64_t n, const double* scale, const double* offset, const double* box_min,
+                             const double* box_max, double spacing, uint8_t* accepted_out, uint16_t* rgb_out);
+
 /* LASzip decode of every point of a LAZ file image (point formats 0-3,
    LASzip's chunked point-wise coding: lasreadpoint.cpp:405-497 with the v2
    item readers of lasreaditemcompressed_v2.cpp) into records_out

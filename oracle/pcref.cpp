@@ -309,6 +309,52 @@ static inline PointCoord lasCoordinates(const Source& src, int64_t i) {  // lasz
 
 struct Chunk { string id; Vec3 min, max; vector<uint8_t> data; };
 
+static void createLUT(const vector<int64_t>& grid, int64_t gridSize, int64_t maxPointsPerChunk, vector<ChunkNode>& nodes,
+                      vector<int32_t>& lut) {  // chunker_countsort_laszip.cpp:1074-1204
+	nodes.clear();
+	lut.assign(gridSize * gridSize * gridSize, -1);
+	vector<int64_t> gridHigh = grid;
+	int64_t levelMax = int64_t(log2(gridSize));
+	for (int64_t levelLow = levelMax - 1; levelLow >= 0; levelLow--) {
+		int64_t levelHigh = levelLow + 1;
+		int64_t gH = int64_t(pow(2, levelHigh)), gL = int64_t(pow(2, levelLow));
+		vector<int64_t> gridLow(gL * gL * gL, 0);
+		for (int64_t x = 0; x < gL; x++) for (int64_t y = 0; y < gL; y++) for (int64_t z = 0; z < gL; z++) {
+			int64_t indexLow = x + y * gL + z * gL * gL;
+			int64_t sum = 0; bool unmergeable = false;
+			for (int64_t j = 0; j < 8; j++) {
+				int64_t nx = 2 * x + ((j & 4) >> 2), ny = 2 * y + ((j & 2) >> 1), nz = 2 * z + (j & 1);
+				int64_t v = gridHigh[nx + ny * gH + nz * gH * gH];
+				if (v == -1) unmergeable = true; else sum += v;
+			}
+			if (unmergeable || sum > maxPointsPerChunk) {
+				for (int64_t j = 0; j < 8; j++) {
+					int64_t nx = 2 * x + ((j & 4) >> 2), ny = 2 * y + ((j & 2) >> 1), nz = 2 * z + (j & 1);
+					int64_t v = gridHigh[nx + ny * gH + nz * gH * gH];
+					if (v > 0) {
+						ChunkNode n;
+						n.id = toNodeID((int)levelHigh, (int)gH, nx, ny, nz);
+						n.numPoints = v; n.x = nx; n.y = ny; n.z = nz;
+						n.size = int64_t(pow(2, levelMax - levelHigh));
+						nodes.push_back(n);
+					}
+				}
+				gridLow[indexLow] = -1;
+			} else {
+				gridLow[indexLow] = sum;
+			}
+		}
+		gridHigh = gridLow;
+	}
+	for (int i = 0; i < (int)nodes.size(); i++) {
+		auto& n = nodes[i];
+		for (int64_t ox = 0; ox < n.size; ox++) for (int64_t oy = 0; oy < n.size; oy++) for (int64_t oz = 0; oz < n.size; oz++) {
+			int64_t x = n.size * n.x + ox, y = n.size * n.y + oy, z = n.size * n.z + oz;
+			lut[x + y * gridSize + z * gridSize * gridSize] = i;
+		}
+	}
+}
+
 static bool doChunking(Job& job, vector<Chunk>& chunksOut, Attributes& attrsOut, Vec3& minOut, Vec3& maxOut) {
 	// chunker_countsort_laszip.cpp:1206-1261
 	int64_t total = job.totalPoints;
@@ -344,49 +390,8 @@ static bool doChunking(Job& job, vector<Chunk>& chunksOut, Attributes& attrsOut,
 
 	// createLUT, :1074-1204
 	vector<ChunkNode> nodes;
-	vector<int32_t> lut(gridSize * gridSize * gridSize, -1);
-	{
-		vector<int64_t> gridHigh = grid;
-		int64_t levelMax = int64_t(log2(gridSize));
-		for (int64_t levelLow = levelMax - 1; levelLow >= 0; levelLow--) {
-			int64_t levelHigh = levelLow + 1;
-			int64_t gH = int64_t(pow(2, levelHigh)), gL = int64_t(pow(2, levelLow));
-			vector<int64_t> gridLow(gL * gL * gL, 0);
-			for (int64_t x = 0; x < gL; x++) for (int64_t y = 0; y < gL; y++) for (int64_t z = 0; z < gL; z++) {
-				int64_t indexLow = x + y * gL + z * gL * gL;
-				int64_t sum = 0; bool unmergeable = false;
-				for (int64_t j = 0; j < 8; j++) {
-					int64_t nx = 2 * x + ((j & 4) >> 2), ny = 2 * y + ((j & 2) >> 1), nz = 2 * z + (j & 1);
-					int64_t v = gridHigh[nx + ny * gH + nz * gH * gH];
-					if (v == -1) unmergeable = true; else sum += v;
-				}
-				if (unmergeable || sum > maxPointsPerChunk) {
-					for (int64_t j = 0; j < 8; j++) {
-						int64_t nx = 2 * x + ((j & 4) >> 2), ny = 2 * y + ((j & 2) >> 1), nz = 2 * z + (j & 1);
-						int64_t v = gridHigh[nx + ny * gH + nz * gH * gH];
-						if (v > 0) {
-							ChunkNode n;
-							n.id = toNodeID((int)levelHigh, (int)gH, nx, ny, nz);
-							n.numPoints = v; n.x = nx; n.y = ny; n.z = nz;
-							n.size = int64_t(pow(2, levelMax - levelHigh));
-							nodes.push_back(n);
-						}
-					}
-					gridLow[indexLow] = -1;
-				} else {
-					gridLow[indexLow] = sum;
-				}
-			}
-			gridHigh = gridLow;
-		}
-		for (int i = 0; i < (int)nodes.size(); i++) {
-			auto& n = nodes[i];
-			for (int64_t ox = 0; ox < n.size; ox++) for (int64_t oy = 0; oy < n.size; oy++) for (int64_t oz = 0; oz < n.size; oz++) {
-				int64_t x = n.size * n.x + ox, y = n.size * n.y + oy, z = n.size * n.z + oz;
-				lut[x + y * gridSize + z * gridSize * gridSize] = i;
-			}
-		}
-	}
+	vector<int32_t> lut;
+	createLUT(grid, gridSize, maxPointsPerChunk, nodes, lut);
 
 	// distributePoints, :660-1003 (handlers :380-658), one batch thread,
 	// sources in order
@@ -1520,4 +1525,172 @@ extern "C" void pcref_std_shuffle(int64_t n, uint32_t seed, int32_t* perm) {
 	for (int64_t i = 0; i < n; i++) v[i] = (int)i;
 	std::shuffle(v.begin(), v.end(), std::default_random_engine(seed));
 	for (int64_t i = 0; i < n; i++) perm[i] = v[i];
+}
+
+// ------------------------------------------------------------ stage hooks
+// One stage of the pipeline at a time, for the parity tests of the library's
+// stage entry points (include/pcgpu.h pcg_kernel_lut, _scatter, _octree,
+// _accept). Each runs the restatement's own function of that stage.
+
+// createLUT (chunker_countsort_laszip.cpp:1074-1204) of a count grid:
+// chunks in file-name order (ids 16 bytes each, info: level, x, y, z,
+// count), the LUT remapped to that order. Returns 1 when the chunk list
+// exceeds capacity (*num_chunks = chunks found).
+extern "C" int pcref_lut(const int64_t* grid, int64_t grid_size, int64_t max_points_per_chunk, int32_t* lut_out, char* ids_out,
+                         int64_t* info_out, int64_t capacity, int64_t* num_chunks) {
+	using namespace pcref;
+	vector<int64_t> g(grid, grid + grid_size * grid_size * grid_size);
+	vector<ChunkNode> nodes;
+	vector<int32_t> lut;
+	createLUT(g, grid_size, max_points_per_chunk, nodes, lut);
+	*num_chunks = (int64_t)nodes.size();
+	if ((int64_t)nodes.size() > capacity) return 1;
+	vector<size_t> order(nodes.size());
+	for (size_t i = 0; i < order.size(); i++) order[i] = i;
+	std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return nodes[a].id + ".bin" < nodes[b].id + ".bin"; });
+	vector<int32_t> rank(nodes.size());
+	for (size_t r = 0; r < order.size(); r++) {
+		const ChunkNode& n = nodes[order[r]];
+		rank[order[r]] = (int32_t)r;
+		memset(ids_out + 16 * r, 0, 16);
+		memcpy(ids_out + 16 * r, n.id.c_str(), std::min<size_t>(n.id.size(), 15));
+		int64_t level = (int64_t)n.id.size() - 1;
+		info_out[5 * r] = level;
+		info_out[5 * r + 1] = n.x;
+		info_out[5 * r + 2] = n.y;
+		info_out[5 * r + 3] = n.z;
+		info_out[5 * r + 4] = n.numPoints;
+	}
+	for (size_t i = 0; i < lut.size(); i++) lut_out[i] = lut[i] < 0 ? -1 : rank[lut[i]];
+	return 0;
+}
+
+// distributePoints' bucket fill (chunker_countsort_laszip.cpp:837-904, one
+// chunker thread): point indices appended to their chunk in input order.
+extern "C" int pcref_scatter(const uint32_t* cell, int64_t n, const int32_t* lut, int32_t num_chunks, uint32_t* ids_out,
+                             int64_t* chunk_start) {
+	std::vector<std::vector<uint32_t>> buckets(num_chunks);
+	for (int64_t i = 0; i < n; i++) {
+		int32_t k = lut[cell[i]];
+		if (k < 0 || k >= num_chunks) return 1;
+		buckets[k].push_back((uint32_t)i);
+	}
+	int64_t off = 0;
+	for (int32_t k = 0; k < num_chunks; k++) {
+		chunk_start[k] = off;
+		memcpy(ids_out + off, buckets[k].data(), buckets[k].size() * sizeof(uint32_t));
+		off += (int64_t)buckets[k].size();
+	}
+	chunk_start[num_chunks] = off;
+	return 0;
+}
+
+namespace {
+
+// Attributes of the stage hooks' records: position, then the point's input
+// index (and rgb for the averaging sampler), so the points can be followed
+// through the restatement's record shuffling.
+pcref::Attributes hookAttributes(const double* scale, const double* offset, bool rgb) {
+	using namespace pcref;
+	vector<Attribute> list = {Attribute("position", 12, 3, 4, AType::INT32), Attribute("index", 4, 1, 4, AType::UINT32)};
+	if (rgb) list.push_back(Attribute("rgb", 6, 3, 2, AType::UINT16));
+	Attributes a(list);
+	a.posScale = {scale[0], scale[1], scale[2]};
+	a.posOffset = {offset[0], offset[1], offset[2]};
+	return a;
+}
+
+void packRecord(uint8_t* p, int32_t X, int32_t Y, int32_t Z, uint32_t index) {
+	memcpy(p, &X, 4); memcpy(p + 4, &Y, 4); memcpy(p + 8, &Z, 4); memcpy(p + 12, &index, 4);
+}
+
+}  // namespace
+
+// buildHierarchy (indexer.cpp:823-1109) of one chunk: its subtree's nodes
+// sorted by name (names 32 bytes each; info: start, count, is_leaf), point
+// indices in the order the restatement leaves them.
+extern "C" int pcref_octree(const int32_t* X, const int32_t* Y, const int32_t* Z, int64_t n, const double* scale, const double* offset,
+                            const double* box_min, const double* box_max, const char* root_name, uint32_t* order_out, char* names_out,
+                            int64_t* info_out, int64_t capacity, int64_t* num_nodes, int64_t* octree_depth) {
+	using namespace pcref;
+	Indexer indexer;
+	indexer.attributes = hookAttributes(scale, offset, false);
+	const int64_t bpp = indexer.attributes.bytes;
+	auto points = std::make_shared<vector<uint8_t>>(n * bpp);
+	for (int64_t i = 0; i < n; i++) packRecord(points->data() + i * bpp, X[i], Y[i], Z[i], (uint32_t)i);
+	auto root = std::make_shared<Node>(root_name, Vec3{box_min[0], box_min[1], box_min[2]}, Vec3{box_max[0], box_max[1], box_max[2]});
+	buildHierarchy(&indexer, root.get(), points, n);
+	vector<Node*> all;
+	traverseNode(root.get(), [&](Node* nd) { all.push_back(nd); });
+	std::sort(all.begin(), all.end(), [](Node* a, Node* b) { return a->name < b->name; });
+	*num_nodes = (int64_t)all.size();
+	*octree_depth = indexer.octreeDepth;
+	if ((int64_t)all.size() > capacity) return 1;
+	int64_t off = 0;
+	for (size_t k = 0; k < all.size(); k++) {
+		Node* nd = all[k];
+		memset(names_out + 32 * k, 0, 32);
+		memcpy(names_out + 32 * k, nd->name.c_str(), std::min<size_t>(nd->name.size(), 31));
+		const bool leaf = nd->isLeaf();
+		int64_t cnt = (leaf && nd->points) ? nd->numPoints : 0;
+		info_out[3 * k] = off;
+		info_out[3 * k + 1] = cnt;
+		info_out[3 * k + 2] = leaf ? 1 : 0;
+		for (int64_t i = 0; i < cnt; i++) order_out[off + i] = rd<uint32_t>(nd->points->data() + i * bpp + 12);
+		off += cnt;
+	}
+	for (int64_t i = off; i < n; i++) order_out[i] = 0xffffffffu;  // dropped by the duplicate rule
+	return 0;
+}
+
+// One inner node sampled by the restatement's sampler (method 0 poisson, 1
+// poisson_average, 2 random): the candidates are the children's points,
+// child[] non-decreasing; the children count as already sampled (no leaf
+// shuffle); the node is named "r" so its spacing is baseSpacing.
+extern "C" int pcref_accept(int32_t method, const int32_t* X, const int32_t* Y, const int32_t* Z, const uint8_t* child, const uint16_t* rgb,
+                            int64_t n, const double* scale, const double* offset, const double* box_min, const double* box_max,
+                            double spacing, uint8_t* accepted_out, uint16_t* rgb_out) {
+	using namespace pcref;
+	Attributes attrs = hookAttributes(scale, offset, method == 1);
+	const int64_t bpp = attrs.bytes;
+	auto node = std::make_shared<Node>("r", Vec3{box_min[0], box_min[1], box_min[2]}, Vec3{box_max[0], box_max[1], box_max[2]});
+	shared_ptr<Node> kids[8];
+	for (int64_t i = 0; i < n; i++) {
+		int c = child[i];
+		if (c > 7 || (i > 0 && child[i - 1] > c)) return 1;
+		if (!kids[c]) {
+			kids[c] = std::make_shared<Node>();
+			childBox(node->min, node->max, c, kids[c]->min, kids[c]->max);
+			kids[c]->name = "r" + std::to_string(c);
+			kids[c]->children.resize(8);
+			kids[c]->points = std::make_shared<vector<uint8_t>>();
+			kids[c]->sampled = true;
+			node->children[c] = kids[c];
+		}
+		auto& buf = *kids[c]->points;
+		size_t at = buf.size();
+		buf.resize(at + bpp);
+		packRecord(buf.data() + at, X[i], Y[i], Z[i], (uint32_t)i);
+		if (method == 1) memcpy(buf.data() + at + 16, rgb + 3 * i, 6);
+		kids[c]->numPoints++;
+	}
+	auto noop = [](Node*) {};
+	memset(accepted_out, 0, n);
+	if (method == 0) samplePoisson(node.get(), attrs, spacing, noop);
+	else if (method == 1) samplePoissonAverage(node.get(), attrs, spacing, noop);
+	else {
+		// the random sampler's visit counter: this node is the thread's first
+		sampleRandom(node.get(), attrs, 0, noop);
+	}
+	for (int64_t i = 0; i < node->numPoints; i++) accepted_out[rd<uint32_t>(node->points->data() + i * bpp + 12)] = 1;
+	if (method == 1 && rgb_out) {
+		// every candidate's record carries the averaged colour (:440-445);
+		// the children were given their rejected and kept points
+		for (int c = 0; c < 8; c++) {
+			if (!kids[c] || !kids[c]->points) continue;
+			const auto& buf = *kids[c]->points;
+			for (size_t k = 0; k + bpp <= buf.size(); k += bpp) memcpy(rgb_out + 3 * rd<uint32_t>(buf.data() + k + 12), buf.data() + k + 16, 6);
+		}
+	}
+	return 0;
 }

@@ -90,10 +90,21 @@ class _Result(ctypes.Structure):
                 ("nodes", ctypes.POINTER(_Node)), ("num_nodes", ctypes.c_uint64)]
 
 
+class _Chunk(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_char * 16), ("level", ctypes.c_int32), ("x", ctypes.c_int32), ("y", ctypes.c_int32),
+                ("z", ctypes.c_int32), ("count", ctypes.c_int64)]
+
+
+class _OctreeNode(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("start", ctypes.c_int64), ("count", ctypes.c_int64),
+                ("is_leaf", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
 # every symbol include/pcgpu.h declares
 EXPORTS = ["pcg_create", "pcg_destroy", "pcg_last_error", "pcg_status_string", "pcg_convert", "pcg_result_free",
            "pcg_write_files", "pcg_submit", "pcg_poll", "pcg_wait", "pcg_kernel_sort_keys", "pcg_kernel_shuffle",
-           "pcg_kernel_sort_keys_noalloc", "pcg_kernel_laz_decode", "pcg_kernel_decode_count"]
+           "pcg_kernel_sort_keys_noalloc", "pcg_kernel_laz_decode", "pcg_kernel_decode_count", "pcg_kernel_lut",
+           "pcg_kernel_scatter", "pcg_kernel_octree", "pcg_kernel_accept"]
 
 _lib = None
 
@@ -125,6 +136,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.pcg_kernel_laz_decode.argtypes = [c.c_void_p, c.c_char_p, c.c_uint64, c.c_void_p, c.c_uint64]
     lib.pcg_kernel_decode_count.argtypes = [c.c_void_p, c.c_char_p, c.c_uint64, c.c_void_p, c.c_void_p, c.c_void_p,
                                             c.c_void_p, c.c_int64, c.c_void_p, c.c_int64, c.POINTER(c.c_int32)]
+    lib.pcg_kernel_lut.argtypes = [c.c_void_p, c.c_void_p, c.c_int32, c.c_int64, c.c_void_p, c.POINTER(_Chunk), c.c_int64,
+                                   c.POINTER(c.c_int32)]
+    lib.pcg_kernel_scatter.argtypes = [c.c_void_p, c.c_void_p, c.c_int64, c.c_void_p, c.c_int32, c.c_int32, c.c_void_p,
+                                       c.c_void_p]
+    lib.pcg_kernel_octree.argtypes = [c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p,
+                                      c.c_void_p, c.c_void_p, c.c_char_p, c.c_void_p, c.POINTER(_OctreeNode), c.c_int64,
+                                      c.POINTER(c.c_int64), c.POINTER(c.c_int64)]
+    lib.pcg_kernel_accept.argtypes = [c.c_void_p, c.c_int32, c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p,
+                                      c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p, c.c_double, c.c_void_p,
+                                      c.c_void_p]
     _lib = lib
     return lib
 
@@ -340,6 +361,85 @@ class Context:
         if st != 0:
             raise self._err(st)
         return X[:n], Y[:n], Z[:n], cell[:n], grid[: gs.value ** 3]
+
+    def lut(self, grid, grid_size: int, max_points_per_chunk: int):
+        """The chunker's LUT merge of a count grid (G^3 counts): (chunks, lut)
+        with chunks a list of (id, level, x, y, z, count) in chunk file-name
+        order and lut every cell's index in that list (-1: no chunk)."""
+        import numpy as np
+        g = np.ascontiguousarray(grid, dtype=np.uint32)
+        lut = np.empty(grid_size ** 3, np.int32)
+        cap = 1 << 16
+        while True:
+            chunks = (_Chunk * cap)()
+            num = ctypes.c_int32()
+            st = self._lib.pcg_kernel_lut(self._h, g.ctypes.data, grid_size, max_points_per_chunk, lut.ctypes.data, chunks, cap,
+                                          ctypes.byref(num))
+            if st == 1 and num.value > cap:
+                cap = num.value
+                continue
+            if st != 0:
+                raise self._err(st)
+            out = [(c.id.decode(), c.level, c.x, c.y, c.z, c.count) for c in chunks[: num.value]]
+            return out, lut
+
+    def scatter(self, cell, lut, grid_size: int, num_chunks: int):
+        """Points distributed to chunks: (ids, chunk_start), ids grouped by
+        chunk in input order, chunk_start num_chunks + 1 offsets."""
+        import numpy as np
+        c = np.ascontiguousarray(cell, dtype=np.uint32)
+        lt = np.ascontiguousarray(lut, dtype=np.int32)
+        ids = np.empty(max(c.shape[0], 1), np.uint32)
+        start = np.empty(num_chunks + 1, np.int64)
+        st = self._lib.pcg_kernel_scatter(self._h, c.ctypes.data, c.shape[0], lt.ctypes.data, grid_size, num_chunks,
+                                          ids.ctypes.data, start.ctypes.data)
+        if st != 0:
+            raise self._err(st)
+        return ids[: c.shape[0]], start
+
+    def octree(self, X, Y, Z, scale, offset, box_min, box_max, root_name: str = "r"):
+        """One chunk's octree: (order, nodes, depth); nodes a list of
+        (name, start, count, is_leaf) sorted by name, order the points'
+        indices in the order the octree build leaves them."""
+        import numpy as np
+        arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in (X, Y, Z)]
+        vecs = [np.ascontiguousarray(v, dtype=np.float64) for v in (scale, offset, box_min, box_max)]
+        n = arrs[0].shape[0]
+        order = np.empty(max(n, 1), np.uint32)
+        cap = 4096
+        while True:
+            nodes = (_OctreeNode * cap)()
+            num, depth = ctypes.c_int64(), ctypes.c_int64()
+            st = self._lib.pcg_kernel_octree(self._h, *[a.ctypes.data for a in arrs], n, *[v.ctypes.data for v in vecs],
+                                             root_name.encode(), order.ctypes.data, nodes, cap, ctypes.byref(num),
+                                             ctypes.byref(depth))
+            if st == 1 and num.value > cap:
+                cap = num.value
+                continue
+            if st != 0:
+                raise self._err(st)
+            out = [(x.name.decode(), x.start, x.count, x.is_leaf) for x in nodes[: num.value]]
+            return order[:n], out, depth.value
+
+    def accept(self, method: str, X, Y, Z, child, scale, offset, box_min, box_max, spacing: float, rgb=None):
+        """One inner node's sampler decision: (accepted, rgb) with accepted
+        a 0/1 mask over the candidates (children's points in order) and rgb
+        the averaged colours (poisson_average) or None."""
+        import numpy as np
+        arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in (X, Y, Z)]
+        ch = np.ascontiguousarray(child, dtype=np.uint8)
+        vecs = [np.ascontiguousarray(v, dtype=np.float64) for v in (scale, offset, box_min, box_max)]
+        n = ch.shape[0]
+        acc = np.empty(max(n, 1), np.uint8)
+        col_in = np.ascontiguousarray(rgb, dtype=np.uint16) if rgb is not None else None
+        col_out = np.empty((max(n, 1), 3), np.uint16) if method == "poisson_average" else None
+        st = self._lib.pcg_kernel_accept(self._h, METHODS[method], *[a.ctypes.data for a in arrs], ch.ctypes.data,
+                                         col_in.ctypes.data if col_in is not None else None, n,
+                                         *[v.ctypes.data for v in vecs], spacing, acc.ctypes.data,
+                                         col_out.ctypes.data if col_out is not None else None)
+        if st != 0:
+            raise self._err(st)
+        return acc[:n], (col_out[:n] if col_out is not None else None)
 
     def laz_decode(self, laz: bytes) -> bytes:
         """Point records of a LAZ file image, decoded on the device."""

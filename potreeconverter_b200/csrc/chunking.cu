@@ -238,11 +238,12 @@ __global__ void lut_fill_kernel(const ChunkCell* __restrict__ chunks, int grid_s
 	}
 }
 
-__global__ void assign_kernel(const uint32_t* __restrict__ cell, const int32_t* __restrict__ lut, int64_t n,
+__global__ void assign_kernel(const uint32_t* __restrict__ cell, const int32_t* __restrict__ lut, int64_t n, int chunk_base,
                               uint32_t* __restrict__ chunk_of, uint32_t* __restrict__ ids, int64_t* error) {
 	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
 	int32_t c = lut[cell[i]];
+	c = c < 0 ? -1 : c - chunk_base;
 	if (c < 0) {
 		atomicCAS((unsigned long long*)&error[1], 0ull, (unsigned long long)(i + 1));
 		c = 0;
@@ -251,7 +252,22 @@ __global__ void assign_kernel(const uint32_t* __restrict__ cell, const int32_t* 
 	ids[i] = (uint32_t)i;
 }
 
+// starts[k] = first position of key k in the ascending keys[0..n), for every
+// k in 0..num_keys (starts[num_keys] = n); keys absent get the next start
+__global__ void segment_starts_kernel(const uint32_t* __restrict__ keys, int64_t n, int num_keys, int64_t* __restrict__ starts) {
+	int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i > n) return;
+	const int64_t lo = i == 0 ? -1 : (int64_t)keys[i - 1];
+	const int64_t hi = i == n ? (int64_t)num_keys : (int64_t)keys[i];
+	for (int64_t k = lo + 1; k <= hi && k <= num_keys; k++) starts[k] = i;
+}
+
 }  // namespace
+
+void launch_segment_starts(const uint32_t* keys, int64_t n, int num_keys, int64_t* starts, DeviceMem& mem) {
+	segment_starts_kernel<<<(unsigned)ceil_div(n + 1, 256), 256, 0, mem.stream()>>>(keys, n, num_keys, starts);
+	PCG_LAUNCHED();
+}
 
 void launch_decode_count(const DecodeParams& p, uint32_t* grid, ChunkingOut& out, DeviceMem& mem) {
 	if (p.n == 0) return;
@@ -296,10 +312,10 @@ void launch_lut_fill(const ChunkCell* chunks, int num_chunks, int grid_size, int
 	PCG_LAUNCHED();
 }
 
-void launch_assign_chunks(const uint32_t* cell, const int32_t* lut, int64_t n, uint32_t* chunk_of, uint32_t* ids,
+void launch_assign_chunks(const uint32_t* cell, const int32_t* lut, int64_t n, int chunk_base, uint32_t* chunk_of, uint32_t* ids,
                           int64_t* error, DeviceMem& mem) {
 	if (n == 0) return;
-	assign_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(cell, lut, n, chunk_of, ids, error);
+	assign_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(cell, lut, n, chunk_base, chunk_of, ids, error);
 	PCG_LAUNCHED();
 }
 

@@ -33,8 +33,13 @@ void launch_lut_merge(const uint32_t* grid, int grid_size, int64_t max_points_pe
                       int32_t* num_chunks, int capacity, DeviceMem& mem);
 // Fills the LUT: chunk k owns cells of chunks[k] (already in chunk order).
 void launch_lut_fill(const ChunkCell* chunks, int num_chunks, int grid_size, int32_t* lut, DeviceMem& mem);
-void launch_assign_chunks(const uint32_t* cell, const int32_t* lut, int64_t n, uint32_t* chunk_of, uint32_t* ids,
+// chunk_of[i] = lut[cell[i]] - chunk_base, ids[i] = i; a cell without a
+// chunk, or one below chunk_base, sets error[1]
+void launch_assign_chunks(const uint32_t* cell, const int32_t* lut, int64_t n, int chunk_base, uint32_t* chunk_of, uint32_t* ids,
                           int64_t* error, DeviceMem& mem);
+// starts[k] = first index of key k in ascending keys[0..n), k = 0..num_keys
+// (starts[num_keys] = n; keys < num_keys)
+void launch_segment_starts(const uint32_t* keys, int64_t n, int num_keys, int64_t* starts, DeviceMem& mem);
 
 // --------------------------------------------------------------- octree.cu
 struct SegmentDesc {        // one node to split with a 32^3 counting sort

@@ -348,39 +348,15 @@ struct Converter {
 		PCG_CUDA(cudaMemsetAsync(co.error, 0, 16, stream));
 		launch_decode_count(p, grid, co, mem);
 
-		const int chunk_cap = 1 << 20;
-		ChunkCell* d_chunks = mem.alloc<ChunkCell>(chunk_cap);
-		int32_t* d_nchunks = mem.alloc<int32_t>(1);
-		PCG_CUDA(cudaMemsetAsync(d_nchunks, 0, 4, stream));
-		launch_lut_merge(grid, G, s.max_points_per_chunk, d_chunks, d_nchunks, chunk_cap, mem);
 		auto errs = download(co.error, 2, stream);
 		if (errs[0]) throw PcgError(PCG_OUT_OF_BOX, "point " + std::to_string(errs[0] - 1) + " lies outside the header bounding box");
-		int nchunks = download(d_nchunks, 1, stream)[0];
-		if (nchunks > chunk_cap) throw PcgError(PCG_INTERNAL, "too many chunks");
-		auto cells_found = download(d_chunks, (size_t)nchunks, stream);
-		// chunk order = chunk file-name order (the oracle's sorted directory scan)
-		std::vector<std::pair<std::string, ChunkCell>> chunks;
-		for (auto& c : cells_found) chunks.push_back({chunk_id(c), c});
-		std::sort(chunks.begin(), chunks.end(), [](const auto& a, const auto& b) { return a.first + ".bin" < b.first + ".bin"; });
-		std::vector<ChunkCell> sorted_cells;
-		for (auto& c : chunks) sorted_cells.push_back(c.second);
-		ChunkCell* d_sorted = upload(sorted_cells, mem);
 		int32_t* lut = mem.alloc<int32_t>(cells);
-		PCG_CUDA(cudaMemsetAsync(lut, 0xff, cells * sizeof(int32_t), stream));
-		launch_lut_fill(d_sorted, nchunks, G, lut, mem);
-		uint32_t* chunk_of = mem.alloc<uint32_t>(N);
+		const std::vector<std::pair<std::string, ChunkCell>> chunks = make_chunks(grid, G, s.max_points_per_chunk, lut, mem);
+		const int nchunks = (int)chunks.size();
 		uint32_t* ids = mem.alloc<uint32_t>(N);
-		launch_assign_chunks(co.cell, lut, N, chunk_of, ids, co.error, mem);
-		{
-			uint32_t* kt = mem.alloc<uint32_t>(N);
-			uint32_t* vt = mem.alloc<uint32_t>(N);
-			radix_sort_pairs(chunk_of, ids, kt, vt, N, 0, std::max(1, bits_for((uint64_t)std::max(nchunks - 1, 0))), mem);
-			mem.free(kt);
-			mem.free(vt);
-		}
+		scatter_chunks(co.cell, lut, N, nchunks, 0, ids, co.error, mem);
 		errs = download(co.error, 2, stream);
 		if (errs[1]) throw PcgError(PCG_INTERNAL, "point to chunk lookup failed");
-		mem.free(chunk_of);
 		mem.free(lut);
 		mem.free(grid);
 		mem.free(co.cell);
@@ -407,91 +383,11 @@ struct Converter {
 			chunk_roots.push_back(cur);
 		}
 		if (off != N) throw PcgError(PCG_INTERNAL, "chunk counts do not add up");
-		int64_t octree_depth = 0;
 		PosParams pp;
 		for (int a = 0; a < 3; a++) { pp.scale[a] = (&s.pos_scale.x)[a]; pp.offset[a] = (&s.pos_offset.x)[a]; }
-		// nodes to split this round: (node, count of the parent call for the
-		// duplicate test, indexer.cpp:1002)
-		struct Pending { int node; int64_t parent_count; };
-		std::vector<Pending> pending;
-		for (int cr : chunk_roots)
-			if (tree.nodes[cr].leaf_count >= kMaxNodePoints) pending.push_back({cr, -1});
-		NodeCand* d_cands = nullptr;
-		int32_t* d_ncands = mem.alloc<int32_t>(1);
-		int64_t cand_cap = 0;
-		while (!pending.empty()) {
-			std::vector<SegmentDesc> segs;
-			int64_t total = 0;
-			for (auto& pd : pending) {
-				TNode& n = tree.nodes[pd.node];
-				SegmentDesc d;
-				d.start = n.leaf_start;
-				d.count = n.leaf_count;
-				d.coff = total;
-				Vec3d size = n.max - n.min;
-				d.min[0] = n.min.x; d.min[1] = n.min.y; d.min[2] = n.min.z;
-				d.size[0] = size.x; d.size[1] = size.y; d.size[2] = size.z;
-				segs.push_back(d);
-				total += d.count;
-			}
-			if (total > cand_cap) {
-				if (d_cands) mem.free(d_cands);
-				cand_cap = total;
-				d_cands = mem.alloc<NodeCand>(cand_cap);
-			}
-			SegmentDesc* d_segs = upload(segs, mem);
-			PCG_CUDA(cudaMemsetAsync(d_ncands, 0, 4, stream));
-			launch_octree_round(ids, co.X, co.Y, co.Z, pp, d_segs, (int)segs.size(), total, d_cands, d_ncands, cand_cap, mem);
-			int ncand = download(d_ncands, 1, stream)[0];
-			if (ncand > cand_cap) throw PcgError(PCG_INTERNAL, "octree round overflow");
-			auto cands = download(d_cands, (size_t)ncand, stream);
-			mem.free(d_segs);
-			// deterministic handling order: by segment, then path
-			std::sort(cands.begin(), cands.end(), [](const NodeCand& a, const NodeCand& b) {
-				if (a.seg != b.seg) return a.seg < b.seg;
-				if (a.level != b.level) return a.level < b.level;
-				return a.path < b.path;
-			});
-			std::vector<Pending> next;
-			std::vector<int64_t> seg_depth(segs.size(), 0);
-			for (auto& c : cands) {
-				int sn = pending[c.seg].node;
-				int cur = sn;
-				for (int l = 0; l < c.level; l++) {
-					int digit = (c.path >> (3 * (c.level - 1 - l))) & 7;
-					cur = tree.child_of(cur, digit, tree.nodes[sn].chunk);
-				}
-				TNode& rn = tree.nodes[cur];
-				rn.leaf_start = tree.nodes[sn].leaf_start + c.start;
-				rn.leaf_count = c.count;
-				octree_depth = std::max<int64_t>(octree_depth, rn.depth);
-				if (rn.leaf_count > kMaxNodePoints) next.push_back({cur, tree.nodes[sn].leaf_count});
-			}
-			// the split node's own points now live in its children (or in the
-			// node itself when createNodes kept it whole)
-			for (auto& pd : pending) {
-				TNode& n = tree.nodes[pd.node];
-				if (n.has_children()) n.leaf_count = 0;
-			}
-			// duplicate handling for nodes that did not split
-			std::vector<Pending> refined;
-			for (auto& nx : next) {
-				TNode& sub = tree.nodes[nx.node];
-				if (sub.leaf_count == nx.parent_count) {
-					int64_t uniq = count_unique_positions(ids + sub.leaf_start, sub.leaf_count, co.X, co.Y, co.Z, mem);
-					int64_t dups = sub.leaf_count - uniq;
-					if (dups >= kMaxNodePoints / 2) {
-						// the reference keeps the first `uniq` records (indexer.cpp:1088-1090)
-						sub.leaf_count = uniq;
-					}
-				}
-				if (sub.leaf_count >= kMaxNodePoints) refined.push_back({nx.node, sub.leaf_count});
-			}
-			pending.swap(refined);
-		}
+		const int64_t octree_depth = refine_octree(tree, chunk_roots, ids, co.X, co.Y, co.Z, pp, mem);
 		res.stats.octree_depth = octree_depth;
 		res.stats.ms_octree = ms_since(t_oct);
-
 		// --------------------------------------------------------- sampling
 		auto t_samp = Clock::now();
 		SampleStats* d_st = mem.alloc<SampleStats>(1);
@@ -635,6 +531,150 @@ struct Converter {
 		res.stats.ms_total = ms_since(t0);
 	}
 
+	// The per-chunk octrees (buildHierarchy, indexer.cpp:823-1109): every
+	// node of `roots` holding at least 10,000 points is split by 32^3
+	// counting-sort rounds, all pending nodes of the tree per round, until
+	// no node is over-full. ids[leaf_start .. leaf_start + leaf_count) are a
+	// node's points; they are reordered in place. Returns the deepest level
+	// created (the reference's octreeDepth, updated only here, :984-991).
+	int64_t refine_octree(Tree& tree, const std::vector<int>& roots, uint32_t* ids, const int32_t* X, const int32_t* Y, const int32_t* Z,
+	                      const PosParams& pp, DeviceMem& mem) {
+		int64_t octree_depth = 0;
+		// nodes to split this round: (node, count of the parent call for the
+		// duplicate test, indexer.cpp:1002)
+		struct Pending { int node; int64_t parent_count; };
+		std::vector<Pending> pending;
+		for (int cr : roots)
+			if (tree.nodes[cr].leaf_count >= kMaxNodePoints) pending.push_back({cr, -1});
+		NodeCand* d_cands = nullptr;
+		int32_t* d_ncands = mem.alloc<int32_t>(1);
+		int64_t cand_cap = 0;
+		while (!pending.empty()) {
+			std::vector<SegmentDesc> segs;
+			int64_t total = 0;
+			for (auto& pd : pending) {
+				TNode& n = tree.nodes[pd.node];
+				SegmentDesc d;
+				d.start = n.leaf_start;
+				d.count = n.leaf_count;
+				d.coff = total;
+				Vec3d size = n.max - n.min;
+				d.min[0] = n.min.x; d.min[1] = n.min.y; d.min[2] = n.min.z;
+				d.size[0] = size.x; d.size[1] = size.y; d.size[2] = size.z;
+				segs.push_back(d);
+				total += d.count;
+			}
+			if (total > cand_cap) {
+				if (d_cands) mem.free(d_cands);
+				cand_cap = total;
+				d_cands = mem.alloc<NodeCand>(cand_cap);
+			}
+			SegmentDesc* d_segs = upload(segs, mem);
+			PCG_CUDA(cudaMemsetAsync(d_ncands, 0, 4, stream));
+			launch_octree_round(ids, X, Y, Z, pp, d_segs, (int)segs.size(), total, d_cands, d_ncands, cand_cap, mem);
+			int ncand = download(d_ncands, 1, stream)[0];
+			if (ncand > cand_cap) throw PcgError(PCG_INTERNAL, "octree round overflow");
+			auto cands = download(d_cands, (size_t)ncand, stream);
+			mem.free(d_segs);
+			// deterministic handling order: by segment, then path
+			std::sort(cands.begin(), cands.end(), [](const NodeCand& a, const NodeCand& b) {
+				if (a.seg != b.seg) return a.seg < b.seg;
+				if (a.level != b.level) return a.level < b.level;
+				return a.path < b.path;
+			});
+			std::vector<Pending> next;
+			std::vector<int64_t> seg_depth(segs.size(), 0);
+			for (auto& c : cands) {
+				int sn = pending[c.seg].node;
+				int cur = sn;
+				for (int l = 0; l < c.level; l++) {
+					int digit = (c.path >> (3 * (c.level - 1 - l))) & 7;
+					cur = tree.child_of(cur, digit, tree.nodes[sn].chunk);
+				}
+				TNode& rn = tree.nodes[cur];
+				rn.leaf_start = tree.nodes[sn].leaf_start + c.start;
+				rn.leaf_count = c.count;
+				octree_depth = std::max<int64_t>(octree_depth, rn.depth);
+				if (rn.leaf_count > kMaxNodePoints) next.push_back({cur, tree.nodes[sn].leaf_count});
+			}
+			// the split node's own points now live in its children (or in the
+			// node itself when createNodes kept it whole)
+			for (auto& pd : pending) {
+				TNode& n = tree.nodes[pd.node];
+				if (n.has_children()) n.leaf_count = 0;
+			}
+			// duplicate handling for nodes that did not split
+			std::vector<Pending> refined;
+			for (auto& nx : next) {
+				TNode& sub = tree.nodes[nx.node];
+				if (sub.leaf_count == nx.parent_count) {
+					int64_t uniq = count_unique_positions(ids + sub.leaf_start, sub.leaf_count, X, Y, Z, mem);
+					int64_t dups = sub.leaf_count - uniq;
+					if (dups >= kMaxNodePoints / 2) {
+						// the reference keeps the first `uniq` records (indexer.cpp:1088-1090)
+						sub.leaf_count = uniq;
+					}
+				}
+				if (sub.leaf_count >= kMaxNodePoints) refined.push_back({nx.node, sub.leaf_count});
+			}
+			pending.swap(refined);
+		}
+		if (d_cands) mem.free(d_cands);
+		mem.free(d_ncands);
+		return octree_depth;
+	}
+
+	// Chunk list and LUT from a count grid of G^3 cells (createLUT,
+	// chunker_countsort_laszip.cpp:1074-1204): the chunks in chunk
+	// file-name order (the order of the pinned reference's sorted directory
+	// scan, indexer.cpp:149), and lut[cell] = index of the chunk covering
+	// the cell in that order, -1 elsewhere (lut: G^3 entries, filled here).
+	std::vector<std::pair<std::string, ChunkCell>> make_chunks(const uint32_t* grid, int G, int64_t max_points_per_chunk, int32_t* lut,
+	                                                           DeviceMem& mem) {
+		const int chunk_cap = 1 << 20;
+		const int64_t cells = (int64_t)G * G * G;
+		ChunkCell* d_chunks = mem.alloc<ChunkCell>(chunk_cap);
+		int32_t* d_nchunks = mem.alloc<int32_t>(1);
+		PCG_CUDA(cudaMemsetAsync(d_nchunks, 0, 4, stream));
+		launch_lut_merge(grid, G, max_points_per_chunk, d_chunks, d_nchunks, chunk_cap, mem);
+		const int nchunks = download(d_nchunks, 1, stream)[0];
+		if (nchunks > chunk_cap) throw PcgError(PCG_INTERNAL, "too many chunks");
+		auto cells_found = download(d_chunks, (size_t)nchunks, stream);
+		std::vector<std::pair<std::string, ChunkCell>> chunks;
+		for (auto& c : cells_found) chunks.push_back({chunk_id(c), c});
+		std::sort(chunks.begin(), chunks.end(), [](const auto& a, const auto& b) { return a.first + ".bin" < b.first + ".bin"; });
+		std::vector<ChunkCell> sorted_cells;
+		for (auto& c : chunks) sorted_cells.push_back(c.second);
+		ChunkCell* d_sorted = upload(sorted_cells, mem);
+		PCG_CUDA(cudaMemsetAsync(lut, 0xff, cells * sizeof(int32_t), stream));
+		launch_lut_fill(d_sorted, nchunks, G, lut, mem);
+		mem.free(d_sorted);
+		mem.free(d_nchunks);
+		mem.free(d_chunks);
+		return chunks;
+	}
+
+	// The distribution of points to chunks (distributePoints,
+	// chunker_countsort_laszip.cpp:837-904, one chunker thread): ids[0..n)
+	// = point indices grouped by chunk, input order inside a chunk (a
+	// stable radix sort by chunk index). chunk_base is subtracted from every
+	// looked-up index (a cloud part holding chunks chunk_base .. + nchunks).
+	// A cell without a chunk sets error[1].
+	// chunk_start (device, nchunks + 1 entries), when given, receives where
+	// every chunk starts in ids.
+	void scatter_chunks(const uint32_t* cell, const int32_t* lut, int64_t n, int nchunks, int chunk_base, uint32_t* ids, int64_t* error,
+	                    DeviceMem& mem, int64_t* chunk_start = nullptr) {
+		uint32_t* chunk_of = mem.alloc<uint32_t>(std::max<int64_t>(n, 1));
+		launch_assign_chunks(cell, lut, n, chunk_base, chunk_of, ids, error, mem);
+		uint32_t* kt = mem.alloc<uint32_t>(std::max<int64_t>(n, 1));
+		uint32_t* vt = mem.alloc<uint32_t>(std::max<int64_t>(n, 1));
+		radix_sort_pairs(chunk_of, ids, kt, vt, n, 0, std::max(1, bits_for((uint64_t)std::max(nchunks - 1, 0))), mem);
+		if (chunk_start) launch_segment_starts(chunk_of, n, nchunks, chunk_start, mem);
+		mem.free(kt);
+		mem.free(vt);
+		mem.free(chunk_of);
+	}
+
 	// Kernel parameters of the decode: the output layout, and per source its
 	// records, coordinate transform and handler byte moves (src_recs: device
 	// pointer of each source's first record). descs / firsts receive the
@@ -705,8 +745,12 @@ struct Converter {
 		return p;
 	}
 
+	// Samples every node of level_nodes (all at one depth). level_cols, when
+	// given, receives the level's packed colours in gather order (every
+	// candidate's averaged colour, poisson_average).
 	void sample_level(Tree& tree, const std::vector<int>& level_nodes, int method, double base_spacing, const PosParamsS& pps,
-	                  const ChunkingOut& co, SampleStats* d_st, GreedyArena& grid_arena, DeviceMem& mem, JobResult& res) {
+	                  const ChunkingOut& co, SampleStats* d_st, GreedyArena& grid_arena, DeviceMem& mem, JobResult& res,
+	                  uint64_t** level_cols = nullptr) {
 		const auto t_level = Clock::now();
 		const double alloc0 = mem.alloc_ms();
 		int sms = 148;
@@ -944,6 +988,7 @@ struct Converter {
 		mem.free(lb.accepted);
 		if (lb.rec) mem.free(lb.rec);
 		if (method != PCG_POISSON_AVERAGE) mem.free(lb.ids);
+		if (level_cols) *level_cols = lb.cols;
 	}
 
 	// The single-threaded reference's completion order (doIndexing,
@@ -1532,6 +1577,205 @@ pcg_status pcg_kernel_decode_count(pcg_ctx* ctx, const void* las, uint64_t size,
 		}
 		PCG_CUDA(cudaMemcpyAsync(grid, d_grid, cells * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
 		PCG_CUDA(cudaStreamSynchronize(stream));
+	});
+}
+
+pcg_status pcg_kernel_lut(pcg_ctx* ctx, const uint32_t* grid, int32_t grid_size, int64_t max_points_per_chunk, int32_t* lut_out,
+                          pcg_chunk* chunks_out, int64_t chunk_capacity, int32_t* num_chunks) {
+	if (!ctx || !grid || !lut_out || !num_chunks) return PCG_BAD_INPUT;
+	if (grid_size < 2 || grid_size > 512 || (grid_size & (grid_size - 1)) != 0 || max_points_per_chunk < 0) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->mtx);
+	return guarded(ctx, [&] {
+		PCG_CUDA(cudaSetDevice(ctx->conv.device));
+		const cudaStream_t stream = ctx->conv.stream;
+		pcg::DeviceMem mem(stream, ctx->conv.arena.get());
+		const int64_t cells = (int64_t)grid_size * grid_size * grid_size;
+		uint32_t* d_grid = mem.alloc<uint32_t>(cells);
+		int32_t* d_lut = mem.alloc<int32_t>(cells);
+		PCG_CUDA(cudaMemcpyAsync(d_grid, grid, cells * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+		const auto chunks = ctx->conv.make_chunks(d_grid, grid_size, max_points_per_chunk, d_lut, mem);
+		*num_chunks = (int32_t)chunks.size();
+		if ((int64_t)chunks.size() > chunk_capacity || (!chunks.empty() && !chunks_out))
+			throw pcg::PcgError(PCG_BAD_INPUT, "more chunks than chunk_capacity");
+		for (size_t k = 0; k < chunks.size(); k++) {
+			pcg_chunk c{};
+			std::snprintf(c.id, sizeof(c.id), "%s", chunks[k].first.c_str());
+			c.level = chunks[k].second.level;
+			c.x = chunks[k].second.x;
+			c.y = chunks[k].second.y;
+			c.z = chunks[k].second.z;
+			c.count = chunks[k].second.count;
+			chunks_out[k] = c;
+		}
+		PCG_CUDA(cudaMemcpyAsync(lut_out, d_lut, cells * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+		PCG_CUDA(cudaStreamSynchronize(stream));
+	});
+}
+
+pcg_status pcg_kernel_scatter(pcg_ctx* ctx, const uint32_t* cell, int64_t n, const int32_t* lut, int32_t grid_size, int32_t num_chunks,
+                              uint32_t* ids_out, int64_t* chunk_start) {
+	if (!ctx || !lut || !chunk_start || n < 0 || n >= (int64_t(1) << 31) || num_chunks < 0) return PCG_BAD_INPUT;
+	if (n > 0 && (!cell || !ids_out)) return PCG_BAD_INPUT;
+	if (grid_size < 2 || grid_size > 512 || (grid_size & (grid_size - 1)) != 0) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->mtx);
+	return guarded(ctx, [&] {
+		PCG_CUDA(cudaSetDevice(ctx->conv.device));
+		const cudaStream_t stream = ctx->conv.stream;
+		pcg::DeviceMem mem(stream, ctx->conv.arena.get());
+		const int64_t cells = (int64_t)grid_size * grid_size * grid_size;
+		// cells beyond the grid would index past the LUT
+		for (int64_t i = 0; i < n; i++)
+			if (cell[i] >= (uint64_t)cells) throw pcg::PcgError(PCG_BAD_INPUT, "cell index outside the grid");
+		uint32_t* d_cell = mem.alloc<uint32_t>(std::max<int64_t>(n, 1));
+		int32_t* d_lut = mem.alloc<int32_t>(cells);
+		uint32_t* d_ids = mem.alloc<uint32_t>(std::max<int64_t>(n, 1));
+		int64_t* d_start = mem.alloc<int64_t>((size_t)num_chunks + 1);
+		int64_t* d_err = mem.alloc<int64_t>(2);
+		PCG_CUDA(cudaMemsetAsync(d_err, 0, 16, stream));
+		if (n > 0) PCG_CUDA(cudaMemcpyAsync(d_cell, cell, n * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+		PCG_CUDA(cudaMemcpyAsync(d_lut, lut, cells * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+		ctx->conv.scatter_chunks(d_cell, d_lut, n, num_chunks, 0, d_ids, d_err, mem, d_start);
+		if (n == 0) {
+			for (int32_t k = 0; k <= num_chunks; k++) chunk_start[k] = 0;
+			return;
+		}
+		const auto err = pcg::download(d_err, 2, stream);
+		if (err[1]) throw pcg::PcgError(PCG_INTERNAL, "point " + std::to_string(err[1] - 1) + ": its cell belongs to no chunk");
+		PCG_CUDA(cudaMemcpyAsync(ids_out, d_ids, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+		PCG_CUDA(cudaMemcpyAsync(chunk_start, d_start, ((size_t)num_chunks + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+		PCG_CUDA(cudaStreamSynchronize(stream));
+	});
+}
+
+pcg_status pcg_kernel_octree(pcg_ctx* ctx, const int32_t* X, const int32_t* Y, const int32_t* Z, int64_t n, const double* scale,
+                             const double* offset, const double* box_min, const double* box_max, const char* root_name,
+                             uint32_t* order_out, pcg_octree_node* nodes_out, int64_t node_capacity, int64_t* num_nodes,
+                             int64_t* octree_depth) {
+	if (!ctx || !scale || !offset || !box_min || !box_max || !root_name || !num_nodes || !octree_depth) return PCG_BAD_INPUT;
+	if (n < 0 || n >= (int64_t(1) << 31) || (n > 0 && (!X || !Y || !Z || !order_out))) return PCG_BAD_INPUT;
+	if (root_name[0] != 'r' || std::strlen(root_name) > 24) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->mtx);
+	return guarded(ctx, [&] {
+		PCG_CUDA(cudaSetDevice(ctx->conv.device));
+		const cudaStream_t stream = ctx->conv.stream;
+		pcg::DeviceMem mem(stream, ctx->conv.arena.get());
+		pcg::Tree tree;
+		tree.add(root_name, -1, pcg::Vec3d{box_min[0], box_min[1], box_min[2]}, pcg::Vec3d{box_max[0], box_max[1], box_max[2]});
+		tree.nodes[0].chunk = 0;
+		tree.nodes[0].chunk_root = true;
+		tree.nodes[0].leaf_start = 0;
+		tree.nodes[0].leaf_count = n;
+		const size_t nb = (size_t)std::max<int64_t>(n, 1);
+		int32_t* d_X = mem.alloc<int32_t>(nb);
+		int32_t* d_Y = mem.alloc<int32_t>(nb);
+		int32_t* d_Z = mem.alloc<int32_t>(nb);
+		std::vector<uint32_t> iota((size_t)n);
+		for (int64_t i = 0; i < n; i++) iota[i] = (uint32_t)i;
+		uint32_t* d_ids = pcg::upload(iota, mem);
+		if (n > 0) {
+			PCG_CUDA(cudaMemcpyAsync(d_X, X, n * 4, cudaMemcpyHostToDevice, stream));
+			PCG_CUDA(cudaMemcpyAsync(d_Y, Y, n * 4, cudaMemcpyHostToDevice, stream));
+			PCG_CUDA(cudaMemcpyAsync(d_Z, Z, n * 4, cudaMemcpyHostToDevice, stream));
+		}
+		pcg::PosParams pp;
+		for (int a = 0; a < 3; a++) { pp.scale[a] = scale[a]; pp.offset[a] = offset[a]; }
+		*octree_depth = ctx->conv.refine_octree(tree, {0}, d_ids, d_X, d_Y, d_Z, pp, mem);
+		std::vector<int> order(tree.nodes.size());
+		for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+		std::sort(order.begin(), order.end(), [&](int a, int b) { return tree.nodes[a].name < tree.nodes[b].name; });
+		*num_nodes = (int64_t)order.size();
+		if ((int64_t)order.size() > node_capacity || !nodes_out) throw pcg::PcgError(PCG_BAD_INPUT, "more nodes than node_capacity");
+		for (size_t k = 0; k < order.size(); k++) {
+			const pcg::TNode& t = tree.nodes[order[k]];
+			pcg_octree_node o{};
+			std::snprintf(o.name, sizeof(o.name), "%s", t.name.c_str());
+			o.is_leaf = t.has_children() ? 0 : 1;
+			o.start = o.is_leaf ? t.leaf_start : 0;
+			o.count = o.is_leaf ? t.leaf_count : 0;
+			nodes_out[k] = o;
+		}
+		if (n > 0) PCG_CUDA(cudaMemcpyAsync(order_out, d_ids, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+		PCG_CUDA(cudaStreamSynchronize(stream));
+	});
+}
+
+pcg_status pcg_kernel_accept(pcg_ctx* ctx, int32_t method, const int32_t* X, const int32_t* Y, const int32_t* Z, const uint8_t* child,
+                             const uint16_t* rgb, int64_t n, const double* scale, const double* offset, const double* box_min,
+                             const double* box_max, double spacing, uint8_t* accepted_out, uint16_t* rgb_out) {
+	if (!ctx || !scale || !offset || !box_min || !box_max || method < 0 || method > 2) return PCG_BAD_INPUT;
+	if (n < 0 || n >= (int64_t(1) << 31) || (n > 0 && (!X || !Y || !Z || !child || !accepted_out))) return PCG_BAD_INPUT;
+	if (method == PCG_POISSON_AVERAGE && n > 0 && !rgb) return PCG_BAD_INPUT;
+	if (!(spacing > 0.0)) return PCG_BAD_INPUT;
+	for (int64_t i = 0; i < n; i++)
+		if (child[i] > 7 || (i > 0 && child[i] < child[i - 1])) return PCG_BAD_INPUT;
+	std::lock_guard<std::mutex> lk(ctx->mtx);
+	return guarded(ctx, [&] {
+		if (n == 0) return;
+		PCG_CUDA(cudaSetDevice(ctx->conv.device));
+		const cudaStream_t stream = ctx->conv.stream;
+		pcg::DeviceMem mem(stream, ctx->conv.arena.get());
+		// the node "r" (level 0, so baseSpacing = spacing) with one leaf per
+		// child holding that child's candidates
+		pcg::Tree tree;
+		tree.add("r", -1, pcg::Vec3d{box_min[0], box_min[1], box_min[2]}, pcg::Vec3d{box_max[0], box_max[1], box_max[2]});
+		int64_t first = 0;
+		for (int64_t i = 1; i <= n; i++) {
+			if (i < n && child[i] == child[first]) continue;
+			const int c = tree.child_of(0, child[first], 0);
+			tree.nodes[c].leaf_start = first;
+			tree.nodes[c].leaf_count = i - first;
+			first = i;
+		}
+		pcg::ChunkingOut co{};
+		co.X = mem.alloc<int32_t>(n);
+		co.Y = mem.alloc<int32_t>(n);
+		co.Z = mem.alloc<int32_t>(n);
+		PCG_CUDA(cudaMemcpyAsync(co.X, X, n * 4, cudaMemcpyHostToDevice, stream));
+		PCG_CUDA(cudaMemcpyAsync(co.Y, Y, n * 4, cudaMemcpyHostToDevice, stream));
+		PCG_CUDA(cudaMemcpyAsync(co.Z, Z, n * 4, cudaMemcpyHostToDevice, stream));
+		std::vector<uint32_t> iota((size_t)n);
+		for (int64_t i = 0; i < n; i++) iota[i] = (uint32_t)i;
+		uint32_t* d_ids = pcg::upload(iota, mem);
+		uint64_t* d_cols = nullptr;
+		if (method == PCG_POISSON_AVERAGE) {
+			std::vector<uint64_t> cols((size_t)n);
+			for (int64_t i = 0; i < n; i++)
+				cols[i] = (uint64_t)rgb[3 * i] | (uint64_t)rgb[3 * i + 1] << 16 | (uint64_t)rgb[3 * i + 2] << 32;
+			d_cols = pcg::upload(cols, mem);
+		}
+		int4* d_rec = nullptr;
+		if (method != PCG_RANDOM) {
+			d_rec = mem.alloc<int4>(n);
+			pcg::launch_gather_records(d_ids, n, co.X, co.Y, co.Z, d_rec, mem);
+		}
+		for (auto& t : tree.nodes) {
+			if (t.has_children()) continue;
+			t.buf_ids = d_ids + t.leaf_start;
+			t.buf_cols = d_cols ? d_cols + t.leaf_start : nullptr;
+			t.buf_rec = d_rec ? d_rec + t.leaf_start : nullptr;
+			t.buf_count = t.leaf_count;
+		}
+		pcg::SampleStats* d_st = mem.alloc<pcg::SampleStats>(1);
+		PCG_CUDA(cudaMemsetAsync(d_st, 0, sizeof(pcg::SampleStats), stream));
+		pcg::GreedyArena grid_arena;
+		pcg::PosParamsS pps;
+		for (int a = 0; a < 3; a++) { pps.scale[a] = scale[a]; pps.offset[a] = offset[a]; }
+		pcg::JobResult res;
+		uint64_t* level_cols = nullptr;
+		ctx->conv.sample_level(tree, {0}, method, spacing, pps, co, d_st, grid_arena, mem, res, &level_cols);
+		const pcg::TNode& root = tree.nodes[0];
+		const auto acc = pcg::download(root.buf_ids, (size_t)root.buf_count, stream);
+		if (pcg::download(d_st, 1, stream)[0].timeouts) throw pcg::PcgError(PCG_TIMEOUT, "a bounded device loop gave up");
+		std::memset(accepted_out, 0, (size_t)n);
+		for (uint32_t id : acc) accepted_out[id] = 1;
+		if (method == PCG_POISSON_AVERAGE && rgb_out) {
+			const auto cols = pcg::download(level_cols, (size_t)n, stream);
+			for (int64_t i = 0; i < n; i++) {
+				rgb_out[3 * i] = (uint16_t)(cols[i] & 0xffff);
+				rgb_out[3 * i + 1] = (uint16_t)((cols[i] >> 16) & 0xffff);
+				rgb_out[3 * i + 2] = (uint16_t)((cols[i] >> 32) & 0xffff);
+			}
+		}
 	});
 }
 

@@ -48,6 +48,15 @@ class Oracle:
         lib.pcref_decode_count.argtypes = [ctypes.c_void_p, ctypes.c_uint64] + [ctypes.c_void_p] * 5 + [
             ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_char_p]
         lib.pcref_std_sort_perm.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+        lib.pcref_lut.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+        lib.pcref_scatter.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+        lib.pcref_octree.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] + [ctypes.c_void_p] * 4 + [
+            ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+            ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+        lib.pcref_accept.argtypes = [ctypes.c_int32] + [ctypes.c_void_p] * 5 + [ctypes.c_int64] + [ctypes.c_void_p] * 4 + [
+            ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
         lib.pcref_std_shuffle.argtypes = [ctypes.c_int64, ctypes.c_uint32, ctypes.c_void_p]
         self.lib = lib
 
@@ -108,6 +117,66 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(err.value.decode())
         return X[:n], Y[:n], Z[:n], cell[:n], grid[: gs.value ** 3]
+
+    def lut(self, grid, grid_size: int, max_points_per_chunk: int):
+        """createLUT of a count grid: (chunks, lut) like Context.lut."""
+        g = np.ascontiguousarray(grid, dtype=np.int64)
+        lut = np.empty(grid_size ** 3, np.int32)
+        cap = 1 << 16
+        ids = ctypes.create_string_buffer(16 * cap)
+        info = np.empty(5 * cap, np.int64)
+        num = ctypes.c_int64()
+        if self.lib.pcref_lut(g.ctypes.data, grid_size, max_points_per_chunk, lut.ctypes.data, ids, info.ctypes.data, cap,
+                              ctypes.byref(num)) != 0:
+            raise RuntimeError("too many chunks")
+        out = []
+        for k in range(num.value):
+            name = ids.raw[16 * k: 16 * k + 16].split(b"\0")[0].decode()
+            out.append((name,) + tuple(int(v) for v in info[5 * k: 5 * k + 5]))
+        return out, lut
+
+    def scatter(self, cell, lut, num_chunks: int):
+        c = np.ascontiguousarray(cell, dtype=np.uint32)
+        lt = np.ascontiguousarray(lut, dtype=np.int32)
+        ids = np.empty(max(c.shape[0], 1), np.uint32)
+        start = np.empty(num_chunks + 1, np.int64)
+        if self.lib.pcref_scatter(c.ctypes.data, c.shape[0], lt.ctypes.data, num_chunks, ids.ctypes.data,
+                                  start.ctypes.data) != 0:
+            raise RuntimeError("cell without chunk")
+        return ids[: c.shape[0]], start
+
+    def octree(self, X, Y, Z, scale, offset, box_min, box_max, root_name: str = "r"):
+        arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in (X, Y, Z)]
+        vecs = [np.ascontiguousarray(v, dtype=np.float64) for v in (scale, offset, box_min, box_max)]
+        n = arrs[0].shape[0]
+        order = np.empty(max(n, 1), np.uint32)
+        cap = 1 << 16
+        names = ctypes.create_string_buffer(32 * cap)
+        info = np.empty(3 * cap, np.int64)
+        num, depth = ctypes.c_int64(), ctypes.c_int64()
+        if self.lib.pcref_octree(*[a.ctypes.data for a in arrs], n, *[v.ctypes.data for v in vecs], root_name.encode(),
+                                 order.ctypes.data, names, info.ctypes.data, cap, ctypes.byref(num), ctypes.byref(depth)) != 0:
+            raise RuntimeError("too many nodes")
+        nodes = []
+        for k in range(num.value):
+            nm = names.raw[32 * k: 32 * k + 32].split(b"\0")[0].decode()
+            nodes.append((nm, int(info[3 * k]), int(info[3 * k + 1]), int(info[3 * k + 2])))
+        return order[:n], nodes, depth.value
+
+    def accept(self, method: str, X, Y, Z, child, scale, offset, box_min, box_max, spacing: float, rgb=None):
+        m = {"poisson": 0, "poisson_average": 1, "random": 2}[method]
+        arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in (X, Y, Z)]
+        ch = np.ascontiguousarray(child, dtype=np.uint8)
+        vecs = [np.ascontiguousarray(v, dtype=np.float64) for v in (scale, offset, box_min, box_max)]
+        n = ch.shape[0]
+        acc = np.empty(max(n, 1), np.uint8)
+        col_in = np.ascontiguousarray(rgb, dtype=np.uint16) if rgb is not None else None
+        col_out = np.empty((max(n, 1), 3), np.uint16) if m == 1 else None
+        if self.lib.pcref_accept(m, *[a.ctypes.data for a in arrs], ch.ctypes.data,
+                                 col_in.ctypes.data if col_in is not None else None, n, *[v.ctypes.data for v in vecs],
+                                 spacing, acc.ctypes.data, col_out.ctypes.data if col_out is not None else None) != 0:
+            raise RuntimeError("children not in order")
+        return acc[:n], (col_out[:n] if col_out is not None else None)
 
     def sort_perm(self, keys):
         k = np.ascontiguousarray(keys, dtype=np.float64)
