@@ -58,14 +58,32 @@ typedef enum pcg_form {
 	PCG_FORM_PLAIN = 1    /* one launch per node, every neighbour test FP64  */
 } pcg_form;
 
+/* Where the point records of a conversion in parts live (pcg_opts.records). */
+typedef enum pcg_records {
+	PCG_RECORDS_AUTO = 0,      /* resident on the device when they fit beside
+	                              one part's working set, else streamed      */
+	PCG_RECORDS_RESIDENT = 1,  /* copied to the device once (the first pass)  */
+	PCG_RECORDS_STREAMED = 2   /* streamed from host memory again for every
+	                              part                                        */
+} pcg_records;
+
 typedef struct pcg_opts {
 	int32_t device;        /* CUDA device ordinal                            */
 	uint32_t random_seed;  /* seed of the random sampler's leaf shuffle; the
 	                          pinned reference uses 1592614637               */
 	int32_t form;          /* pcg_form                                        */
-	int32_t reserved;
+	int32_t records;       /* pcg_records: record placement of conversions in
+	                          parts                                           */
 	void* stream;          /* cudaStream_t for all device work, or NULL for a
 	                          stream owned by the context                     */
+	/* Conversion in parts (clouds beyond the device's working set, the
+	   reference's out-of-core chunking + indexing, chunker_countsort_laszip.
+	   cpp:1206-1261, indexer.cpp:181-281): a job of one uncompressed LAS
+	   source with more points than group_points is indexed in parts of
+	   consecutive chunks of at most group_points points (a chunk larger than
+	   that is a part by itself). 0 = parts only when the whole cloud would
+	   not fit the device, sized from its free memory. */
+	int64_t group_points;
 } pcg_opts;
 
 enum {
@@ -131,6 +149,14 @@ typedef struct pcg_stats {
 	int64_t cluster_nodes;        /* nodes accepted by a cluster of CTAs    */
 	double ms_decode;             /* LAZ decode of the job's .laz sources   */
 	int64_t laz_chunks;           /* LASzip chunks decoded                  */
+	int64_t device_peak_bytes;    /* high-water mark of the job's device
+	                                 allocations                            */
+	int64_t parts;                /* parts of a conversion in parts, else 0 */
+	int64_t survivors;            /* chunk-root points carried from the
+	                                 parts to the levels above them          */
+	int64_t records_resident;     /* 1: the records stayed on the device
+	                                 between the passes of a conversion in
+	                                 parts                                   */
 } pcg_stats;
 
 /* One completed node: what the reference's hierarchy flusher records for it
@@ -142,9 +168,20 @@ typedef struct pcg_node {
 	uint64_t byte_size;
 } pcg_node;
 
+/* One piece of octree.bin: the file is its pieces back to back. */
+typedef struct pcg_octree_part {
+	const uint8_t* data;   /* host memory (owned by the result)             */
+	uint64_t size;
+} pcg_octree_part;
+
 typedef struct pcg_result {
 	uint8_t* octree;       uint64_t octree_size;     /* host memory unless the
-	                                                    job asked for device */
+	                                                    job asked for device;
+	                                                    NULL for a conversion
+	                                                    in parts, whose
+	                                                    octree.bin is
+	                                                    octree_parts[] (size
+	                                                    still the total)     */
 	uint8_t* hierarchy;    uint64_t hierarchy_size;
 	char* metadata;        uint64_t metadata_size;   /* NUL terminated */
 	pcg_stats stats;
@@ -152,6 +189,11 @@ typedef struct pcg_result {
 	                          the payloads in octree.bin); NULL if the host had
 	                          no memory for the list */
 	uint64_t num_nodes;
+	pcg_octree_part* octree_parts; /* octree.bin in pieces, in file order: one
+	                          piece (octree itself) for a conversion in one
+	                          piece, one per part plus one for the levels
+	                          above the parts otherwise                      */
+	uint64_t num_octree_parts;
 } pcg_result;
 
 typedef struct pcg_ctx pcg_ctx;

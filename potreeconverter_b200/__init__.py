@@ -22,6 +22,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpcgpu.so")
 
 METHODS = {"poisson": 0, "poisson_average": 1, "random": 2}
+RECORDS = {"auto": 0, "resident": 1, "streamed": 2}
 FORMS = {"batched": 0, "plain": 1}
 PINNED_SEED = 1592614637
 
@@ -37,7 +38,11 @@ class PcgError(RuntimeError):
 
 class _Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("random_seed", ctypes.c_uint32), ("form", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("stream", ctypes.c_void_p)]
+                ("records", ctypes.c_int32), ("stream", ctypes.c_void_p), ("group_points", ctypes.c_int64)]
+
+
+class _Part(ctypes.Structure):
+    _fields_ = [("data", ctypes.POINTER(ctypes.c_uint8)), ("size", ctypes.c_uint64)]
 
 
 class _Source(ctypes.Structure):
@@ -75,7 +80,9 @@ class _Stats(ctypes.Structure):
                 ("ms_sort", ctypes.c_double), ("ms_greedy", ctypes.c_double), ("sampled_nodes", ctypes.c_int64),
                 ("candidates", ctypes.c_int64), ("replayed_nodes", ctypes.c_int64),
                 ("replayed_candidates", ctypes.c_int64), ("ms_lists", ctypes.c_double), ("list_entries", ctypes.c_int64),
-                ("cluster_nodes", ctypes.c_int64), ("ms_decode", ctypes.c_double), ("laz_chunks", ctypes.c_int64)]
+                ("cluster_nodes", ctypes.c_int64), ("ms_decode", ctypes.c_double), ("laz_chunks", ctypes.c_int64),
+                ("device_peak_bytes", ctypes.c_int64), ("parts", ctypes.c_int64), ("survivors", ctypes.c_int64),
+                ("records_resident", ctypes.c_int64)]
 
 
 class _Node(ctypes.Structure):
@@ -87,7 +94,8 @@ class _Result(ctypes.Structure):
     _fields_ = [("octree", ctypes.POINTER(ctypes.c_uint8)), ("octree_size", ctypes.c_uint64),
                 ("hierarchy", ctypes.POINTER(ctypes.c_uint8)), ("hierarchy_size", ctypes.c_uint64),
                 ("metadata", ctypes.c_char_p), ("metadata_size", ctypes.c_uint64), ("stats", _Stats),
-                ("nodes", ctypes.POINTER(_Node)), ("num_nodes", ctypes.c_uint64)]
+                ("nodes", ctypes.POINTER(_Node)), ("num_nodes", ctypes.c_uint64),
+                ("octree_parts", ctypes.POINTER(_Part)), ("num_octree_parts", ctypes.c_uint64)]
 
 
 class _Chunk(ctypes.Structure):
@@ -183,7 +191,11 @@ def _copy_out(ptr, size: int) -> bytes:
 
 
 def _take(lib, res: _Result) -> Conversion:
-    octree = _copy_out(res.octree, res.octree_size)
+    if res.octree or res.num_octree_parts <= 1:
+        octree = _copy_out(res.octree, res.octree_size)
+    else:  # a conversion in parts: octree.bin is its pieces back to back
+        octree = b"".join(_copy_out(res.octree_parts[i].data, res.octree_parts[i].size)
+                          for i in range(res.num_octree_parts))
     hierarchy = _copy_out(res.hierarchy, res.hierarchy_size)
     metadata = ctypes.string_at(res.metadata, res.metadata_size).decode() if res.metadata_size else ""
     stats = {name: getattr(res.stats, name) for name, _ in _Stats._fields_}
@@ -196,9 +208,13 @@ def _take(lib, res: _Result) -> Conversion:
 class Context:
     """A device context (pcg_create/pcg_destroy)."""
 
-    def __init__(self, device: int = 0, seed: int = PINNED_SEED, form: str = "batched", stream: int | None = None):
+    def __init__(self, device: int = 0, seed: int = PINNED_SEED, form: str = "batched", stream: int | None = None,
+                 group_points: int = 0, records: str = "auto"):
+        """group_points > 0 converts one-file jobs of more points in parts
+        of at most that many points; records ("auto", "resident",
+        "streamed") places the records of such conversions."""
         self._lib = load_library()
-        opts = _Opts(device, seed, FORMS[form], 0, stream)
+        opts = _Opts(device, seed, FORMS[form], RECORDS[records], stream, group_points)
         h = ctypes.c_void_p()
         st = self._lib.pcg_create(ctypes.byref(h), ctypes.byref(opts))
         if st != 0:
@@ -278,6 +294,23 @@ class Context:
         if st != 0:
             raise self._err(st)
         return _take(self._lib, res)
+
+    def write_files(self, las, out_dir: str, method: str = "poisson", name: str = "cloud", attributes=None) -> dict:
+        """Converts and writes octree.bin, hierarchy.bin and metadata.json
+        into out_dir (pcg_write_files); returns the statistics."""
+        keep = []
+        job = self._job(las, method, name, "", keep, attributes=attributes)
+        res = _Result()
+        st = self._lib.pcg_convert(self._h, ctypes.byref(job), ctypes.byref(res))
+        if st != 0:
+            raise self._err(st)
+        try:
+            st = self._lib.pcg_write_files(ctypes.byref(res), out_dir.encode())
+            if st != 0:
+                raise PcgError(st, f"cannot write into {out_dir}")
+            return {n: getattr(res.stats, n) for n, _ in _Stats._fields_}
+        finally:
+            self._lib.pcg_result_free(ctypes.byref(res))
 
     def convert_stats(self, las, method: str = "poisson", name: str = "cloud", attributes=None) -> dict:
         """Converts like :meth:`convert` (octree.bin lands in pinned host

@@ -46,6 +46,25 @@ __device__ void flush_int(AttrStatsDev* st, int comp, const IntRange& r, unsigne
 	}
 }
 
+// The count-grid cell of a quantized point (countPointsInCells, :232-257):
+// unit-cube coordinates from the output transform, out-of-box test, cell
+// index ix + iy G + iz G^2. False when the point lies outside the box.
+__device__ __forceinline__ bool grid_cell(const DecodeParams& p, int32_t X, int32_t Y, int32_t Z, uint32_t& cell) {
+	const int G = p.grid;
+	const double dG = (double)G;
+	double ux = ((double)X * p.pos_scale[0] + p.pos_offset[0] - p.cmin[0]) / p.csize;
+	double uy = ((double)Y * p.pos_scale[1] + p.pos_offset[1] - p.cmin[1]) / p.csize;
+	double uz = ((double)Z * p.pos_scale[2] + p.pos_offset[2] - p.cmin[2]) / p.csize;
+	bool in_box = ux >= 0.0 && uy >= 0.0 && uz >= 0.0 && ux <= 1.0 && uy <= 1.0 && uz <= 1.0;
+	cell = 0;
+	if (!in_box) return false;
+	int64_t ix = (int64_t)dmin(dG * ux, dG - 1.0);
+	int64_t iy = (int64_t)dmin(dG * uy, dG - 1.0);
+	int64_t iz = (int64_t)dmin(dG * uz, dG - 1.0);
+	cell = (uint32_t)(ix + iy * G + iz * (int64_t)G * G);
+	return true;
+}
+
 // One thread per point (grid-stride). Writes the quantized position SoA and
 // the count-grid cell, counts into the grid with warp-aggregated atomics and
 // reduces attribute min/max (in registers, then shared memory, then one
@@ -69,27 +88,14 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodePara
 	r_int.init(); r_ret.init(); r_nret.init(); r_cls.init(); r_sar.init(); r_user.init(); r_psid.init(); r_r.init(); r_g.init(); r_b.init();
 
 	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-	const int G = p.grid;
-	const double dG = (double)G;
 	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride) with_source<kMulti>(p, i, [&](const SourceDesc& sd) {
 		const uint8_t* r = sd.recs + (i - sd.first) * sd.rec_len;
 		double x, y, z;
 		int32_t X, Y, Z;
 		quantize_record(p, sd, r, x, y, z, X, Y, Z);
-		// unit cube coordinates and cell (:232-257)
-		double ux = ((double)X * p.pos_scale[0] + p.pos_offset[0] - p.cmin[0]) / p.csize;
-		double uy = ((double)Y * p.pos_scale[1] + p.pos_offset[1] - p.cmin[1]) / p.csize;
-		double uz = ((double)Z * p.pos_scale[2] + p.pos_offset[2] - p.cmin[2]) / p.csize;
-		bool in_box = ux >= 0.0 && uy >= 0.0 && uz >= 0.0 && ux <= 1.0 && uy <= 1.0 && uz <= 1.0;
-		uint32_t cell = 0;
-		if (!in_box) {
-			atomicCAS((unsigned long long*)&out.error[0], 0ull, (unsigned long long)(i + 1));
-		} else {
-			int64_t ix = (int64_t)dmin(dG * ux, dG - 1.0);
-			int64_t iy = (int64_t)dmin(dG * uy, dG - 1.0);
-			int64_t iz = (int64_t)dmin(dG * uz, dG - 1.0);
-			cell = (uint32_t)(ix + iy * G + iz * (int64_t)G * G);
-		}
+		uint32_t cell;
+		const bool in_box = grid_cell(p, X, Y, Z, cell);
+		if (!in_box) atomicCAS((unsigned long long*)&out.error[0], 0ull, (unsigned long long)(i + 1));
 		out.X[i] = X;
 		out.Y[i] = Y;
 		out.Z[i] = Z;
@@ -252,6 +258,94 @@ __global__ void assign_kernel(const uint32_t* __restrict__ cell, const int32_t* 
 	ids[i] = (uint32_t)i;
 }
 
+// ---------------------------------------------------- parts of a large cloud
+// A part of a cloud is the run of chunks k0 .. k1 - 1; its points are
+// selected from the records of one source in input order (the order the
+// reference's single chunker thread appends them to the chunk files).
+constexpr int kSelThreads = 256;
+constexpr int kSelItems = 8;
+constexpr int64_t kSelTile = (int64_t)kSelThreads * kSelItems;
+
+__device__ __forceinline__ bool in_part(const DecodeParams& p, const uint8_t* r, const int32_t* __restrict__ lut, int k0, int k1) {
+	double x, y, z;
+	int32_t X, Y, Z;
+	quantize_record(p, p.src0, r, x, y, z, X, Y, Z);
+	uint32_t cell;
+	if (!grid_cell(p, X, Y, Z, cell)) return false;
+	const int c = __ldg(lut + cell);
+	return c >= k0 && c < k1;
+}
+
+// points of the part among recs[0..n), per tile of kSelTile points
+__global__ void __launch_bounds__(kSelThreads) select_count_kernel(DecodeParams p, const uint8_t* __restrict__ recs, int64_t n,
+                                                                  const int32_t* __restrict__ lut, int k0, int k1,
+                                                                  uint32_t* __restrict__ counts) {
+	__shared__ uint32_t s_cnt;
+	if (threadIdx.x == 0) s_cnt = 0;
+	__syncthreads();
+	const int64_t base = (int64_t)blockIdx.x * kSelTile;
+	const int rl = p.src0.rec_len;
+	uint32_t c = 0;
+	for (int e = 0; e < kSelItems; e++) {
+		const int64_t i = base + (int64_t)e * kSelThreads + threadIdx.x;
+		if (i < n && in_part(p, recs + i * rl, lut, k0, k1)) c++;
+	}
+	for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+	if ((threadIdx.x & 31) == 0 && c) atomicAdd(&s_cnt, c);
+	__syncthreads();
+	if (threadIdx.x == 0) counts[blockIdx.x] = s_cnt;
+}
+
+// copies the part's records, in input order, to out at *fill + tile offset
+__global__ void __launch_bounds__(kSelThreads) select_copy_kernel(DecodeParams p, const uint8_t* __restrict__ recs, int64_t n,
+                                                                 const int32_t* __restrict__ lut, int k0, int k1,
+                                                                 const uint32_t* __restrict__ tile_off, const int64_t* __restrict__ fill,
+                                                                 uint8_t* __restrict__ out) {
+	__shared__ uint32_t s_warp[kSelThreads / 32];
+	const int64_t base = (int64_t)blockIdx.x * kSelTile;
+	const int rl = p.src0.rec_len;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	int64_t pos = *fill + tile_off[blockIdx.x];
+	for (int e = 0; e < kSelItems; e++) {
+		const int64_t i = base + (int64_t)e * kSelThreads + threadIdx.x;
+		const bool f = i < n && in_part(p, recs + i * rl, lut, k0, k1);
+		const unsigned ballot = __ballot_sync(0xffffffffu, f);
+		if (lane == 0) s_warp[warp] = __popc(ballot);
+		__syncthreads();
+		uint32_t before = 0, total = 0;
+		for (int w = 0; w < kSelThreads / 32; w++) {
+			const uint32_t v = s_warp[w];
+			before += w < warp ? v : 0;
+			total += v;
+		}
+		if (f) {
+			const uint8_t* r = recs + i * rl;
+			uint8_t* o = out + (pos + before + __popc(ballot & ((1u << lane) - 1))) * rl;
+			for (int b = 0; b < rl; b++) o[b] = r[b];
+		}
+		pos += total;
+		__syncthreads();
+	}
+}
+
+__global__ void select_advance_kernel(int64_t* fill, const uint32_t* __restrict__ tile_off, int64_t tiles) { *fill += tile_off[tiles]; }
+
+// out_recs[i] = recs[ids[i]], oX/oY/oZ[i] = X/Y/Z[ids[i]]
+__global__ void gather_points_kernel(const uint32_t* __restrict__ ids, int64_t n, const uint8_t* __restrict__ recs, int rec_len,
+                                     const int32_t* __restrict__ X, const int32_t* __restrict__ Y, const int32_t* __restrict__ Z,
+                                     uint8_t* __restrict__ out_recs, int32_t* __restrict__ oX, int32_t* __restrict__ oY,
+                                     int32_t* __restrict__ oZ) {
+	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	const uint32_t id = ids[i];
+	const uint8_t* r = recs + (int64_t)id * rec_len;
+	uint8_t* o = out_recs + i * rec_len;
+	for (int b = 0; b < rec_len; b++) o[b] = r[b];
+	oX[i] = X[id];
+	oY[i] = Y[id];
+	oZ[i] = Z[id];
+}
+
 // starts[k] = first position of key k in the ascending keys[0..n), for every
 // k in 0..num_keys (starts[num_keys] = n); keys absent get the next start
 __global__ void segment_starts_kernel(const uint32_t* __restrict__ keys, int64_t n, int num_keys, int64_t* __restrict__ starts) {
@@ -262,10 +356,45 @@ __global__ void segment_starts_kernel(const uint32_t* __restrict__ keys, int64_t
 	for (int64_t k = lo + 1; k <= hi && k <= num_keys; k++) starts[k] = i;
 }
 
+__global__ void iota_kernel(uint32_t* __restrict__ out, int64_t n) {
+	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = (uint32_t)i;
+}
+
 }  // namespace
+
+void launch_iota(uint32_t* out, int64_t n, DeviceMem& mem) {
+	if (n == 0) return;
+	iota_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(out, n);
+	PCG_LAUNCHED();
+}
 
 void launch_segment_starts(const uint32_t* keys, int64_t n, int num_keys, int64_t* starts, DeviceMem& mem) {
 	segment_starts_kernel<<<(unsigned)ceil_div(n + 1, 256), 256, 0, mem.stream()>>>(keys, n, num_keys, starts);
+	PCG_LAUNCHED();
+}
+
+void launch_select_part(const DecodeParams& p, const uint8_t* recs, int64_t n, const int32_t* lut, int k0, int k1, int64_t* fill,
+                        uint8_t* out, DeviceMem& mem) {
+	if (n == 0) return;
+	const int64_t tiles = ceil_div(n, kSelTile);
+	uint32_t* counts = mem.alloc<uint32_t>(tiles);
+	uint32_t* offs = mem.alloc<uint32_t>(tiles + 1);
+	select_count_kernel<<<(unsigned)tiles, kSelThreads, 0, mem.stream()>>>(p, recs, n, lut, k0, k1, counts);
+	PCG_LAUNCHED();
+	exclusive_scan_u32(counts, offs, tiles, true, mem);
+	select_copy_kernel<<<(unsigned)tiles, kSelThreads, 0, mem.stream()>>>(p, recs, n, lut, k0, k1, offs, fill, out);
+	PCG_LAUNCHED();
+	select_advance_kernel<<<1, 1, 0, mem.stream()>>>(fill, offs, tiles);
+	PCG_LAUNCHED();
+	mem.free(counts);
+	mem.free(offs);
+}
+
+void launch_gather_points(const uint32_t* ids, int64_t n, const uint8_t* recs, int rec_len, const int32_t* X, const int32_t* Y,
+                          const int32_t* Z, uint8_t* out_recs, int32_t* oX, int32_t* oY, int32_t* oZ, DeviceMem& mem) {
+	if (n == 0) return;
+	gather_points_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(ids, n, recs, rec_len, X, Y, Z, out_recs, oX, oY, oZ);
 	PCG_LAUNCHED();
 }
 

@@ -46,7 +46,7 @@ static bool ends_with_ci(const std::string& s, const char* suffix) {  // iEndsWi
 int main(int argc, char** argv) {
 	std::vector<std::string> source, attributes;
 	std::string outdir, method = "poisson", encoding = "DEFAULT", projection;
-	pcg_opts opts{0, 1592614637u, PCG_FORM_BATCHED, 0};
+	pcg_opts opts{0, 1592614637u, PCG_FORM_BATCHED, PCG_RECORDS_AUTO, nullptr, 0};
 	bool in_attributes = false;
 	for (int i = 1; i < argc; i++) {
 		std::string a = argv[i];

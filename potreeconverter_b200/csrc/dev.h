@@ -121,6 +121,7 @@ public:
 		Chunk& c = chunks_[it->second.first];
 		size_t off = static_cast<char*>(p) - c.base, len = it->second.second;
 		live_.erase(it);
+		live_bytes_ -= len;
 		auto nx = c.free.lower_bound(off);
 		if (nx != c.free.end() && off + len == nx->first) {  // merge with the next range
 			len += nx->second;
@@ -158,6 +159,7 @@ public:
 		for (Chunk& c : chunks_) cudaFreeAsync(c.base, stream_);
 		chunks_.clear();
 		live_.clear();
+		live_bytes_ = 0;
 	}
 
 	size_t reserved() const {
@@ -165,6 +167,11 @@ public:
 		for (const Chunk& c : chunks_) r += c.size;
 		return r;
 	}
+	// bytes handed out and not yet freed, and their high-water mark since
+	// the last reset_peak()
+	size_t live_bytes() const { return live_bytes_; }
+	size_t peak_bytes() const { return peak_bytes_; }
+	void reset_peak() { peak_bytes_ = live_bytes_; }
 	cudaStream_t stream() const { return stream_; }
 
 private:
@@ -183,6 +190,8 @@ private:
 			if (len > bytes) c.free[off + bytes] = len - bytes;
 			void* p = c.base + off;
 			live_[p] = {ci, bytes};
+			live_bytes_ += bytes;
+			if (live_bytes_ > peak_bytes_) peak_bytes_ = live_bytes_;
 			return p;
 		}
 		return nullptr;
@@ -193,6 +202,7 @@ private:
 	cudaEvent_t fork_ = nullptr, join_ = nullptr;
 	std::vector<Chunk> chunks_;
 	std::unordered_map<void*, std::pair<size_t, size_t>> live_;  // range -> (chunk, length)
+	size_t live_bytes_ = 0, peak_bytes_ = 0;
 };
 
 // Stream-ordered device allocations owned by one job, from an arena when the

@@ -37,6 +37,16 @@ void launch_lut_fill(const ChunkCell* chunks, int num_chunks, int grid_size, int
 // chunk, or one below chunk_base, sets error[1]
 void launch_assign_chunks(const uint32_t* cell, const int32_t* lut, int64_t n, int chunk_base, uint32_t* chunk_of, uint32_t* ids,
                           int64_t* error, DeviceMem& mem);
+// Appends the records among recs[0..n) (one source, p.src0's layout) whose
+// count-grid cell lies in chunks k0 .. k1 - 1 to out, in input order, at
+// record index *fill onwards; *fill (device) advances by their count.
+void launch_select_part(const DecodeParams& p, const uint8_t* recs, int64_t n, const int32_t* lut, int k0, int k1, int64_t* fill,
+                        uint8_t* out, DeviceMem& mem);
+// out_recs[i] = recs[ids[i]] (rec_len bytes each), oX/oY/oZ[i] = X/Y/Z[ids[i]]
+void launch_gather_points(const uint32_t* ids, int64_t n, const uint8_t* recs, int rec_len, const int32_t* X, const int32_t* Y,
+                          const int32_t* Z, uint8_t* out_recs, int32_t* oX, int32_t* oY, int32_t* oZ, DeviceMem& mem);
+// out[i] = i, i < n
+void launch_iota(uint32_t* out, int64_t n, DeviceMem& mem);
 // starts[k] = first index of key k in ascending keys[0..n), k = 0..num_keys
 // (starts[num_keys] = n; keys < num_keys)
 void launch_segment_starts(const uint32_t* keys, int64_t n, int num_keys, int64_t* starts, DeviceMem& mem);

@@ -30,6 +30,7 @@
 #include <mutex>
 #include <thread>
 #include <unordered_map>
+#include <unistd.h>
 
 #include "../../include/pcgpu.h"
 #include "kernels.h"
@@ -165,7 +166,7 @@ public:
 		if (it == owned_.end()) return false;
 		free_.insert({it->second, p});
 		cached_ += it->second;
-		while (cached_ > kMaxCached && !free_.empty()) {  // drop the largest
+		while (cached_ > max_cached() && !free_.empty()) {  // drop the largest
 			auto last = std::prev(free_.end());
 			cached_ -= last->first;
 			owned_.erase(last->second);
@@ -176,7 +177,16 @@ public:
 	}
 
 private:
-	static constexpr size_t kMaxCached = size_t(8) << 30;
+	// pinned memory kept for reuse: a quarter of the host's memory, at most
+	// 64 GiB (the pieces of a large conversion are reused by the next one)
+	static size_t max_cached() {
+		static const size_t m = [] {
+			const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGE_SIZE);
+			const size_t phys = pages > 0 && page > 0 ? (size_t)pages * (size_t)page : (size_t(32) << 30);
+			return std::max(size_t(8) << 30, std::min(size_t(64) << 30, phys / 4));
+		}();
+		return m;
+	}
 	std::mutex m_;
 	std::multimap<size_t, void*> free_;
 	std::unordered_map<void*, size_t> owned_;
@@ -214,8 +224,119 @@ struct JobResult {
 	uint8_t* octree = nullptr;  // pinned host memory, or device memory
 	uint64_t octree_size = 0;
 	bool octree_on_device = false;
+	// a conversion in parts: octree.bin in pieces (pinned host memory, from
+	// g_pinned), octree stays null
+	std::vector<std::pair<uint8_t*, uint64_t>> parts;
 	pcg_stats stats{};
 	std::vector<HierRecord> nodes;  // completion order
+	void release_parts() {
+		for (auto& pt : parts)
+			if (pt.first && !g_pinned.give(pt.first)) cudaFreeHost(pt.first);
+		parts.clear();
+	}
+};
+
+// Streams the records of one host source to the device in tiles of
+// `tile_points` points on a side stream, ahead of the kernels that read
+// them on the compute stream. Page-locked source memory is copied directly;
+// other memory goes through two pinned staging buffers that host threads
+// fill. With `resident` set, tile t lands in resident + t * tile bytes (the
+// records stay on the device); else in one of two device buffers that
+// alternate between tiles.
+class TileFeeder {
+public:
+	TileFeeder(const uint8_t* host, int64_t n, int rec_len, int64_t tile_points, cudaStream_t compute, uint8_t* resident, DeviceMem& mem)
+	    : host_(host), n_(n), rec_(rec_len), tile_(tile_points), compute_(compute), resident_(resident) {
+		tiles_ = n == 0 ? 0 : (n + tile_ - 1) / tile_;
+		cudaPointerAttributes a{};
+		pinned_ = cudaPointerGetAttributes(&a, host) == cudaSuccess && a.type == cudaMemoryTypeHost;
+		cudaGetLastError();
+		PCG_CUDA(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
+		const size_t tile_bytes = (size_t)tile_ * rec_;
+		for (int b = 0; b < 2; b++) {
+			PCG_CUDA(cudaEventCreateWithFlags(&copied_[b], cudaEventDisableTiming));
+			PCG_CUDA(cudaEventCreateWithFlags(&consumed_[b], cudaEventDisableTiming));
+			PCG_CUDA(cudaEventCreateWithFlags(&staged_[b], cudaEventDisableTiming));
+			if (!resident_ && tiles_ > 0) dev_[b] = mem.alloc<uint8_t>(tile_bytes);
+			if (!pinned_ && tiles_ > 0) {
+				stage_[b] = g_pinned.take(tile_bytes);
+				if (!stage_[b]) throw PcgError(PCG_OOM, "no pinned staging memory");
+			}
+		}
+	}
+	~TileFeeder() {
+		cudaStreamSynchronize(copy_);
+		for (int b = 0; b < 2; b++) {
+			cudaEventDestroy(copied_[b]);
+			cudaEventDestroy(consumed_[b]);
+			cudaEventDestroy(staged_[b]);
+			if (stage_[b]) g_pinned.give(stage_[b]);
+		}
+		cudaStreamDestroy(copy_);
+	}
+	int64_t tiles() const { return tiles_; }
+	int64_t tile_points() const { return tile_; }
+	// Device records of tile t (points first .. first + count); the compute
+	// stream waits for their copy. Tiles are taken in order.
+	const uint8_t* acquire(int64_t t, int64_t& first, int64_t& count) {
+		if (issued_ <= t) issue(t);
+		first = t * tile_;
+		count = std::min<int64_t>(tile_, n_ - first);
+		PCG_CUDA(cudaStreamWaitEvent(compute_, copied_[t & 1], 0));
+		return buffer(t);
+	}
+	// The compute stream's work on tile t is enqueued: its buffer may be
+	// refilled once that work is done; the copy of tile t + 1 starts.
+	void release(int64_t t) {
+		PCG_CUDA(cudaEventRecord(consumed_[t & 1], compute_));
+		if (t + 1 < tiles_ && issued_ <= t + 1) issue(t + 1);
+	}
+
+private:
+	uint8_t* buffer(int64_t t) const { return resident_ ? resident_ + (size_t)t * tile_ * rec_ : dev_[t & 1]; }
+	void issue(int64_t t) {
+		const int b = (int)(t & 1);
+		const int64_t first = t * tile_;
+		const size_t bytes = (size_t)std::min<int64_t>(tile_, n_ - first) * rec_;
+		const uint8_t* src = host_ + (size_t)first * rec_;
+		if (!resident_ && t >= 2) PCG_CUDA(cudaStreamWaitEvent(copy_, consumed_[b], 0));
+		if (!pinned_) {
+			// the staging buffer's previous copy must have left it
+			if (t >= 2) PCG_CUDA(cudaEventSynchronize(staged_[b]));
+			parallel_copy(stage_[b], src, bytes);
+			src = stage_[b];
+		}
+		PCG_CUDA(cudaMemcpyAsync(buffer(t), src, bytes, cudaMemcpyHostToDevice, copy_));
+		if (!pinned_) PCG_CUDA(cudaEventRecord(staged_[b], copy_));
+		PCG_CUDA(cudaEventRecord(copied_[b], copy_));
+		issued_ = t + 1;
+	}
+	static void parallel_copy(uint8_t* dst, const uint8_t* src, size_t bytes) {
+		const int nt = (int)std::min<size_t>(8, std::max<size_t>(1, bytes >> 26));
+		if (nt == 1) {
+			std::memcpy(dst, src, bytes);
+			return;
+		}
+		std::vector<std::thread> th;
+		const size_t per = (bytes + nt - 1) / nt;
+		for (int k = 0; k < nt; k++) {
+			const size_t o = k * per;
+			if (o >= bytes) break;
+			th.emplace_back([=] { std::memcpy(dst + o, src + o, std::min(per, bytes - o)); });
+		}
+		for (auto& x : th) x.join();
+	}
+
+	const uint8_t* host_;
+	int64_t n_;
+	int rec_;
+	int64_t tile_, tiles_ = 0, issued_ = 0;
+	cudaStream_t compute_, copy_ = nullptr;
+	uint8_t* resident_;
+	bool pinned_ = false;
+	uint8_t* dev_[2] = {nullptr, nullptr};
+	uint8_t* stage_[2] = {nullptr, nullptr};
+	cudaEvent_t copied_[2], consumed_[2], staged_[2];
 };
 
 // PCG_TRACE_LEVELS=1 prints one line per sampled octree level to stderr
@@ -226,6 +347,107 @@ static bool trace_levels() {
 	}();
 	return on;
 }
+
+// The completion order of the single-threaded reference (doIndexing,
+// indexer.cpp:1639-1745), built in two steps so a conversion in parts can
+// place each part's nodes as soon as the part is sampled: chunk(cr) appends
+// the nodes completed while chunk cr is sampled (post-order, :1639-1671);
+// finish() appends the merged chunk-root tasks (processChunkRoots, :202-281)
+// in pre-order and then the root.
+struct CompletionOrder {
+	Tree& tree;
+	int method;
+	std::vector<int> order;
+	std::vector<char> sampled, cleared;  // cleared: children.clear() was called
+
+	CompletionOrder(Tree& t, int m) : tree(t), method(m) {}
+
+	void grow() {
+		if (sampled.size() < tree.nodes.size()) {
+			sampled.resize(tree.nodes.size(), 0);
+			cleared.resize(tree.nodes.size(), 0);
+		}
+	}
+	void complete_children(int ni) {
+		const TNode& n = tree.nodes[ni];
+		for (int c = 0; c < 8; c++) {
+			int ci = n.child[c];
+			if (ci < 0) continue;
+			const TNode& ch = tree.nodes[ci];
+			if (method == PCG_POISSON_AVERAGE && ch.unlinked) continue;
+			order.push_back(ci);
+		}
+	}
+	void post(int ni) {
+		if (!cleared[ni]) {
+			for (int c = 0; c < 8; c++) {
+				int ci = tree.nodes[ni].child[c];
+				if (ci >= 0 && !sampled[ci]) post(ci);
+			}
+		}
+		sampled[ni] = 1;
+		if (!cleared[ni] && tree.nodes[ni].has_children()) complete_children(ni);
+	}
+	void chunk(int cr) {
+		grow();
+		post(cr);
+		cleared[cr] = 1;
+	}
+	void finish(const std::vector<int>& chunk_roots) {
+		grow();
+		struct CR { int node; std::vector<int> kids; std::vector<int> fcrs; int64_t num_points = 0; };
+		std::vector<CR> crs;
+		std::unordered_map<int, int> cr_of;
+		std::function<void(int)> build = [&](int ni) {
+			int me = (int)crs.size();
+			crs.push_back(CR{ni, {}, {}, 0});
+			cr_of[ni] = me;
+			if (cleared[ni]) return;
+			for (int c = 0; c < 8; c++) {
+				int ci = tree.nodes[ni].child[c];
+				if (ci >= 0) {
+					build(ci);
+					crs[me].kids.push_back(cr_of[ci]);
+				}
+			}
+		};
+		build(0);
+		for (int cr : chunk_roots) {
+			auto it = cr_of.find(cr);
+			if (it == cr_of.end()) continue;
+			crs[it->second].fcrs.push_back(cr);
+			// numPoints of the chunk root after its chunk was sampled
+			crs[it->second].num_points += tree.nodes[cr].buf_count;
+		}
+		std::function<void(int)> merge = [&](int ci) {
+			CR& c = crs[ci];
+			for (int k : c.kids) merge(k);
+			if (c.kids.empty()) return;
+			int64_t np = 0;
+			for (int k : crs[ci].kids) np += crs[k].num_points;
+			crs[ci].num_points = np;
+			if (np < kChunkRootMergeThreshold) {
+				std::vector<int> f = crs[ci].fcrs;
+				for (int k : crs[ci].kids) f.insert(f.end(), crs[k].fcrs.begin(), crs[k].fcrs.end());
+				crs[ci].fcrs = f;
+				crs[ci].kids.clear();
+			}
+		};
+		merge(0);
+		std::vector<int> tasks;
+		std::function<void(int)> pre = [&](int ci) {
+			if (!crs[ci].fcrs.empty()) tasks.push_back(crs[ci].node);
+			for (int k : crs[ci].kids) pre(k);
+		};
+		pre(0);
+		for (int t : tasks) {
+			post(t);
+			cleared[t] = 1;
+		}
+		if (!sampled[0]) post(0);
+		order.push_back(0);
+	}
+};
 
 struct Converter {
 	int device = 0;
@@ -268,10 +490,23 @@ struct Converter {
 		if (!make_setup(infos, requested, s, err)) throw PcgError(PCG_BAD_INPUT, err);
 		if (job.method < 0 || job.method > 2) throw PcgError(PCG_BAD_INPUT, "unknown sampling method");
 		if (s.total_points < 2) throw PcgError(PCG_BAD_INPUT, "need at least two points");
+		// one uncompressed file in host memory may convert in parts
+		if (sources.size() == 1 && !infos[0].compressed && !sources[0].device_records && !(job.flags & PCG_JOB_OCTREE_ON_DEVICE)) {
+			bool resident = true;
+			const int64_t gp = part_plan(s.total_points, infos[0].record_length, resident);
+			if (gp > 0) {
+				pcg_job one = job;
+				one.las = sources[0].las;
+				one.las_size = sources[0].las_size;
+				run_streamed(one, s, infos[0], static_cast<const uint8_t*>(sources[0].las), gp, resident, res);
+				return;
+			}
+		}
 		if (s.total_points >= (int64_t(1) << 31)) throw PcgError(PCG_BAD_INPUT, "more than 2^31 points per job");
 		const int64_t N = s.total_points;
 		const int method = job.method;
 		DeviceMem mem(stream, arena.get());
+		if (arena) arena->reset_peak();
 		res.stats.num_points = N;
 
 		// ---------------------------------------------------------- input
@@ -498,36 +733,15 @@ struct Converter {
 
 		// ---------------------------------------------------- host writers
 		auto t_w = Clock::now();
-		int64_t first_chunk = 0;
-		if (!build_hierarchy(recs, res.hierarchy, first_chunk, err)) throw PcgError(PCG_INTERNAL, err);
-		std::vector<AttrStats> astats(s.attrs.size());
-		for (size_t i = 0; i < s.attrs.size(); i++) {
-			const auto& sd = stats_dev[i];
-			astats[i].min = {decode_ordered(sd.mn[0]), decode_ordered(sd.mn[1]), decode_ordered(sd.mn[2])};
-			astats[i].max = {decode_ordered(sd.mx[0]), decode_ordered(sd.mx[1]), decode_ordered(sd.mx[2])};
-			// the reference passes the statistics through the chunks'
-			// metadata.json, where a non-finite value (or none at all: an
-			// attribute no point carries) comes back as +Infinity
-			// (chunker_countsort_laszip.cpp:1005-1070, indexer.cpp:72-130)
-			for (int c = 0; c < s.attrs[i].numElements && c < 3; c++) {
-				double* mn = &astats[i].min.x + c;
-				double* mx = &astats[i].max.x + c;
-				if (!std::isfinite(*mn)) *mn = INFINITY;
-				if (!std::isfinite(*mx)) *mx = INFINITY;
-			}
-			astats[i].histogram.assign(256, 0);
-			if (s.attrs[i].kind == AK_CLASSIFICATION)
-				for (int k = 0; k < 256; k++) astats[i].histogram[k] = (int64_t)hist[k];
-		}
-		res.metadata = build_metadata(job.name ? job.name : "", job.projection ? job.projection : "", N, first_chunk, octree_depth, s,
-		                              astats, base_spacing);
+		const int64_t num_nodes = (int64_t)recs.size();
+		finish_writers(job, s, N, recs, stats_dev, hist, octree_depth, base_spacing, res);
 		res.stats.ms_host_writers = ms_since(t_w);
 		PCG_CUDA(cudaStreamSynchronize(stream));
 		res.stats.ms_d2h = ms_since(t_d2h);  // the copy, overlapped with the host writers
-		res.stats.num_nodes = (int64_t)recs.size();
-		res.nodes = std::move(recs);
+		res.stats.num_nodes = num_nodes;
 		res.stats.output_points = out_points;
 		res.stats.gpu_launches = g_launch_count;
+		if (arena) res.stats.device_peak_bytes = (int64_t)arena->peak_bytes();
 		res.stats.ms_total = ms_since(t0);
 	}
 
@@ -673,6 +887,487 @@ struct Converter {
 		mem.free(kt);
 		mem.free(vt);
 		mem.free(chunk_of);
+	}
+
+	// ------------------------------------------------ conversion in parts
+	// Device bytes one point of a part needs beside its record (positions,
+	// ids, the level buffers of the sampler, sort and conflict-list scratch;
+	// calibrated against pcg_stats.device_peak_bytes), and the tile of the
+	// streamed passes.
+	static constexpr int64_t kPartBytesPerPoint = 400;
+	static constexpr int64_t kTilePoints = int64_t(1) << 24;
+	int records_mode = PCG_RECORDS_AUTO;  // pcg_records
+	int64_t group_points = 0;             // pcg_opts.group_points
+
+	// Whether a one-file job converts in parts: the part size in points (0:
+	// in one piece) and whether its records stay on the device.
+	int64_t part_plan(int64_t N, int rec_len, bool& resident) const {
+		size_t free_b = 0, total_b = 0;
+		PCG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+		int64_t avail = (int64_t)((double)free_b * 0.85);
+		if (arena) avail += (int64_t)(arena->reserved() - arena->live_bytes());
+		const int64_t rec_bytes = N * (int64_t)rec_len;
+		const int64_t stream_bytes = 2 * std::min<int64_t>(kTilePoints, N) * rec_len;
+		int64_t gp = group_points;
+		if (gp <= 0) {
+			if (N < (int64_t(1) << 31) && rec_bytes + N * kPartBytesPerPoint <= avail) return 0;
+			const int64_t gp_res = (avail - rec_bytes) / kPartBytesPerPoint;
+			const int64_t gp_str = (avail - stream_bytes) / kPartBytesPerPoint;
+			// resident records when they leave room for parts of a few chunks
+			const bool res_ok = records_mode != PCG_RECORDS_STREAMED && gp_res >= 40'000'000;
+			gp = std::min<int64_t>(res_ok ? gp_res : gp_str, (int64_t(1) << 31) - 1);
+			if (gp < 10'000'000) throw PcgError(PCG_OOM, "not enough device memory for one chunk of the cloud");
+			resident = records_mode == PCG_RECORDS_RESIDENT || (records_mode == PCG_RECORDS_AUTO && res_ok);
+			return gp;
+		}
+		if (N <= gp) return 0;
+		resident = records_mode == PCG_RECORDS_RESIDENT ||
+		           (records_mode == PCG_RECORDS_AUTO && rec_bytes + std::min(gp, N) * kPartBytesPerPoint <= avail);
+		return gp;
+	}
+
+	// Hands the device image of a finished piece of octree.bin to the host
+	// on the side stream `d2h` (after the compute stream's work so far) and
+	// frees it there; the piece joins res.parts.
+	void emit_part(uint8_t* d_part, uint64_t bytes, cudaStream_t d2h, JobResult& res) {
+		if (bytes == 0) return;
+		uint8_t* h = host_buffers ? host_buffers->take(bytes) : nullptr;
+		if (!h) PCG_CUDA(cudaMallocHost((void**)&h, bytes));
+		res.parts.push_back({h, bytes});
+		cudaEvent_t ev;
+		PCG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+		PCG_CUDA(cudaEventRecord(ev, stream));
+		PCG_CUDA(cudaStreamWaitEvent(d2h, ev, 0));
+		PCG_CUDA(cudaEventDestroy(ev));
+		PCG_CUDA(cudaMemcpyAsync(h, d_part, bytes, cudaMemcpyDeviceToHost, d2h));
+		PCG_CUDA(cudaFreeAsync(d_part, d2h));
+	}
+
+	// Payloads of the nodes order[o0 ..) (completed since the last call) into
+	// a new piece of octree.bin; their hierarchy records join `recs`.
+	void write_piece(const Tree& tree, const std::vector<int>& order, size_t o0, const DecodeParams& p, const Setup& s,
+	                 std::vector<HierRecord>& recs, int64_t& out_points, cudaStream_t d2h, DeviceMem& mem, JobResult& res) {
+		std::vector<PayloadItem> items;
+		int64_t piece = 0;
+		for (size_t i = o0; i < order.size(); i++) {
+			const TNode& n = tree.nodes[order[i]];
+			HierRecord r;
+			r.name = n.name;
+			r.num_points = n.fin_count;
+			if (n.fin_count > 0) {
+				r.byte_offset = (out_points + piece) * s.bpp;
+				r.byte_size = n.fin_count * s.bpp;
+				items.push_back({n.fin_ids, n.fin_cols, n.fin_count, piece});
+				piece += n.fin_count;
+			}
+			recs.push_back(r);
+		}
+		out_points += piece;
+		if (piece == 0) return;
+		uint8_t* d_part = nullptr;
+		PCG_CUDA(cudaMallocAsync((void**)&d_part, (size_t)piece * s.bpp, stream));
+		PayloadItem* d_items = upload(items, mem);
+		launch_write_payloads(p, items, d_items, d_part, mem);
+		emit_part(d_part, (uint64_t)piece * s.bpp, d2h, res);
+		mem.free(d_items);
+	}
+
+	// Sampler-ready leaves: buffers of every leaf of `nodes` (chunk-local
+	// ids into the part's arrays), shuffled for random, with colours for
+	// poisson_average and coordinates for the poisson samplers.
+	void prepare_leaves(Tree& tree, const std::vector<int>& nodes, int method, const DecodeParams& p, const uint32_t* ids, int64_t n,
+	                    const ChunkingOut& co, DeviceMem& mem) {
+		const uint32_t* leaf_ids = ids;
+		uint64_t* leaf_cols = nullptr;
+		if (method == PCG_RANDOM) {
+			std::vector<int64_t> loff, lcnt;
+			for (int ni : nodes) {
+				const TNode& t = tree.nodes[ni];
+				if (!t.has_children() && t.leaf_count > 0) { loff.push_back(t.leaf_start); lcnt.push_back(t.leaf_count); }
+			}
+			uint32_t* shuffled = mem.alloc<uint32_t>(std::max<int64_t>(n, 1));
+			int32_t* scratch = mem.alloc<int32_t>(std::max<int64_t>(n, 1));
+			int64_t* d_off = upload(loff, mem);
+			int64_t* d_cnt = upload(lcnt, mem);
+			launch_shuffle_leaves(d_off, d_cnt, (int)loff.size(), ids, shuffled, scratch, seed, mem);
+			mem.free(scratch);
+			leaf_ids = shuffled;
+		}
+		if (method == PCG_POISSON_AVERAGE) {
+			if (p.off_rgb < 0) throw PcgError(PCG_BAD_INPUT, "poisson_average needs an rgb attribute");
+			leaf_cols = mem.alloc<uint64_t>(std::max<int64_t>(n, 1));
+			launch_fill_colors(p, ids, n, leaf_cols, mem);
+		}
+		int4* leaf_rec = nullptr;
+		if (method != PCG_RANDOM) {
+			leaf_rec = mem.alloc<int4>(std::max<int64_t>(n, 1));
+			launch_gather_records(leaf_ids, n, co.X, co.Y, co.Z, leaf_rec, mem);
+		}
+		for (int ni : nodes) {
+			TNode& t = tree.nodes[ni];
+			if (t.has_children()) continue;
+			t.buf_ids = leaf_ids + t.leaf_start;
+			t.buf_cols = leaf_cols ? leaf_cols + t.leaf_start : nullptr;
+			t.buf_rec = leaf_rec ? leaf_rec + t.leaf_start : nullptr;
+			t.buf_count = t.leaf_count;
+		}
+	}
+
+	// Samples, deepest level first, the inner nodes among `nodes`.
+	void sample_nodes(Tree& tree, const std::vector<int>& nodes, int method, double base_spacing, const PosParamsS& pps,
+	                  const ChunkingOut& co, SampleStats* d_st, GreedyArena& grid_arena, DeviceMem& mem, JobResult& res) {
+		int max_depth = -1;
+		for (int ni : nodes)
+			if (tree.nodes[ni].has_children()) max_depth = std::max(max_depth, tree.nodes[ni].depth);
+		for (int d = max_depth; d >= 0; d--) {
+			std::vector<int> level_nodes;
+			for (int ni : nodes)
+				if (tree.nodes[ni].depth == d && tree.nodes[ni].has_children()) level_nodes.push_back(ni);
+			if (!level_nodes.empty()) sample_level(tree, level_nodes, method, base_spacing, pps, co, d_st, grid_arena, mem, res);
+		}
+	}
+
+	// A one-file cloud converted in parts (the reference's out-of-core
+	// path: chunker_countsort_laszip.cpp:1206-1261 counts and distributes
+	// in batches through chunk files, indexer.cpp:1581-1745 indexes chunk by
+	// chunk and flushes the chunk roots, :181-281). The counting pass streams
+	// the records through the device in tiles; the chunks (file-name order)
+	// are cut into parts of consecutive chunks of at most part_points
+	// points; each part's records are selected from all records (kept on the
+	// device, or streamed again), indexed and sampled down to its chunk
+	// roots, and its finished nodes' payloads leave for the host while the
+	// next part runs. The chunk roots' points survive the part; the levels
+	// above them are sampled last. Output bytes equal the one-piece form's.
+	void run_streamed(const pcg_job& job, const Setup& s, const LasInfo& info, const uint8_t* las, int64_t part_points, bool resident,
+	                  JobResult& res) {
+		const auto t0 = Clock::now();
+		const int64_t N = s.total_points;
+		const int method = job.method;
+		const int rec = info.record_length;
+		const uint8_t* host_recs = las + info.offset_to_points;
+		if (info.offset_to_points + (uint64_t)N * rec > job.las_size) throw PcgError(PCG_BAD_INPUT, "truncated point records");
+		DeviceMem mem(stream, arena.get());
+		if (arena) arena->reset_peak();
+		res.stats.num_points = N;
+		res.stats.records_resident = resident ? 1 : 0;
+		cudaStream_t d2h = nullptr;
+		PCG_CUDA(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
+		struct StreamGuard {
+			cudaStream_t s;
+			~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+		} d2h_guard{d2h};
+
+		// ------------------------------------------ counting pass, in tiles
+		auto t_chunk = Clock::now();
+		std::vector<SourceDesc> descs;
+		std::vector<int64_t> firsts;
+		const DecodeParams p = decode_params(s, {nullptr}, descs, firsts);
+		const int G = s.grid_size;
+		const int64_t cells = (int64_t)G * G * G;
+		uint32_t* grid = mem.alloc<uint32_t>(cells);
+		PCG_CUDA(cudaMemsetAsync(grid, 0, cells * sizeof(uint32_t), stream));
+		ChunkingOut co{};
+		std::vector<AttrStatsDev> st_init(MAX_ATTRS);
+		for (auto& a : st_init) for (int c = 0; c < 3; c++) { a.mn[c] = ~0ull; a.mx[c] = 0ull; }
+		co.stats = upload(st_init, mem);
+		co.histogram = mem.alloc<unsigned long long>(256);
+		PCG_CUDA(cudaMemsetAsync(co.histogram, 0, 256 * 8, stream));
+		co.error = mem.alloc<int64_t>(2);
+		PCG_CUDA(cudaMemsetAsync(co.error, 0, 16, stream));
+		uint8_t* d_all = resident ? mem.alloc<uint8_t>((size_t)N * rec) : nullptr;
+		const int64_t T = std::min<int64_t>(kTilePoints, N);
+		{
+			ChunkingOut ct = co;
+			ct.X = mem.alloc<int32_t>(T);
+			ct.Y = mem.alloc<int32_t>(T);
+			ct.Z = mem.alloc<int32_t>(T);
+			ct.cell = mem.alloc<uint32_t>(T);
+			TileFeeder feed(host_recs, N, rec, T, stream, d_all, mem);
+			for (int64_t t = 0; t < feed.tiles(); t++) {
+				int64_t first = 0, count = 0;
+				const uint8_t* d = feed.acquire(t, first, count);
+				DecodeParams pt = p;
+				pt.n = count;
+				pt.src0.recs = d;
+				pt.src0.first = 0;
+				pt.src0.count = count;
+				launch_decode_count(pt, grid, ct, mem);
+				feed.release(t);
+			}
+			PCG_CUDA(cudaStreamSynchronize(stream));
+			mem.free(ct.X); mem.free(ct.Y); mem.free(ct.Z); mem.free(ct.cell);
+		}
+		res.stats.ms_h2d = ms_since(t_chunk);
+		if (download(co.error, 2, stream)[0]) throw PcgError(PCG_OUT_OF_BOX, "a point lies outside the header bounding box");
+		int32_t* lut = mem.alloc<int32_t>(cells);
+		const std::vector<std::pair<std::string, ChunkCell>> chunks = make_chunks(grid, G, s.max_points_per_chunk, lut, mem);
+		const int nchunks = (int)chunks.size();
+		res.stats.num_chunks = nchunks;
+		std::vector<std::pair<int, int>> parts;
+		{
+			int k0 = 0;
+			int64_t acc = 0;
+			for (int k = 0; k < nchunks; k++) {
+				if (k > k0 && acc + chunks[k].second.count > part_points) {
+					parts.push_back({k0, k});
+					k0 = k;
+					acc = 0;
+				}
+				acc += chunks[k].second.count;
+			}
+			if (nchunks > k0) parts.push_back({k0, nchunks});
+		}
+		res.stats.parts = (int64_t)parts.size();
+		res.stats.ms_chunking = ms_since(t_chunk);
+
+		// the tree down to the chunk roots
+		Tree tree;
+		const Vec3d rmin = s.cube_min, rmax = s.root_max;
+		tree.add("r", -1, rmin, rmax);
+		std::vector<int> chunk_roots;
+		for (int k = 0; k < nchunks; k++) {
+			const std::string& id = chunks[k].first;
+			int cur = 0;
+			for (size_t i = 1; i < id.size(); i++) cur = tree.child_of(cur, id[i] - '0', i + 1 == id.size() ? k : -1);
+			tree.nodes[cur].chunk = k;
+			tree.nodes[cur].chunk_root = true;
+			chunk_roots.push_back(cur);
+		}
+		PosParams pp;
+		PosParamsS pps;
+		for (int a = 0; a < 3; a++) {
+			pp.scale[a] = pps.scale[a] = (&s.pos_scale.x)[a];
+			pp.offset[a] = pps.offset[a] = (&s.pos_offset.x)[a];
+		}
+		const double base_spacing = (rmax - rmin).x / 128.0;  // indexer.cpp:1603
+		SampleStats* d_st = mem.alloc<SampleStats>(1);
+		PCG_CUDA(cudaMemsetAsync(d_st, 0, sizeof(SampleStats), stream));
+		CompletionOrder corder(tree, method);
+		std::vector<HierRecord> recs;
+		int64_t out_points = 0, octree_depth = 0;
+
+		// survivors: the chunk roots' points after their part, one block of
+		// device memory per part
+		struct Block {
+			std::unique_ptr<DeviceMem> mem;
+			uint8_t* recs = nullptr;
+			int32_t *X = nullptr, *Y = nullptr, *Z = nullptr;
+			uint64_t* cols = nullptr;
+			int64_t count = 0;
+		};
+		std::vector<Block> blocks;
+		std::vector<int64_t> surv_off(nchunks, 0);
+		int64_t S = 0;
+
+		// ------------------------------------------------------------ parts
+		for (const auto& part : parts) {
+			const int k0 = part.first, k1 = part.second;
+			int64_t n_g = 0;
+			for (int k = k0; k < k1; k++) n_g += chunks[k].second.count;
+			DeviceMem gm(stream, arena.get());
+			auto t_sel = Clock::now();
+			uint8_t* g_recs = gm.alloc<uint8_t>((size_t)n_g * rec);
+			int64_t* fill = gm.alloc<int64_t>(1);
+			PCG_CUDA(cudaMemsetAsync(fill, 0, 8, stream));
+			if (resident) {
+				launch_select_part(p, d_all, N, lut, k0, k1, fill, g_recs, gm);
+			} else {
+				TileFeeder feed(host_recs, N, rec, T, stream, nullptr, gm);
+				for (int64_t t = 0; t < feed.tiles(); t++) {
+					int64_t first = 0, count = 0;
+					const uint8_t* d = feed.acquire(t, first, count);
+					launch_select_part(p, d, count, lut, k0, k1, fill, g_recs, gm);
+					feed.release(t);
+				}
+			}
+			if (download(fill, 1, stream)[0] != n_g) throw PcgError(PCG_INTERNAL, "part selection lost points");
+			res.stats.ms_h2d += ms_since(t_sel);
+			// the part as a cloud of its own: positions, cells, chunk order
+			auto t_oct = Clock::now();
+			DecodeParams pg = p;
+			pg.n = n_g;
+			pg.src0.recs = g_recs;
+			pg.src0.first = 0;
+			pg.src0.count = n_g;
+			ChunkingOut cg{};
+			cg.X = gm.alloc<int32_t>(n_g);
+			cg.Y = gm.alloc<int32_t>(n_g);
+			cg.Z = gm.alloc<int32_t>(n_g);
+			cg.cell = gm.alloc<uint32_t>(n_g);
+			cg.stats = upload(st_init, gm);
+			cg.histogram = gm.alloc<unsigned long long>(256);
+			cg.error = gm.alloc<int64_t>(2);
+			PCG_CUDA(cudaMemsetAsync(cg.error, 0, 16, stream));
+			launch_decode_count(pg, grid, cg, gm);  // the grid is scratch by now
+			uint32_t* ids = gm.alloc<uint32_t>(n_g);
+			scatter_chunks(cg.cell, lut, n_g, k1 - k0, k0, ids, cg.error, gm);
+			if (download(cg.error, 2, stream)[1]) throw PcgError(PCG_INTERNAL, "point to chunk lookup failed");
+			gm.free(cg.cell);
+			std::vector<int> roots;
+			int64_t off = 0;
+			for (int k = k0; k < k1; k++) {
+				TNode& cr = tree.nodes[chunk_roots[k]];
+				cr.leaf_start = off;
+				cr.leaf_count = chunks[k].second.count;
+				off += cr.leaf_count;
+				roots.push_back(chunk_roots[k]);
+			}
+			octree_depth = std::max(octree_depth, refine_octree(tree, roots, ids, cg.X, cg.Y, cg.Z, pp, gm));
+			res.stats.ms_octree += ms_since(t_oct);
+			auto t_samp = Clock::now();
+			std::vector<int> nodes;
+			for (int i = 0; i < (int)tree.nodes.size(); i++)
+				if (tree.nodes[i].chunk >= k0 && tree.nodes[i].chunk < k1) nodes.push_back(i);
+			prepare_leaves(tree, nodes, method, pg, ids, n_g, cg, gm);
+			GreedyArena grid_arena;
+			sample_nodes(tree, nodes, method, base_spacing, pps, cg, d_st, grid_arena, gm, res);
+			res.stats.ms_sampling += ms_since(t_samp);
+			// the part's finished nodes, in completion order
+			auto t_out = Clock::now();
+			const size_t o0 = corder.order.size();
+			for (int cr : roots) corder.chunk(cr);
+			write_piece(tree, corder.order, o0, pg, s, recs, out_points, d2h, gm, res);
+			// the chunk roots' points, carried to the levels above the parts
+			Block b;
+			for (int cr : roots) b.count += tree.nodes[cr].buf_count;
+			b.mem = std::make_unique<DeviceMem>(stream);
+			b.recs = b.mem->alloc<uint8_t>((size_t)std::max<int64_t>(b.count, 1) * rec);
+			b.X = b.mem->alloc<int32_t>(std::max<int64_t>(b.count, 1));
+			b.Y = b.mem->alloc<int32_t>(std::max<int64_t>(b.count, 1));
+			b.Z = b.mem->alloc<int32_t>(std::max<int64_t>(b.count, 1));
+			if (method == PCG_POISSON_AVERAGE) b.cols = b.mem->alloc<uint64_t>(std::max<int64_t>(b.count, 1));
+			int64_t o = 0;
+			for (int k = k0; k < k1; k++) {
+				const TNode& cr = tree.nodes[chunk_roots[k]];
+				surv_off[k] = S + o;
+				if (cr.buf_count == 0) continue;
+				launch_gather_points(cr.buf_ids, cr.buf_count, g_recs, rec, cg.X, cg.Y, cg.Z, b.recs + (size_t)o * rec, b.X + o, b.Y + o,
+				                     b.Z + o, gm);
+				if (b.cols)
+					PCG_CUDA(cudaMemcpyAsync(b.cols + o, cr.buf_cols, cr.buf_count * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream));
+				o += cr.buf_count;
+			}
+			S += b.count;
+			blocks.push_back(std::move(b));
+			// nothing of the part's device memory is referenced any more
+			for (int ni : nodes) {
+				TNode& t = tree.nodes[ni];
+				t.buf_ids = nullptr; t.buf_cols = nullptr; t.buf_rec = nullptr;
+				t.fin_ids = nullptr; t.fin_cols = nullptr;
+			}
+			res.stats.ms_output += ms_since(t_out);
+		}
+		res.stats.survivors = S;
+		res.stats.octree_depth = octree_depth;
+
+		// ---------------------------------- levels above the chunk roots
+		auto t_top = Clock::now();
+		if (d_all) mem.free(d_all);
+		uint8_t* s_recs = mem.alloc<uint8_t>((size_t)std::max<int64_t>(S, 1) * rec);
+		ChunkingOut ctop{};
+		ctop.X = mem.alloc<int32_t>(std::max<int64_t>(S, 1));
+		ctop.Y = mem.alloc<int32_t>(std::max<int64_t>(S, 1));
+		ctop.Z = mem.alloc<int32_t>(std::max<int64_t>(S, 1));
+		uint64_t* s_cols = method == PCG_POISSON_AVERAGE ? mem.alloc<uint64_t>(std::max<int64_t>(S, 1)) : nullptr;
+		{
+			int64_t o = 0;
+			for (Block& b : blocks) {
+				if (b.count) {
+					PCG_CUDA(cudaMemcpyAsync(s_recs + (size_t)o * rec, b.recs, (size_t)b.count * rec, cudaMemcpyDeviceToDevice, stream));
+					PCG_CUDA(cudaMemcpyAsync(ctop.X + o, b.X, b.count * 4, cudaMemcpyDeviceToDevice, stream));
+					PCG_CUDA(cudaMemcpyAsync(ctop.Y + o, b.Y, b.count * 4, cudaMemcpyDeviceToDevice, stream));
+					PCG_CUDA(cudaMemcpyAsync(ctop.Z + o, b.Z, b.count * 4, cudaMemcpyDeviceToDevice, stream));
+					if (s_cols) PCG_CUDA(cudaMemcpyAsync(s_cols + o, b.cols, b.count * 8, cudaMemcpyDeviceToDevice, stream));
+				}
+				o += b.count;
+				b.mem.reset();
+			}
+		}
+		uint32_t* s_ids = mem.alloc<uint32_t>(std::max<int64_t>(S, 1));
+		launch_iota(s_ids, S, mem);
+		int4* s_rec4 = nullptr;
+		if (method != PCG_RANDOM) {
+			s_rec4 = mem.alloc<int4>(std::max<int64_t>(S, 1));
+			launch_gather_records(s_ids, S, ctop.X, ctop.Y, ctop.Z, s_rec4, mem);
+		}
+		for (int k = 0; k < nchunks; k++) {
+			TNode& cr = tree.nodes[chunk_roots[k]];
+			cr.buf_ids = s_ids + surv_off[k];
+			cr.buf_cols = s_cols ? s_cols + surv_off[k] : nullptr;
+			cr.buf_rec = s_rec4 ? s_rec4 + surv_off[k] : nullptr;
+		}
+		DecodeParams ptop = p;
+		ptop.n = S;
+		ptop.src0.recs = s_recs;
+		ptop.src0.first = 0;
+		ptop.src0.count = S;
+		std::vector<int> upper;
+		for (int i = 0; i < (int)tree.nodes.size(); i++)
+			if (tree.nodes[i].chunk < 0) upper.push_back(i);
+		GreedyArena grid_arena;
+		sample_nodes(tree, upper, method, base_spacing, pps, ctop, d_st, grid_arena, mem, res);
+		TNode& root = tree.nodes[0];
+		root.fin_ids = root.buf_ids;
+		root.fin_cols = root.buf_cols;
+		root.fin_count = root.buf_count;
+		const size_t o0 = corder.order.size();
+		corder.finish(chunk_roots);
+		write_piece(tree, corder.order, o0, ptop, s, recs, out_points, d2h, mem, res);
+		const auto hst = download(d_st, 1, stream)[0];
+		if (hst.timeouts) throw PcgError(PCG_TIMEOUT, "a bounded device loop gave up");
+		res.stats.escalated_pairs = (int64_t)hst.escalated;
+		res.stats.heapsort_fallbacks = (int64_t)hst.heapsorts;
+		res.stats.list_entries = (int64_t)hst.list_entries;
+		res.stats.cluster_nodes = (int64_t)hst.cluster_nodes;
+		res.stats.ms_sampling += ms_since(t_top);
+
+		// ------------------------------------------------------ host writers
+		const auto stats_dev = download(co.stats, MAX_ATTRS, stream);
+		const auto hist = download(co.histogram, 256, stream);
+		auto t_w = Clock::now();
+		finish_writers(job, s, N, recs, stats_dev, hist, octree_depth, base_spacing, res);
+		res.stats.ms_host_writers = ms_since(t_w);
+		auto t_d2h = Clock::now();
+		PCG_CUDA(cudaStreamSynchronize(d2h));
+		res.stats.ms_d2h = ms_since(t_d2h);
+		res.octree = nullptr;
+		res.octree_size = (uint64_t)(out_points * s.bpp);
+		res.stats.output_points = out_points;
+		res.stats.num_nodes = (int64_t)res.nodes.size();
+		res.stats.gpu_launches = g_launch_count;
+		if (arena) res.stats.device_peak_bytes = (int64_t)arena->peak_bytes();
+		res.stats.ms_total = ms_since(t0);
+	}
+
+	// hierarchy.bin and metadata.json from the completed nodes and the
+	// counting pass's attribute statistics; res.nodes takes the records
+	void finish_writers(const pcg_job& job, const Setup& s, int64_t N, std::vector<HierRecord>& recs, const std::vector<AttrStatsDev>& stats_dev,
+	                    const std::vector<unsigned long long>& hist, int64_t octree_depth, double base_spacing, JobResult& res) {
+		std::string err;
+		int64_t first_chunk = 0;
+		if (!build_hierarchy(recs, res.hierarchy, first_chunk, err)) throw PcgError(PCG_INTERNAL, err);
+		std::vector<AttrStats> astats(s.attrs.size());
+		for (size_t i = 0; i < s.attrs.size(); i++) {
+			const auto& sd = stats_dev[i];
+			astats[i].min = {decode_ordered(sd.mn[0]), decode_ordered(sd.mn[1]), decode_ordered(sd.mn[2])};
+			astats[i].max = {decode_ordered(sd.mx[0]), decode_ordered(sd.mx[1]), decode_ordered(sd.mx[2])};
+			// the reference passes the statistics through the chunks'
+			// metadata.json, where a non-finite value (or none at all: an
+			// attribute no point carries) comes back as +Infinity
+			// (chunker_countsort_laszip.cpp:1005-1070, indexer.cpp:72-130)
+			for (int c = 0; c < s.attrs[i].numElements && c < 3; c++) {
+				double* mn = &astats[i].min.x + c;
+				double* mx = &astats[i].max.x + c;
+				if (!std::isfinite(*mn)) *mn = INFINITY;
+				if (!std::isfinite(*mx)) *mx = INFINITY;
+			}
+			astats[i].histogram.assign(256, 0);
+			if (s.attrs[i].kind == AK_CLASSIFICATION)
+				for (int k = 0; k < 256; k++) astats[i].histogram[k] = (int64_t)hist[k];
+		}
+		res.metadata = build_metadata(job.name ? job.name : "", job.projection ? job.projection : "", N, first_chunk, octree_depth, s,
+		                              astats, base_spacing);
+		res.nodes = std::move(recs);
 	}
 
 	// Kernel parameters of the decode: the output layout, and per source its
@@ -996,86 +1691,10 @@ struct Converter {
 	// post-order; then the merged chunk-root tasks (processChunkRoots,
 	// :202-281) in pre-order; then the root.
 	static std::vector<int> completion_order(Tree& tree, const std::vector<int>& chunk_roots, int method) {
-		std::vector<int> order;
-		std::vector<char> sampled(tree.nodes.size(), 0);
-		std::vector<char> cleared(tree.nodes.size(), 0);  // children.clear() was called
-		auto complete_children = [&](int ni) {
-			const TNode& n = tree.nodes[ni];
-			for (int c = 0; c < 8; c++) {
-				int ci = n.child[c];
-				if (ci < 0) continue;
-				const TNode& ch = tree.nodes[ci];
-				if (method == PCG_POISSON_AVERAGE && ch.unlinked) continue;
-				order.push_back(ci);
-			}
-		};
-		std::function<void(int)> post = [&](int ni) {
-			if (!cleared[ni]) {
-				for (int c = 0; c < 8; c++) {
-					int ci = tree.nodes[ni].child[c];
-					if (ci >= 0 && !sampled[ci]) post(ci);
-				}
-			}
-			sampled[ni] = 1;
-			if (!cleared[ni] && tree.nodes[ni].has_children()) complete_children(ni);
-		};
-		for (int cr : chunk_roots) {
-			post(cr);
-			cleared[cr] = 1;
-		}
-		// chunk-root tasks
-		struct CR { int node; std::vector<int> kids; std::vector<int> fcrs; int num_points = 0; bool cleared = false; };
-		std::vector<CR> crs;
-		std::unordered_map<int, int> cr_of;
-		std::function<void(int)> build = [&](int ni) {
-			int me = (int)crs.size();
-			crs.push_back(CR{ni, {}, {}, 0, false});
-			cr_of[ni] = me;
-			if (cleared[ni]) return;
-			for (int c = 0; c < 8; c++) {
-				int ci = tree.nodes[ni].child[c];
-				if (ci >= 0) {
-					build(ci);
-					crs[me].kids.push_back(cr_of[ci]);
-				}
-			}
-		};
-		build(0);
-		for (int cr : chunk_roots) {
-			auto it = cr_of.find(cr);
-			if (it == cr_of.end()) continue;
-			crs[it->second].fcrs.push_back(cr);
-			// numPoints of the chunk root after its chunk was sampled
-			crs[it->second].num_points += (int)tree.nodes[cr].buf_count;
-		}
-		std::function<void(int)> merge = [&](int ci) {
-			CR& c = crs[ci];
-			for (int k : c.kids) merge(k);
-			if (c.kids.empty()) return;
-			int np = 0;
-			for (int k : crs[ci].kids) np += crs[k].num_points;
-			crs[ci].num_points = np;
-			if (np < kChunkRootMergeThreshold) {
-				std::vector<int> f = crs[ci].fcrs;
-				for (int k : crs[ci].kids) f.insert(f.end(), crs[k].fcrs.begin(), crs[k].fcrs.end());
-				crs[ci].fcrs = f;
-				crs[ci].kids.clear();
-			}
-		};
-		merge(0);
-		std::vector<int> tasks;
-		std::function<void(int)> pre = [&](int ci) {
-			if (!crs[ci].fcrs.empty()) tasks.push_back(crs[ci].node);
-			for (int k : crs[ci].kids) pre(k);
-		};
-		pre(0);
-		for (int t : tasks) {
-			post(t);
-			cleared[t] = 1;
-		}
-		if (!sampled[0]) post(0);
-		order.push_back(0);
-		return order;
+		CompletionOrder co(tree, method);
+		for (int cr : chunk_roots) co.chunk(cr);
+		co.finish(chunk_roots);
+		return co.order;
 	}
 };
 
@@ -1162,6 +1781,18 @@ void move_result(pcg::JobResult& r, pcg_result* out, int device) {
 	out->metadata[r.metadata.size()] = 0;
 	out->metadata_size = r.metadata.size();
 	out->stats = r.stats;
+	// octree.bin in pieces: the one image, or the parts (owned by the result)
+	const size_t np = r.octree || r.parts.empty() ? 1 : r.parts.size();
+	out->octree_parts = (pcg_octree_part*)malloc(sizeof(pcg_octree_part) * np);
+	if (out->octree_parts) {
+		if (r.octree || r.parts.empty()) {
+			out->octree_parts[0] = {out->octree, out->octree_size};
+		} else {
+			for (size_t i = 0; i < np; i++) out->octree_parts[i] = {r.parts[i].first, r.parts[i].second};
+			r.parts.clear();
+		}
+		out->num_octree_parts = np;
+	}
 	// node list: the records, then their names, in one block
 	size_t chars = 0;
 	for (auto& n : r.nodes) chars += n.name.size() + 1;
@@ -1256,6 +1887,7 @@ void worker_main(pcg_ctx* ctx, int wi) {
 		} catch (const std::exception& e) {
 			st = PCG_INTERNAL; err = e.what();
 		}
+		if (st != PCG_OK) job->result.release_parts();
 		conv.arena->release_all();
 		if (job->las_pinned) {
 			pcg::g_pinned.give(job->las_pinned);
@@ -1301,6 +1933,10 @@ pcg_status pcg_create(pcg_ctx** out, const pcg_opts* opts) {
 			ctx->conv.device = opts->device;
 			ctx->conv.seed = opts->random_seed;
 			ctx->conv.form = opts->form;
+			if (opts->records < PCG_RECORDS_AUTO || opts->records > PCG_RECORDS_STREAMED || opts->group_points < 0)
+				throw pcg::PcgError(PCG_BAD_INPUT, "bad records placement or part size");
+			ctx->conv.records_mode = opts->records;
+			ctx->conv.group_points = opts->group_points;
 		}
 		int n = 0;
 		PCG_CUDA(cudaGetDeviceCount(&n));
@@ -1335,8 +1971,10 @@ void pcg_destroy(pcg_ctx* ctx) {
 	}
 	ctx->qcv.notify_all();
 	for (auto& t : ctx->workers) t.join();
-	for (auto& kv : ctx->jobs)
+	for (auto& kv : ctx->jobs) {
 		if (kv.second->result.octree && !pcg::g_pinned.give(kv.second->result.octree)) cudaFreeHost(kv.second->result.octree);
+		kv.second->result.release_parts();
+	}
 	for (auto& kv : ctx->jobs)
 		if (kv.second->las_pinned) pcg::g_pinned.give(kv.second->las_pinned);
 	cudaSetDevice(ctx->conv.device);
@@ -1360,6 +1998,7 @@ pcg_status pcg_convert(pcg_ctx* ctx, const pcg_job* job, pcg_result* out) {
 	if (st != PCG_OK) {
 		if (r.octree_on_device && r.octree) cudaFree(r.octree);
 		else if (r.octree && !pcg::g_pinned.give(r.octree)) cudaFreeHost(r.octree);
+		r.release_parts();  // their copies ended with the conversion's side stream
 		return st;
 	}
 	move_result(r, out, ctx->conv.device);
@@ -1368,6 +2007,9 @@ pcg_status pcg_convert(pcg_ctx* ctx, const pcg_job* job, pcg_result* out) {
 
 void pcg_result_free(pcg_result* r) {
 	if (!r) return;
+	if (!r->octree && r->octree_parts)  // the pieces of a conversion in parts
+		for (uint64_t i = 0; i < r->num_octree_parts; i++) pcg::release_octree(const_cast<uint8_t*>(r->octree_parts[i].data));
+	free(r->octree_parts);
 	pcg::release_octree(r->octree);
 	free(r->hierarchy);
 	free(r->metadata);
@@ -1383,7 +2025,14 @@ pcg_status pcg_write_files(const pcg_result* r, const char* dir) {
 		f.write((const char*)data, (std::streamsize)size);
 		return (bool)f;
 	};
-	if (!wr("octree.bin", r->octree, r->octree_size)) return PCG_BAD_INPUT;
+	if (r->octree || !r->octree_parts) {
+		if (!wr("octree.bin", r->octree, r->octree_size)) return PCG_BAD_INPUT;
+	} else {
+		std::ofstream f(std::string(dir) + "/octree.bin", std::ios::binary);
+		for (uint64_t i = 0; f && i < r->num_octree_parts; i++)
+			f.write((const char*)r->octree_parts[i].data, (std::streamsize)r->octree_parts[i].size);
+		if (!f) return PCG_BAD_INPUT;
+	}
 	if (!wr("hierarchy.bin", r->hierarchy, r->hierarchy_size)) return PCG_BAD_INPUT;
 	if (!wr("metadata.json", r->metadata, r->metadata_size)) return PCG_BAD_INPUT;
 	return PCG_OK;

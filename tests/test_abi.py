@@ -51,10 +51,11 @@ def test_binding_structs_match_the_header(tmp_path):
     import ctypes
     import subprocess
     structs = {"pcg_opts": pc._Opts, "pcg_source": pc._Source, "pcg_job": pc._Job, "pcg_stats": pc._Stats,
-               "pcg_node": pc._Node, "pcg_result": pc._Result}
+               "pcg_node": pc._Node, "pcg_result": pc._Result, "pcg_chunk": pc._Chunk, "pcg_octree_node": pc._OctreeNode,
+               "pcg_octree_part": pc._Part}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pcgpu.h"', "int main(void) {"]
     for cname, py in structs.items():
-        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        lines.append(f'printf("{cname} sizeof() %zu\\n", sizeof({cname}));')
         for field, _ in py._fields_:
             lines.append(f'printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
     lines.append("return 0; }")
@@ -67,7 +68,7 @@ def test_binding_structs_match_the_header(tmp_path):
     for line in filter(None, out):
         cname, what, value = line.split()
         py = structs[cname]
-        got = ctypes.sizeof(py) if what == "size" else getattr(py, what).offset
+        got = ctypes.sizeof(py) if what == "sizeof()" else getattr(py, what).offset
         assert got == int(value), (cname, what)
         seen += 1
     assert seen == sum(len(p._fields_) + 1 for p in structs.values())
