@@ -112,7 +112,6 @@ def write_las(X, Y, Z, attrs: dict, *, pdrf: int, version_minor: int,
         recs["extra"] = extra
     for e in extras:
         recs[e["name"]] = e["values"]
-    header_size = 227 if version_minor <= 2 else 375
     if extras:
         descs = b"" if extra is None else _extra_descriptor("extra", 9, "N(0,1) float")
         for e in extras:
@@ -122,12 +121,27 @@ def write_las(X, Y, Z, attrs: dict, *, pdrf: int, version_minor: int,
         vlrs = _extra_bytes_vlr(descriptors=descs)
     else:
         vlrs = _extra_bytes_vlr() if extra is not None else b""
-    offset_to_points = header_size + len(vlrs)
 
     # LASzip's coordinate: scale * X + offset (the header box holds them all)
     xs = X.astype(np.float64) * sc[0] + of[0]
     ys = Y.astype(np.float64) * sc[1] + of[1]
     zs = Z.astype(np.float64) * sc[2] + of[2]
+    ret = (recs["bits"] & 7).astype(np.int64)
+    byret = np.bincount(np.clip(ret, 1, 5) - 1, minlength=5)[:5] if n else np.zeros(5, np.int64)
+    bbox = (xs.max(), xs.min(), ys.max(), ys.min(), zs.max(), zs.min()) if n else None
+    h = las_header(n, pdrf=pdrf, version_minor=version_minor, record_length=dt.itemsize, vlrs=vlrs,
+                   has_extra=extra is not None or bool(extras), scale=sc, offset=of, bbox=bbox, by_return=byret)
+    return h + recs.tobytes()
+
+
+def las_header(n: int, *, pdrf: int, version_minor: int, record_length: int, vlrs: bytes, has_extra: bool, scale, offset,
+               bbox, by_return) -> bytes:
+    """Header and VLRs of an uncompressed LAS file of n points: bbox is
+    (max x, min x, max y, min y, max z, min z) of the coordinates,
+    by_return the point counts by return number 1-5."""
+    header_size = 227 if version_minor <= 2 else 375
+    offset_to_points = header_size + len(vlrs)
+    sc, of, byret = scale, offset, by_return
     h = bytearray(header_size)
     h[0:4] = b"LASF"
     h[24], h[25] = 1, version_minor
@@ -136,23 +150,21 @@ def write_las(X, Y, Z, attrs: dict, *, pdrf: int, version_minor: int,
     struct.pack_into("<HH", h, 90, 1, 2024)
     struct.pack_into("<H", h, 94, header_size)
     struct.pack_into("<I", h, 96, offset_to_points)
-    struct.pack_into("<I", h, 100, 1 if (extra is not None or extras) else 0)
+    struct.pack_into("<I", h, 100, 1 if has_extra else 0)
     struct.pack_into("<B", h, 104, pdrf)
-    struct.pack_into("<H", h, 105, dt.itemsize)
+    struct.pack_into("<H", h, 105, record_length)
     struct.pack_into("<I", h, 107, n if n < 2**32 else 0)
-    ret = (recs["bits"] & 7).astype(np.int64)
-    byret = np.bincount(np.clip(ret, 1, 5) - 1, minlength=5)[:5] if n else np.zeros(5, np.int64)
     struct.pack_into("<5I", h, 111, *[int(v) if n < 2**32 else 0 for v in byret])
     struct.pack_into("<3d", h, 131, *sc)
     struct.pack_into("<3d", h, 155, *of)
     if n:
-        struct.pack_into("<6d", h, 179, xs.max(), xs.min(), ys.max(), ys.min(), zs.max(), zs.min())
+        struct.pack_into("<6d", h, 179, *bbox)
     if version_minor >= 4:
         struct.pack_into("<Q", h, 235, 0)
         struct.pack_into("<I", h, 243, 0)
         struct.pack_into("<Q", h, 247, n)
         struct.pack_into("<15Q", h, 255, *([int(v) for v in byret] + [0] * 10))
-    return bytes(h) + vlrs + recs.tobytes()
+    return bytes(h) + vlrs
 
 
 def _common_attrs(rng, n, z):

@@ -23,3 +23,19 @@ def test_header_box_is_exact(kind):
     assert mnx == xyz[:, 0].min() * 0.001 and mx == xyz[:, 0].max() * 0.001
     assert mny == xyz[:, 1].min() * 0.001 and my == xyz[:, 1].max() * 0.001
     assert mnz == xyz[:, 2].min() * 0.001 and mz == xyz[:, 2].max() * 0.001
+
+
+@pytest.mark.parametrize("kind,kw", [("strips", {}), ("terrain", {"pdrf": 2}), ("terrain", {"pdrf": 3, "extent": 1500.0})])
+def test_gpu_generator_images_are_valid_las(oracle, kind, kw):
+    # the torch generator of the large workloads, run on the CPU here: the
+    # image parses, every point lies in its header box, and the oracle
+    # converts it
+    import torch
+    from potreeconverter_b200 import synth_gpu
+    n = 60_000
+    host = torch.empty(400 + n * 34, dtype=torch.uint8)
+    img = getattr(synth_gpu, kind)(n, 5, device="cpu", host=host, **kw)
+    las = bytes(img.numpy())
+    X, Y, Z, cell, grid = oracle.decode_count(las)
+    assert X.shape[0] == n and int(grid.sum()) == n
+    assert len(oracle.convert(las, "poisson")["octree.bin"]) > 0
