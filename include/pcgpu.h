@@ -157,6 +157,9 @@ typedef struct pcg_stats {
 	int64_t records_resident;     /* 1: the records stayed on the device
 	                                 between the passes of a conversion in
 	                                 parts                                   */
+	int64_t device_estimate_bytes; /* the request loop's admission estimate
+	                                 of this job's device memory (a job in
+	                                 one piece)                              */
 } pcg_stats;
 
 /* One completed node: what the reference's hierarchy flusher records for it

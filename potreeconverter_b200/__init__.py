@@ -82,7 +82,7 @@ class _Stats(ctypes.Structure):
                 ("replayed_candidates", ctypes.c_int64), ("ms_lists", ctypes.c_double), ("list_entries", ctypes.c_int64),
                 ("cluster_nodes", ctypes.c_int64), ("ms_decode", ctypes.c_double), ("laz_chunks", ctypes.c_int64),
                 ("device_peak_bytes", ctypes.c_int64), ("parts", ctypes.c_int64), ("survivors", ctypes.c_int64),
-                ("records_resident", ctypes.c_int64)]
+                ("records_resident", ctypes.c_int64), ("device_estimate_bytes", ctypes.c_int64)]
 
 
 class _Node(ctypes.Structure):

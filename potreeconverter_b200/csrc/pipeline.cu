@@ -449,6 +449,15 @@ struct CompletionOrder {
 	}
 };
 
+// Device memory a job of `points` points and `record_bytes` bytes of point
+// records is expected to hold at its peak (the request loop's admission
+// figure): the records, a per-point working set and the count grid and LUT.
+// Checked against pcg_stats.device_peak_bytes by the request-loop tests.
+constexpr int64_t kJobBytesPerPoint = 400;
+inline size_t estimate_footprint(int64_t points, int64_t record_bytes) {
+	return (size_t)(record_bytes + points * kJobBytesPerPoint) + (size_t(256) << 20);
+}
+
 struct Converter {
 	int device = 0;
 	cudaStream_t stream = nullptr;
@@ -508,6 +517,11 @@ struct Converter {
 		DeviceMem mem(stream, arena.get());
 		if (arena) arena->reset_peak();
 		res.stats.num_points = N;
+		{
+			int64_t rb = 0;
+			for (auto& L : infos) rb += L.num_points * (int64_t)L.record_length;
+			res.stats.device_estimate_bytes = (int64_t)estimate_footprint(N, rb);
+		}
 
 		// ---------------------------------------------------------- input
 		// host sources are copied back to back (16-byte aligned) into one
@@ -894,7 +908,7 @@ struct Converter {
 	// ids, the level buffers of the sampler, sort and conflict-list scratch;
 	// calibrated against pcg_stats.device_peak_bytes), and the tile of the
 	// streamed passes.
-	static constexpr int64_t kPartBytesPerPoint = 400;
+	static constexpr int64_t kPartBytesPerPoint = kJobBytesPerPoint;
 	static constexpr int64_t kTilePoints = int64_t(1) << 24;
 	int records_mode = PCG_RECORDS_AUTO;  // pcg_records
 	int64_t group_points = 0;             // pcg_opts.group_points
@@ -1727,6 +1741,7 @@ struct pcg_ctx {
 		std::string error;
 		pcg::JobResult result;
 		size_t footprint = 0;
+		int bypassed = 0;  // times a later job was admitted before it
 	};
 	std::mutex qmtx;
 	std::condition_variable qcv;
@@ -1811,10 +1826,11 @@ void move_result(pcg::JobResult& r, pcg_result* out, int device) {
 	}
 }
 
-// Bytes of point records a source image stands for: its header's point
-// count x record length (a LAZ image is several times smaller than the
-// records it decodes to), at least the image size.
-size_t record_bytes(const void* image, size_t size) {
+// Points and bytes of point records a source image stands for: its
+// header's point count x record length (a LAZ image is several times
+// smaller than the records it decodes to), at least the image size.
+size_t record_bytes(const void* image, size_t size, size_t* points = nullptr) {
+	if (points) *points = size / 20;
 	const uint8_t* h = static_cast<const uint8_t*>(image);
 	if (size < 227 || std::memcmp(h, "LASF", 4) != 0) return size;
 	uint16_t header_size, rec_len;
@@ -1829,14 +1845,13 @@ size_t record_bytes(const void* image, size_t size) {
 		if (ext > count) count = ext;
 	}
 	if (count > (uint64_t(1) << 32)) return size;  // implausible; parsing will refuse it
+	if (points) *points = count;
 	const uint64_t bytes = count * rec_len;
 	return bytes > size ? (size_t)bytes : size;
 }
 
-size_t estimate_footprint(size_t record_bytes) {
-	// point records + positions/ids/keys per point, plus headroom
-	return record_bytes * 3 + (record_bytes / 20) * 64 + (size_t(64) << 20);
-}
+
+constexpr int kMaxBypass = 16;
 
 void worker_main(pcg_ctx* ctx, int wi) {
 	pcg::Converter conv = ctx->conv;
@@ -1848,14 +1863,23 @@ void worker_main(pcg_ctx* ctx, int wi) {
 		std::shared_ptr<pcg_ctx::Job> job;
 		{
 			std::unique_lock<std::mutex> lk(ctx->qmtx);
-			ctx->qcv.wait(lk, [&] {
-				if (ctx->stopping) return true;
-				return !ctx->queue.empty() && (ctx->in_use == 0 || ctx->in_use + ctx->queue.front()->footprint <= ctx->budget);
-			});
+			// first fit: the oldest job whose footprint fits the memory left
+			// (any job when nothing runs); a job bypassed kMaxBypass times
+			// blocks the ones behind it until it fits
+			auto pick = [&]() -> std::deque<std::shared_ptr<pcg_ctx::Job>>::iterator {
+				for (auto it = ctx->queue.begin(); it != ctx->queue.end(); ++it) {
+					if (ctx->in_use == 0 || ctx->in_use + (*it)->footprint <= ctx->budget) return it;
+					if ((*it)->bypassed >= kMaxBypass) break;
+				}
+				return ctx->queue.end();
+			};
+			ctx->qcv.wait(lk, [&] { return ctx->stopping || pick() != ctx->queue.end(); });
 			if (ctx->stopping && ctx->queue.empty()) return;
-			if (ctx->queue.empty()) continue;
-			job = ctx->queue.front();
-			ctx->queue.pop_front();
+			auto it = pick();
+			if (it == ctx->queue.end()) continue;
+			for (auto b = ctx->queue.begin(); b != it; ++b) (*b)->bypassed++;
+			job = *it;
+			ctx->queue.erase(it);
 			ctx->in_use += job->footprint;
 		}
 		pcg_job pj{};
@@ -2054,22 +2078,9 @@ pcg_status pcg_submit(pcg_ctx* ctx, const pcg_job* job, uint64_t* job_id) {
 	for (int32_t i = 0; i < job->num_attributes; i++)
 		if (!job->attributes[i]) return PCG_BAD_INPUT;
 	return guarded(ctx, [&] {
-		std::lock_guard<std::mutex> lk(ctx->qmtx);
-		if (ctx->workers.empty()) {
-			size_t free_b = 0, total_b = 0;
-			PCG_CUDA(cudaSetDevice(ctx->conv.device));
-			PCG_CUDA(cudaMemGetInfo(&free_b, &total_b));
-			ctx->budget = (size_t)(free_b * 0.8);
-			const int nworkers = 4;
-			for (int i = 0; i < nworkers; i++) {
-				cudaStream_t s;
-				PCG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-				ctx->worker_streams.push_back(s);
-			}
-			for (int i = 0; i < nworkers; i++) ctx->workers.emplace_back(worker_main, ctx, i);
-		}
+		// the images are copied before the queue is locked, so a large job's
+		// copy does not hold up the workers
 		auto j = std::make_shared<pcg_ctx::Job>();
-		j->id = ctx->next_id++;
 		size_t total = 0;
 		for (auto& src : srcs) {
 			j->src_off.push_back(total);
@@ -2090,9 +2101,28 @@ pcg_status pcg_submit(pcg_ctx* ctx, const pcg_job* job, uint64_t* job_id) {
 		j->name = job->name ? job->name : "";
 		j->projection = job->projection ? job->projection : "";
 		j->method = job->method;
-		size_t records = 0;
-		for (auto& src : srcs) records += record_bytes(src.las, src.las_size);
-		j->footprint = estimate_footprint(records);
+		size_t records = 0, points = 0;
+		for (auto& src : srcs) {
+			size_t np = 0;
+			records += record_bytes(src.las, src.las_size, &np);
+			points += np;
+		}
+		j->footprint = pcg::estimate_footprint((int64_t)points, (int64_t)records);
+		std::lock_guard<std::mutex> lk(ctx->qmtx);
+		if (ctx->workers.empty()) {
+			size_t free_b = 0, total_b = 0;
+			PCG_CUDA(cudaSetDevice(ctx->conv.device));
+			PCG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+			ctx->budget = (size_t)(free_b * 0.8);
+			const int nworkers = 4;
+			for (int i = 0; i < nworkers; i++) {
+				cudaStream_t s;
+				PCG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+				ctx->worker_streams.push_back(s);
+			}
+			for (int i = 0; i < nworkers; i++) ctx->workers.emplace_back(worker_main, ctx, i);
+		}
+		j->id = ctx->next_id++;
 		ctx->jobs[j->id] = j;
 		ctx->queue.push_back(j);
 		*job_id = j->id;

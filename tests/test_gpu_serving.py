@@ -35,3 +35,28 @@ def test_poll_reports_completion_and_unknown_jobs_fail(gpu_ctx):
         assert conv.octree
         with pytest.raises(pc.PcgError):
             ctx.poll(j + 1000)
+
+
+@pytest.mark.parametrize("kind", ["terrain", "hotspots", "lattice", "strips"])
+@pytest.mark.parametrize("n", [100_000, 1_000_000, 5_000_000])
+def test_admission_estimate_covers_the_device_peak(gpu_ctx, kind, n):
+    # the request loop admits jobs by an estimate of their device memory;
+    # it must never be below what the job actually held at its peak
+    las = synth.generate(kind, n, 60 + n // 100_000)
+    for method in ("poisson", "poisson_average", "random"):
+        st = gpu_ctx.convert_stats(las, method=method, name="fp")
+        assert st["device_peak_bytes"] > 0
+        assert st["device_estimate_bytes"] >= st["device_peak_bytes"], (method, st["device_peak_bytes"])
+
+
+def test_large_job_ahead_of_small_jobs():
+    # a large job at the head of the queue and small jobs behind it, which
+    # the first-fit admission may start before it: every result is exact
+    big = synth.generate("hotspots", 3_000_000, 61)
+    small = [synth.generate("terrain", 100_000, 62 + i) for i in range(6)]
+    with pc.Context() as ctx:
+        alone = [ctx.convert(las, method="poisson", name="s").octree for las in small]
+        ids = [ctx.submit(big, method="poisson", name="b")] + [ctx.submit(las, method="poisson", name="s") for las in small]
+        res = [ctx.wait(j) for j in ids]
+    assert [r.octree for r in res[1:]] == alone
+    assert res[0].stats["num_points"] == 3_000_000
