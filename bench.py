@@ -18,9 +18,19 @@ all sampler levels, octree.bin payloads, hierarchy.bin, metadata.json).
          on the host cores, each step a bounded sample of the workload
   plain_form  the plain form (one launch per node, every neighbour test in
          FP64) on the same workload, one step, and the batched/plain ratio
-  serving  eight jobs of 0.5-4M points submitted together to the request
-         loop after one warm-up round of the same mix; p50/p99 latency from
-         submit to completion, and the makespan
+  parity   one conversion of the benchmarked cloud with each sampler, md5 of
+         octree.bin, hierarchy.bin and metadata.json against the pinned
+         reference's digests (tests/golden/golden.json large_cases)
+  parts_form  the aerial-strip cloud (config-3 shape, poisson_average) at
+         the largest size half the host memory holds (at most 3B points),
+         converted in parts from page-locked host memory; Mpts/s host to
+         host, beside the plain form on a 10M-point cloud of the same
+         generator
+  serving  the request-loop replay (config-4 shape): jobs of log-uniform
+         100k-50M points (terrain generator, own seed and extent 100-2000 m,
+         point format 2 or 3, samplers 60/30/10 % poisson / poisson_average
+         / random) submitted at Poisson arrival times; p50/p99 latency from
+         arrival to completion and the aggregate Mpts/s
 
 Multi-GPU: the build path does not shard within one cloud (one GPU per cloud,
 replicas only); with N ranks every rank converts its own seeded cloud and
@@ -48,6 +58,7 @@ WORKLOAD = {"workload": "hotspots-50M", "points": 50_000_000, "las": "1.4", "poi
             "extra_attributes": "1 x float32", "extent_m": [2000, 2000, 50], "hotspots": 20,
             "sampler": "poisson", "form": "batched", "l2": "inputs larger than L2 (1.9 GB records)"}
 REF_SAMPLE_POINTS = 2_000_000
+GOLDEN = os.path.join(REPO, "tests", "golden", "golden.json")
 # DRAM bytes (read + write) per candidate of the acceptance kernel, from the
 # ncu capture summarised in profiles/accept_hotspots-5M_poisson.md
 ACCEPT_DRAM_BYTES_PER_CANDIDATE = 225.6
@@ -196,6 +207,138 @@ def run_reference_arm(args):
     }))
 
 
+def parity_leg(ctx, pinned, n):
+    """md5 of the three outputs of the benchmarked cloud with each sampler
+    against the pinned reference's digests (golden large_cases)."""
+    import hashlib
+    try:
+        with open(GOLDEN) as f:
+            case = next(c for c in json.load(f).get("large_cases", []) if c["name"] == "hotspots_50m")
+    except (OSError, StopIteration):
+        return {"md5_match": None, "why": "no golden digests for the 50M hot-spot cloud"}
+    if n != case["points"]:
+        return {"md5_match": None, "why": f"workload of {n} points, digests for {case['points']}"}
+    las_md5 = hashlib.md5(memoryview(pinned.numpy())).hexdigest()
+    out = {"las_md5_match": las_md5 == case["las_md5"], "samplers": {}}
+    for method in ("poisson", "poisson_average", "random"):
+        conv = ctx.convert((pinned.data_ptr(), pinned.numel()), method=method, name=case["name"])
+        got = {"octree.bin": conv.octree, "hierarchy.bin": conv.hierarchy, "metadata.json": conv.metadata.encode()}
+        out["samplers"][method] = all(hashlib.md5(got[f]).hexdigest() == case["outputs"][method][f]["md5"] for f in got)
+        del conv, got
+    out["md5_match"] = out["las_md5_match"] and all(out["samplers"].values())
+    out["reference"] = "pinned reference digests, tests/golden/golden.json large_cases hotspots_50m"
+    return out
+
+
+def host_points_budget(bytes_per_point: float) -> int:
+    """Points whose page-locked input and output fit half the host memory
+    available now."""
+    try:
+        with open("/proc/meminfo") as f:
+            avail = next(int(l.split()[1]) * 1024 for l in f if l.startswith("MemAvailable"))
+    except (OSError, StopIteration):
+        avail = 64 << 30
+    return int(avail / 2 / bytes_per_point)
+
+
+def parts_leg(local, stream, points, steps):
+    """Config-3 shape: the aerial-strip cloud, poisson_average, converted in
+    parts from page-locked host memory; Mpts/s from host records to the
+    three outputs in host memory (the pieces of octree.bin included)."""
+    import torch
+    import potreeconverter_b200 as pc
+    from potreeconverter_b200 import synth_gpu
+    t0 = time.perf_counter()
+    img = synth_gpu.strips(points, 1003, device=torch.device("cuda", local))
+    gen_s = time.perf_counter() - t0
+    out = {"workload": "strips", "points": points, "point_format": 3, "sampler": "poisson_average",
+           "extent_m": [20000, 20000], "strips": 40, "generator": "potreeconverter_b200.synth_gpu.strips seed 1003",
+           "generate_s": round(gen_s, 1)}
+    with pc.Context(device=local, stream=stream.cuda_stream) as ctx:
+        st = ctx.convert_stats((img.data_ptr(), img.numel()), method="poisson_average", name="strips")  # warm-up
+        times = []
+        for _ in range(steps):
+            t = time.perf_counter()
+            st = ctx.convert_stats((img.data_ptr(), img.numel()), method="poisson_average", name="strips")
+            times.append(time.perf_counter() - t)
+    ms = 1e3 * statistics.median(times)
+    out.update({"value": points / (ms * 1e3), "unit": "Mpts/s", "ms_per_step": ms, "steps": steps,
+                "parts": int(st["parts"]), "survivors": int(st["survivors"]), "records_resident": bool(st["records_resident"]),
+                "device_peak_gb": round(st["device_peak_bytes"] / 1e9, 2), "output_points": int(st["output_points"]),
+                "h2d_bytes_per_step": int(img.numel()), "d2h_bytes_per_step": int(st["octree_size"]),
+                "stages_ms": {k: round(st[k], 1) for k in ("ms_h2d", "ms_chunking", "ms_octree", "ms_sampling", "ms_output",
+                                                          "ms_d2h", "ms_host_writers", "ms_total")}})
+    del img
+    # the plain form on a cloud of the same generator (one launch per node,
+    # every neighbour test in FP64), 10M points
+    pn = 10_000_000
+    small = synth_gpu.strips(pn, 1003, device=torch.device("cuda", local))
+    with pc.Context(device=local, stream=stream.cuda_stream, form="plain") as pctx:
+        t = time.perf_counter()
+        pctx.convert_stats((small.data_ptr(), small.numel()), method="poisson_average", name="strips")
+        p_s = time.perf_counter() - t
+    with pc.Context(device=local, stream=stream.cuda_stream) as bctx:
+        bctx.convert_stats((small.data_ptr(), small.numel()), method="poisson_average", name="strips")
+        t = time.perf_counter()
+        bctx.convert_stats((small.data_ptr(), small.numel()), method="poisson_average", name="strips")
+        b_s = time.perf_counter() - t
+    out["plain_form_10M"] = {"value": pn / (p_s * 1e6), "unit": "Mpts/s", "batched_value": pn / (b_s * 1e6),
+                             "batched_over_plain": p_s / b_s}
+    out["parts_over_plain"] = out["value"] / (pn / (p_s * 1e6))
+    return out
+
+
+def serving_leg(local, jobs: int, rate: float, seed: int = 2000):
+    """Config-4 shape replay: `jobs` jobs with Poisson arrivals at `rate`
+    jobs/s (log-uniform 100k-50M points, terrain generator with its own seed
+    and extent 100-2000 m, point format 2 or 3, samplers 60/30/10 %),
+    submitted at their arrival times; latency = arrival to completion."""
+    import numpy as np
+    import torch
+    import potreeconverter_b200 as pc
+    from potreeconverter_b200 import synth_gpu
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(1e5), np.log(5e7), jobs)).astype(np.int64)
+    extents = rng.uniform(100.0, 2000.0, jobs)
+    methods = rng.choice(["poisson", "poisson_average", "random"], jobs, p=[0.6, 0.3, 0.1])
+    pdrfs = rng.choice([2, 3], jobs)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, jobs))
+    dev = torch.device("cuda", local)
+    t0 = time.perf_counter()
+    images = [synth_gpu.terrain(int(sizes[j]), seed + j, float(extents[j]), int(pdrfs[j]), device=dev) for j in range(jobs)]
+    gen_s = time.perf_counter() - t0
+    with pc.Context(device=local) as ctx:
+        # warm-up: the worker streams, their arenas and the pinned pool
+        for j in [ctx.submit((images[i].data_ptr(), images[i].numel()), method=methods[i], name="w") for i in range(min(8, jobs))]:
+            ctx.wait(j)
+        ids, t_done = [None] * jobs, [None] * jobs
+        start = time.perf_counter()
+        nxt = 0
+        pending = set()
+        while nxt < jobs or pending:
+            now = time.perf_counter() - start
+            while nxt < jobs and arrivals[nxt] <= now:
+                ids[nxt] = ctx.submit((images[nxt].data_ptr(), images[nxt].numel()), method=methods[nxt], name=f"job{nxt}")
+                pending.add(nxt)
+                nxt += 1
+            for i in list(pending):
+                if ctx.poll(ids[i]):
+                    t_done[i] = time.perf_counter() - start
+                    pending.discard(i)
+            time.sleep(0.0005)
+        makespan = max(t_done)
+        for j in ids:
+            ctx.wait(j)
+    del images
+    lat = np.array([1e3 * (t_done[i] - arrivals[i]) for i in range(jobs)])
+    return {"jobs": jobs, "arrival_rate_per_s": rate, "offered_mpts_per_s": float(sizes.sum() / arrivals[-1] / 1e6),
+            "points_total": int(sizes.sum()), "sizes": "log-uniform 100k-50M", "samplers": "60/30/10 % poisson/poisson_average/random",
+            "point_formats": [2, 3], "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(lat.max()), "makespan_s": makespan, "mpts_per_s": float(sizes.sum() / makespan / 1e6),
+            "worker_streams": 4, "generate_s": round(gen_s, 1),
+            "time_compression": f"{rate / 4.0:g}x the configuration's 4 jobs/s, {jobs} of its 2,000 jobs"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -206,6 +349,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form leg (one-launch-per-node form)")
     ap.add_argument("--no-serving", action="store_true", help="skip the request-loop latency leg")
+    ap.add_argument("--no-parity", action="store_true", help="skip the md5 check against the pinned reference")
+    ap.add_argument("--no-parts", action="store_true", help="skip the conversion-in-parts leg (config-3 shape)")
+    ap.add_argument("--parts-points", type=int, default=0, help="points of the parts leg (0: as many as host memory holds, <= 3B)")
+    ap.add_argument("--serving-jobs", type=int, default=200)
+    ap.add_argument("--serving-rate", type=float, default=16.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -306,36 +454,21 @@ def main():
         plain = {"value": n / (p_ms * 1e3), "unit": "Mpts/s", "ms_per_step": p_ms, "steps": 1,
                  "batched_over_plain": (n / (ms * 1e3)) / (n / (p_ms * 1e3))}
 
-    # ---- request loop: jobs of mixed sizes submitted together (from host
-    # memory, through pcg_submit), latency = submit to completion
+    # ---- parity of the benchmarked workload (one conversion per sampler,
+    # outside the timed region)
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = parity_leg(ctx, pinned, n)
+
+    # ---- the request-loop replay (config-4 shape) and the conversion in
+    # parts (config-3 shape), single GPU runs only
     serving = None
     if world == 1 and not args.no_serving:
-        sizes = [500_000, 1_000_000, 2_000_000, 4_000_000] * 2
-        jobs = [synth.hotspots(m, 3000 + i) for i, m in enumerate(sizes)]
-        with pc.Context(device=local) as sctx:
-            # warm-up: one round of the whole mix, so every worker stream,
-            # its device arena and the pinned staging buffers are in use
-            for j in [sctx.submit(las, method="poisson", name="warm") for las in jobs]:
-                sctx.wait(j)
-            t_sub, t_done, ids = {}, {}, []
-            t0 = time.perf_counter()
-            for i, las in enumerate(jobs):
-                ids.append(sctx.submit(las, method="poisson", name=f"job{i}"))
-                t_sub[i] = time.perf_counter()
-            pending = set(range(len(ids)))
-            while pending:
-                for i in list(pending):
-                    if sctx.poll(ids[i]):
-                        t_done[i] = time.perf_counter()
-                        pending.discard(i)
-                time.sleep(0.0005)
-            makespan = max(t_done.values()) - t0
-            for j in ids:
-                sctx.wait(j)
-        lat = sorted(1e3 * (t_done[i] - t_sub[i]) for i in range(len(ids)))
-        serving = {"jobs": len(sizes), "points": sizes, "sampler": "poisson", "p50_ms": statistics.median(lat),
-                   "p99_ms": lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))], "makespan_ms": 1e3 * makespan,
-                   "mpts_per_s": sum(sizes) / (makespan * 1e6), "worker_streams": 4}
+        serving = serving_leg(local, args.serving_jobs, args.serving_rate)
+    parts = None
+    if world == 1 and not args.no_parts:
+        pts = args.parts_points or min(3_000_000_000, host_points_budget(34 + 35 * 1.7))
+        parts = parts_leg(local, stream, pts, 2)
 
     if rank == 0:
         cpu = None
@@ -345,10 +478,10 @@ def main():
                 p = os.path.join(tmp, "sample.las")
                 with open(p, "wb") as f:
                     f.write(sample)
-                pts, secs = cpu_reference_step(p, os.path.join(tmp, "out"))
+                secs = statistics.median(cpu_reference_step(p, os.path.join(tmp, f"out{k}"))[1] for k in range(3))
             cpu = {"value": REF_SAMPLE_POINTS / secs / 1e6, "unit": "Mpts/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"{REF_SAMPLE_POINTS} points of the same generator, stock reference converter, "
-                             f"duration(chunking-total)+duration(indexing), {os.cpu_count()} threads"}
+                             f"duration(chunking-total)+duration(indexing), median of 3, {os.cpu_count()} threads"}
         line = {
             "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -368,6 +501,8 @@ def main():
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "plain_form": plain,
+            "parity": parity,
+            "parts_form": parts,
             "serving": serving,
             "escalated_pairs": int(s["escalated_pairs"]),
             "sampler": {k: int(s[k]) for k in ("sampled_nodes", "candidates", "replayed_nodes", "replayed_candidates",

@@ -177,13 +177,13 @@ public:
 	}
 
 private:
-	// pinned memory kept for reuse: a quarter of the host's memory, at most
+	// pinned memory kept for reuse: a third of the host's memory, at most
 	// 64 GiB (the pieces of a large conversion are reused by the next one)
 	static size_t max_cached() {
 		static const size_t m = [] {
 			const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGE_SIZE);
 			const size_t phys = pages > 0 && page > 0 ? (size_t)pages * (size_t)page : (size_t(32) << 30);
-			return std::max(size_t(8) << 30, std::min(size_t(64) << 30, phys / 4));
+			return std::max(size_t(8) << 30, std::min(size_t(64) << 30, phys / 3));
 		}();
 		return m;
 	}

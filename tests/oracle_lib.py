@@ -122,7 +122,7 @@ class Oracle:
         """createLUT of a count grid: (chunks, lut) like Context.lut."""
         g = np.ascontiguousarray(grid, dtype=np.int64)
         lut = np.empty(grid_size ** 3, np.int32)
-        cap = 1 << 16
+        cap = grid_size ** 3  # at most one chunk per cell
         ids = ctypes.create_string_buffer(16 * cap)
         info = np.empty(5 * cap, np.int64)
         num = ctypes.c_int64()
