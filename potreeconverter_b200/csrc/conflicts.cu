@@ -20,9 +20,19 @@
 //  4. one thread per candidate in cell order (a warp shares neighbourhoods)
 //     scans the occupied cells among its 27 up to its own sorted position:
 //     the FP32 distance on node-relative coordinates decides every pair
-//     outside the band s^2 (1 -/+ 1e-3) (its rounding error is below 1e-4 of
-//     s^2); pairs inside the band are decided by the reference's FP64 test
-//     and counted as escalated; then the early-exit bound.
+//     outside the band s^2 (1 -/+ 1e-3); pairs inside the band are decided
+//     by the reference's FP64 test and counted as escalated; then the
+//     early-exit bound. Error bound (u = 2^-24): a node-relative coordinate
+//     v lies in [0, L], L = 128 s, so its float differs from the FP64 value
+//     by at most L u = 128 s u; a coordinate difference d (|d| about s in the
+//     band) then carries at most 256 s u + |d| u, its square a relative
+//     error of 2 (257 u) + u, and the sum of three squares at most 517 u
+//     = 3.1e-5 of the squared distance D. The FP64 values the reference
+//     compares are themselves within 1.1e-16 |x| of the exact coordinates,
+//     below 1.1e-10 s when |x| < 1e6 s (checked per node; beyond it the
+//     node uses FP64 alone). So D32 >= s^2 (1 + 1e-3) (rounded up by at
+//     most u) implies D64 > s^2, and D32 < s^2 (1 - 1e-3) implies D64 < s^2:
+//     the margin is 30x the error.
 // A candidate with more than kListCap such predecessors marks its node
 // dense; dense nodes keep the grid-based acceptance kernel.
 
@@ -175,7 +185,12 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 		lim = limit * limit;
 	}
 	// node-relative FP32 coordinates: error far below the 1e-3 margin on s^2
-	const bool pre32 = s2 > 1e-30 && s2 < 1e30;
+	// (the bound on its error, derived for node-relative coordinates below
+	// 128 spacings, holds while the FP64 coordinates themselves carry a
+	// rounding error far below the spacing: |coordinate| < 1e6 spacings)
+	double amax = 0.0;
+	for (int a = 0; a < 3; a++) amax = fmax(amax, fmax(fabs(nd.min[a]), fabs(nd.max[a])));
+	const bool pre32 = s2 > 1e-30 && s2 < 1e30 && amax < 1e6 * sp;
 	const float s2hi = (float)(s2 * 1.001), s2lo = (float)(s2 * 0.999);
 	unsigned escalated = 0;  // pairs inside the band, decided in FP64
 	const uint64_t c = ck[j];
