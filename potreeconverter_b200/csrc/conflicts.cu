@@ -195,7 +195,10 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 	unsigned escalated = 0;  // pairs inside the band, decided in FP64
 	const uint64_t c = ck[j];
 	const int cx = (int)(c % kCellsPerAxis), cy = (int)((c / kCellsPerAxis) % kCellsPerAxis), cz = (int)(c / (kCellsPerAxis * kCellsPerAxis));
-	int32_t* out = cl.entries + (co + t) * (int64_t)kListCap;
+	// the first kListInline entries in registers, the rest (rare) in a
+	// per-thread array; both are stored once the search is done
+	int4 head = make_int4(0, 0, 0, 0);
+	int32_t rest[kListCap - kListInline];
 	int n = 0;
 	const int64_t boff = bm_off[node];
 	for (int dz = -1; dz <= 1; dz++) {
@@ -244,16 +247,32 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 						if (!(dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < s2)) continue;
 					}
 					if (MODE == 0 && !(lb.keys[co + u] >= lim)) continue;
-					if (n < kListCap) out[n] = u;
+					if (n == 0) head.x = u;
+					else if (n == 1) head.y = u;
+					else if (n == 2) head.z = u;
+					else if (n == 3) head.w = u;
+					else if (n < kListCap) rest[n - kListInline] = u;
 					n++;
 				}
 			}
 		}
 	}
-	cl.count[co + t] = (uint8_t)(n <= kListCap ? n : kListDense);
-	if (n > kListCap) cl.node_dense[node] = 1;
+	cl.inl[co + t] = head;
+	bool dense = n > kListCap;
+	if (!dense && n > kListInline) {
+		const int extra = n - kListInline;
+		const unsigned long long at = atomicAdd(cl.pool_used, (unsigned long long)extra);
+		if ((int64_t)(at + extra) <= cl.pool_cap) {
+			cl.ovf_off[co + t] = (int32_t)at;
+			for (int e = 0; e < extra; e++) cl.pool[at + e] = rest[e];
+		} else {
+			dense = true;  // the pool is full: this node keeps the lookup kernels
+		}
+	}
+	cl.count[co + t] = (uint8_t)(dense ? kListDense : n);
+	if (dense) cl.node_dense[node] = 1;
 	const unsigned active = __activemask();
-	const unsigned sum = __reduce_add_sync(active, (unsigned)(n <= kListCap ? n : kListCap));
+	const unsigned sum = __reduce_add_sync(active, (unsigned)(dense ? 0 : n));
 	const unsigned esc = __reduce_add_sync(active, escalated);
 	if ((int)(threadIdx.x & 31) == __ffs(active) - 1) {
 		atomicAdd(&st->list_entries, (unsigned long long)sum);
@@ -311,7 +330,15 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 		conf_bitmap_kernel<<<blocks, 256, 0, s>>>(lb.node_of, ck, M, d_bm_off, bm);
 		PCG_LAUNCHED();
 	}
-	cl.entries = mem.alloc<int32_t>((size_t)M * kListCap);
+	cl.inl = mem.alloc<int4>(M);
+	cl.ovf_off = mem.alloc<int32_t>(M);
+	// entries past the inline ones: room for 4 more per candidate on
+	// average (lists average about one entry); a node whose candidates find
+	// the pool full keeps the lookup kernels
+	cl.pool_cap = std::min<int64_t>((int64_t)M * kListInline, (int64_t)INT32_MAX);
+	cl.pool = mem.alloc<int32_t>(cl.pool_cap > 0 ? cl.pool_cap : 1);
+	cl.pool_used = mem.alloc<unsigned long long>(1);
+	PCG_CUDA(cudaMemsetAsync(cl.pool_used, 0, sizeof(unsigned long long), s));
 	cl.count = mem.alloc<uint8_t>(M);
 	cl.node_dense = mem.alloc<uint8_t>(K);
 	PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
@@ -332,7 +359,10 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 }
 
 void free_conflict_lists(ConflictLists& cl, DeviceMem& mem) {
-	if (cl.entries) mem.free(cl.entries);
+	if (cl.inl) mem.free(cl.inl);
+	if (cl.ovf_off) mem.free(cl.ovf_off);
+	if (cl.pool) mem.free(cl.pool);
+	if (cl.pool_used) mem.free(cl.pool_used);
 	if (cl.count) mem.free(cl.count);
 	if (cl.node_dense) mem.free(cl.node_dense);
 	cl = ConflictLists{};

@@ -936,8 +936,7 @@ __global__ void __launch_bounds__(kBigThreads) greedy_big_kernel(const LevelNode
 // ahead of the round that reads them (they were written by an earlier kernel
 // and usually sit in DRAM).
 __device__ __forceinline__ void prefetch_list(const ConflictLists& cl, const LevelBuffers& lb, int64_t co, int64_t u) {
-	const int32_t* row = cl.entries + (co + u) * (int64_t)kListCap;
-	asm volatile("prefetch.global.L2 [%0];" ::"l"(row));
+	asm volatile("prefetch.global.L2 [%0];" ::"l"(cl.inl + co + u));
 	asm volatile("prefetch.global.L2 [%0];" ::"l"(cl.count + co + u));
 	asm volatile("prefetch.global.L2 [%0];" ::"l"(lb.cq + co + u));
 }
@@ -1030,11 +1029,11 @@ __global__ void __launch_bounds__(kListThreads) greedy_list_kernel(const LevelNo
 		}
 		{
 			// lists are short (about one entry on average): loop to the
-			// warp's longest list, four entries per 16-byte load
-			const int4* lp = reinterpret_cast<const int4*>(cl.entries + (co + t) * (int64_t)kListCap);
+			// warp's longest list, four entries at a time (the first four in one
+			// 16-byte load)
 			const int wmax = (int)__reduce_max_sync(FULL, (unsigned)nl);
 			for (int w = 0; 4 * w < wmax; w++) {
-				const int4 v = 4 * w < nl ? lp[w] : make_int4(0, 0, 0, 0);
+				const int4 v = 4 * w < nl ? list_quad(cl, co + t, nl, w) : make_int4(0, 0, 0, 0);
 				const int32_t u4[4] = {v.x, v.y, v.z, v.w};
 				int32_t rk4[4];
 #pragma unroll
@@ -1254,10 +1253,9 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 			nl = cl.count[co + t];
 		}
 		{
-			const int4* lp = reinterpret_cast<const int4*>(cl.entries + (co + t) * (int64_t)kListCap);
 			const int wmax = (int)__reduce_max_sync(FULL, (unsigned)nl);
 			for (int w = 0; 4 * w < wmax; w++) {
-				const int4 v = 4 * w < nl ? lp[w] : make_int4(0, 0, 0, 0);
+				const int4 v = 4 * w < nl ? list_quad(cl, co + t, nl, w) : make_int4(0, 0, 0, 0);
 				const int32_t u4[4] = {v.x, v.y, v.z, v.w};
 				int32_t rk4[4];
 #pragma unroll
@@ -1478,10 +1476,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) greedy_list_warp_kernel(c
 				nl = cl.count[co + t];
 			}
 			{
-				const int4* lp = reinterpret_cast<const int4*>(cl.entries + (co + t) * (int64_t)kListCap);
 				const int wmax = (int)__reduce_max_sync(FULL, (unsigned)nl);
 				for (int w = 0; 4 * w < wmax; w++) {
-					const int4 v = 4 * w < nl ? lp[w] : make_int4(0, 0, 0, 0);
+					const int4 v = 4 * w < nl ? list_quad(cl, co + t, nl, w) : make_int4(0, 0, 0, 0);
 					const int32_t u4[4] = {v.x, v.y, v.z, v.w};
 					int32_t rk4[4];
 #pragma unroll

@@ -97,13 +97,31 @@ void launch_node_pos(const LevelNode* nodes, const std::vector<uint8_t>& pick, L
 // Earlier candidates of the same node that would reject a candidate if
 // accepted (within the spacing and, for poisson, not before the early-exit
 // bound), by sorted position; built for the nodes flagged in `use`.
+// A list holds at most kListCap entries: the first kListInline in the
+// candidate's own 16-byte slot, the rest in a pool shared by the level
+// (lists average about one entry, so a fixed row per candidate would be
+// mostly empty).
 constexpr int kListCap = 32;
+constexpr int kListInline = 4;
 constexpr uint8_t kListDense = 255;
 struct ConflictLists {
-	int32_t* entries = nullptr;     // [M * kListCap] node-local sorted positions
+	int4* inl = nullptr;            // [M] first entries (node-local sorted positions)
+	int32_t* ovf_off = nullptr;     // [M] where entries kListInline.. start in pool
+	int32_t* pool = nullptr;        // [pool_cap] the longer lists' remaining entries
+	unsigned long long* pool_used = nullptr;  // entries handed out of pool
+	int64_t pool_cap = 0;
 	uint8_t* count = nullptr;       // [M] by sorted position: entries, or kListDense past kListCap
 	uint8_t* node_dense = nullptr;  // [K] some candidate has more than kListCap
 };
+
+// entries 4w .. 4w + 3 of the list of candidate slot `idx` (nl entries);
+// positions past the list read as 0
+__device__ __forceinline__ int4 list_quad(const ConflictLists& cl, int64_t idx, int nl, int w) {
+	if (w == 0) return cl.inl[idx];
+	const int32_t* p = cl.pool + cl.ovf_off[idx] + 4 * (w - 1);
+	const int e = 4 * w;
+	return make_int4(e < nl ? p[0] : 0, e + 1 < nl ? p[1] : 0, e + 2 < nl ? p[2] : 0, e + 3 < nl ? p[3] : 0);
+}
 void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<LevelNode>& ln, const std::vector<uint8_t>& use,
                           const PosParamsS& pp, LevelBuffers& lb, ConflictLists& cl, std::vector<uint8_t>& dense, SampleStats* st,
                           DeviceMem& mem);
