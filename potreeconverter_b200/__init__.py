@@ -183,6 +183,8 @@ def _copy_out(ptr, size: int) -> bytes:
     images of 2 GiB and more are copied with memmove."""
     if not size:
         return b""
+    if not ptr:
+        raise ValueError("no buffer behind a non-empty result")
     if size < (1 << 31):
         return ctypes.string_at(ptr, size)
     buf = bytearray(size)
@@ -191,7 +193,7 @@ def _copy_out(ptr, size: int) -> bytes:
 
 
 def _take(lib, res: _Result) -> Conversion:
-    if res.octree or res.num_octree_parts <= 1:
+    if res.octree or not res.octree_parts:
         octree = _copy_out(res.octree, res.octree_size)
     else:  # a conversion in parts: octree.bin is its pieces back to back
         octree = b"".join(_copy_out(res.octree_parts[i].data, res.octree_parts[i].size)

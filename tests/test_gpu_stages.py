@@ -25,10 +25,23 @@ def stage(request, oracle):
     return StageInputs(oracle, case_las(kind, n, seed, json.dumps(kw, sort_keys=True)))
 
 
+def _same_chunks(got, exp):
+    # element by element, reporting the first difference (a plain list
+    # comparison of 10^5 chunks makes pytest's failure diff very slow)
+    assert len(got) == len(exp), f"{len(got)} chunks, expected {len(exp)}"
+    bad = next((i for i, (a, b) in enumerate(zip(got, exp)) if a != b), None)
+    assert bad is None, f"chunk {bad}: {got[bad]} != {exp[bad]}"
+
+
+def _same_lut(got, exp):
+    bad = np.nonzero(got != exp)[0]
+    assert bad.size == 0, f"{bad.size} LUT cells differ, first {bad[0]}: {got[bad[0]]} != {exp[bad[0]]}"
+
+
 def test_lut_matches_oracle(gpu_ctx, stage):
     chunks, lut = gpu_ctx.lut(stage.grid, stage.G, stage.mpc)
-    assert chunks == stage.chunks
-    assert (lut == stage.lut).all()
+    _same_chunks(chunks, stage.chunks)
+    _same_lut(lut, stage.lut)
 
 
 @pytest.mark.parametrize("mpc", [1, 5_000, 10**9])
@@ -36,14 +49,14 @@ def test_lut_merge_limits(gpu_ctx, oracle, stage, mpc):
     # every cell its own chunk, a mid-size limit, and one chunk for all
     exp_chunks, exp_lut = oracle.lut(stage.grid, stage.G, mpc)
     chunks, lut = gpu_ctx.lut(stage.grid, stage.G, mpc)
-    assert chunks == exp_chunks
-    assert (lut == exp_lut).all()
+    _same_chunks(chunks, exp_chunks)
+    _same_lut(lut, exp_lut)
 
 
 def test_scatter_matches_oracle(gpu_ctx, stage):
     ids, start = gpu_ctx.scatter(stage.cell, stage.lut, stage.G, len(stage.chunks))
-    assert (start == stage.chunk_start).all()
-    assert (ids == stage.ids).all()
+    assert np.array_equal(start, stage.chunk_start)
+    assert np.array_equal(ids, stage.ids)
 
 
 def test_scatter_empty_and_reversed(gpu_ctx, oracle, stage):
