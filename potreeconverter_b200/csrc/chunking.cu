@@ -65,12 +65,22 @@ __device__ __forceinline__ bool grid_cell(const DecodeParams& p, int32_t X, int3
 	return true;
 }
 
-// One thread per point (grid-stride). Writes the quantized position SoA and
-// the count-grid cell, counts into the grid with warp-aggregated atomics and
-// reduces attribute min/max (in registers, then shared memory, then one
-// global atomic per block and statistic).
-template <bool kMulti>
+// Records per tile of the staged decode: a block copies a tile of records
+// into shared memory with 16-byte loads (the tile is 16-byte aligned when the
+// source's records are, since kDecodeTile x record length is a multiple of
+// 16) and decodes its points from there.
+constexpr int kDecodeTile = 512;
+constexpr int kDecodeStageMaxRec = 96;  // 48 KB of shared memory per block
+
+// One thread per point. Writes the quantized position SoA and the count-grid
+// cell, counts into the grid with warp-aggregated atomics and reduces
+// attribute min/max (in registers, then shared memory, then one global atomic
+// per block and statistic). With kStaged (one source, 16-byte aligned
+// records, short records) the block walks tiles of kDecodeTile records staged
+// in shared memory; else it reads each record in place (grid-stride).
+template <bool kMulti, bool kStaged>
 __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodeParams p, uint32_t* __restrict__ grid, ChunkingOut out) {
+	extern __shared__ uint4 stage16[];
 	// shared statistics: [attr][comp] ordered min / max
 	__shared__ unsigned long long s_mn[MAX_ATTRS][3];
 	__shared__ unsigned long long s_mx[MAX_ATTRS][3];
@@ -87,9 +97,7 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodePara
 	IntRange r_int, r_ret, r_nret, r_cls, r_sar, r_user, r_psid, r_r, r_g, r_b;
 	r_int.init(); r_ret.init(); r_nret.init(); r_cls.init(); r_sar.init(); r_user.init(); r_psid.init(); r_r.init(); r_g.init(); r_b.init();
 
-	const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride) with_source<kMulti>(p, i, [&](const SourceDesc& sd) {
-		const uint8_t* r = sd.recs + (i - sd.first) * sd.rec_len;
+	auto point = [&](int64_t i, const uint8_t* r, const SourceDesc& sd) {
 		double x, y, z;
 		int32_t X, Y, Z;
 		quantize_record(p, sd, r, x, y, z, X, Y, Z);
@@ -155,7 +163,27 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodePara
 				atomicMax(&s_mx[d.stat_index][c], ordered(v));
 			}
 		}
-	});
+	};
+	if constexpr (kStaged) {
+		const SourceDesc& sd = p.src0;
+		const int rl = sd.rec_len;
+		const uint8_t* stage = reinterpret_cast<const uint8_t*>(stage16);
+		for (int64_t t0 = (int64_t)blockIdx.x * kDecodeTile; t0 < p.n; t0 += (int64_t)gridDim.x * kDecodeTile) {
+			const int cnt = (int)(p.n - t0 < kDecodeTile ? p.n - t0 : kDecodeTile);
+			const uint8_t* src = sd.recs + (t0 - sd.first) * rl;
+			const int bytes = cnt * rl, words = bytes >> 4;
+			for (int w = threadIdx.x; w < words; w += blockDim.x) stage16[w] = __ldg(reinterpret_cast<const uint4*>(src) + w);
+			for (int b = (words << 4) + threadIdx.x; b < bytes; b += blockDim.x)
+				reinterpret_cast<uint8_t*>(stage16)[b] = src[b];
+			__syncthreads();
+			for (int j = threadIdx.x; j < cnt; j += blockDim.x) point(t0 + j, stage + j * rl, sd);
+			__syncthreads();
+		}
+	} else {
+		const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+		for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.n; i += stride)
+			with_source<kMulti>(p, i, [&](const SourceDesc& sd) { point(i, sd.recs + (i - sd.first) * sd.rec_len, sd); });
+	}
 	// block reduction of the register accumulators
 	if (pmn[0] <= pmx[0]) {
 		for (int c = 0; c < 3; c++) {
@@ -408,8 +436,17 @@ void launch_decode_count(const DecodeParams& p, uint32_t* grid, ChunkingOut& out
 	int64_t cap = (int64_t)sms * 8;
 	if (blocks > cap) blocks = cap;
 	if (blocks < 1) blocks = 1;
-	if (p.nsrc > 1) decode_count_kernel<true><<<(unsigned)blocks, kDecodeThreads, 0, mem.stream()>>>(p, grid, out);
-	else decode_count_kernel<false><<<(unsigned)blocks, kDecodeThreads, 0, mem.stream()>>>(p, grid, out);
+	const bool staged = p.nsrc == 1 && p.src0.rec_len <= kDecodeStageMaxRec && (reinterpret_cast<uintptr_t>(p.src0.recs) & 15) == 0;
+	if (p.nsrc > 1) {
+		decode_count_kernel<true, false><<<(unsigned)blocks, kDecodeThreads, 0, mem.stream()>>>(p, grid, out);
+	} else if (staged) {
+		const size_t smem = (size_t)kDecodeTile * p.src0.rec_len;
+		int64_t tb = ceil_div(p.n, kDecodeTile);
+		if (tb > cap) tb = cap;
+		decode_count_kernel<false, true><<<(unsigned)tb, kDecodeThreads, smem, mem.stream()>>>(p, grid, out);
+	} else {
+		decode_count_kernel<false, false><<<(unsigned)blocks, kDecodeThreads, 0, mem.stream()>>>(p, grid, out);
+	}
 	PCG_LAUNCHED();
 }
 
