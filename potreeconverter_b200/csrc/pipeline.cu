@@ -1536,7 +1536,8 @@ struct Converter {
 			// large nodes get a CTA each; on levels with few nodes every node
 			// of some size does, so the GPU is not left to a handful of warps
 			int num_big = 0;
-			const int64_t big_min = K < 2 * sms ? kSmallLevelCtaCandidates : kBigNodeCandidates;
+			const LevelSchedule sch = level_schedule();
+			const int64_t big_min = K < 2 * sms ? sch.small_level_cta_min : sch.cta_min;
 			while (num_big < K && ln[order[num_big]].count >= big_min) num_big++;
 			int list_nodes = 0;
 			cudaEvent_t ev_lists;

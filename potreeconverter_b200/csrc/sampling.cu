@@ -30,8 +30,12 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <cstdio>
+#include <cstdlib>
+
 #include "devutil.cuh"
 #include "sampling.h"
+#include "tuned_schedule.h"
 
 namespace pcg {
 
@@ -1195,7 +1199,7 @@ __global__ void __launch_bounds__(kListThreads) greedy_list_kernel(const LevelNo
 // every CTA reaches the same number of times.
 constexpr int kClusterCtas = 4;
 constexpr int kSuper = kListRound * kClusterCtas;  // 4096
-constexpr int64_t kClusterMinCandidates = 65536;
+constexpr int64_t kClusterMinCandidates = 65536;  // smallest cluster node the shared-memory layout is sized for
 static_assert(kSuper <= 32767, "conflict indices are int16");
 
 struct ClusterRound {
@@ -1642,6 +1646,17 @@ void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int3
 	}
 }
 
+LevelSchedule level_schedule() {
+	// read at every level, so the autotuner can sweep in one process
+	LevelSchedule v{PCG_TUNED_CTA_MIN, PCG_TUNED_SMALL_LEVEL_CTA_MIN, PCG_TUNED_CLUSTER_MIN, PCG_TUNED_WARP_BLOCKS_PER_SM};
+	if (const char* e = std::getenv("PCG_SCHEDULE")) {
+		long long a = 0, b = 0, c = 0, d = 0;
+		if (std::sscanf(e, "%lld,%lld,%lld,%lld", &a, &b, &c, &d) == 4 && a > 0 && b > 0 && c > 0 && d > 0 && d <= 64)
+			v = LevelSchedule{a, b, c, (int)d};
+	}
+	return v;
+}
+
 void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int32_t>& cta_nodes, const std::vector<int32_t>& warp_nodes,
                          const PosParamsS& pp, LevelBuffers& lb, uint64_t* hash_keys, int32_t* hash_heads, double* acc_xyz,
                          double* acc_key, int32_t* acc_next, int32_t* acc_pos, const ConflictLists& cl, SampleStats* st, DeviceMem& mem,
@@ -1652,7 +1667,8 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 	// the largest nodes (cta_nodes is largest first) on a cluster each, the
 	// other CTA nodes on one CTA, the rest on a warp
 	std::vector<int32_t> clu, one;
-	for (int32_t k : cta_nodes) (ln[k].count >= kClusterMinCandidates ? clu : one).push_back(k);
+	const int64_t cluster_min = std::max(level_schedule().cluster_min, kClusterMinCandidates);
+	for (int32_t k : cta_nodes) (ln[k].count >= cluster_min ? clu : one).push_back(k);
 	int32_t* srank = mem.alloc<int32_t>((size_t)lb.M);
 	int32_t* d_clu = clu.empty() ? nullptr : mem.alloc<int32_t>(clu.size());
 	int32_t* d_one = one.empty() ? nullptr : mem.alloc<int32_t>(one.size());
@@ -1708,7 +1724,7 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 		cudaStream_t ws = stream_for_set();
 		const int nw = (int)warp_nodes.size();
 		int blocks = (int)ceil_div(nw, kWarpsPerBlock);
-		const int cap = sm_count() * 16;
+		const int cap = sm_count() * level_schedule().warp_blocks_per_sm;
 		if (blocks > cap) blocks = cap;
 		if (mode == 0) greedy_list_warp_kernel<0><<<blocks, kWarpsPerBlock * 32, 0, ws>>>(nodes, d_warp, nw, pp, lb, ga, cl, srank, st, counter);
 		else greedy_list_warp_kernel<1><<<blocks, kWarpsPerBlock * 32, 0, ws>>>(nodes, d_warp, nw, pp, lb, ga, cl, srank, st, counter);

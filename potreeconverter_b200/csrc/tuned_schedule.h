@@ -1,0 +1,9 @@
+// Level schedule of the samplers (sampling.h LevelSchedule). Written by
+// potreeconverter_b200/autotune.py from a sweep on the target GPU; the
+// values below are the sweep's best for the benchmarked workload, or the
+// hand-set defaults until a sweep has run.
+#pragma once
+#define PCG_TUNED_CTA_MIN 32768
+#define PCG_TUNED_SMALL_LEVEL_CTA_MIN 2048
+#define PCG_TUNED_CLUSTER_MIN 65536
+#define PCG_TUNED_WARP_BLOCKS_PER_SM 16
