@@ -13,6 +13,7 @@ made by tests/golden/make_golden.py --large-only):
 md5 equality of octree.bin and hierarchy.bin means every node holds the
 reference's points in the reference's order: zero acceptance mismatches."""
 
+import functools
 import hashlib
 
 import pytest
@@ -26,11 +27,17 @@ LARGE = {c["name"]: c for c in load_golden().get("large_cases", [])}
 FILES = {"octree.bin": "octree", "hierarchy.bin": "hierarchy", "metadata.json": "metadata"}
 
 
-def _las(case):
+@functools.lru_cache(maxsize=2)
+def _las_named(name):
     from potreeconverter_b200 import synth
+    case = LARGE[name]
     las = synth.generate(case["kind"], case["points"], case["seed"], **case["kwargs"])
     assert hashlib.md5(las).hexdigest() == case["las_md5"], "synthetic generator output changed"
     return las
+
+
+def _las(case):
+    return _las_named(case["name"])
 
 
 def _check(conv, case, method):
