@@ -449,6 +449,23 @@ struct CompletionOrder {
 	}
 };
 
+// Device memory this process can allocate now: what the driver reports free
+// plus what the stream-ordered allocator's default pool holds without using
+// it (the library keeps freed memory in the pool, so the driver counts it
+// as taken).
+inline size_t device_available(int device) {
+	size_t free_b = 0, total_b = 0;
+	PCG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+	cudaMemPool_t pool;
+	uint64_t reserved = 0, used = 0;
+	if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess &&
+	    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+	    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+		free_b += (size_t)(reserved - used);
+	cudaGetLastError();
+	return free_b;
+}
+
 // Device memory a job of `points` points and `record_bytes` bytes of point
 // records is expected to hold at its peak (the request loop's admission
 // figure): the records, a per-point working set and the count grid and LUT.
@@ -916,8 +933,7 @@ struct Converter {
 	// Whether a one-file job converts in parts: the part size in points (0:
 	// in one piece) and whether its records stay on the device.
 	int64_t part_plan(int64_t N, int rec_len, bool& resident) const {
-		size_t free_b = 0, total_b = 0;
-		PCG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+		const size_t free_b = device_available(device);
 		int64_t avail = (int64_t)((double)free_b * 0.85);
 		if (arena) avail += (int64_t)(arena->reserved() - arena->live_bytes());
 		const int64_t rec_bytes = N * (int64_t)rec_len;
@@ -2111,9 +2127,8 @@ pcg_status pcg_submit(pcg_ctx* ctx, const pcg_job* job, uint64_t* job_id) {
 		j->footprint = pcg::estimate_footprint((int64_t)points, (int64_t)records);
 		std::lock_guard<std::mutex> lk(ctx->qmtx);
 		if (ctx->workers.empty()) {
-			size_t free_b = 0, total_b = 0;
 			PCG_CUDA(cudaSetDevice(ctx->conv.device));
-			PCG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+			const size_t free_b = pcg::device_available(ctx->conv.device);
 			ctx->budget = (size_t)(free_b * 0.8);
 			const int nworkers = 4;
 			for (int i = 0; i < nworkers; i++) {

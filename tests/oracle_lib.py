@@ -130,8 +130,9 @@ class Oracle:
                               ctypes.byref(num)) != 0:
             raise RuntimeError("too many chunks")
         out = []
+        raw = ids.raw  # one copy of the buffer, not one per chunk
         for k in range(num.value):
-            name = ids.raw[16 * k: 16 * k + 16].split(b"\0")[0].decode()
+            name = raw[16 * k: 16 * k + 16].split(b"\0")[0].decode()
             out.append((name,) + tuple(int(v) for v in info[5 * k: 5 * k + 5]))
         return out, lut
 
@@ -158,8 +159,9 @@ class Oracle:
                                  order.ctypes.data, names, info.ctypes.data, cap, ctypes.byref(num), ctypes.byref(depth)) != 0:
             raise RuntimeError("too many nodes")
         nodes = []
+        raw = names.raw
         for k in range(num.value):
-            nm = names.raw[32 * k: 32 * k + 32].split(b"\0")[0].decode()
+            nm = raw[32 * k: 32 * k + 32].split(b"\0")[0].decode()
             nodes.append((nm, int(info[3 * k]), int(info[3 * k + 1]), int(info[3 * k + 2])))
         return order[:n], nodes, depth.value
 
