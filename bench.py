@@ -471,19 +471,26 @@ def main():
 
     # ---- parity of the benchmarked workload (one conversion per sampler,
     # outside the timed region)
+    def leg(fn, *a):
+        # a failing side leg is reported in the line, not fatal to it
+        try:
+            return fn(*a)
+        except Exception as e:  # noqa: BLE001
+            return {"error": f"{type(e).__name__}: {e}"}
+
     parity = None
     if rank == 0 and not args.no_parity:
-        parity = parity_leg(ctx, pinned, n)
+        parity = leg(parity_leg, ctx, pinned, n)
 
     # ---- the request-loop replay (config-4 shape) and the conversion in
     # parts (config-3 shape), single GPU runs only
     serving = None
     if world == 1 and not args.no_serving:
-        serving = serving_leg(local, args.serving_jobs, args.serving_rate)
+        serving = leg(serving_leg, local, args.serving_jobs, args.serving_rate)
     parts = None
     if world == 1 and not args.no_parts:
         pts = args.parts_points or min(3_000_000_000, host_points_budget(34 + 35 * 1.7))
-        parts = parts_leg(local, stream, pts, 2)
+        parts = leg(parts_leg, local, stream, pts, 2)
 
     if rank == 0:
         cpu = None
