@@ -1,5 +1,6 @@
 """Autotuner of the samplers' level schedule (csrc/sampling.h LevelSchedule):
-which nodes of a level get a CTA, a cluster of CTAs or a warp.
+which nodes of a level get a CTA, a cluster of CTAs or a warp, and how many
+resident blocks per SM pull warp-sized nodes from the device work queue.
 
 Run on the target GPU:
 
@@ -24,9 +25,10 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 
-CTA_MIN = [4096, 8192, 16384, 32768, 65536]
-SMALL_LEVEL_CTA_MIN = [512, 1024, 2048, 4096]
+CTA_MIN = [8192, 16384, 32768, 65536]
+SMALL_LEVEL_CTA_MIN = [1024, 2048, 4096]
 CLUSTER_MIN = [65536, 131072, 1 << 40]
+WARP_BLOCKS = [8, 16, 32]
 
 
 def sweep(points: int) -> list:
@@ -44,8 +46,8 @@ def sweep(points: int) -> list:
         clouds.append((kind, las[:off], recs))
     rows = []
     with pc.Context(stream=stream.cuda_stream) as ctx:
-        for cta, small, clu in itertools.product(CTA_MIN, SMALL_LEVEL_CTA_MIN, CLUSTER_MIN):
-            os.environ["PCG_SCHEDULE"] = f"{cta},{small},{clu}"
+        for cta, small, clu, warp in itertools.product(CTA_MIN, SMALL_LEVEL_CTA_MIN, CLUSTER_MIN, WARP_BLOCKS):
+            os.environ["PCG_SCHEDULE"] = f"{cta},{small},{clu},{warp}"
             ms = {}
             for kind, header, recs in clouds:
                 for method in ("poisson", "poisson_average"):
@@ -59,7 +61,7 @@ def sweep(points: int) -> list:
                         b.synchronize()
                         times.append(a.elapsed_time(b))
                     ms[f"{kind}-{method}"] = statistics.median(times)
-            rows.append({"schedule": [cta, small, clu], "ms": ms, "total_ms": sum(ms.values())})
+            rows.append({"schedule": [cta, small, clu, warp], "ms": ms, "total_ms": sum(ms.values())})
             print(json.dumps(rows[-1]), flush=True)
     os.environ.pop("PCG_SCHEDULE", None)
     return rows
@@ -68,14 +70,14 @@ def sweep(points: int) -> list:
 def write(rows: list, points: int):
     ok = [r for r in rows if "total_ms" in r]
     best = min(ok, key=lambda r: r["total_ms"])
-    cta, small, clu = best["schedule"]
+    cta, small, clu, warp = best["schedule"]
     with open(os.path.join(CSRC, "tuned_schedule.h"), "w") as f:
         f.write("// Level schedule of the samplers (sampling.h LevelSchedule). Written by\n"
                 "// potreeconverter_b200/autotune.py from a sweep on the target GPU; the\n"
                 "// values below are the sweep's best for the benchmarked workload, or the\n"
                 "// hand-set defaults until a sweep has run.\n#pragma once\n"
                 f"#define PCG_TUNED_CTA_MIN {cta}\n#define PCG_TUNED_SMALL_LEVEL_CTA_MIN {small}\n"
-                f"#define PCG_TUNED_CLUSTER_MIN {clu}\n")
+                f"#define PCG_TUNED_CLUSTER_MIN {clu}\n#define PCG_TUNED_WARP_BLOCKS_PER_SM {warp}\n")
     with open(os.path.join(CSRC, "tuned_schedule.json"), "w") as f:
         json.dump({"points": points, "best": best, "rows": rows}, f, indent=1)
     return best

@@ -1667,10 +1667,11 @@ void launch_greedy(int mode, bool fp32_guard, const LevelNode* nodes, const int3
 
 LevelSchedule level_schedule() {
 	// read at every level, so the autotuner can sweep in one process
-	LevelSchedule v{PCG_TUNED_CTA_MIN, PCG_TUNED_SMALL_LEVEL_CTA_MIN, PCG_TUNED_CLUSTER_MIN};
+	LevelSchedule v{PCG_TUNED_CTA_MIN, PCG_TUNED_SMALL_LEVEL_CTA_MIN, PCG_TUNED_CLUSTER_MIN, PCG_TUNED_WARP_BLOCKS_PER_SM};
 	if (const char* e = std::getenv("PCG_SCHEDULE")) {
-		long long a = 0, b = 0, c = 0;
-		if (std::sscanf(e, "%lld,%lld,%lld", &a, &b, &c) == 3 && a > 0 && b > 0 && c > 0) v = LevelSchedule{a, b, c};
+		long long a = 0, b = 0, c = 0, d = 0;
+		if (std::sscanf(e, "%lld,%lld,%lld,%lld", &a, &b, &c, &d) == 4 && a > 0 && b > 0 && c > 0 && d > 0 && d <= 64)
+			v = LevelSchedule{a, b, c, (int)d};
 	}
 	return v;
 }

@@ -75,16 +75,17 @@ void launch_gather_records(const uint32_t* ids, int64_t n, const int32_t* X, con
 // Which kernel shape samples which node of a level: nodes of at least
 // cta_min candidates get a CTA each (small_level_cta_min on levels with
 // fewer nodes than 2 x SMs), those of at least cluster_min a cluster of
-// CTAs, the rest a warp each (CTA- and warp-sized nodes are pulled from
-// device work queues by one persistent launch per level). The compiled-in
-// values come from the autotuner's table (tuned_schedule.h, written by
-// potreeconverter_b200/autotune.py); PCG_SCHEDULE="cta_min,
-// small_level_cta_min,cluster_min" in the environment overrides them (read
-// at every level, for the autotuner's sweep).
+// CTAs, the rest a warp each, pulled from a device work queue by
+// warp_blocks_per_sm resident blocks per SM. The compiled-in values come from
+// the autotuner's table (tuned_schedule.h, written by
+// potreeconverter_b200/autotune.py); PCG_SCHEDULE="cta_min,small_level_cta_min,
+// cluster_min,warp_blocks_per_sm" in the environment overrides them (read at
+// every level, for the autotuner's sweep).
 struct LevelSchedule {
 	int64_t cta_min;
 	int64_t small_level_cta_min;
 	int64_t cluster_min;
+	int warp_blocks_per_sm;
 };
 LevelSchedule level_schedule();
 void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, LevelBuffers& lb, SampleStats* st, DeviceMem& mem,

@@ -6,3 +6,4 @@
 #define PCG_TUNED_CTA_MIN 32768
 #define PCG_TUNED_SMALL_LEVEL_CTA_MIN 2048
 #define PCG_TUNED_CLUSTER_MIN 65536
+#define PCG_TUNED_WARP_BLOCKS_PER_SM 16
