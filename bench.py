@@ -440,9 +440,7 @@ def main():
     bpp = 39
     out_pts = s["output_points"]
     # roofline: the dominant kernel of a step (ncu launch list) is the
-    # acceptance from conflict lists (greedy_level_kernel, the persistent
-    # per-level launch of the CTA- and warp-sized nodes, and
-    # greedy_list_cluster_kernel),
+    # acceptance from conflict lists (greedy_list_kernel and its warp form),
     # launched once per octree level. Algorithmic bytes: per candidate its
     # record (16 B), list length (1 B) and its decision, rank and flag
     # (9 B); per list entry the entry (4 B) and that candidate's decision
@@ -513,7 +511,7 @@ def main():
             "e2e": {"value": e2e, "unit": "Mpts/s", "h2d_bytes_per_step": int(pinned.numel()),
                     "d2h_bytes_per_step": int(octree_bytes)},
             "gpu_launches": int(s["gpu_launches"]) * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "greedy_level_kernel + greedy_list_cluster_kernel (all levels of a step)",
+            "roofline": {"bound": "hbm", "kernel": "greedy_list_kernel + greedy_list_warp_kernel (all levels of a step)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "traffic_source": "DRAM bytes per candidate from ncu, profiles/accept_hotspots-5M_poisson.md",
                          "algorithmic_bytes": accept_bytes, "kernel_ms": accept_ms,

@@ -996,9 +996,13 @@ struct ListRound {
 };
 
 template <int MODE>
-__device__ __forceinline__ void list_accept_cta(const LevelNode nd, ListRound& R, PosParamsS pp, LevelBuffers lb, GreedyArgs ga,
-                                                ConflictLists cl, int32_t* __restrict__ srank, SampleStats* st) {
+__global__ void __launch_bounds__(kListThreads) greedy_list_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order,
+                                                                 int node_begin, PosParamsS pp, LevelBuffers lb, GreedyArgs ga,
+                                                                 ConflictLists cl, int32_t* __restrict__ srank, SampleStats* st) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	ListRound& R = *reinterpret_cast<ListRound*>(smem_raw);
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const LevelNode nd = nodes[order[node_begin + blockIdx.x]];
 	const int64_t n = nd.count, co = nd.cand_off;
 	uint64_t* hk = ga.hkeys + nd.hash_off;
 	int32_t* hh = ga.hheads + nd.hash_off;
@@ -1439,11 +1443,19 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 // lane decides once its earlier conflicting lanes have) or, when a lane's
 // old conflict sits at the edge of the 10,001-check window, in lane order.
 template <int MODE>
-__device__ __forceinline__ void list_accept_warp(const LevelNode nd, PosParamsS pp, LevelBuffers lb, GreedyArgs ga, ConflictLists cl,
-                                                 int32_t* __restrict__ srank, SampleStats* st) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) greedy_list_warp_kernel(const LevelNode* __restrict__ nodes,
+                                                                              const int32_t* __restrict__ order, int num, PosParamsS pp,
+                                                                              LevelBuffers lb, GreedyArgs ga, ConflictLists cl,
+                                                                              int32_t* __restrict__ srank, SampleStats* st,
+                                                                              int* next_node) {
 	const int lane = threadIdx.x & 31;
 	const uint32_t lt = lanemask_lt();
-	{
+	while (true) {
+		int idx = 0;
+		if (lane == 0) idx = atomicAdd(next_node, 1);
+		idx = __shfl_sync(FULL, idx, 0);
+		if (idx >= num) break;
+		const LevelNode nd = nodes[order[idx]];
 		const int64_t n = nd.count, co = nd.cand_off;
 		uint64_t* hk = ga.hkeys + nd.hash_off;
 		int32_t* hh = ga.hheads + nd.hash_off;
@@ -1542,37 +1554,6 @@ __device__ __forceinline__ void list_accept_warp(const LevelNode nd, PosParamsS 
 			}
 			cnt += __popc(accmask);
 		}
-	}
-}
-
-// One persistent launch for a level's CTA-sized and warp-sized nodes: each
-// resident 1024-thread CTA pulls CTA-sized nodes (largest first) from a
-// device work queue and accepts them with all its threads; once that queue
-// is empty its warps pull the warp-sized nodes from a second queue.
-template <int MODE>
-__global__ void __launch_bounds__(kListThreads, 1) greedy_level_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ cta_order,
-                                                                    int num_cta, const int32_t* __restrict__ warp_order, int num_warp,
-                                                                    PosParamsS pp, LevelBuffers lb, GreedyArgs ga, ConflictLists cl,
-                                                                    int32_t* __restrict__ srank, SampleStats* st, int* queues) {
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	ListRound& R = *reinterpret_cast<ListRound*>(smem_raw);
-	__shared__ int s_item;
-	while (true) {
-		if (threadIdx.x == 0) s_item = atomicAdd(&queues[0], 1);
-		__syncthreads();
-		const int item = s_item;
-		__syncthreads();
-		if (item >= num_cta) break;
-		list_accept_cta<MODE>(nodes[cta_order[item]], R, pp, lb, ga, cl, srank, st);
-		__syncthreads();
-	}
-	const int lane = threadIdx.x & 31;
-	while (true) {
-		int idx = 0;
-		if (lane == 0) idx = atomicAdd(&queues[1], 1);
-		idx = __shfl_sync(FULL, idx, 0);
-		if (idx >= num_warp) break;
-		list_accept_warp<MODE>(nodes[warp_order[idx]], pp, lb, ga, cl, srank, st);
 	}
 }
 
@@ -1692,17 +1673,16 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 	int32_t* d_clu = clu.empty() ? nullptr : mem.alloc<int32_t>(clu.size());
 	int32_t* d_one = one.empty() ? nullptr : mem.alloc<int32_t>(one.size());
 	int32_t* d_warp = warp_nodes.empty() ? nullptr : mem.alloc<int32_t>(warp_nodes.size());
-	int* counter = mem.alloc<int>(2);  // the level kernel's two work queues
+	int* counter = mem.alloc<int>(1);
 	if (d_clu) PCG_CUDA(cudaMemcpyAsync(d_clu, clu.data(), clu.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 	if (d_one) PCG_CUDA(cudaMemcpyAsync(d_one, one.data(), one.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 	if (d_warp) PCG_CUDA(cudaMemcpyAsync(d_warp, warp_nodes.data(), warp_nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-	PCG_CUDA(cudaMemsetAsync(counter, 0, 2 * sizeof(int), s));
+	PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), s));
 	// the node sets are independent: the smaller ones run beside the
 	// largest on a forked stream
 	cudaStream_t side = nullptr;
 	cudaEvent_t fork = nullptr, join = nullptr;
-	// the CTA- and warp-sized nodes share one persistent launch
-	const int sets = (d_clu ? 1 : 0) + ((d_one || d_warp) ? 1 : 0);
+	const int sets = (d_clu ? 1 : 0) + (d_one ? 1 : 0) + (d_warp ? 1 : 0);
 	if (sets > 1 && mem.arena()) {
 		side = mem.arena()->side_stream(fork, join);
 		PCG_CUDA(cudaEventRecord(fork, s));
@@ -1727,19 +1707,27 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 		}
 		PCG_LAUNCHED();
 	}
-	if (d_one || d_warp) {
+	if (d_one) {
 		const size_t smem = sizeof(ListRound);
-		const int nc = (int)one.size(), nw = (int)warp_nodes.size();
+		const int nc = (int)one.size();
 		cudaStream_t cs = stream_for_set();
-		const int64_t want = (int64_t)nc + ceil_div((int64_t)nw, kListWarps);
-		const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, sm_count()));
 		if (mode == 0) {
-			PCG_CUDA(cudaFuncSetAttribute(greedy_level_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_level_kernel<0><<<grid, kListThreads, smem, cs>>>(nodes, d_one, nc, d_warp, nw, pp, lb, ga, cl, srank, st, counter);
+			PCG_CUDA(cudaFuncSetAttribute(greedy_list_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			greedy_list_kernel<0><<<nc, kListThreads, smem, cs>>>(nodes, d_one, 0, pp, lb, ga, cl, srank, st);
 		} else {
-			PCG_CUDA(cudaFuncSetAttribute(greedy_level_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_level_kernel<1><<<grid, kListThreads, smem, cs>>>(nodes, d_one, nc, d_warp, nw, pp, lb, ga, cl, srank, st, counter);
+			PCG_CUDA(cudaFuncSetAttribute(greedy_list_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+			greedy_list_kernel<1><<<nc, kListThreads, smem, cs>>>(nodes, d_one, 0, pp, lb, ga, cl, srank, st);
 		}
+		PCG_LAUNCHED();
+	}
+	if (d_warp) {
+		cudaStream_t ws = stream_for_set();
+		const int nw = (int)warp_nodes.size();
+		int blocks = (int)ceil_div(nw, kWarpsPerBlock);
+		const int cap = sm_count() * level_schedule().warp_blocks_per_sm;
+		if (blocks > cap) blocks = cap;
+		if (mode == 0) greedy_list_warp_kernel<0><<<blocks, kWarpsPerBlock * 32, 0, ws>>>(nodes, d_warp, nw, pp, lb, ga, cl, srank, st, counter);
+		else greedy_list_warp_kernel<1><<<blocks, kWarpsPerBlock * 32, 0, ws>>>(nodes, d_warp, nw, pp, lb, ga, cl, srank, st, counter);
 		PCG_LAUNCHED();
 	}
 	if (side) {
