@@ -17,9 +17,8 @@
 //     a candidate's own;
 //  2. segmented radix sort of (cell, sorted position) per node;
 //  3. a hash table (node, cell) -> range of the cell-sorted records;
-//  4. one thread per candidate in cell order: a block looks up the runs of
-//     the 27 cells around each of its cells once, into shared memory, and
-//     every candidate scans them up to its own sorted position:
+//  4. one thread per candidate in cell order (a warp shares neighbourhoods)
+//     scans the occupied cells among its 27 up to its own sorted position:
 //     the FP32 distance on node-relative coordinates decides every pair
 //     outside the band s^2 (1 -/+ 1e-3); pairs inside the band are decided
 //     by the reference's FP64 test and counted as escalated; then the
@@ -100,6 +99,22 @@ __global__ void conf_gather_kernel(const LevelNode* __restrict__ nodes, PosParam
 	                     (float)(qcoord(r.z, 2, pp) - nd.min[2]), __int_as_float((int)u));
 }
 
+// occupancy bitmap of a node's cells: 128 bits per (z, y) row, 4 words
+constexpr int kRowWords = kCellsPerAxis / 32;
+constexpr int64_t kBitmapWords = (int64_t)kCellsPerAxis * kCellsPerAxis * kRowWords;
+constexpr int64_t kBitmapMinCandidates = 2048;  // smaller nodes probe the hash for every cell
+
+__global__ void conf_bitmap_kernel(const int32_t* __restrict__ node_of, const uint64_t* __restrict__ ck, int64_t M,
+                                   const int64_t* __restrict__ bm_off, uint32_t* __restrict__ bm) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= M) return;
+	const int64_t off = bm_off[node_of[j]];
+	if (off < 0) return;
+	const uint64_t c = ck[j];
+	const int cx = (int)(c % kCellsPerAxis);
+	atomicOr(&bm[off + (int64_t)(c / kCellsPerAxis) * kRowWords + (cx >> 5)], 1u << (cx & 31));
+}
+
 __device__ __forceinline__ bool run_head(const LevelNode* nodes, const int32_t* node_of, const uint64_t* ck, int64_t j) {
 	return j == nodes[node_of[j]].cand_off || ck[j] != ck[j - 1];
 }
@@ -146,73 +161,15 @@ __device__ __forceinline__ int2 find_run(const RunSlot* table, int64_t cap, uint
 	return make_int2(0, 0);
 }
 
-// One thread per candidate, in cell order (a block covers 128 consecutive
-// candidates, several to a cell). The block first finds the runs of the 27
-// cells around each of its distinct (node, cell) groups -- one hash probe per
-// group and neighbour cell, spread over all threads, into shared memory --
-// so the scans below read run bounds from shared memory and only the
-// candidates' records from global memory.
-constexpr int kConfThreads = 128;
-constexpr int kNeighbours = 27;
-
 template <int MODE>
-__global__ void __launch_bounds__(kConfThreads) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use,
-                                                                 PosParamsS pp, LevelBuffers lb, const uint64_t* __restrict__ ck,
-                                                                 const int4* __restrict__ crec, const float4* __restrict__ crf,
-                                                                 const RunSlot* __restrict__ table, int64_t cap, ConflictLists cl,
-                                                                 SampleStats* st) {
-	extern __shared__ int2 s_run[];  // [groups][27] (start, count) of the neighbour cells' runs
-	__shared__ uint64_t s_key[kConfThreads];
-	__shared__ int32_t s_grp[kConfThreads];
-	__shared__ uint64_t s_gkey[kConfThreads];
-	__shared__ int32_t s_ngroups;
-	const int tid = threadIdx.x;
-	const int64_t j = (int64_t)blockIdx.x * kConfThreads + tid;
-	int32_t node = -1;
-	bool valid = j < lb.M;
-	if (valid) {
-		node = lb.node_of[j];
-		valid = use[node] != 0;
-	}
-	// groups: runs of equal (node, cell) among the block's candidates
-	const uint64_t key = valid ? (((uint64_t)(uint32_t)node << 32) | ck[j]) : ~0ull - (uint64_t)tid;
-	s_key[tid] = key;
-	__syncthreads();
-	const bool head = valid && (tid == 0 || s_key[tid - 1] != key);
-	{
-		const unsigned b = __ballot_sync(FULL, head);
-		__shared__ int32_t s_warp[kConfThreads / 32];
-		const int lane = tid & 31, warp = tid >> 5;
-		if (lane == 0) s_warp[warp] = __popc(b);
-		__syncthreads();
-		int before = 0, total = 0;
-		for (int w = 0; w < kConfThreads / 32; w++) {
-			before += w < warp ? s_warp[w] : 0;
-			total += s_warp[w];
-		}
-		const int incl = before + __popc(b & ((2u << lane) - 1));  // heads up to and including this thread
-		s_grp[tid] = incl - 1;
-		if (head) s_gkey[incl - 1] = key;
-		if (tid == 0) s_ngroups = total;
-	}
-	__syncthreads();
-	const int ngroups = s_ngroups;
-	for (int f = tid; f < ngroups * kNeighbours; f += kConfThreads) {
-		const int g = f / kNeighbours, q = f % kNeighbours;
-		const uint64_t gk = s_gkey[g];
-		const uint64_t c = gk & 0xffffffffull;
-		const int cx = (int)(c % kCellsPerAxis) + q % 3 - 1;
-		const int cy = (int)((c / kCellsPerAxis) % kCellsPerAxis) + (q / 3) % 3 - 1;
-		const int cz = (int)(c / (kCellsPerAxis * kCellsPerAxis)) + q / 9 - 1;
-		int2 run = make_int2(0, 0);
-		if (cx >= 0 && cx < kCellsPerAxis && cy >= 0 && cy < kCellsPerAxis && cz >= 0 && cz < kCellsPerAxis) {
-			const uint64_t cell = ((uint64_t)cz * kCellsPerAxis + (uint64_t)cy) * kCellsPerAxis + (uint64_t)cx;
-			run = find_run(table, cap, (gk & 0xffffffff00000000ull) | cell);
-		}
-		s_run[f] = run;
-	}
-	__syncthreads();
-	if (!valid) return;
+__global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, PosParamsS pp,
+                                                        LevelBuffers lb, const uint64_t* __restrict__ ck, const int4* __restrict__ crec,
+                                                        const float4* __restrict__ crf, const RunSlot* __restrict__ table, int64_t cap, const int64_t* __restrict__ bm_off, const uint32_t* __restrict__ bm,
+                                                        ConflictLists cl, SampleStats* st) {
+	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= lb.M) return;
+	const int32_t node = lb.node_of[j];
+	if (!use[node]) return;
 	const LevelNode& nd = nodes[node];
 	const int64_t co = nd.cand_off;
 	const int4 me = crec[j];
@@ -236,47 +193,71 @@ __global__ void __launch_bounds__(kConfThreads) conf_lists_kernel(const LevelNod
 	const bool pre32 = s2 > 1e-30 && s2 < 1e30 && amax < 1e6 * sp;
 	const float s2hi = (float)(s2 * 1.001), s2lo = (float)(s2 * 0.999);
 	unsigned escalated = 0;  // pairs inside the band, decided in FP64
+	const uint64_t c = ck[j];
+	const int cx = (int)(c % kCellsPerAxis), cy = (int)((c / kCellsPerAxis) % kCellsPerAxis), cz = (int)(c / (kCellsPerAxis * kCellsPerAxis));
 	// the first kListInline entries in registers, the rest (rare) in a
 	// per-thread array; both are stored once the search is done
-	int4 head4 = make_int4(0, 0, 0, 0);
+	int4 head = make_int4(0, 0, 0, 0);
 	int32_t rest[kListCap - kListInline];
 	int n = 0;
-	const int2* runs = s_run + s_grp[tid] * kNeighbours;
-	for (int q = 0; q < kNeighbours; q++) {
-		const int2 run = runs[q];
-		const int4* rp = crec + co + run.x;
-		const float4* rf = crf + co + run.x;
-		for (int i = 0; i < run.y; i++) {
-			const float4 qf = rf[i];
-			const int32_t u = __float_as_int(qf.w);
-			if (u >= t) break;  // a cell's records are in sorted order: only earlier candidates
-			bool inside = false;
-			if (pre32) {
-				// FP32 decides outside the band s^2 (1 -/+ 1e-3), well clear
-				// of its rounding error; pairs in the band go to FP64
-				const float fx = qf.x - mf.x, fy = qf.y - mf.y, fz = qf.z - mf.z;
-				const float d2 = fx * fx + fy * fy + fz * fz;
-				if (d2 >= s2hi) continue;
-				inside = d2 < s2lo;
+	const int64_t boff = bm_off[node];
+	for (int dz = -1; dz <= 1; dz++) {
+		const int qz = cz + dz;
+		if (qz < 0 || qz >= kCellsPerAxis) continue;
+		for (int dy = -1; dy <= 1; dy++) {
+			const int qy = cy + dy;
+			if (qy < 0 || qy >= kCellsPerAxis) continue;
+			// occupied cells among x = cx-1 .. cx+1 of this row
+			uint32_t occ = 7u;
+			if (boff >= 0) {
+				const uint32_t* row = bm + boff + ((int64_t)qz * kCellsPerAxis + qy) * kRowWords;
+				const int x0 = cx - 1;
+				occ = 0;
+				for (int b = 0; b < 3; b++) {
+					const int qx = x0 + b;
+					if (qx >= 0 && qx < kCellsPerAxis && ((row[qx >> 5] >> (qx & 31)) & 1u)) occ |= 1u << b;
+				}
 			}
-			if (!inside) {
-				const int4 qq = rp[i];
-				const double ax = qcoord(qq.x, 0, pp), ay = qcoord(qq.y, 1, pp), az = qcoord(qq.z, 2, pp);
-				// squaredDistance(point, candidate), sampler_poisson.h:117-125
-				const double dx_ = ax - x, dy_ = ay - y, dz_ = az - z;
-				escalated++;
-				if (!(dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < s2)) continue;
+			for (int dx = -1; dx <= 1; dx++) {
+				const int qx = cx + dx;
+				if (qx < 0 || qx >= kCellsPerAxis || !((occ >> (dx + 1)) & 1u)) continue;
+				const uint64_t cell = ((uint64_t)qz * kCellsPerAxis + (uint64_t)qy) * kCellsPerAxis + (uint64_t)qx;
+				const int2 run = find_run(table, cap, ((uint64_t)(uint32_t)node << 32) | cell);
+				const int4* rp = crec + co + run.x;
+				const float4* rf = crf + co + run.x;
+				for (int i = 0; i < run.y; i++) {
+					const float4 qf = rf[i];
+					const int32_t u = __float_as_int(qf.w);
+					if (u >= t) break;  // a cell's records are in sorted order: only earlier candidates
+					bool inside = false;
+					if (pre32) {
+						// FP32 decides outside the band s^2 (1 -/+ 1e-3), well clear
+						// of its rounding error; pairs in the band go to FP64
+						const float fx = qf.x - mf.x, fy = qf.y - mf.y, fz = qf.z - mf.z;
+						const float d2 = fx * fx + fy * fy + fz * fz;
+						if (d2 >= s2hi) continue;
+						inside = d2 < s2lo;
+					}
+					if (!inside) {
+						const int4 q = rp[i];
+						const double ax = qcoord(q.x, 0, pp), ay = qcoord(q.y, 1, pp), az = qcoord(q.z, 2, pp);
+						// squaredDistance(point, candidate), sampler_poisson.h:117-125
+						const double dx_ = ax - x, dy_ = ay - y, dz_ = az - z;
+						escalated++;
+						if (!(dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < s2)) continue;
+					}
+					if (MODE == 0 && !(lb.keys[co + u] >= lim)) continue;
+					if (n == 0) head.x = u;
+					else if (n == 1) head.y = u;
+					else if (n == 2) head.z = u;
+					else if (n == 3) head.w = u;
+					else if (n < kListCap) rest[n - kListInline] = u;
+					n++;
+				}
 			}
-			if (MODE == 0 && !(lb.keys[co + u] >= lim)) continue;
-			if (n == 0) head4.x = u;
-			else if (n == 1) head4.y = u;
-			else if (n == 2) head4.z = u;
-			else if (n == 3) head4.w = u;
-			else if (n < kListCap) rest[n - kListInline] = u;
-			n++;
 		}
 	}
-	cl.inl[co + t] = head4;
+	cl.inl[co + t] = head;
 	bool dense = n > kListCap;
 	if (!dense && n > kListInline) {
 		const int extra = n - kListInline;
@@ -336,6 +317,19 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	PCG_CUDA(cudaMemsetAsync(table, 0xff, cap * sizeof(RunSlot), s));
 	conf_insert_runs_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb.node_of, ck, M, table, cap, st);
 	PCG_LAUNCHED();
+	// occupancy bitmaps of the larger nodes
+	std::vector<int64_t> bm_off(K, -1);
+	int64_t bm_words = 0;
+	for (int k = 0; k < K; k++)
+		if (use[k] && ln[k].count >= kBitmapMinCandidates) { bm_off[k] = bm_words; bm_words += kBitmapWords; }
+	int64_t* d_bm_off = mem.alloc<int64_t>(K);
+	PCG_CUDA(cudaMemcpyAsync(d_bm_off, bm_off.data(), K * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+	uint32_t* bm = mem.alloc<uint32_t>(bm_words > 0 ? bm_words : 1);
+	if (bm_words > 0) {
+		PCG_CUDA(cudaMemsetAsync(bm, 0, bm_words * sizeof(uint32_t), s));
+		conf_bitmap_kernel<<<blocks, 256, 0, s>>>(lb.node_of, ck, M, d_bm_off, bm);
+		PCG_LAUNCHED();
+	}
 	cl.inl = mem.alloc<int4>(M);
 	cl.ovf_off = mem.alloc<int32_t>(M);
 	// entries past the inline ones: room for 4 more per candidate on
@@ -350,20 +344,14 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
 	uint8_t* d_use = mem.alloc<uint8_t>(K);
 	PCG_CUDA(cudaMemcpyAsync(d_use, use.data(), K, cudaMemcpyHostToDevice, s));
-	const size_t smem = (size_t)kConfThreads * kNeighbours * sizeof(int2);  // every candidate its own cell, at worst
-	static_assert(kConfThreads * kNeighbours * sizeof(int2) <= 48 * 1024, "run table of a block");
-	const unsigned lblocks = (unsigned)ceil_div(M, kConfThreads);
-	if (mode == 0) {
-		PCG_CUDA(cudaFuncSetAttribute(conf_lists_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-		conf_lists_kernel<0><<<lblocks, kConfThreads, smem, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, cl, st);
-	} else {
-		PCG_CUDA(cudaFuncSetAttribute(conf_lists_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-		conf_lists_kernel<1><<<lblocks, kConfThreads, smem, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, cl, st);
-	}
+	if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, st);
+	else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, st);
 	PCG_LAUNCHED();
 	PCG_CUDA(cudaMemcpyAsync(dense.data(), cl.node_dense, K, cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));
 	mem.free(d_use);
+	mem.free(d_bm_off);
+	mem.free(bm);
 	mem.free(table);
 	mem.free(crec);
 	mem.free(crf);
