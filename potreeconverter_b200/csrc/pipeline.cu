@@ -956,27 +956,49 @@ struct Converter {
 		return gp;
 	}
 
+	// Device images of pieces of octree.bin whose copy to the host runs on
+	// the side stream; each is returned to the job's memory once its copy
+	// has finished (`done`), one part later, so the copy overlaps the next
+	// part's work.
+	struct PieceInFlight {
+		uint8_t* dev;
+		cudaEvent_t done;
+	};
+
 	// Hands the device image of a finished piece of octree.bin to the host
-	// on the side stream `d2h` (after the compute stream's work so far) and
-	// frees it there; the piece joins res.parts.
-	void emit_part(uint8_t* d_part, uint64_t bytes, cudaStream_t d2h, JobResult& res) {
-		if (bytes == 0) return;
+	// on the side stream `d2h` (after the compute stream's work so far); the
+	// piece joins res.parts.
+	void emit_part(uint8_t* d_part, uint64_t bytes, cudaStream_t d2h, std::vector<PieceInFlight>& inflight, JobResult& res) {
 		uint8_t* h = host_buffers ? host_buffers->take(bytes) : nullptr;
 		if (!h) PCG_CUDA(cudaMallocHost((void**)&h, bytes));
 		res.parts.push_back({h, bytes});
-		cudaEvent_t ev;
+		cudaEvent_t ev, done;
 		PCG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
 		PCG_CUDA(cudaEventRecord(ev, stream));
 		PCG_CUDA(cudaStreamWaitEvent(d2h, ev, 0));
 		PCG_CUDA(cudaEventDestroy(ev));
 		PCG_CUDA(cudaMemcpyAsync(h, d_part, bytes, cudaMemcpyDeviceToHost, d2h));
-		PCG_CUDA(cudaFreeAsync(d_part, d2h));
+		PCG_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+		PCG_CUDA(cudaEventRecord(done, d2h));
+		inflight.push_back({d_part, done});
+	}
+
+	// Returns the device images of all pieces but the last `keep` to the
+	// job's memory, waiting for their copies first.
+	static void retire_pieces(std::vector<PieceInFlight>& inflight, size_t keep, DeviceMem& mem) {
+		while (inflight.size() > keep) {
+			PCG_CUDA(cudaEventSynchronize(inflight.front().done));
+			cudaEventDestroy(inflight.front().done);
+			mem.free(inflight.front().dev);
+			inflight.erase(inflight.begin());
+		}
 	}
 
 	// Payloads of the nodes order[o0 ..) (completed since the last call) into
 	// a new piece of octree.bin; their hierarchy records join `recs`.
 	void write_piece(const Tree& tree, const std::vector<int>& order, size_t o0, const DecodeParams& p, const Setup& s,
-	                 std::vector<HierRecord>& recs, int64_t& out_points, cudaStream_t d2h, DeviceMem& mem, JobResult& res) {
+	                 std::vector<HierRecord>& recs, int64_t& out_points, cudaStream_t d2h, std::vector<PieceInFlight>& inflight,
+	                 DeviceMem& piece_mem, DeviceMem& mem, JobResult& res) {
 		std::vector<PayloadItem> items;
 		int64_t piece = 0;
 		for (size_t i = o0; i < order.size(); i++) {
@@ -994,11 +1016,10 @@ struct Converter {
 		}
 		out_points += piece;
 		if (piece == 0) return;
-		uint8_t* d_part = nullptr;
-		PCG_CUDA(cudaMallocAsync((void**)&d_part, (size_t)piece * s.bpp, stream));
+		uint8_t* d_part = piece_mem.alloc<uint8_t>((size_t)piece * s.bpp);
 		PayloadItem* d_items = upload(items, mem);
 		launch_write_payloads(p, items, d_items, d_part, mem);
-		emit_part(d_part, (uint64_t)piece * s.bpp, d2h, res);
+		emit_part(d_part, (uint64_t)piece * s.bpp, d2h, inflight, res);
 		mem.free(d_items);
 	}
 
@@ -1188,6 +1209,13 @@ struct Converter {
 		std::vector<Block> blocks;
 		std::vector<int64_t> surv_off(nchunks, 0);
 		int64_t S = 0;
+		std::vector<PieceInFlight> inflight;
+		struct PiecesGuard {  // on any exit: no piece copy outlives its memory
+			std::vector<PieceInFlight>& v;
+			~PiecesGuard() {
+				for (auto& pc : v) { cudaEventSynchronize(pc.done); cudaEventDestroy(pc.done); }
+			}
+		} pieces_guard{inflight};
 
 		// ------------------------------------------------------------ parts
 		for (const auto& part : parts) {
@@ -1256,7 +1284,8 @@ struct Converter {
 			auto t_out = Clock::now();
 			const size_t o0 = corder.order.size();
 			for (int cr : roots) corder.chunk(cr);
-			write_piece(tree, corder.order, o0, pg, s, recs, out_points, d2h, gm, res);
+			retire_pieces(inflight, 1, mem);  // the previous part's piece has been copied meanwhile
+			write_piece(tree, corder.order, o0, pg, s, recs, out_points, d2h, inflight, mem, gm, res);
 			// the chunk roots' points, carried to the levels above the parts
 			Block b;
 			for (int cr : roots) b.count += tree.nodes[cr].buf_count;
@@ -1342,7 +1371,7 @@ struct Converter {
 		root.fin_count = root.buf_count;
 		const size_t o0 = corder.order.size();
 		corder.finish(chunk_roots);
-		write_piece(tree, corder.order, o0, ptop, s, recs, out_points, d2h, mem, res);
+		write_piece(tree, corder.order, o0, ptop, s, recs, out_points, d2h, inflight, mem, mem, res);
 		const auto hst = download(d_st, 1, stream)[0];
 		if (hst.timeouts) throw PcgError(PCG_TIMEOUT, "a bounded device loop gave up");
 		res.stats.escalated_pairs = (int64_t)hst.escalated;
@@ -1359,6 +1388,7 @@ struct Converter {
 		res.stats.ms_host_writers = ms_since(t_w);
 		auto t_d2h = Clock::now();
 		PCG_CUDA(cudaStreamSynchronize(d2h));
+		retire_pieces(inflight, 0, mem);
 		res.stats.ms_d2h = ms_since(t_d2h);
 		res.octree = nullptr;
 		res.octree_size = (uint64_t)(out_points * s.bpp);
