@@ -368,7 +368,7 @@ def main():
     ap.add_argument("--no-parts", action="store_true", help="skip the conversion-in-parts leg (config-3 shape)")
     ap.add_argument("--parts-points", type=int, default=0, help="points of the parts leg (0: as many as host memory holds, <= 3B)")
     ap.add_argument("--serving-jobs", type=int, default=200)
-    ap.add_argument("--serving-rate", type=float, default=16.0)
+    ap.add_argument("--serving-rate", type=float, default=4.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
