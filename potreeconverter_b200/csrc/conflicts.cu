@@ -280,6 +280,13 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 	}
 }
 
+// st += the list build's own counters
+__global__ void add_list_stats_kernel(SampleStats* st, const SampleStats* lst) {
+	atomicAdd(&st->list_entries, lst->list_entries);
+	atomicAdd(&st->escalated, lst->escalated);
+	atomicAdd(&st->timeouts, lst->timeouts);
+}
+
 }  // namespace
 
 void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<LevelNode>& ln, const std::vector<uint8_t>& use,
@@ -333,22 +340,36 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	cl.inl = mem.alloc<int4>(M);
 	cl.ovf_off = mem.alloc<int32_t>(M);
 	// entries past the inline ones: room for 4 more per candidate on
-	// average (lists average about one entry); a node whose candidates find
-	// the pool full keeps the lookup kernels
+	// average (lists average about one entry); when the lists need more, the
+	// build runs again with a pool of the exact size it asked for
 	cl.pool_cap = std::min<int64_t>((int64_t)M * kListInline, (int64_t)INT32_MAX);
 	cl.pool = mem.alloc<int32_t>(cl.pool_cap > 0 ? cl.pool_cap : 1);
 	cl.pool_used = mem.alloc<unsigned long long>(1);
-	PCG_CUDA(cudaMemsetAsync(cl.pool_used, 0, sizeof(unsigned long long), s));
 	cl.count = mem.alloc<uint8_t>(M);
 	cl.node_dense = mem.alloc<uint8_t>(K);
-	PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
 	uint8_t* d_use = mem.alloc<uint8_t>(K);
 	PCG_CUDA(cudaMemcpyAsync(d_use, use.data(), K, cudaMemcpyHostToDevice, s));
-	if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, st);
-	else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, st);
+	SampleStats* lst = mem.alloc<SampleStats>(1);
+	for (int attempt = 0; attempt < 2; attempt++) {
+		PCG_CUDA(cudaMemsetAsync(cl.pool_used, 0, sizeof(unsigned long long), s));
+		PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
+		PCG_CUDA(cudaMemsetAsync(lst, 0, sizeof(SampleStats), s));
+		if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, lst);
+		else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, lst);
+		PCG_LAUNCHED();
+		unsigned long long used = 0;
+		PCG_CUDA(cudaMemcpyAsync(&used, cl.pool_used, sizeof(used), cudaMemcpyDeviceToHost, s));
+		PCG_CUDA(cudaStreamSynchronize(s));
+		if ((int64_t)used <= cl.pool_cap || attempt == 1 || (int64_t)used > (int64_t)INT32_MAX) break;
+		mem.free(cl.pool);
+		cl.pool_cap = (int64_t)used;
+		cl.pool = mem.alloc<int32_t>(cl.pool_cap);
+	}
+	add_list_stats_kernel<<<1, 1, 0, s>>>(st, lst);
 	PCG_LAUNCHED();
 	PCG_CUDA(cudaMemcpyAsync(dense.data(), cl.node_dense, K, cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));
+	mem.free(lst);
 	mem.free(d_use);
 	mem.free(d_bm_off);
 	mem.free(bm);
