@@ -339,10 +339,10 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	}
 	cl.inl = mem.alloc<int4>(M);
 	cl.ovf_off = mem.alloc<int32_t>(M);
-	// entries past the inline ones: room for 4 more per candidate on
+	// entries past the inline ones: room for 8 more per candidate on
 	// average (lists average about one entry); when the lists need more, the
 	// build runs again with a pool of the exact size it asked for
-	cl.pool_cap = std::min<int64_t>((int64_t)M * kListInline, (int64_t)INT32_MAX);
+	cl.pool_cap = std::min<int64_t>((int64_t)M * 2 * kListInline, (int64_t)INT32_MAX);
 	cl.pool = mem.alloc<int32_t>(cl.pool_cap > 0 ? cl.pool_cap : 1);
 	cl.pool_used = mem.alloc<unsigned long long>(1);
 	cl.count = mem.alloc<uint8_t>(M);
