@@ -16,7 +16,7 @@
 //     every point closer than the spacing lies in the 3 x 3 x 3 cells around
 //     a candidate's own;
 //  2. segmented radix sort of (cell, sorted position) per node;
-//  3. a hash table (node, cell) -> range of the cell-sorted records;
+//  3. a hash table per node, cell -> range of the cell-sorted records;
 //  4. one thread per candidate in cell order (a warp shares neighbourhoods)
 //     scans the occupied cells among its 27 up to its own sorted position:
 //     the FP32 distance on node-relative coordinates decides every pair
@@ -51,7 +51,7 @@ constexpr uint64_t kEmptyRun = ~0ull;
 constexpr int kCellsPerAxis = 128;  // node box = 128 spacings
 
 struct alignas(16) RunSlot {  // run table entry, one 16-byte load per probe
-	uint64_t key;             // node << 32 | cell, kEmptyRun when free
+	uint64_t key;             // cell, kEmptyRun when free
 	int32_t start, count;     // first record in the node, records
 };
 
@@ -119,30 +119,39 @@ __device__ __forceinline__ bool run_head(const LevelNode* nodes, const int32_t* 
 	return j == nodes[node_of[j]].cand_off || ck[j] != ck[j - 1];
 }
 
+// occupied cells (runs) per node
 __global__ void conf_count_runs_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ node_of, const uint64_t* __restrict__ ck,
-                                       int64_t M, unsigned long long* __restrict__ runs) {
+                                       int64_t M, unsigned long long* __restrict__ node_runs) {
 	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	const bool h = j < M && run_head(nodes, node_of, ck, j);
-	const unsigned b = __ballot_sync(FULL, h);
-	if ((threadIdx.x & 31) == 0 && b) atomicAdd(runs, (unsigned long long)__popc(b));
+	const int32_t node = j < M ? node_of[j] : -1;
+	const unsigned peers = __match_any_sync(FULL, node);
+	const unsigned heads = __ballot_sync(FULL, h) & peers;
+	if (node >= 0 && heads && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&node_runs[node], (unsigned long long)__popc(heads));
 }
 
-// run table: key (node << 32 | cell) -> (first record, count)
-__global__ void conf_insert_runs_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ node_of, const uint64_t* __restrict__ ck,
-                                        int64_t M, RunSlot* __restrict__ table, int64_t cap, SampleStats* st) {
+// run tables, one per node: cell -> (first record, count). A node's table
+// is its own region (tab_off, power-of-two tab_cap), so the probes of the
+// candidates in flight stay within the few nodes being searched and hit L2.
+__global__ void conf_insert_runs_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, const int32_t* __restrict__ node_of,
+                                        const uint64_t* __restrict__ ck, int64_t M, RunSlot* __restrict__ table,
+                                        const int64_t* __restrict__ tab_off, const int64_t* __restrict__ tab_cap, SampleStats* st) {
 	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (j >= M || !run_head(nodes, node_of, ck, j)) return;
+	if (j >= M) return;
 	const int32_t node = node_of[j];
+	if (!use[node] || !run_head(nodes, node_of, ck, j)) return;
 	const int64_t end = nodes[node].cand_off + nodes[node].count;
 	int64_t e = j + 1;
 	while (e < end && ck[e] == ck[j]) e++;
-	const uint64_t key = ((uint64_t)(uint32_t)node << 32) | ck[j];
+	const uint64_t key = ck[j];
+	RunSlot* tb = table + tab_off[node];
+	const int64_t cap = tab_cap[node];
 	uint64_t s = run_hash(key, cap);
 	for (int64_t probe = 0; probe < cap; probe++) {
-		const unsigned long long prev = atomicCAS((unsigned long long*)&table[s].key, (unsigned long long)kEmptyRun, (unsigned long long)key);
+		const unsigned long long prev = atomicCAS((unsigned long long*)&tb[s].key, (unsigned long long)kEmptyRun, (unsigned long long)key);
 		if (prev == kEmptyRun) {
-			table[s].start = (int32_t)(j - nodes[node].cand_off);
-			table[s].count = (int32_t)(e - j);
+			tb[s].start = (int32_t)(j - nodes[node].cand_off);
+			tb[s].count = (int32_t)(e - j);
 			return;
 		}
 		s = (s + 1) & (uint64_t)(cap - 1);
@@ -161,10 +170,15 @@ __device__ __forceinline__ int2 find_run(const RunSlot* table, int64_t cap, uint
 	return make_int2(0, 0);
 }
 
+// The search waits on dependent loads (bitmap row, run table, runs): five
+// resident blocks of 256 threads per SM (48 registers) hide more of it than
+// four would.
 template <int MODE>
-__global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, PosParamsS pp,
+__global__ void __launch_bounds__(256, 5) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, PosParamsS pp,
                                                         LevelBuffers lb, const uint64_t* __restrict__ ck, const int4* __restrict__ crec,
-                                                        const float4* __restrict__ crf, const RunSlot* __restrict__ table, int64_t cap, const int64_t* __restrict__ bm_off, const uint32_t* __restrict__ bm,
+                                                        const float4* __restrict__ crf, const RunSlot* __restrict__ table,
+                                                        const int64_t* __restrict__ tab_off, const int64_t* __restrict__ tab_cap,
+                                                        const int64_t* __restrict__ bm_off, const uint32_t* __restrict__ bm,
                                                         ConflictLists cl, SampleStats* st) {
 	const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= lb.M) return;
@@ -172,10 +186,8 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 	if (!use[node]) return;
 	const LevelNode& nd = nodes[node];
 	const int64_t co = nd.cand_off;
-	const int4 me = crec[j];
 	const float4 mf = crf[j];
-	const int32_t t = me.w;
-	const double x = qcoord(me.x, 0, pp), y = qcoord(me.y, 1, pp), z = qcoord(me.z, 2, pp);
+	const int32_t t = __float_as_int(mf.w);
 	const double sp = nd.spacing, s2 = sp * sp;
 	double lim = 0.0;
 	if (MODE == 0) {
@@ -195,12 +207,16 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 	unsigned escalated = 0;  // pairs inside the band, decided in FP64
 	const uint64_t c = ck[j];
 	const int cx = (int)(c % kCellsPerAxis), cy = (int)((c / kCellsPerAxis) % kCellsPerAxis), cz = (int)(c / (kCellsPerAxis * kCellsPerAxis));
-	// the first kListInline entries in registers, the rest (rare) in a
-	// per-thread array; both are stored once the search is done
-	int4 head = make_int4(0, 0, 0, 0);
-	int32_t rest[kListCap - kListInline];
+	// the first kListInline entries go to the candidate's own slot (positions
+	// past the list read as 0); a list that outgrows it takes a block of
+	// kListCap - kListInline entries of the pool for the rest
+	int32_t* inl = reinterpret_cast<int32_t*>(cl.inl + co + t);
+	cl.inl[co + t] = make_int4(0, 0, 0, 0);
+	int64_t at = -1;
 	int n = 0;
 	const int64_t boff = bm_off[node];
+	const RunSlot* tb = table + tab_off[node];
+	const int64_t cap = tab_cap[node];
 	for (int dz = -1; dz <= 1; dz++) {
 		const int qz = cz + dz;
 		if (qz < 0 || qz >= kCellsPerAxis) continue;
@@ -222,7 +238,7 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 				const int qx = cx + dx;
 				if (qx < 0 || qx >= kCellsPerAxis || !((occ >> (dx + 1)) & 1u)) continue;
 				const uint64_t cell = ((uint64_t)qz * kCellsPerAxis + (uint64_t)qy) * kCellsPerAxis + (uint64_t)qx;
-				const int2 run = find_run(table, cap, ((uint64_t)(uint32_t)node << 32) | cell);
+				const int2 run = find_run(tb, cap, cell);
 				const int4* rp = crec + co + run.x;
 				const float4* rf = crf + co + run.x;
 				for (int i = 0; i < run.y; i++) {
@@ -239,35 +255,37 @@ __global__ void __launch_bounds__(256) conf_lists_kernel(const LevelNode* __rest
 						inside = d2 < s2lo;
 					}
 					if (!inside) {
+						// the FP64 positions are recomputed here, not held in
+						// registers through the search (pairs in the band are rare)
 						const int4 q = rp[i];
+						const int4 me = crec[j];
 						const double ax = qcoord(q.x, 0, pp), ay = qcoord(q.y, 1, pp), az = qcoord(q.z, 2, pp);
+						const double x = qcoord(me.x, 0, pp), y = qcoord(me.y, 1, pp), z = qcoord(me.z, 2, pp);
 						// squaredDistance(point, candidate), sampler_poisson.h:117-125
 						const double dx_ = ax - x, dy_ = ay - y, dz_ = az - z;
 						escalated++;
 						if (!(dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < s2)) continue;
 					}
 					if (MODE == 0 && !(lb.keys[co + u] >= lim)) continue;
-					if (n == 0) head.x = u;
-					else if (n == 1) head.y = u;
-					else if (n == 2) head.z = u;
-					else if (n == 3) head.w = u;
-					else if (n < kListCap) rest[n - kListInline] = u;
+					if (n < kListInline) {
+						inl[n] = u;
+					} else if (n < kListCap) {
+						if (n == kListInline) {
+							constexpr int kBlock = kListCap - kListInline;
+							const unsigned long long a = atomicAdd(cl.pool_used, (unsigned long long)kBlock);
+							at = (int64_t)a + kBlock <= cl.pool_cap ? (int64_t)a : -2;
+						}
+						if (at >= 0) cl.pool[at + (n - kListInline)] = u;
+					}
 					n++;
 				}
 			}
 		}
 	}
-	cl.inl[co + t] = head;
 	bool dense = n > kListCap;
 	if (!dense && n > kListInline) {
-		const int extra = n - kListInline;
-		const unsigned long long at = atomicAdd(cl.pool_used, (unsigned long long)extra);
-		if ((int64_t)(at + extra) <= cl.pool_cap) {
-			cl.ovf_off[co + t] = (int32_t)at;
-			for (int e = 0; e < extra; e++) cl.pool[at + e] = rest[e];
-		} else {
-			dense = true;  // the pool is full: this node keeps the lookup kernels
-		}
+		if (at >= 0) cl.ovf_off[co + t] = (int32_t)at;
+		else dense = true;  // the pool is full: the level builds its lists again with a larger pool
 	}
 	cl.count[co + t] = (uint8_t)(dense ? kListDense : n);
 	if (dense) cl.node_dense[node] = 1;
@@ -310,19 +328,36 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	conf_gather_kernel<<<blocks, 256, 0, s>>>(d_nodes, pp, lb, cv, crec, crf);
 	PCG_LAUNCHED();
 	mem.free(cv);
-	unsigned long long* d_runs = mem.alloc<unsigned long long>(1);
-	PCG_CUDA(cudaMemsetAsync(d_runs, 0, sizeof(unsigned long long), s));
+	unsigned long long* d_runs = mem.alloc<unsigned long long>(K);
+	PCG_CUDA(cudaMemsetAsync(d_runs, 0, K * sizeof(unsigned long long), s));
 	conf_count_runs_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb.node_of, ck, M, d_runs);
 	PCG_LAUNCHED();
-	unsigned long long runs = 0;
-	PCG_CUDA(cudaMemcpyAsync(&runs, d_runs, sizeof(runs), cudaMemcpyDeviceToHost, s));
+	std::vector<unsigned long long> runs(K);
+	PCG_CUDA(cudaMemcpyAsync(runs.data(), d_runs, K * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));
 	mem.free(d_runs);
-	int64_t cap = 64;
-	while (cap < 2 * (int64_t)runs) cap <<= 1;
-	RunSlot* table = mem.alloc<RunSlot>(cap);
-	PCG_CUDA(cudaMemsetAsync(table, 0xff, cap * sizeof(RunSlot), s));
-	conf_insert_runs_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb.node_of, ck, M, table, cap, st);
+	// per-node tables at most half full
+	std::vector<int64_t> tab(2 * (size_t)K, 0);  // offsets, then capacities
+	int64_t slots = 0;
+	for (int k = 0; k < K; k++) {
+		int64_t cap = 0;
+		if (use[k] && runs[k] > 0) {
+			cap = 16;
+			while (cap < 2 * (int64_t)runs[k]) cap <<= 1;
+		}
+		tab[k] = slots;
+		tab[K + k] = cap;
+		slots += cap;
+	}
+	int64_t* d_tab = mem.alloc<int64_t>(2 * (size_t)K);
+	PCG_CUDA(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+	const int64_t* tab_off = d_tab;
+	const int64_t* tab_cap = d_tab + K;
+	RunSlot* table = mem.alloc<RunSlot>(slots > 0 ? slots : 1);
+	if (slots > 0) PCG_CUDA(cudaMemsetAsync(table, 0xff, slots * sizeof(RunSlot), s));
+	uint8_t* d_use = mem.alloc<uint8_t>(K);
+	PCG_CUDA(cudaMemcpyAsync(d_use, use.data(), K, cudaMemcpyHostToDevice, s));
+	conf_insert_runs_kernel<<<blocks, 256, 0, s>>>(d_nodes, d_use, lb.node_of, ck, M, table, tab_off, tab_cap, st);
 	PCG_LAUNCHED();
 	// occupancy bitmaps of the larger nodes
 	std::vector<int64_t> bm_off(K, -1);
@@ -339,23 +374,23 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	}
 	cl.inl = mem.alloc<int4>(M);
 	cl.ovf_off = mem.alloc<int32_t>(M);
-	// entries past the inline ones: room for 8 more per candidate on
-	// average (lists average about one entry); when the lists need more, the
-	// build runs again with a pool of the exact size it asked for
+	// entries past the inline ones: a list longer than kListInline takes a
+	// block of kListCap - kListInline entries; room for 8 entries per
+	// candidate (lists average about one entry, a few percent outgrow the
+	// inline slot). When the lists need more, the build runs again with a
+	// pool of the exact size they asked for (the same lists outgrow it).
 	cl.pool_cap = std::min<int64_t>((int64_t)M * 2 * kListInline, (int64_t)INT32_MAX);
 	cl.pool = mem.alloc<int32_t>(cl.pool_cap > 0 ? cl.pool_cap : 1);
 	cl.pool_used = mem.alloc<unsigned long long>(1);
 	cl.count = mem.alloc<uint8_t>(M);
 	cl.node_dense = mem.alloc<uint8_t>(K);
-	uint8_t* d_use = mem.alloc<uint8_t>(K);
-	PCG_CUDA(cudaMemcpyAsync(d_use, use.data(), K, cudaMemcpyHostToDevice, s));
 	SampleStats* lst = mem.alloc<SampleStats>(1);
 	for (int attempt = 0; attempt < 2; attempt++) {
 		PCG_CUDA(cudaMemsetAsync(cl.pool_used, 0, sizeof(unsigned long long), s));
 		PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
 		PCG_CUDA(cudaMemsetAsync(lst, 0, sizeof(SampleStats), s));
-		if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, lst);
-		else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, cap, d_bm_off, bm, cl, lst);
+		if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, tab_off, tab_cap, d_bm_off, bm, cl, lst);
+		else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, tab_off, tab_cap, d_bm_off, bm, cl, lst);
 		PCG_LAUNCHED();
 		unsigned long long used = 0;
 		PCG_CUDA(cudaMemcpyAsync(&used, cl.pool_used, sizeof(used), cudaMemcpyDeviceToHost, s));
@@ -374,6 +409,7 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	mem.free(d_bm_off);
 	mem.free(bm);
 	mem.free(table);
+	mem.free(d_tab);
 	mem.free(crec);
 	mem.free(crf);
 	mem.free(ck);

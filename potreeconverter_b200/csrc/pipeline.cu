@@ -698,6 +698,8 @@ struct Converter {
 		int max_depth = 0;
 		for (auto& n : tree.nodes) max_depth = std::max(max_depth, n.depth);
 		for (int d = max_depth - 1; d >= 0; d--) {
+			// the chunk roots one level down are final once their level ran
+			if (method == PCG_RANDOM) reshuffle_chunk_root_tasks(tree, chunk_roots, d + 1, mem);
 			std::vector<int> level_nodes;
 			for (int i = 0; i < (int)tree.nodes.size(); i++)
 				if (tree.nodes[i].depth == d && tree.nodes[i].has_children()) level_nodes.push_back(i);
@@ -1065,6 +1067,50 @@ struct Converter {
 	}
 
 	// Samples, deepest level first, the inner nodes among `nodes`.
+	// processChunkRoots (indexer.cpp:202-281) merges the chunk roots below a
+	// node into one task when they hold fewer than 5M points after their
+	// chunks were sampled; a chunk root whose parent is not merged stays a
+	// task of its own, and sampling that task (indexer.cpp:1717-1730) runs the
+	// sampler's callback on the chunk root once more. Its children were
+	// cleared after its chunk (:1675), so it is a leaf by then: the random
+	// sampler shuffles its points again with the same seed
+	// (sampler_random.h:89-121), the poisson samplers return at a leaf. Called
+	// for the chunk roots at `depth` (all of them for depth < 0) once the
+	// chunk roots below their parents have all been sampled.
+	void reshuffle_chunk_root_tasks(Tree& tree, const std::vector<int>& chunk_roots, int depth, DeviceMem& mem) {
+		if (chunk_roots.size() < 2) return;  // one chunk: its root is the octree's root
+		std::vector<int64_t> below(tree.nodes.size(), 0);  // CRNode::numPoints
+		for (int cr : chunk_roots)
+			for (int a = tree.nodes[cr].parent; a >= 0; a = tree.nodes[a].parent) below[a] += tree.nodes[cr].buf_count;
+		std::vector<int> sel;
+		std::vector<int64_t> off, cnt;
+		int64_t total = 0;
+		for (int cr : chunk_roots) {
+			const TNode& n = tree.nodes[cr];
+			if ((depth >= 0 && n.depth != depth) || n.parent < 0 || n.buf_count < 2) continue;
+			if (below[n.parent] < kChunkRootMergeThreshold) continue;  // merged into an ancestor's task
+			sel.push_back(cr);
+			off.push_back(total);
+			cnt.push_back(n.buf_count);
+			total += n.buf_count;
+		}
+		if (sel.empty()) return;
+		const cudaStream_t stream = mem.stream();
+		uint32_t* in = mem.alloc<uint32_t>(total);
+		uint32_t* out = mem.alloc<uint32_t>(total);
+		int32_t* scratch = mem.alloc<int32_t>(total);
+		for (size_t i = 0; i < sel.size(); i++)
+			PCG_CUDA(cudaMemcpyAsync(in + off[i], tree.nodes[sel[i]].buf_ids, cnt[i] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
+		int64_t* d_off = upload(off, mem);
+		int64_t* d_cnt = upload(cnt, mem);
+		launch_shuffle_leaves(d_off, d_cnt, (int)sel.size(), in, out, scratch, seed, mem);
+		for (size_t i = 0; i < sel.size(); i++) tree.nodes[sel[i]].buf_ids = out + off[i];
+		mem.free(d_cnt);
+		mem.free(d_off);
+		mem.free(scratch);
+		mem.free(in);
+	}
+
 	void sample_nodes(Tree& tree, const std::vector<int>& nodes, int method, double base_spacing, const PosParamsS& pps,
 	                  const ChunkingOut& co, SampleStats* d_st, GreedyArena& grid_arena, DeviceMem& mem, JobResult& res) {
 		int max_depth = -1;
@@ -1363,6 +1409,7 @@ struct Converter {
 		std::vector<int> upper;
 		for (int i = 0; i < (int)tree.nodes.size(); i++)
 			if (tree.nodes[i].chunk < 0) upper.push_back(i);
+		if (method == PCG_RANDOM) reshuffle_chunk_root_tasks(tree, chunk_roots, -1, mem);
 		GreedyArena grid_arena;
 		sample_nodes(tree, upper, method, base_spacing, pps, ctop, d_st, grid_arena, mem, res);
 		TNode& root = tree.nodes[0];

@@ -63,6 +63,13 @@ def test_hotspots_10m_matches_reference(gpu_ctx, method):
     _check(gpu_ctx.convert(_las(case), method=method, name=case["name"]), case, method)
 
 
+def test_hotspots_50m_random_matches_reference(gpu_ctx):
+    """Above 5M chunk-root points under a parent the chunk roots are tasks of
+    their own and the random sampler shuffles each of them a second time."""
+    case = _need("hotspots_50m")
+    _check(gpu_ctx.convert(_las(case), method="random", name=case["name"]), case, "random")
+
+
 def test_hotspots_50m_in_parts_matches_reference():
     case = _need("hotspots_50m")
     las = _las(case)
