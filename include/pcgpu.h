@@ -338,11 +338,11 @@ pcg_status pcg_kernel_laz_decode(pcg_ctx* ctx, const void* laz_file, uint64_t si
  * cudaMalloc/cudaFree is called.
  *  - n > PCG_NOALLOC_SORT_MAX returns PCG_BAD_INPUT and does nothing;
  *  - the first call on a device looks up the array's device address (set-up
- *    per device); make that first call before any stream capture. The
- *    address is kept for the life of the process: do not call this entry
- *    point again on a device after cudaDeviceReset;
+ *    per device). The address is kept for the life of the process: do not
+ *    call this entry point again on a device after cudaDeviceReset;
  *  - work runs on `stream` (a cudaStream_t, NULL = legacy default) and the
- *    call waits for it to finish (it reads back a small error word);
+ *    call waits for it to finish (it reads back a small error word), so it
+ *    cannot be part of a stream capture;
  *  - a CUDA error left pending by earlier work is reported as PCG_CUDA
  *    before anything is launched, and left pending for the caller;
  *  - all calls share the one array: calls that overlap on the GPU (other

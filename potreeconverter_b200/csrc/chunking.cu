@@ -10,6 +10,7 @@
 
 #include <math_constants.h>
 
+#include "bulk.cuh"
 #include "devutil.cuh"
 #include "kernels.h"
 
@@ -32,6 +33,12 @@ __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b 
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max(a, b)
 
 constexpr int kDecodeThreads = 256;
+
+// min / max of one extra-attribute element as ordered bit patterns
+struct ExtraRange {
+	unsigned long long mn = ~0ull, mx = 0ull;
+	__device__ void add(unsigned long long o) { mn = o < mn ? o : mn; mx = o > mx ? o : mx; }
+};
 
 struct IntRange {
 	int mn, mx;
@@ -65,12 +72,13 @@ __device__ __forceinline__ bool grid_cell(const DecodeParams& p, int32_t X, int3
 	return true;
 }
 
-// Records per tile of the staged decode: a block copies a tile of records
-// into shared memory with 16-byte loads (the tile is 16-byte aligned when the
+// Records per tile of the staged decode: a block brings tiles of records
+// into shared memory by bulk copies (the tile is 16-byte aligned when the
 // source's records are, since kDecodeTile x record length is a multiple of
-// 16) and decodes its points from there.
+// 16), two buffers deep, and decodes its points from there.
 constexpr int kDecodeTile = 512;
-constexpr int kDecodeStageMaxRec = 96;  // 48 KB of shared memory per block
+constexpr int kRegExtras = 2;
+constexpr int kDecodeStageMaxRec = 96;  // two buffers: 96 KB of shared memory per block
 
 // One thread per point. Writes the quantized position SoA and the count-grid
 // cell, counts into the grid with warp-aggregated atomics and reduces
@@ -79,7 +87,7 @@ constexpr int kDecodeStageMaxRec = 96;  // 48 KB of shared memory per block
 // records, short records) the block walks tiles of kDecodeTile records staged
 // in shared memory; else it reads each record in place (grid-stride).
 template <bool kMulti, bool kStaged>
-__global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodeParams p, uint32_t* __restrict__ grid, ChunkingOut out) {
+__global__ void __launch_bounds__(kDecodeThreads, 3) decode_count_kernel(DecodeParams p, uint32_t* __restrict__ grid, ChunkingOut out) {
 	extern __shared__ uint4 stage16[];
 	// shared statistics: [attr][comp] ordered min / max
 	__shared__ unsigned long long s_mn[MAX_ATTRS][3];
@@ -94,6 +102,9 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodePara
 
 	double pmn[3] = {CUDART_INF, CUDART_INF, CUDART_INF}, pmx[3] = {-CUDART_INF, -CUDART_INF, -CUDART_INF};
 	double gmn = CUDART_INF, gmx = -CUDART_INF;
+	// the first kRegExtras extra-attribute elements keep their min / max in
+	// registers (ordered bit patterns), the others go to shared memory
+	ExtraRange ex[kRegExtras];
 	IntRange r_int, r_ret, r_nret, r_cls, r_sar, r_user, r_psid, r_r, r_g, r_b;
 	r_int.init(); r_ret.init(); r_nret.init(); r_cls.init(); r_sar.init(); r_user.init(); r_psid.init(); r_r.init(); r_g.init(); r_b.init();
 
@@ -126,7 +137,10 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodePara
 		if (p.stat_class >= 0) {
 			int c = r[15] & 31;
 			r_cls.add(c);
-			atomicAdd(&s_hist[c], 1u);
+			// one shared-memory add per class present in the warp
+			const unsigned act = __activemask();
+			const unsigned peers = __match_any_sync(act, c);
+			if ((__ffs(peers) - 1) == (int)(threadIdx.x & 31)) atomicAdd(&s_hist[c], (unsigned)__popc(peers));
 		}
 		if (p.stat_sar >= 0) r_sar.add((int8_t)r[16]);
 		if (p.stat_user >= 0) r_user.add(r[17]);
@@ -141,9 +155,10 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodePara
 			r_g.add(ld<uint16_t>(r + sd.src_rgb + 2));
 			r_b.add(ld<uint16_t>(r + sd.src_rgb + 4));
 		}
+		int k = 0;  // element index over all extra attributes
 		for (int e = 0; e < sd.n_extra; e++) {
 			const ExtraDesc& d = sd.extra[e];
-			for (int c = 0; c < d.num_elements && c < 3; c++) {
+			for (int c = 0; c < d.num_elements && c < 3; c++, k++) {
 				const uint8_t* q = r + d.src_off + c * d.element_size;
 				double v = 0.0;
 				switch (d.type) {
@@ -159,25 +174,73 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodePara
 				case 21: v = ld<double>(q); break;
 				default: v = 0.0;
 				}
-				atomicMin(&s_mn[d.stat_index][c], ordered(v));
-				atomicMax(&s_mx[d.stat_index][c], ordered(v));
+				const unsigned long long o = ordered(v);
+				if (!kMulti && k < kRegExtras) {  // one source: element k is the same statistic for every point
+					// constant indices keep the accumulators in registers
+#pragma unroll
+					for (int q = 0; q < kRegExtras; q++)
+						if (q == k) ex[q].add(o);
+				} else {
+					atomicMin(&s_mn[d.stat_index][c], o);
+					atomicMax(&s_mx[d.stat_index][c], o);
+				}
 			}
 		}
 	};
 	if constexpr (kStaged) {
+		// tiles t0 = (blockIdx.x + k gridDim.x) kDecodeTile, k = 0, 1, ...;
+		// tile k lands in buffer k & 1 by a bulk copy issued two tiles ahead,
+		// so the copy of the next tile runs while this one is decoded
+		__shared__ uint64_t bars[2];
 		const SourceDesc& sd = p.src0;
 		const int rl = sd.rec_len;
-		const uint8_t* stage = reinterpret_cast<const uint8_t*>(stage16);
-		for (int64_t t0 = (int64_t)blockIdx.x * kDecodeTile; t0 < p.n; t0 += (int64_t)gridDim.x * kDecodeTile) {
-			const int cnt = (int)(p.n - t0 < kDecodeTile ? p.n - t0 : kDecodeTile);
-			const uint8_t* src = sd.recs + (t0 - sd.first) * rl;
-			const int bytes = cnt * rl, words = bytes >> 4;
-			for (int w = threadIdx.x; w < words; w += blockDim.x) stage16[w] = __ldg(reinterpret_cast<const uint4*>(src) + w);
-			for (int b = (words << 4) + threadIdx.x; b < bytes; b += blockDim.x)
-				reinterpret_cast<uint8_t*>(stage16)[b] = src[b];
-			__syncthreads();
-			for (int j = threadIdx.x; j < cnt; j += blockDim.x) point(t0 + j, stage + j * rl, sd);
-			__syncthreads();
+		uint8_t* const stage = reinterpret_cast<uint8_t*>(stage16);
+		const size_t buf_bytes = (size_t)kDecodeTile * rl;
+		auto buf = [&](int b) { return stage + b * buf_bytes; };
+		const int64_t step = (int64_t)gridDim.x * kDecodeTile;
+		const int64_t first = (int64_t)blockIdx.x * kDecodeTile;
+		auto tile_count = [&](int64_t t0) { return (int)(p.n - t0 < kDecodeTile ? p.n - t0 : kDecodeTile); };
+		// every tile but the cloud's last is a multiple of 16 bytes (kDecodeTile is)
+		auto by_bulk = [&](int64_t t0) { return t0 < p.n && ((int64_t)tile_count(t0) * rl) % 16 == 0; };
+		auto issue = [&](int64_t t0, int b) {
+			bulk_load(buf(b), sd.recs + (t0 - sd.first) * rl, (uint32_t)(tile_count(t0) * rl), &bars[b]);
+		};
+		if (threadIdx.x == 0) {
+			bulk_bar_init(&bars[0]);
+			bulk_bar_init(&bars[1]);
+			bulk_bar_fence_init();
+		}
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			if (by_bulk(first)) issue(first, 0);
+			if (by_bulk(first + step)) issue(first + step, 1);
+		}
+		uint32_t parity = 0u;  // bit b: phase parity of buffer b's barrier
+		int k = 0;
+		for (int64_t t0 = first; t0 < p.n; t0 += step, k++) {
+			const int b = k & 1;
+			const int cnt = tile_count(t0);
+			if (by_bulk(t0)) {
+				const bool ok = bulk_wait(&bars[b], (parity >> b) & 1u);
+				parity ^= 1u << b;
+				if (__syncthreads_or(!ok)) {
+					// a copy that did not complete: report it; the other
+					// buffer's copy, if one was issued, gets a bounded wait
+					if (threadIdx.x == 0) {
+						atomicCAS((unsigned long long*)&out.error[0], 0ull, (unsigned long long)(long long)-1);
+						if (by_bulk(t0 + step)) bulk_wait(&bars[b ^ 1], (parity >> (b ^ 1)) & 1u);
+					}
+					return;
+				}
+			} else {
+				// the cloud's last tile, not a multiple of 16 bytes
+				const uint8_t* src = sd.recs + (t0 - sd.first) * rl;
+				for (int i = threadIdx.x; i < cnt * rl; i += blockDim.x) buf(b)[i] = src[i];
+				__syncthreads();
+			}
+			for (int j = threadIdx.x; j < cnt; j += blockDim.x) point(t0 + j, buf(b) + (size_t)j * rl, sd);
+			__syncthreads();  // buffer b is free again
+			if (threadIdx.x == 0 && by_bulk(t0 + 2 * step)) issue(t0 + 2 * step, b);
 		}
 	} else {
 		const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -206,6 +269,21 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_count_kernel(DecodePara
 	if (p.stat_gps >= 0 && gmn <= gmx) {
 		atomicMin(&s_mn[p.stat_gps][0], ordered(gmn));
 		atomicMax(&s_mx[p.stat_gps][0], ordered(gmx));
+	}
+	if (!kMulti) {
+		const SourceDesc& sd = p.src0;
+		int k = 0;
+		for (int e = 0; e < sd.n_extra; e++) {
+			const ExtraDesc& d = sd.extra[e];
+			for (int c = 0; c < d.num_elements && c < 3 && k < kRegExtras; c++, k++) {
+#pragma unroll
+				for (int q = 0; q < kRegExtras; q++) {
+					if (q != k) continue;
+					if (ex[q].mn != ~0ull) atomicMin(&s_mn[d.stat_index][c], ex[q].mn);
+					if (ex[q].mx != 0ull) atomicMax(&s_mx[d.stat_index][c], ex[q].mx);
+				}
+			}
+		}
 	}
 	__syncthreads();
 	for (int i = threadIdx.x; i < MAX_ATTRS * 3; i += blockDim.x) {
@@ -436,11 +514,16 @@ void launch_decode_count(const DecodeParams& p, uint32_t* grid, ChunkingOut& out
 	int64_t cap = (int64_t)sms * 8;
 	if (blocks > cap) blocks = cap;
 	if (blocks < 1) blocks = 1;
-	const bool staged = p.nsrc == 1 && p.src0.rec_len <= kDecodeStageMaxRec && (reinterpret_cast<uintptr_t>(p.src0.recs) & 15) == 0;
+	// bulk copies of whole tiles: 16-byte aligned records (kDecodeTile
+	// records are a multiple of 16 bytes, so every tile starts aligned)
+	const bool staged = p.nsrc == 1 && p.src0.rec_len <= kDecodeStageMaxRec && (reinterpret_cast<uintptr_t>(p.src0.recs) & 15) == 0 &&
+	                    p.src0.first == 0;
 	if (p.nsrc > 1) {
 		decode_count_kernel<true, false><<<(unsigned)blocks, kDecodeThreads, 0, mem.stream()>>>(p, grid, out);
 	} else if (staged) {
-		const size_t smem = (size_t)kDecodeTile * p.src0.rec_len;
+		const size_t smem = 2 * (size_t)kDecodeTile * p.src0.rec_len;
+		if (smem > 48 * 1024)
+			PCG_CUDA(cudaFuncSetAttribute(decode_count_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 		int64_t tb = ceil_div(p.n, kDecodeTile);
 		if (tb > cap) tb = cap;
 		decode_count_kernel<false, true><<<(unsigned)tb, kDecodeThreads, smem, mem.stream()>>>(p, grid, out);

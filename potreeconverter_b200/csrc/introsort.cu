@@ -873,10 +873,10 @@ void launch_sort_keys_single(double* keys, int32_t* vals, int64_t n, DeviceMem& 
 // pcg_kernel_sort_keys_noalloc: the std::sort replay for callers that cannot
 // allocate device memory themselves or let a library do it -- code running
 // inside a host framework that owns every device allocation (a plugin under
-// a fixed memory budget), or code enqueuing work while a stream is being
-// captured, where cudaMalloc is not permitted. Its scratch is this
-// file-scope array, reserved on every GPU that loads the library until the
-// process exits.
+// a fixed memory budget). Its scratch is this file-scope array, reserved on
+// every GPU that loads the library until the process exits. The call waits
+// on its stream for the error word, so it cannot be part of a stream
+// capture.
 
 #include "../../include/pcgpu.h"
 

@@ -45,6 +45,14 @@ namespace {
 using Clock = std::chrono::steady_clock;
 double ms_since(Clock::time_point t) { return std::chrono::duration<double, std::milli>(Clock::now() - t).count(); }
 
+// error word of the counting pass: the first point outside the header's
+// box (index + 1), or -1 when a record copy into shared memory did not
+// complete within its bounded wait
+void check_counting_pass(int64_t e) {
+	if (e < 0) throw PcgError(PCG_TIMEOUT, "a record copy of the counting pass did not complete");
+	if (e > 0) throw PcgError(PCG_OUT_OF_BOX, "point " + std::to_string(e - 1) + " lies outside the header bounding box");
+}
+
 constexpr int64_t kMaxNodePoints = 10'000;          // indexer.h:47
 constexpr int kChunkRootMergeThreshold = 5'000'000; // indexer.cpp:241
 
@@ -615,7 +623,7 @@ struct Converter {
 		launch_decode_count(p, grid, co, mem);
 
 		auto errs = download(co.error, 2, stream);
-		if (errs[0]) throw PcgError(PCG_OUT_OF_BOX, "point " + std::to_string(errs[0] - 1) + " lies outside the header bounding box");
+		check_counting_pass(errs[0]);
 		int32_t* lut = mem.alloc<int32_t>(cells);
 		const std::vector<std::pair<std::string, ChunkCell>> chunks = make_chunks(grid, G, s.max_points_per_chunk, lut, mem);
 		const int nchunks = (int)chunks.size();
@@ -1195,7 +1203,7 @@ struct Converter {
 			mem.free(ct.X); mem.free(ct.Y); mem.free(ct.Z); mem.free(ct.cell);
 		}
 		res.stats.ms_h2d = ms_since(t_chunk);
-		if (download(co.error, 2, stream)[0]) throw PcgError(PCG_OUT_OF_BOX, "a point lies outside the header bounding box");
+		check_counting_pass(download(co.error, 2, stream)[0]);
 		int32_t* lut = mem.alloc<int32_t>(cells);
 		const std::vector<std::pair<std::string, ChunkCell>> chunks = make_chunks(grid, G, s.max_points_per_chunk, lut, mem);
 		const int nchunks = (int)chunks.size();
@@ -2340,7 +2348,7 @@ pcg_status pcg_kernel_decode_count(pcg_ctx* ctx, const void* las, uint64_t size,
 		PCG_CUDA(cudaMemsetAsync(co.error, 0, 16, stream));
 		pcg::launch_decode_count(p, d_grid, co, mem);
 		const auto errs = pcg::download(co.error, 2, stream);
-		if (errs[0]) throw pcg::PcgError(PCG_OUT_OF_BOX, "point " + std::to_string(errs[0] - 1) + " lies outside the header bounding box");
+		pcg::check_counting_pass(errs[0]);
 		if (N > 0) {
 			PCG_CUDA(cudaMemcpyAsync(X, co.X, N * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
 			PCG_CUDA(cudaMemcpyAsync(Y, co.Y, N * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
