@@ -208,21 +208,37 @@ __global__ void __launch_bounds__(256, 5) conf_lists_kernel(const LevelNode* __r
 	const uint64_t c = ck[j];
 	const int cx = (int)(c % kCellsPerAxis), cy = (int)((c / kCellsPerAxis) % kCellsPerAxis), cz = (int)(c / (kCellsPerAxis * kCellsPerAxis));
 	// the first kListInline entries go to the candidate's own slot (positions
-	// past the list read as 0); a list that outgrows it takes a block of
-	// kListCap - kListInline entries of the pool for the rest
+	// past the list read as 0); the rest (rare) wait in a per-thread array
+	// and take exactly their room in the pool once the search is done
 	int32_t* inl = reinterpret_cast<int32_t*>(cl.inl + co + t);
 	cl.inl[co + t] = make_int4(0, 0, 0, 0);
-	int64_t at = -1;
+	int32_t rest[kListCap - kListInline];
 	int n = 0;
 	const int64_t boff = bm_off[node];
 	const RunSlot* tb = table + tab_off[node];
 	const int64_t cap = tab_cap[node];
+	// gaps from the candidate to the faces it shares with the cells below
+	// and above it on each axis: a neighbour cell whose nearest point is
+	// at least the band's upper edge away holds no pair (with the
+	// prefilter's margin over the FP32 error; nodes without the prefilter
+	// visit every cell)
+	const float cs = (float)(sp * 1.000001);
+	auto gap2 = [&](int d, float v, int c) {
+		const float g = d < 0 ? v - (float)c * cs : (float)(c + 1) * cs - v;
+		return pre32 && d != 0 && g > 0.f ? g * g : 0.f;
+	};
+#pragma unroll 1
 	for (int dz = -1; dz <= 1; dz++) {
 		const int qz = cz + dz;
 		if (qz < 0 || qz >= kCellsPerAxis) continue;
+		const float dz2 = gap2(dz, mf.z, cz);
+		if (dz2 >= s2hi) continue;
+#pragma unroll 1
 		for (int dy = -1; dy <= 1; dy++) {
 			const int qy = cy + dy;
 			if (qy < 0 || qy >= kCellsPerAxis) continue;
+			const float dzy2 = dz2 + gap2(dy, mf.y, cy);
+			if (dzy2 >= s2hi) continue;
 			// occupied cells among x = cx-1 .. cx+1 of this row
 			uint32_t occ = 7u;
 			if (boff >= 0) {
@@ -237,6 +253,7 @@ __global__ void __launch_bounds__(256, 5) conf_lists_kernel(const LevelNode* __r
 			for (int dx = -1; dx <= 1; dx++) {
 				const int qx = cx + dx;
 				if (qx < 0 || qx >= kCellsPerAxis || !((occ >> (dx + 1)) & 1u)) continue;
+				if (dzy2 + gap2(dx, mf.x, cx) >= s2hi) continue;
 				const uint64_t cell = ((uint64_t)qz * kCellsPerAxis + (uint64_t)qy) * kCellsPerAxis + (uint64_t)qx;
 				const int2 run = find_run(tb, cap, cell);
 				const int4* rp = crec + co + run.x;
@@ -267,16 +284,8 @@ __global__ void __launch_bounds__(256, 5) conf_lists_kernel(const LevelNode* __r
 						if (!(dx_ * dx_ + dy_ * dy_ + dz_ * dz_ < s2)) continue;
 					}
 					if (MODE == 0 && !(lb.keys[co + u] >= lim)) continue;
-					if (n < kListInline) {
-						inl[n] = u;
-					} else if (n < kListCap) {
-						if (n == kListInline) {
-							constexpr int kBlock = kListCap - kListInline;
-							const unsigned long long a = atomicAdd(cl.pool_used, (unsigned long long)kBlock);
-							at = (int64_t)a + kBlock <= cl.pool_cap ? (int64_t)a : -2;
-						}
-						if (at >= 0) cl.pool[at + (n - kListInline)] = u;
-					}
+					if (n < kListInline) inl[n] = u;
+					else if (n < kListCap) rest[n - kListInline] = u;
 					n++;
 				}
 			}
@@ -284,8 +293,14 @@ __global__ void __launch_bounds__(256, 5) conf_lists_kernel(const LevelNode* __r
 	}
 	bool dense = n > kListCap;
 	if (!dense && n > kListInline) {
-		if (at >= 0) cl.ovf_off[co + t] = (int32_t)at;
-		else dense = true;  // the pool is full: the level builds its lists again with a larger pool
+		const int extra = n - kListInline;
+		const unsigned long long at = atomicAdd(cl.pool_used, (unsigned long long)extra);
+		if ((int64_t)(at + extra) <= cl.pool_cap) {
+			cl.ovf_off[co + t] = (int32_t)at;
+			for (int e = 0; e < extra; e++) cl.pool[at + e] = rest[e];
+		} else {
+			dense = true;  // the pool is full: the level builds its lists again with a larger pool
+		}
 	}
 	cl.count[co + t] = (uint8_t)(dense ? kListDense : n);
 	if (dense) cl.node_dense[node] = 1;
@@ -374,13 +389,25 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	}
 	cl.inl = mem.alloc<int4>(M);
 	cl.ovf_off = mem.alloc<int32_t>(M);
-	// entries past the inline ones: a list longer than kListInline takes a
-	// block of kListCap - kListInline entries; room for 8 entries per
-	// candidate (lists average about one entry, a few percent outgrow the
-	// inline slot). When the lists need more, the build runs again with a
-	// pool of the exact size they asked for (the same lists outgrow it).
-	cl.pool_cap = std::min<int64_t>((int64_t)M * 2 * kListInline, (int64_t)INT32_MAX);
-	cl.pool = mem.alloc<int32_t>(cl.pool_cap > 0 ? cl.pool_cap : 1);
+	// entries past the inline ones: room for 4 more per candidate on
+	// average (lists average about one entry). When the lists need more,
+	// the build runs again with a pool of the exact size they asked for. A
+	// pool the device cannot hold is made smaller: the candidates it cannot
+	// take mark their nodes dense, which keep the lookup kernels.
+	auto alloc_pool = [&](int64_t want) {
+		int64_t cap = std::max<int64_t>(want, 1);
+		while (true) {
+			try {
+				cl.pool = mem.alloc<int32_t>(cap);
+				cl.pool_cap = cap;
+				return;
+			} catch (const PcgError& e) {
+				if (e.status != 3 || cap <= 4096) throw;  // 3: PCG_OOM
+				cap /= 2;
+			}
+		}
+	};
+	alloc_pool(std::min<int64_t>((int64_t)M * kListInline, (int64_t)INT32_MAX));
 	cl.pool_used = mem.alloc<unsigned long long>(1);
 	cl.count = mem.alloc<uint8_t>(M);
 	cl.node_dense = mem.alloc<uint8_t>(K);
@@ -397,8 +424,7 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 		PCG_CUDA(cudaStreamSynchronize(s));
 		if ((int64_t)used <= cl.pool_cap || attempt == 1 || (int64_t)used > (int64_t)INT32_MAX) break;
 		mem.free(cl.pool);
-		cl.pool_cap = (int64_t)used;
-		cl.pool = mem.alloc<int32_t>(cl.pool_cap);
+		alloc_pool((int64_t)used);
 	}
 	add_list_stats_kernel<<<1, 1, 0, s>>>(st, lst);
 	PCG_LAUNCHED();

@@ -15,6 +15,7 @@
 //    node) run the replay for the nodes of one octree level.
 
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 #include <algorithm>
 #include <climits>
@@ -636,14 +637,157 @@ __global__ void __launch_bounds__(kWideThreads) wide_swap_kernel(const WideTile*
 	}
 }
 
+// ------------------------------------------- segments with distinct keys
+// The smallest and largest key of a segment, how often each occurs and
+// where (first occurrence).
+struct SegExtremes {
+	double kmin, kmax;
+	int cmin, cmax;
+	int64_t imin, imax;
+};
+
+__device__ __forceinline__ void extremes_init(SegExtremes& e) {
+	e.kmin = CUDART_INF;
+	e.kmax = -CUDART_INF;
+	e.cmin = e.cmax = 0;
+	e.imin = e.imax = INT64_MAX;
+}
+
+__device__ __forceinline__ void extremes_merge(SegExtremes& e, const SegExtremes& o) {
+	if (o.kmin < e.kmin) { e.kmin = o.kmin; e.cmin = o.cmin; e.imin = o.imin; }
+	else if (o.kmin == e.kmin) { e.cmin += o.cmin; e.imin = o.imin < e.imin ? o.imin : e.imin; }
+	if (o.kmax > e.kmax) { e.kmax = o.kmax; e.cmax = o.cmax; e.imax = o.imax; }
+	else if (o.kmax == e.kmax) { e.cmax += o.cmax; e.imax = o.imax < e.imax ? o.imax : e.imax; }
+}
+
+__device__ __forceinline__ void extremes_point(SegExtremes& e, double k, int64_t i) {
+	SegExtremes o;
+	o.kmin = o.kmax = k;
+	o.cmin = o.cmax = 1;
+	o.imin = o.imax = i;
+	extremes_merge(e, o);
+}
+
+__device__ __forceinline__ void extremes_warp(SegExtremes& e) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		SegExtremes x;
+		x.kmin = __shfl_xor_sync(FULL, e.kmin, o);
+		x.kmax = __shfl_xor_sync(FULL, e.kmax, o);
+		x.cmin = __shfl_xor_sync(FULL, e.cmin, o);
+		x.cmax = __shfl_xor_sync(FULL, e.cmax, o);
+		x.imin = __shfl_xor_sync(FULL, (long long)e.imin, o);
+		x.imax = __shfl_xor_sync(FULL, (long long)e.imax, o);
+		extremes_merge(e, x);
+	}
+}
+
+// Whether segment [f, l) (its extremes e) has pairwise distinct keys; if so
+// *a is the first sorted position of its inner elements (keys strictly
+// between its smallest and largest), which are sorted[a, a + (l - f) - 2).
+__device__ bool distinct_segment(const SortedLevel& sl, int64_t f, int64_t l, const SegExtremes& e, int64_t* a) {
+	const int64_t n = l - f;
+	if (e.cmin != 1 || e.cmax != 1 || !(e.kmin < e.kmax)) return false;
+	const LevelNode nd = sl.nodes[sl.node_of[f]];
+	const uint64_t bmin = (uint64_t)__double_as_longlong(e.kmin), bmax = (uint64_t)__double_as_longlong(e.kmax);
+	// keys are >= +0, so their bit patterns order like their values
+	int64_t lo = nd.cand_off, hi = nd.cand_off + nd.count;
+	while (lo < hi) {
+		const int64_t mid = lo + (hi - lo) / 2;
+		if (sl.sk[mid] <= bmin) lo = mid + 1;
+		else hi = mid;
+	}
+	const int64_t first = lo;
+	hi = nd.cand_off + nd.count;
+	while (lo < hi) {
+		const int64_t mid = lo + (hi - lo) / 2;
+		if (sl.sk[mid] < bmax) lo = mid + 1;
+		else hi = mid;
+	}
+	const int64_t last = lo;  // inner elements: sorted[first, last)
+	if (last - first != n - 2) return false;
+	if (last - first >= 2 && sl.ties[last - 1] != sl.ties[first]) return false;
+	*a = first;
+	return true;
+}
+
+// writes a distinct segment in ascending order (e and a from above); the
+// caller's threads t = 0 .. nt-1 share the work and have all read
+// vmin = val[e.imin], vmax = val[e.imax] before
+__device__ void write_distinct(const SortedLevel& sl, double* key, int32_t* val, int64_t f, int64_t l, const SegExtremes& e, int64_t a,
+                               int32_t vmin, int32_t vmax, int t, int nt) {
+	const int64_t n = l - f;
+	for (int64_t i = t; i < n; i += nt) {
+		if (i == 0) {
+			key[f] = e.kmin;
+			val[f] = vmin;
+		} else if (i == n - 1) {
+			key[l - 1] = e.kmax;
+			val[l - 1] = vmax;
+		} else {
+			key[f + i] = __longlong_as_double((long long)sl.sk[a + i - 1]);
+			val[f + i] = (int32_t)sl.sv[a + i - 1];
+		}
+	}
+}
+
+// one warp: true when [f, l) had distinct keys and has been written
+__device__ bool warp_finish_distinct(const SortedLevel& sl, double* key, int32_t* val, int64_t f, int64_t l) {
+	const int lane = threadIdx.x & 31;
+	SegExtremes e;
+	extremes_init(e);
+	for (int64_t i = f + lane; i < l; i += 32) extremes_point(e, key[i], i);
+	extremes_warp(e);
+	int64_t a = 0;
+	const bool ok = distinct_segment(sl, f, l, e, &a);  // same values on every lane
+	if (!ok) return false;
+	const int32_t vmin = val[e.imin], vmax = val[e.imax];
+	__syncwarp();
+	write_distinct(sl, key, val, f, l, e, a, vmin, vmax, lane, 32);
+	__syncwarp();
+	return true;
+}
+
+// one CTA of kBigThreads: the same
+__device__ bool block_finish_distinct(const SortedLevel& sl, double* key, int32_t* val, int64_t f, int64_t l) {
+	__shared__ SegExtremes part[kBigWarps];
+	__shared__ int verdict;
+	__shared__ int64_t sa;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	SegExtremes e;
+	extremes_init(e);
+	for (int64_t i = f + tid; i < l; i += kBigThreads) extremes_point(e, key[i], i);
+	extremes_warp(e);
+	if (lane == 0) part[warp] = e;
+	__syncthreads();
+	if (tid == 0) {
+		SegExtremes all = part[0];
+		for (int w = 1; w < kBigWarps; w++) extremes_merge(all, part[w]);
+		int64_t a = 0;
+		verdict = distinct_segment(sl, f, l, all, &a) ? 1 : 0;
+		sa = a;
+		part[0] = all;
+	}
+	__syncthreads();
+	if (!verdict) return false;
+	const SegExtremes all = part[0];
+	const int64_t a = sa;
+	const int32_t vmin = val[all.imin], vmax = val[all.imax];
+	__syncthreads();
+	write_distinct(sl, key, val, f, l, all, a, vmin, vmax, tid, kBigThreads);
+	__syncthreads();
+	return true;
+}
+
 __global__ void __launch_bounds__(kBigThreads) seg_cta_kernel(const Seg* __restrict__ segs, double* key, int32_t* val, SortScratch sc,
-                                                             SampleStats* st) {
+                                                             SampleStats* st, SortedLevel sl) {
 	const Seg g = segs[blockIdx.x];
+	if (sl.sk && block_finish_distinct(sl, key, val, g.f, g.l)) return;
 	block_std_sort(key + g.f, val + g.f, g.l - g.f, sc.SL + g.f, sc.SR + g.f, sc.blk + 2 * g.f, st, g.d);
 }
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) seg_warp_kernel(const Seg* __restrict__ segs, int n, double* key, int32_t* val,
-                                                                      SortScratch sc, SampleStats* st, int* next_seg) {
+                                                                      SortScratch sc, SampleStats* st, int* next_seg, SortedLevel sl) {
 	__shared__ Seg stacks[kWarpsPerBlock][kStackDepth];
 	__shared__ int nblk[kWarpsPerBlock];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -654,6 +798,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) seg_warp_kernel(const Seg
 		if (idx >= n) break;
 		const Seg g = segs[idx];
 		const int64_t len = g.l - g.f;
+		if (sl.sk && warp_finish_distinct(sl, key, val, g.f, g.l)) continue;
 		if (lane == 0) nblk[warp] = 0;
 		__syncwarp();
 		warp_introsort(key + g.f, val + g.f, 0, len, g.d, sc.SL + g.f, sc.SR + g.f, sc.blk + 2 * g.f, &nblk[warp], stacks[warp], st);
@@ -715,8 +860,10 @@ void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, Level
 	mem.free(sc.blk);
 }
 
-void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<SortSeg>& segs, SampleStats* st, DeviceMem& mem) {
+void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<SortSeg>& segs, SampleStats* st, DeviceMem& mem,
+                     const SortedLevel* sorted) {
 	if (segs.empty() || M == 0) return;
+	const SortedLevel sl = sorted ? *sorted : SortedLevel{};
 	cudaStream_t s = mem.stream();
 	SortScratch sc;
 	sc.SL = mem.alloc<int32_t>(M);
@@ -824,7 +971,7 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 	PCG_CUDA(cudaStreamSynchronize(s));
 	if (h_counts[1] > L.cap_seg || h_counts[2] > L.cap_seg || h_counts[3] > L.cap_blk) throw PcgError(5, "sort replay: list overflow");
 	if (h_counts[1] > 0) {
-		seg_cta_kernel<<<h_counts[1], kBigThreads, 0, s>>>(L.cta, key, val, sc, st);
+		seg_cta_kernel<<<h_counts[1], kBigThreads, 0, s>>>(L.cta, key, val, sc, st, sl);
 		PCG_LAUNCHED();
 	}
 	if (h_counts[2] > 0) {
@@ -832,7 +979,7 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 		int blocks = (int)ceil_div(h_counts[2], kWarpsPerBlock);
 		const int cap = sm_count() * 16;
 		if (blocks > cap) blocks = cap;
-		seg_warp_kernel<<<blocks, kWarpsPerBlock * 32, 0, s>>>(L.warp, h_counts[2], key, val, sc, st, counters + 4);
+		seg_warp_kernel<<<blocks, kWarpsPerBlock * 32, 0, s>>>(L.warp, h_counts[2], key, val, sc, st, counters + 4, sl);
 		PCG_LAUNCHED();
 	}
 	if (h_counts[3] > 0) {
@@ -862,9 +1009,9 @@ void launch_node_pos(const LevelNode* nodes, const std::vector<uint8_t>& pick, L
 
 int sort_depth_budget(int64_t n) { return host_introsort_depth(n); }
 
-void launch_sort_keys_single(double* keys, int32_t* vals, int64_t n, DeviceMem& mem, SampleStats* st) {
+void launch_sort_keys_single(double* keys, int32_t* vals, int64_t n, DeviceMem& mem, SampleStats* st, const SortedLevel* sorted) {
 	if (n <= 0) return;
-	replay_segments(keys, vals, n, {SortSeg{0, n, host_introsort_depth(n), 0}}, st, mem);
+	replay_segments(keys, vals, n, {SortSeg{0, n, host_introsort_depth(n), 0}}, st, mem, sorted);
 }
 
 }  // namespace pcg

@@ -933,10 +933,15 @@ struct Converter {
 	// ------------------------------------------------ conversion in parts
 	// Device bytes one point of a part needs beside its record (positions,
 	// ids, the level buffers of the sampler, sort and conflict-list scratch;
-	// calibrated against pcg_stats.device_peak_bytes), and the tile of the
+	// the request loop's figure, calibrated against pcg_stats.device_peak_bytes,
+	// plus headroom for the power-of-two tables of the very large levels a
+	// part of hundreds of millions of points has), and the tile of the
 	// streamed passes.
-	static constexpr int64_t kPartBytesPerPoint = kJobBytesPerPoint;
+	static constexpr int64_t kPartBytesPerPoint = kJobBytesPerPoint + 80;
 	static constexpr int64_t kTilePoints = int64_t(1) << 24;
+	// largest part an automatic plan makes: parts of this size keep the GPU
+	// busy, and smaller level buffers fragment the device memory less
+	static constexpr int64_t kMaxPartPoints = 100'000'000;
 	int records_mode = PCG_RECORDS_AUTO;  // pcg_records
 	int64_t group_points = 0;             // pcg_opts.group_points
 
@@ -951,11 +956,15 @@ struct Converter {
 		int64_t gp = group_points;
 		if (gp <= 0) {
 			if (N < (int64_t(1) << 31) && rec_bytes + N * kPartBytesPerPoint <= avail) return 0;
-			const int64_t gp_res = (avail - rec_bytes) / kPartBytesPerPoint;
-			const int64_t gp_str = (avail - stream_bytes) / kPartBytesPerPoint;
+			// per point of a part: its working set, and its piece of
+			// octree.bin, which stays on the device until the next part has
+			// run (the copy to the host overlaps it)
+			const int64_t per_point = kPartBytesPerPoint + rec_len;
+			const int64_t gp_res = (avail - rec_bytes) / per_point;
+			const int64_t gp_str = (avail - stream_bytes) / per_point;
 			// resident records when they leave room for parts of a few chunks
 			const bool res_ok = records_mode != PCG_RECORDS_STREAMED && gp_res >= 40'000'000;
-			gp = std::min<int64_t>(res_ok ? gp_res : gp_str, (int64_t(1) << 31) - 1);
+			gp = std::min<int64_t>(res_ok ? gp_res : gp_str, kMaxPartPoints);
 			if (gp < 10'000'000) throw PcgError(PCG_OOM, "not enough device memory for one chunk of the cloud");
 			resident = records_mode == PCG_RECORDS_RESIDENT || (records_mode == PCG_RECORDS_AUTO && res_ok);
 			return gp;
@@ -1611,7 +1620,7 @@ struct Converter {
 		lb.rec = method == PCG_RANDOM ? nullptr : mem.alloc<int4>(M);
 		LevelNode* d_nodes = upload(ln, mem);
 		GatherItem* d_items = upload(items, mem);
-		launch_gather(d_items, (int)items.size(), lb, mem);
+		launch_gather(items, d_items, lb, mem);
 		// node order for the warp-per-node kernels: largest first
 		std::vector<int32_t> order(K);
 		for (int k = 0; k < K; k++) order[k] = k;
@@ -1657,7 +1666,8 @@ struct Converter {
 				// distinct keys: one exact radix sort of the level; equal keys:
 				// the introsort replay, for those nodes only
 				std::vector<uint8_t> tie;
-				sort_level_distinct(d_nodes, ln, lb, mem, tie);
+				SortedLevel sorted;
+				sort_level_distinct(d_nodes, ln, lb, mem, tie, &sorted);
 				std::vector<int32_t> tie_nodes;
 				std::vector<SortSeg> tie_segs;
 				for (int k = 0; k < K; k++) {
@@ -1668,9 +1678,10 @@ struct Converter {
 				}
 				res.stats.replayed_nodes += (int64_t)tie_nodes.size();
 				if (!tie_nodes.empty()) {
-					replay_segments(lb.keys, lb.perm, M, tie_segs, d_st, mem);
+					replay_segments(lb.keys, lb.perm, M, tie_segs, d_st, mem, &sorted);
 					launch_node_pos(d_nodes, tie, lb, mem);
 				}
+				free_sorted_level(sorted, mem);
 				launch_cand_records(d_nodes, co.X, co.Y, co.Z, lb, mem);
 				PCG_CUDA(cudaEventRecord(ev[1], s));
 				// conflict lists for every node; a node where some candidate has
@@ -2275,7 +2286,26 @@ pcg_status pcg_kernel_sort_keys(pcg_ctx* ctx, const double* keys, int64_t n, int
 		std::vector<int32_t> iota(n);
 		for (int64_t i = 0; i < n; i++) iota[i] = (int32_t)i;
 		PCG_CUDA(cudaMemcpyAsync(dv, iota.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, mem.stream()));
-		pcg::launch_sort_keys_single(dk, dv, n, mem, st);
+		// keys >= +0 (the samplers' squared distances): the replay finishes
+		// the partitions whose keys are distinct from their radix order
+		bool nonneg = true;
+		for (int64_t i = 0; i < n && nonneg; i++) nonneg = keys[i] >= 0.0 && !std::signbit(keys[i]);
+		pcg::SortedLevel sorted;
+		int32_t* d_node_of = nullptr;
+		pcg::LevelNode* d_one = nullptr;
+		if (nonneg) {
+			std::vector<pcg::LevelNode> one(1);
+			one[0].cand_off = 0;
+			one[0].count = n;
+			d_one = pcg::upload(one, mem);
+			d_node_of = mem.alloc<int32_t>(n);
+			PCG_CUDA(cudaMemsetAsync(d_node_of, 0, n * sizeof(int32_t), mem.stream()));
+			pcg::build_sorted_level(d_one, one, d_node_of, reinterpret_cast<const uint64_t*>(dk), n, sorted, mem);
+		}
+		pcg::launch_sort_keys_single(dk, dv, n, mem, st, nonneg ? &sorted : nullptr);
+		pcg::free_sorted_level(sorted, mem);
+		if (d_node_of) mem.free(d_node_of);
+		if (d_one) mem.free(d_one);
 		PCG_CUDA(cudaMemcpyAsync(perm_out, dv, n * sizeof(int32_t), cudaMemcpyDeviceToHost, mem.stream()));
 		PCG_CUDA(cudaStreamSynchronize(mem.stream()));
 	});

@@ -44,9 +44,14 @@ namespace {
 constexpr uint64_t EMPTY_KEY = ~0ull;
 
 // ---------------------------------------------------------------- gather
-__global__ void gather_kernel(const GatherItem* __restrict__ items, LevelBuffers lb) {
-	const GatherItem it = items[blockIdx.x];
-	for (int64_t t = threadIdx.x; t < it.count; t += blockDim.x) {
+// one CTA per piece of kGatherPiece ids of an item (piece_item / piece_start
+// give the item and the piece's first id in it)
+__global__ void gather_kernel(const GatherItem* __restrict__ items, const int32_t* __restrict__ piece_item,
+                              const int64_t* __restrict__ piece_start, LevelBuffers lb) {
+	const GatherItem it = items[piece_item[blockIdx.x]];
+	const int64_t t0 = piece_start[blockIdx.x];
+	const int64_t t1 = t0 + kGatherPiece < it.count ? t0 + kGatherPiece : it.count;
+	for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
 		int64_t j = it.dst_off + t;
 		lb.ids[j] = it.src_ids[t];
 		if (lb.cols) lb.cols[j] = it.src_cols ? it.src_cols[t] : 0ull;
@@ -1560,10 +1565,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) greedy_list_warp_kernel(c
 }  // namespace
 
 // ----------------------------------------------------------------- launchers
-void launch_gather(const GatherItem* items, int num_items, LevelBuffers& lb, DeviceMem& mem) {
-	if (num_items == 0) return;
-	gather_kernel<<<num_items, 256, 0, mem.stream()>>>(items, lb);
+void launch_gather(const std::vector<GatherItem>& h_items, const GatherItem* items, LevelBuffers& lb, DeviceMem& mem) {
+	std::vector<int32_t> pi;
+	std::vector<int64_t> ps;
+	for (size_t k = 0; k < h_items.size(); k++)
+		for (int64_t t = 0; t < h_items[k].count; t += kGatherPiece) {
+			pi.push_back((int32_t)k);
+			ps.push_back(t);
+		}
+	if (pi.empty()) return;
+	int32_t* d_pi = mem.alloc<int32_t>(pi.size());
+	int64_t* d_ps = mem.alloc<int64_t>(ps.size());
+	PCG_CUDA(cudaMemcpyAsync(d_pi, pi.data(), pi.size() * sizeof(int32_t), cudaMemcpyHostToDevice, mem.stream()));
+	PCG_CUDA(cudaMemcpyAsync(d_ps, ps.data(), ps.size() * sizeof(int64_t), cudaMemcpyHostToDevice, mem.stream()));
+	gather_kernel<<<(unsigned)pi.size(), 256, 0, mem.stream()>>>(items, d_pi, d_ps, lb);
 	PCG_LAUNCHED();
+	mem.free(d_ps);
+	mem.free(d_pi);
 }
 
 void launch_keys(const LevelNode* nodes, const PosParamsS& pp, LevelBuffers& lb, DeviceMem& mem) {

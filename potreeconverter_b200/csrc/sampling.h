@@ -1,6 +1,8 @@
 // Sampler kernels (one octree level across all its nodes per launch).
 #pragma once
 
+#include <vector>
+
 #include "dev.h"
 
 namespace pcg {
@@ -25,6 +27,9 @@ struct GatherItem {         // copy `count` ids (and colours, records) of one ch
 	int32_t child;
 	int32_t node;
 };
+// the gather launch takes the items cut into pieces of at most this many
+// ids, one CTA each, so a large child buffer does not keep one CTA busy
+constexpr int64_t kGatherPiece = 4096;
 
 struct LevelBuffers {
 	int64_t M = 0;                 // candidates at this level
@@ -65,7 +70,7 @@ struct SampleStats {
 	unsigned long long cycles[7];  // CTA greedy: SM cycles of thread 0 in phases A, B, C1, C2, D; cells read past 3 and 7 points
 };
 
-void launch_gather(const GatherItem* items, int num_items, LevelBuffers& lb, DeviceMem& mem);
+void launch_gather(const std::vector<GatherItem>& h_items, const GatherItem* items, LevelBuffers& lb, DeviceMem& mem);
 // keys from the gathered records lb.rec
 void launch_keys(const LevelNode* nodes, const PosParamsS& pp, LevelBuffers& lb, DeviceMem& mem);
 // records (X, Y, Z, -) of ids[0..n)
@@ -100,11 +105,36 @@ void launch_node_sort(const LevelNode* nodes, const int32_t* order, int K, Level
 // keys_in must not alias keys_out.
 void segmented_sort_pairs(const std::vector<LevelNode>& ln, int64_t M, const uint64_t* keys_in, const uint32_t* vals_in,
                           uint64_t* keys_out, uint32_t* vals_out, int begin_bit, int end_bit, DeviceMem& mem);
+// The radix-sorted keys of a level, kept for the replay of the nodes with
+// equal keys. A segment of the replay whose keys are pairwise distinct ends
+// in ascending order whatever its partitions do (the unique sorted order of
+// its elements), so the replay writes it from here instead of partitioning
+// it further: its smallest and largest element (which may equal keys
+// outside the segment) at the ends, between them the sorted elements whose
+// keys lie strictly between those two -- exactly the segment's other
+// elements, since a partition keeps every key strictly between its pivots
+// on one side.
+struct SortedLevel {
+	const uint64_t* sk = nullptr;     // [M] key bits, ascending within each node
+	const uint32_t* sv = nullptr;     // [M] candidate index in its node
+	const int32_t* ties = nullptr;    // [M] adjacent equal keys within the node up to each position (inclusive count)
+	const int32_t* node_of = nullptr; // [M] node of each level position
+	const LevelNode* nodes = nullptr;
+	void* owned[3] = {nullptr, nullptr, nullptr};
+};
+// keep != nullptr: when some node has equal keys, the sorted keys stay
+// allocated in *keep for the replay (release with free_sorted_level)
 void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, LevelBuffers& lb, DeviceMem& mem,
-                         std::vector<uint8_t>& tie);
+                         std::vector<uint8_t>& tie, SortedLevel* keep = nullptr);
+void free_sorted_level(SortedLevel& keep, DeviceMem& mem);
+// the same for keys >= +0 (bit patterns) of nodes `ln`, sorted on all 64 bits
+void build_sorted_level(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, const int32_t* node_of, const uint64_t* keys, int64_t M,
+                        SortedLevel& out, DeviceMem& mem);
 // std::sort replayed on every segment [f, l) of key/val independently, each
-// with depth budget d (2 * floor(log2(l - f)) for a whole node).
-void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<SortSeg>& segs, SampleStats* st, DeviceMem& mem);
+// with depth budget d (2 * floor(log2(l - f)) for a whole node). With
+// `sorted`, segments whose keys are pairwise distinct are written from it.
+void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<SortSeg>& segs, SampleStats* st, DeviceMem& mem,
+                     const SortedLevel* sorted = nullptr);
 int sort_depth_budget(int64_t n);
 // lb.pos of the nodes k with pick[k] != 0, from their sorted lb.perm
 void launch_node_pos(const LevelNode* nodes, const std::vector<uint8_t>& pick, LevelBuffers& lb, DeviceMem& mem);
@@ -175,7 +205,7 @@ void launch_random_accept_sized(const LevelNode* nodes, const int32_t* X, const 
 void launch_shuffle_leaves(const int64_t* leaf_off, const int64_t* leaf_cnt, int num_leaves, const uint32_t* ids_in,
                            uint32_t* ids_out, int32_t* scratch, uint32_t seed, DeviceMem& mem);
 // stand-alone entry points for the parity tests
-void launch_sort_keys_single(double* keys, int32_t* vals, int64_t n, DeviceMem& mem, SampleStats* st);
+void launch_sort_keys_single(double* keys, int32_t* vals, int64_t n, DeviceMem& mem, SampleStats* st, const SortedLevel* sorted = nullptr);
 void launch_shuffle_single(int64_t n, uint32_t seed, int32_t* perm, DeviceMem& mem);
 
 }  // namespace pcg

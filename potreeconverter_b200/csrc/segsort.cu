@@ -270,8 +270,61 @@ void segmented_sort_pairs(const std::vector<LevelNode>& ln, int64_t M, const uin
 	mem.free(d_tiles);
 }
 
+namespace {
+
+// ties[j]: adjacent equal keys of j's node up to j (inclusive prefix of
+// "sk[j] equals its predecessor in the node")
+__global__ void seg_tie_flags_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ node_of, const uint64_t* __restrict__ sk,
+                                     int64_t M, uint32_t* __restrict__ flags) {
+	const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= M) return;
+	flags[t] = t > nodes[node_of[t]].cand_off && sk[t] == sk[t - 1] ? 1u : 0u;
+}
+
+__global__ void seg_inclusive_kernel(const uint32_t* __restrict__ flags, const uint32_t* __restrict__ excl, int64_t M, int32_t* __restrict__ incl) {
+	const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t < M) incl[t] = (int32_t)(excl[t] + flags[t]);
+}
+
+}  // namespace
+
+void build_sorted_level(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, const int32_t* node_of, const uint64_t* keys, int64_t M,
+                        SortedLevel& out, DeviceMem& mem) {
+	out = SortedLevel{};
+	if (M == 0) return;
+	cudaStream_t s = mem.stream();
+	uint64_t* sk = mem.alloc<uint64_t>(M);
+	uint32_t* sv = mem.alloc<uint32_t>(M);
+	segmented_sort_pairs(ln, M, keys, nullptr, sk, sv, 0, 64, mem);
+	const unsigned blocks = (unsigned)ceil_div(M, 256);
+	uint32_t* f = mem.alloc<uint32_t>(M);
+	uint32_t* ex = mem.alloc<uint32_t>(M);
+	int32_t* ties = mem.alloc<int32_t>(M);
+	seg_tie_flags_kernel<<<blocks, 256, 0, s>>>(d_nodes, node_of, sk, M, f);
+	PCG_LAUNCHED();
+	exclusive_scan_u32(f, ex, M, false, mem);
+	seg_inclusive_kernel<<<blocks, 256, 0, s>>>(f, ex, M, ties);
+	PCG_LAUNCHED();
+	mem.free(ex);
+	mem.free(f);
+	out.sk = sk;
+	out.sv = sv;
+	out.ties = ties;
+	out.node_of = node_of;
+	out.nodes = d_nodes;
+	out.owned[0] = sk;
+	out.owned[1] = sv;
+	out.owned[2] = ties;
+}
+
+void free_sorted_level(SortedLevel& keep, DeviceMem& mem) {
+	for (void*& p : keep.owned)
+		if (p) { mem.free(p); p = nullptr; }
+	keep = SortedLevel{};
+}
+
 void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>& ln, LevelBuffers& lb, DeviceMem& mem,
-                         std::vector<uint8_t>& tie) {
+                         std::vector<uint8_t>& tie, SortedLevel* keep) {
 	const int K = (int)ln.size();
 	const int64_t M = lb.M;
 	tie.assign(K, 0);
@@ -304,6 +357,30 @@ void sort_level_distinct(const LevelNode* d_nodes, const std::vector<LevelNode>&
 	PCG_CUDA(cudaMemcpyAsync(tie.data(), d_flags, K, cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));
 	mem.free(d_flags);
+	bool any_tie = false;
+	for (uint8_t t : tie) any_tie |= t != 0;
+	if (keep && any_tie) {
+		uint32_t* f = mem.alloc<uint32_t>(M);
+		uint32_t* ex = mem.alloc<uint32_t>(M);
+		int32_t* ties = mem.alloc<int32_t>(M);
+		seg_tie_flags_kernel<<<blocks, 256, 0, s>>>(d_nodes, lb.node_of, sk, M, f);
+		PCG_LAUNCHED();
+		exclusive_scan_u32(f, ex, M, false, mem);
+		seg_inclusive_kernel<<<blocks, 256, 0, s>>>(f, ex, M, ties);
+		PCG_LAUNCHED();
+		mem.free(ex);
+		mem.free(f);
+		*keep = SortedLevel{};
+		keep->sk = sk;
+		keep->sv = sv;
+		keep->ties = ties;
+		keep->node_of = lb.node_of;
+		keep->nodes = d_nodes;
+		keep->owned[0] = sk;
+		keep->owned[1] = sv;
+		keep->owned[2] = ties;
+		return;
+	}
 	mem.free(sk);
 	mem.free(sv);
 }
