@@ -62,7 +62,7 @@ REF_SAMPLE_POINTS = 2_000_000
 GOLDEN = os.path.join(REPO, "tests", "golden", "golden.json")
 # DRAM bytes (read + write) per candidate of the acceptance kernel, from the
 # ncu capture summarised in profiles/accept_hotspots-5M_poisson.md
-ACCEPT_DRAM_BYTES_PER_CANDIDATE = 225.6
+ACCEPT_DRAM_BYTES_PER_CANDIDATE = 36.9
 MEASURED_PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
 
 

@@ -39,6 +39,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "devutil.cuh"
 #include "sampling.h"
@@ -48,6 +49,7 @@ namespace pcg {
 namespace {
 
 constexpr uint64_t kEmptyRun = ~0ull;
+constexpr int kListsVariant = 2;  // see lists_variant(); measured fastest on the benchmark's 50M cloud
 constexpr int kCellsPerAxis = 128;  // node box = 128 spacings
 
 struct alignas(16) RunSlot {  // run table entry, one 16-byte load per probe
@@ -170,11 +172,12 @@ __device__ __forceinline__ int2 find_run(const RunSlot* table, int64_t cap, uint
 	return make_int2(0, 0);
 }
 
-// The search waits on dependent loads (bitmap row, run table, runs): five
-// resident blocks of 256 threads per SM (48 registers) hide more of it than
-// four would.
-template <int MODE>
-__global__ void __launch_bounds__(256, 5) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, PosParamsS pp,
+// The search waits on dependent loads (bitmap row, run table, runs) and is
+// near its issue limit: MINB resident blocks of 256 threads per SM (5: 48
+// registers, 4: 64), GAPS skips the neighbour cells beyond the band. The
+// variant is chosen by lists_variant() (measured; PCG_LISTS overrides).
+template <int MODE, int MINB, bool GAPS>
+__global__ void __launch_bounds__(256, MINB) conf_lists_kernel(const LevelNode* __restrict__ nodes, const uint8_t* __restrict__ use, PosParamsS pp,
                                                         LevelBuffers lb, const uint64_t* __restrict__ ck, const int4* __restrict__ crec,
                                                         const float4* __restrict__ crf, const RunSlot* __restrict__ table,
                                                         const int64_t* __restrict__ tab_off, const int64_t* __restrict__ tab_cap,
@@ -225,7 +228,7 @@ __global__ void __launch_bounds__(256, 5) conf_lists_kernel(const LevelNode* __r
 	const float cs = (float)(sp * 1.000001);
 	auto gap2 = [&](int d, float v, int c) {
 		const float g = d < 0 ? v - (float)c * cs : (float)(c + 1) * cs - v;
-		return pre32 && d != 0 && g > 0.f ? g * g : 0.f;
+		return GAPS && pre32 && d != 0 && g > 0.f ? g * g : 0.f;
 	};
 #pragma unroll 1
 	for (int dz = -1; dz <= 1; dz++) {
@@ -311,6 +314,16 @@ __global__ void __launch_bounds__(256, 5) conf_lists_kernel(const LevelNode* __r
 		atomicAdd(&st->list_entries, (unsigned long long)sum);
 		if (esc) atomicAdd(&st->escalated, (unsigned long long)esc);
 	}
+}
+
+// 0: five blocks per SM with the cell skip, 1: four blocks with it, 2: five
+// blocks without it; PCG_LISTS=<n> overrides the measured default
+int lists_variant() {
+	static const int v = [] {
+		const char* e = std::getenv("PCG_LISTS");
+		return e ? std::atoi(e) : kListsVariant;
+	}();
+	return v;
 }
 
 // st += the list build's own counters
@@ -416,8 +429,19 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 		PCG_CUDA(cudaMemsetAsync(cl.pool_used, 0, sizeof(unsigned long long), s));
 		PCG_CUDA(cudaMemsetAsync(cl.node_dense, 0, K, s));
 		PCG_CUDA(cudaMemsetAsync(lst, 0, sizeof(SampleStats), s));
-		if (mode == 0) conf_lists_kernel<0><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, tab_off, tab_cap, d_bm_off, bm, cl, lst);
-		else conf_lists_kernel<1><<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, tab_off, tab_cap, d_bm_off, bm, cl, lst);
+		auto run = [&](auto kernel) {
+			kernel<<<blocks, 256, 0, s>>>(d_nodes, d_use, pp, lb, ck, crec, crf, table, tab_off, tab_cap, d_bm_off, bm, cl, lst);
+		};
+		const int v = lists_variant();
+		if (mode == 0) {
+			if (v == 1) run(conf_lists_kernel<0, 4, true>);
+			else if (v == 2) run(conf_lists_kernel<0, 5, false>);
+			else run(conf_lists_kernel<0, 5, true>);
+		} else {
+			if (v == 1) run(conf_lists_kernel<1, 4, true>);
+			else if (v == 2) run(conf_lists_kernel<1, 5, false>);
+			else run(conf_lists_kernel<1, 5, true>);
+		}
 		PCG_LAUNCHED();
 		unsigned long long used = 0;
 		PCG_CUDA(cudaMemcpyAsync(&used, cl.pool_used, sizeof(used), cudaMemcpyDeviceToHost, s));

@@ -59,27 +59,29 @@ public:
 	explicit DeviceArena(cudaStream_t s) : stream_(s) {}
 	~DeviceArena() {
 		release_all();
-		if (side_) {
-			cudaStreamSynchronize(side_);
-			cudaStreamDestroy(side_);
-			cudaEventDestroy(fork_);
-			cudaEventDestroy(join_);
+		for (int k = 0; k < kSides; k++) {
+			if (!side_[k]) continue;
+			cudaStreamSynchronize(side_[k]);
+			cudaStreamDestroy(side_[k]);
+			cudaEventDestroy(fork_[k]);
+			cudaEventDestroy(join_[k]);
 		}
 	}
 
-	// A second stream for work that runs beside the arena's stream, with the
-	// events that fork it from and join it back to the arena's stream;
-	// created once (stream creation can stall the host).
-	cudaStream_t side_stream(cudaEvent_t& fork, cudaEvent_t& join) {
-		if (!side_) {
-			cudaError_t e = cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking);
-			if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming);
-			if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join_, cudaEventDisableTiming);
+	// Streams for work that runs beside the arena's stream (k < kSides), with
+	// the events that fork each from and join it back to the arena's
+	// stream; created once (stream creation can stall the host).
+	static constexpr int kSides = 2;
+	cudaStream_t side_stream(cudaEvent_t& fork, cudaEvent_t& join, int k = 0) {
+		if (!side_[k]) {
+			cudaError_t e = cudaStreamCreateWithFlags(&side_[k], cudaStreamNonBlocking);
+			if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork_[k], cudaEventDisableTiming);
+			if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join_[k], cudaEventDisableTiming);
 			if (e != cudaSuccess) throw CudaError(e, std::string("side stream: ") + cudaGetErrorString(e));
 		}
-		fork = fork_;
-		join = join_;
-		return side_;
+		fork = fork_[k];
+		join = join_[k];
+		return side_[k];
 	}
 	DeviceArena(const DeviceArena&) = delete;
 	DeviceArena& operator=(const DeviceArena&) = delete;
@@ -198,8 +200,8 @@ private:
 	}
 
 	cudaStream_t stream_;
-	cudaStream_t side_ = nullptr;
-	cudaEvent_t fork_ = nullptr, join_ = nullptr;
+	cudaStream_t side_[kSides] = {nullptr, nullptr};
+	cudaEvent_t fork_[kSides] = {nullptr, nullptr}, join_[kSides] = {nullptr, nullptr};
 	std::vector<Chunk> chunks_;
 	std::unordered_map<void*, std::pair<size_t, size_t>> live_;  // range -> (chunk, length)
 	size_t live_bytes_ = 0, peak_bytes_ = 0;

@@ -1193,19 +1193,26 @@ __global__ void __launch_bounds__(kListThreads) greedy_list_kernel(const LevelNo
 }
 
 
-// Greedy acceptance for the largest nodes on a cluster of kClusterCtas CTAs
-// (4 x 1024 threads): a super-round decides 4096 candidates, CTA k holding
-// candidates [1024k, 1024k + 1024) of it. Each CTA keeps its candidates'
-// states in its own shared memory; a candidate's conflicts inside the
-// super-round (always with lower indices) are read from the owning CTA's
-// shared memory through the cluster's distributed shared memory. Passes,
-// the in-order warp (CTA 0, warp 0, reading and writing all four CTAs'
-// states) and the rank prefix are separated by cluster barriers, which
-// every CTA reaches the same number of times.
+// Greedy acceptance for the largest nodes on a cluster of CS CTAs (CS x
+// 1024 threads, CS = 4, or 8 for the few largest nodes of a level): a
+// super-round decides CS x 1024 candidates, CTA k holding candidates
+// [1024k, 1024k + 1024) of it. Each CTA keeps its candidates' states in its
+// own shared memory; a candidate's conflicts inside the super-round (always
+// with lower indices) are read from the owning CTA's shared memory through
+// the cluster's distributed shared memory. Passes, the in-order warp (CTA
+// 0, warp 0, reading and writing all CTAs' states) and the rank prefix are
+// separated by cluster barriers, which every CTA reaches the same number of
+// times. A node's serial chain of super-rounds sets a level's acceptance
+// time, so its largest nodes take the wider cluster: half the super-rounds.
 constexpr int kClusterCtas = 4;
-constexpr int kSuper = kListRound * kClusterCtas;  // 4096
+constexpr int kWideClusterCtas = 8;  // portable maximum cluster size
 constexpr int64_t kClusterMinCandidates = 65536;  // smallest cluster node the shared-memory layout is sized for
-static_assert(kSuper <= 32767, "conflict indices are int16");
+static_assert(kListRound * kWideClusterCtas <= 32767, "conflict indices are int16");
+// A level's cluster nodes take 8-CTA clusters only when there are at most
+// this many of them (the top levels): an 8-CTA cluster needs eight free SMs
+// of one GPC at once, and beside many other nodes' CTAs it waits for them
+// (measured: the 50M cloud's levels 3-5 lost 2-4x).
+constexpr int kMaxWideClusterNodes = 4;
 
 struct ClusterRound {
 	int32_t maxrank[kListRound];
@@ -1220,10 +1227,11 @@ struct ClusterRound {
 	int32_t total;               // accepted in this CTA's part of the super-round
 };
 
-template <int MODE>
-__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThreads, 1)
+template <int MODE, int CS>
+__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(kListThreads, 1)
     greedy_list_cluster_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ order, PosParamsS pp, LevelBuffers lb,
                                GreedyArgs ga, ConflictLists cl, int32_t* __restrict__ srank, SampleStats* st) {
+	constexpr int kSuper = kListRound * CS;
 	namespace cgr = cooperative_groups;
 	cgr::cluster_group cluster = cgr::this_cluster();
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1232,7 +1240,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 	const int crank = (int)cluster.block_rank();
 	// another CTA's round state (distributed shared memory)
 	auto peer = [&](int r) { return cluster.map_shared_rank(&R, r); };
-	const LevelNode nd = nodes[order[blockIdx.x / kClusterCtas]];
+	const LevelNode nd = nodes[order[blockIdx.x / CS]];
 	const int64_t n = nd.count, co = nd.cand_off;
 	uint64_t* hk = ga.hkeys + nd.hash_off;
 	int32_t* hh = ga.hheads + nd.hash_off;
@@ -1333,7 +1341,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 			cluster.sync();
 			int all = 0;
 #pragma unroll
-			for (int r = 0; r < kClusterCtas; r++) all |= *(volatile int32_t*)&peer(r)->changed[gpass & 1];
+			for (int r = 0; r < CS; r++) all |= *(volatile int32_t*)&peer(r)->changed[gpass & 1];
 			if (!all) break;
 		}
 		if (tid == 0 && crank == 0) atomicAdd(&st->passes, (unsigned long long)passes);
@@ -1342,7 +1350,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 		cluster.sync();
 		int left = 0;
 #pragma unroll
-		for (int r = 0; r < kClusterCtas; r++) left |= *(volatile int32_t*)&peer(r)->left;
+		for (int r = 0; r < CS; r++) left |= *(volatile int32_t*)&peer(r)->left;
 		if (crank == 0 && tid == 0) {
 			atomicAdd(&st->rounds, 1ull);
 			if (left) atomicAdd(&st->serial, 1ull);
@@ -1401,7 +1409,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kListThre
 		cluster.sync();
 		int32_t before = 0, all_acc = 0;
 #pragma unroll
-		for (int r = 0; r < kClusterCtas; r++) {
+		for (int r = 0; r < CS; r++) {
 			const int32_t tr = *(volatile int32_t*)&peer(r)->total;
 			if (r < crank) before += tr;
 			all_acc += tr;
@@ -1684,46 +1692,54 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 	cudaStream_t s = mem.stream();
 	// the largest nodes (cta_nodes is largest first) on a cluster each, the
 	// other CTA nodes on one CTA, the rest on a warp
-	std::vector<int32_t> clu, one;
+	std::vector<int32_t> wide, clu, one;
 	const int64_t cluster_min = std::max(level_schedule().cluster_min, kClusterMinCandidates);
 	for (int32_t k : cta_nodes) (ln[k].count >= cluster_min ? clu : one).push_back(k);
+	if (!clu.empty() && (int)clu.size() <= kMaxWideClusterNodes) wide.swap(clu);
 	int32_t* srank = mem.alloc<int32_t>((size_t)lb.M);
+	int32_t* d_wide = wide.empty() ? nullptr : mem.alloc<int32_t>(wide.size());
 	int32_t* d_clu = clu.empty() ? nullptr : mem.alloc<int32_t>(clu.size());
 	int32_t* d_one = one.empty() ? nullptr : mem.alloc<int32_t>(one.size());
 	int32_t* d_warp = warp_nodes.empty() ? nullptr : mem.alloc<int32_t>(warp_nodes.size());
 	int* counter = mem.alloc<int>(1);
+	if (d_wide) PCG_CUDA(cudaMemcpyAsync(d_wide, wide.data(), wide.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 	if (d_clu) PCG_CUDA(cudaMemcpyAsync(d_clu, clu.data(), clu.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 	if (d_one) PCG_CUDA(cudaMemcpyAsync(d_one, one.data(), one.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 	if (d_warp) PCG_CUDA(cudaMemcpyAsync(d_warp, warp_nodes.data(), warp_nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
 	PCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), s));
-	// the node sets are independent: the smaller ones run beside the
-	// largest on a forked stream
-	cudaStream_t side = nullptr;
-	cudaEvent_t fork = nullptr, join = nullptr;
-	const int sets = (d_clu ? 1 : 0) + (d_one ? 1 : 0) + (d_warp ? 1 : 0);
-	if (sets > 1 && mem.arena()) {
-		side = mem.arena()->side_stream(fork, join);
-		PCG_CUDA(cudaEventRecord(fork, s));
-		PCG_CUDA(cudaStreamWaitEvent(side, fork, 0));
+	// the node sets are independent: the first runs on the job's stream, the
+	// second on one forked stream, the others on a second one
+	constexpr int kSides = DeviceArena::kSides;
+	cudaStream_t side[kSides] = {nullptr, nullptr};
+	cudaEvent_t fork[kSides] = {nullptr, nullptr}, join[kSides] = {nullptr, nullptr};
+	const int sets = (d_wide ? 1 : 0) + (d_clu ? 1 : 0) + (d_one ? 1 : 0) + (d_warp ? 1 : 0);
+	const int nsides = mem.arena() ? std::min(sets - 1, kSides) : 0;
+	for (int k = 0; k < nsides; k++) {
+		side[k] = mem.arena()->side_stream(fork[k], join[k], k);
+		PCG_CUDA(cudaEventRecord(fork[k], s));
+		PCG_CUDA(cudaStreamWaitEvent(side[k], fork[k], 0));
 	}
-	cudaStream_t next = s;  // the first set runs on s, the others on the side stream
+	int next_set = 0;
 	auto stream_for_set = [&]() {
-		cudaStream_t r = next;
-		if (side) next = side;
-		return r;
+		const int i = next_set++;
+		if (i == 0 || nsides == 0) return s;
+		return side[std::min(i, nsides) - 1];
 	};
-	if (d_clu) {
+	auto launch_cluster = [&](auto kernel, int cs_ctas, const int32_t* d_set, size_t count, cudaStream_t cs) {
 		const size_t smem = sizeof(ClusterRound);
-		const unsigned grid = (unsigned)(clu.size() * kClusterCtas);
-		cudaStream_t cs = stream_for_set();
-		if (mode == 0) {
-			PCG_CUDA(cudaFuncSetAttribute(greedy_list_cluster_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_list_cluster_kernel<0><<<grid, kListThreads, smem, cs>>>(nodes, d_clu, pp, lb, ga, cl, srank, st);
-		} else {
-			PCG_CUDA(cudaFuncSetAttribute(greedy_list_cluster_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-			greedy_list_cluster_kernel<1><<<grid, kListThreads, smem, cs>>>(nodes, d_clu, pp, lb, ga, cl, srank, st);
-		}
+		PCG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		kernel<<<(unsigned)(count * cs_ctas), kListThreads, smem, cs>>>(nodes, d_set, pp, lb, ga, cl, srank, st);
 		PCG_LAUNCHED();
+	};
+	if (d_wide) {
+		cudaStream_t cs = stream_for_set();
+		if (mode == 0) launch_cluster(greedy_list_cluster_kernel<0, kWideClusterCtas>, kWideClusterCtas, d_wide, wide.size(), cs);
+		else launch_cluster(greedy_list_cluster_kernel<1, kWideClusterCtas>, kWideClusterCtas, d_wide, wide.size(), cs);
+	}
+	if (d_clu) {
+		cudaStream_t cs = stream_for_set();
+		if (mode == 0) launch_cluster(greedy_list_cluster_kernel<0, kClusterCtas>, kClusterCtas, d_clu, clu.size(), cs);
+		else launch_cluster(greedy_list_cluster_kernel<1, kClusterCtas>, kClusterCtas, d_clu, clu.size(), cs);
 	}
 	if (d_one) {
 		const size_t smem = sizeof(ListRound);
@@ -1748,11 +1764,12 @@ void launch_greedy_lists(int mode, const LevelNode* nodes, const std::vector<int
 		else greedy_list_warp_kernel<1><<<blocks, kWarpsPerBlock * 32, 0, ws>>>(nodes, d_warp, nw, pp, lb, ga, cl, srank, st, counter);
 		PCG_LAUNCHED();
 	}
-	if (side) {
-		PCG_CUDA(cudaEventRecord(join, side));
-		PCG_CUDA(cudaStreamWaitEvent(s, join, 0));
+	for (int k = 0; k < nsides; k++) {
+		PCG_CUDA(cudaEventRecord(join[k], side[k]));
+		PCG_CUDA(cudaStreamWaitEvent(s, join[k], 0));
 	}
 	mem.free(srank);
+	if (d_wide) mem.free(d_wide);
 	if (d_clu) mem.free(d_clu);
 	if (d_one) mem.free(d_one);
 	if (d_warp) mem.free(d_warp);
