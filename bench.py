@@ -488,13 +488,13 @@ def main():
 
     # ---- the request-loop replay (config-4 shape) and the conversion in
     # parts (config-3 shape), single GPU runs only
-    serving = None
-    if world == 1 and not args.no_serving:
-        serving = leg(serving_leg, local, args.serving_jobs, args.serving_rate)
     parts = None
     if world == 1 and not args.no_parts:
         pts = args.parts_points or min(3_000_000_000, host_points_budget(34 + 35 * 1.7))
         parts = leg(parts_leg, local, stream, pts, 1)
+    serving = None
+    if world == 1 and not args.no_serving:
+        serving = leg(serving_leg, local, args.serving_jobs, args.serving_rate)
 
     if rank == 0:
         cpu = None

@@ -402,11 +402,12 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 	}
 	cl.inl = mem.alloc<int4>(M);
 	cl.ovf_off = mem.alloc<int32_t>(M);
-	// entries past the inline ones: room for 4 more per candidate on
-	// average (lists average about one entry). When the lists need more,
-	// the build runs again with a pool of the exact size they asked for. A
-	// pool the device cannot hold is made smaller: the candidates it cannot
-	// take mark their nodes dense, which keep the lookup kernels.
+	// entries past the inline ones: room for 8 more per candidate on
+	// average (lists average about one entry; the top levels' dense nodes
+	// need more than 4). When the lists need more, the build runs again
+	// with a pool of the exact size they asked for. A pool the device cannot
+	// hold is made smaller: the candidates it cannot take mark their nodes
+	// dense, which keep the lookup kernels.
 	auto alloc_pool = [&](int64_t want) {
 		int64_t cap = std::max<int64_t>(want, 1);
 		while (true) {
@@ -420,7 +421,7 @@ void build_conflict_lists(int mode, const LevelNode* d_nodes, const std::vector<
 			}
 		}
 	};
-	alloc_pool(std::min<int64_t>((int64_t)M * kListInline, (int64_t)INT32_MAX));
+	alloc_pool(std::min<int64_t>((int64_t)M * 2 * kListInline, (int64_t)INT32_MAX));
 	cl.pool_used = mem.alloc<unsigned long long>(1);
 	cl.count = mem.alloc<uint8_t>(M);
 	cl.node_dense = mem.alloc<uint8_t>(K);

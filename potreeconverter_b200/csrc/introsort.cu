@@ -19,6 +19,8 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
+#include <limits>
 
 #include "devutil.cuh"
 #include "sampling.h"
@@ -424,12 +426,15 @@ __global__ void __launch_bounds__(kBigThreads) sort_single_big_kernel(double* ke
 // with the decremented depth budget (std::__introsort_loop), so the order in
 // which disjoint segments are processed does not change the result.
 // Segments at most kWideMin long finish on one warp each with their
-// remaining depth budget (a whole CTA for a segment of exactly kBigSortMin or
-// one whose budget is spent, which is heap-sorted); <= 16-element segments
-// go to the final insertion pass. kWideMin = 4096 measured fastest: the
-// rounds are HBM-efficient, a CTA replaying a segment in global memory is
-// not.
-constexpr int64_t kWideMin = 4096;
+// remaining depth budget (a CTA for one whose budget is spent, which is
+// heap-sorted); <= 16-element segments go to the final insertion pass, and
+// segments whose keys became distinct are written from the sorted keys.
+// kWideMin = 1024 measured fastest on the 50M benchmark cloud (sort 36.6 ms
+// per conversion against 40.1 with 4096 and 37.0 with 512): once finished
+// segments leave the rounds, the rounds only carry the segments around
+// equal keys, and the less of them a warp replays in global memory, the
+// better.
+constexpr int64_t kWideMin = 1024;
 constexpr int kWideThreads = 256;
 constexpr int kWideWarps = kWideThreads / 32;
 constexpr int kWideSteps = 16;
@@ -443,13 +448,44 @@ struct WideTile {
 	int32_t last_tile;   // the segment's last tile
 };
 
+// The key range a segment's elements lie in, from the pivots of the
+// partitions that made it: lo <= key <= hi. Bit 0 of inc: the element keyed
+// lo is in the segment, bit 1: the element keyed hi (meaningful when that
+// key occurs once in the node: a partition leaves its pivot at the front of
+// its left half, and an element keyed strictly between two pivots stays
+// between them).
+struct SegBounds {
+	double lo, hi;
+	int32_t inc;
+	int32_t pad;
+};
+
+struct FinSeg {          // a segment written from the sorted keys
+	int64_t f, l;        // its range in key/val
+	int64_t a;           // its first element in the sorted order
+};
+
 struct WideLists {       // outputs of a round (device counters)
 	Seg* next; int* n_next;   // still longer than kWideMin
+	SegBounds* next_b;        // their key ranges
 	Seg* cta;  int* n_cta;    // CTA replay (>= kBigSortMin elements, or heapsort)
 	Seg* warp; int* n_warp;   // warp replay
 	int32_t* blk; int* n_blk; // <= 16 elements: final insertion pass (absolute f, l)
+	FinSeg* fin; int* n_fin;  // distinct keys: written from the sorted keys
 	int64_t cap_seg, cap_blk;
+	SortedLevel sl;           // the sorted keys (sl.sk == nullptr: none)
+	int64_t wide_min;         // segments longer than this go on with the GPU-wide rounds
 };
+
+// kWideMin, or PCG_WIDE_MIN for measurements
+int64_t wide_min() {
+	static const int64_t v = [] {
+		const char* e = std::getenv("PCG_WIDE_MIN");
+		const int64_t x = e ? std::atoll(e) : kWideMin;
+		return x >= 32 ? x : kWideMin;
+	}();
+	return v;
+}
 
 __global__ void wide_pivot_kernel(const Seg* __restrict__ segs, int n, double* key, int32_t* val) {
 	const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -545,8 +581,48 @@ __device__ __forceinline__ void wide_push(Seg* list, int* n, int64_t cap, const 
 	else atomicAdd(&st->timeouts, 1ull);
 }
 
-__device__ void wide_classify(int64_t f, int64_t l, int d, const WideLists& L, SampleStats* st) {
+// position of key v in the node's sorted keys [n0, n1): the first with key
+// >= v (upper = false) or > v (upper = true); keys are >= +0, so their bit
+// patterns order like their values, and the open ends (-inf, +inf) map to
+// the node's ends
+__device__ int64_t sorted_bound(const uint64_t* sk, int64_t n0, int64_t n1, double v, bool upper) {
+	if (v == -CUDART_INF) return n0;
+	if (v == CUDART_INF) return n1;
+	const uint64_t bv = (uint64_t)__double_as_longlong(v);
+	int64_t lo = n0, hi = n1;
+	while (lo < hi) {
+		const int64_t mid = lo + (hi - lo) / 2;
+		if (upper ? sk[mid] <= bv : sk[mid] < bv) lo = mid + 1;
+		else hi = mid;
+	}
+	return lo;
+}
+
+// Whether segment [f, l) with bounds b holds pairwise distinct keys, and
+// where its elements sit in the sorted order: the four positions
+// lower(lo), upper(lo), lower(hi), upper(hi) are given. Requires lo < hi,
+// each bound key at most once in the node, and a slice of the segment's
+// size without adjacent equal keys.
+__device__ bool distinct_slice(const SortedLevel& sl, int64_t f, int64_t l, const SegBounds& b, int64_t llo, int64_t ulo, int64_t lhi,
+                               int64_t uhi, int64_t* a) {
+	if (!(b.lo < b.hi) || ulo - llo > 1 || uhi - lhi > 1) return false;
+	const int64_t first = (b.inc & 1) ? llo : ulo, last = (b.inc & 2) ? uhi : lhi;
+	if (last - first != l - f) return false;
+	if (last - first >= 2 && sl.ties[last - 1] != sl.ties[first]) return false;
+	*a = first;
+	return true;
+}
+
+// slice_a >= 0: the segment's keys are distinct, its elements are
+// sorted[slice_a, slice_a + l - f)
+__device__ void wide_classify(int64_t f, int64_t l, int d, const SegBounds& b, int64_t slice_a, const WideLists& L, SampleStats* st) {
 	const int64_t n = l - f;
+	if (n > 16 && slice_a >= 0) {
+		const int i = atomicAdd(L.n_fin, 1);
+		if (i < L.cap_seg) L.fin[i] = {f, l, slice_a};
+		else atomicAdd(&st->timeouts, 1ull);
+		return;
+	}
 	if (n <= 16) {
 		if (n > 1) {
 			const int i = atomicAdd(L.n_blk, 1);
@@ -557,20 +633,27 @@ __device__ void wide_classify(int64_t f, int64_t l, int d, const WideLists& L, S
 				atomicAdd(&st->timeouts, 1ull);
 			}
 		}
-	} else if (d == 0 || (n >= kBigSortMin && n <= kWideMin)) {
+	} else if (d == 0 || (n >= kBigSortMin && n <= L.wide_min)) {
 		wide_push(L.cta, L.n_cta, L.cap_seg, {f, l, d, 0}, st);
-	} else if (n > kWideMin) {
-		wide_push(L.next, L.n_next, L.cap_seg, {f, l, d, 0}, st);
+	} else if (n > L.wide_min) {
+		const int i = atomicAdd(L.n_next, 1);
+		if (i < L.cap_seg) {
+			L.next[i] = {f, l, d, 0};
+			L.next_b[i] = b;
+		} else {
+			atomicAdd(&st->timeouts, 1ull);
+		}
 	} else {
 		wide_push(L.warp, L.n_warp, L.cap_seg, {f, l, d, 0}, st);
 	}
 }
 
 // one warp per segment: Hoare's pair count K, the cut, the two halves
-__global__ void wide_split_kernel(const Seg* __restrict__ segs, int n, const WideTile* __restrict__ tiles, const int32_t* __restrict__ seg_tile,
-                                  const unsigned long long* __restrict__ counts, const unsigned long long* __restrict__ offs,
-                                  const int32_t* __restrict__ SL, const int32_t* __restrict__ SR, int64_t* __restrict__ segK,
-                                  int64_t* __restrict__ segCR, WideLists L, SampleStats* st) {
+__global__ void wide_split_kernel(const Seg* __restrict__ segs, const SegBounds* __restrict__ bounds, int n, const WideTile* __restrict__ tiles,
+                                  const int32_t* __restrict__ seg_tile, const unsigned long long* __restrict__ counts,
+                                  const unsigned long long* __restrict__ offs, const int32_t* __restrict__ SL, const int32_t* __restrict__ SR,
+                                  const double* __restrict__ key, int64_t* __restrict__ segK, int64_t* __restrict__ segCR, WideLists L,
+                                  SampleStats* st) {
 	const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
 	const int lane = threadIdx.x & 31;
 	if (s >= n) return;
@@ -604,20 +687,57 @@ __global__ void wide_split_kernel(const Seg* __restrict__ segs, int n, const Wid
 		if (b) hi = lo + __ffs(b) - 1;
 	}
 	const int64_t K = hi;
-	if (lane != 0) return;
 	const int64_t c1 = K < cL ? (int64_t)sl[K] : INT64_MAX;
 	const int64_t c2 = K >= 1 ? (int64_t)sr[cR - K] : INT64_MAX;
 	const int64_t cut = g.f + (c1 < c2 ? c1 : c2);
-	segK[s] = K;
-	segCR[s] = cR;
 	if (cut <= g.f || cut >= g.l) {
-		atomicAdd(&st->timeouts, 1ull);
-		segK[s] = 0;
+		if (lane == 0) {
+			segK[s] = 0;
+			segCR[s] = cR;
+			atomicAdd(&st->timeouts, 1ull);
+		}
 		return;
 	}
 	const int d = g.d - 1;
-	wide_classify(cut, g.l, d, L, st);
-	wide_classify(g.f, cut, d, L, st);
+	// the halves' key ranges: the pivot (key[g.f], moved there by
+	// wide_pivot_kernel) stays at the front of the left half
+	const SegBounds pb = bounds[s];
+	const double P = key[g.f];
+	const SegBounds bR{P, pb.hi, pb.inc & 2, 0}, bL{pb.lo, P, (pb.inc & 1) | 2, 0};
+	// lanes 0-7 find the halves' bound keys in the sorted order at once
+	int64_t pos = 0;
+	if (L.sl.sk && lane < 8) {
+		const LevelNode nd = L.sl.nodes[L.sl.node_of[g.f]];
+		const SegBounds& hb = lane < 4 ? bR : bL;
+		const int w = lane & 3;
+		pos = sorted_bound(L.sl.sk, nd.cand_off, nd.cand_off + nd.count, w < 2 ? hb.lo : hb.hi, (w & 1) != 0);
+	}
+	int64_t q[8];
+#pragma unroll
+	for (int i = 0; i < 8; i++) q[i] = __shfl_sync(FULL, pos, i);
+	if (lane != 0) return;
+	segK[s] = K;
+	segCR[s] = cR;
+	int64_t aR = -1, aL = -1;
+	if (L.sl.sk) {
+		if (!distinct_slice(L.sl, cut, g.l, bR, q[0], q[1], q[2], q[3], &aR)) aR = -1;
+		if (!distinct_slice(L.sl, g.f, cut, bL, q[4], q[5], q[6], q[7], &aL)) aL = -1;
+	}
+	wide_classify(cut, g.l, d, bR, aR, L, st);
+	wide_classify(g.f, cut, d, bL, aL, L, st);
+}
+
+// the segments with distinct keys get their sorted keys in order; one CTA
+// per tile of kFinTile elements of a segment (tile_seg / tile_off)
+constexpr int64_t kFinTile = 4096;
+__global__ void __launch_bounds__(256) fin_copy_kernel(const FinSeg* __restrict__ fin, const int32_t* __restrict__ tile_seg,
+                                                       const int64_t* __restrict__ tile_off, SortedLevel sl, double* key, int32_t* val) {
+	const FinSeg g = fin[tile_seg[blockIdx.x]];
+	const int64_t i0 = tile_off[blockIdx.x], i1 = i0 + kFinTile < g.l - g.f ? i0 + kFinTile : g.l - g.f;
+	for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+		key[g.f + i] = __longlong_as_double((long long)sl.sk[g.a + i]);
+		val[g.f + i] = (int32_t)sl.sv[g.a + i];
+	}
 }
 
 __global__ void __launch_bounds__(kWideThreads) wide_swap_kernel(const WideTile* __restrict__ tiles, const Seg* __restrict__ segs,
@@ -637,157 +757,14 @@ __global__ void __launch_bounds__(kWideThreads) wide_swap_kernel(const WideTile*
 	}
 }
 
-// ------------------------------------------- segments with distinct keys
-// The smallest and largest key of a segment, how often each occurs and
-// where (first occurrence).
-struct SegExtremes {
-	double kmin, kmax;
-	int cmin, cmax;
-	int64_t imin, imax;
-};
-
-__device__ __forceinline__ void extremes_init(SegExtremes& e) {
-	e.kmin = CUDART_INF;
-	e.kmax = -CUDART_INF;
-	e.cmin = e.cmax = 0;
-	e.imin = e.imax = INT64_MAX;
-}
-
-__device__ __forceinline__ void extremes_merge(SegExtremes& e, const SegExtremes& o) {
-	if (o.kmin < e.kmin) { e.kmin = o.kmin; e.cmin = o.cmin; e.imin = o.imin; }
-	else if (o.kmin == e.kmin) { e.cmin += o.cmin; e.imin = o.imin < e.imin ? o.imin : e.imin; }
-	if (o.kmax > e.kmax) { e.kmax = o.kmax; e.cmax = o.cmax; e.imax = o.imax; }
-	else if (o.kmax == e.kmax) { e.cmax += o.cmax; e.imax = o.imax < e.imax ? o.imax : e.imax; }
-}
-
-__device__ __forceinline__ void extremes_point(SegExtremes& e, double k, int64_t i) {
-	SegExtremes o;
-	o.kmin = o.kmax = k;
-	o.cmin = o.cmax = 1;
-	o.imin = o.imax = i;
-	extremes_merge(e, o);
-}
-
-__device__ __forceinline__ void extremes_warp(SegExtremes& e) {
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) {
-		SegExtremes x;
-		x.kmin = __shfl_xor_sync(FULL, e.kmin, o);
-		x.kmax = __shfl_xor_sync(FULL, e.kmax, o);
-		x.cmin = __shfl_xor_sync(FULL, e.cmin, o);
-		x.cmax = __shfl_xor_sync(FULL, e.cmax, o);
-		x.imin = __shfl_xor_sync(FULL, (long long)e.imin, o);
-		x.imax = __shfl_xor_sync(FULL, (long long)e.imax, o);
-		extremes_merge(e, x);
-	}
-}
-
-// Whether segment [f, l) (its extremes e) has pairwise distinct keys; if so
-// *a is the first sorted position of its inner elements (keys strictly
-// between its smallest and largest), which are sorted[a, a + (l - f) - 2).
-__device__ bool distinct_segment(const SortedLevel& sl, int64_t f, int64_t l, const SegExtremes& e, int64_t* a) {
-	const int64_t n = l - f;
-	if (e.cmin != 1 || e.cmax != 1 || !(e.kmin < e.kmax)) return false;
-	const LevelNode nd = sl.nodes[sl.node_of[f]];
-	const uint64_t bmin = (uint64_t)__double_as_longlong(e.kmin), bmax = (uint64_t)__double_as_longlong(e.kmax);
-	// keys are >= +0, so their bit patterns order like their values
-	int64_t lo = nd.cand_off, hi = nd.cand_off + nd.count;
-	while (lo < hi) {
-		const int64_t mid = lo + (hi - lo) / 2;
-		if (sl.sk[mid] <= bmin) lo = mid + 1;
-		else hi = mid;
-	}
-	const int64_t first = lo;
-	hi = nd.cand_off + nd.count;
-	while (lo < hi) {
-		const int64_t mid = lo + (hi - lo) / 2;
-		if (sl.sk[mid] < bmax) lo = mid + 1;
-		else hi = mid;
-	}
-	const int64_t last = lo;  // inner elements: sorted[first, last)
-	if (last - first != n - 2) return false;
-	if (last - first >= 2 && sl.ties[last - 1] != sl.ties[first]) return false;
-	*a = first;
-	return true;
-}
-
-// writes a distinct segment in ascending order (e and a from above); the
-// caller's threads t = 0 .. nt-1 share the work and have all read
-// vmin = val[e.imin], vmax = val[e.imax] before
-__device__ void write_distinct(const SortedLevel& sl, double* key, int32_t* val, int64_t f, int64_t l, const SegExtremes& e, int64_t a,
-                               int32_t vmin, int32_t vmax, int t, int nt) {
-	const int64_t n = l - f;
-	for (int64_t i = t; i < n; i += nt) {
-		if (i == 0) {
-			key[f] = e.kmin;
-			val[f] = vmin;
-		} else if (i == n - 1) {
-			key[l - 1] = e.kmax;
-			val[l - 1] = vmax;
-		} else {
-			key[f + i] = __longlong_as_double((long long)sl.sk[a + i - 1]);
-			val[f + i] = (int32_t)sl.sv[a + i - 1];
-		}
-	}
-}
-
-// one warp: true when [f, l) had distinct keys and has been written
-__device__ bool warp_finish_distinct(const SortedLevel& sl, double* key, int32_t* val, int64_t f, int64_t l) {
-	const int lane = threadIdx.x & 31;
-	SegExtremes e;
-	extremes_init(e);
-	for (int64_t i = f + lane; i < l; i += 32) extremes_point(e, key[i], i);
-	extremes_warp(e);
-	int64_t a = 0;
-	const bool ok = distinct_segment(sl, f, l, e, &a);  // same values on every lane
-	if (!ok) return false;
-	const int32_t vmin = val[e.imin], vmax = val[e.imax];
-	__syncwarp();
-	write_distinct(sl, key, val, f, l, e, a, vmin, vmax, lane, 32);
-	__syncwarp();
-	return true;
-}
-
-// one CTA of kBigThreads: the same
-__device__ bool block_finish_distinct(const SortedLevel& sl, double* key, int32_t* val, int64_t f, int64_t l) {
-	__shared__ SegExtremes part[kBigWarps];
-	__shared__ int verdict;
-	__shared__ int64_t sa;
-	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	SegExtremes e;
-	extremes_init(e);
-	for (int64_t i = f + tid; i < l; i += kBigThreads) extremes_point(e, key[i], i);
-	extremes_warp(e);
-	if (lane == 0) part[warp] = e;
-	__syncthreads();
-	if (tid == 0) {
-		SegExtremes all = part[0];
-		for (int w = 1; w < kBigWarps; w++) extremes_merge(all, part[w]);
-		int64_t a = 0;
-		verdict = distinct_segment(sl, f, l, all, &a) ? 1 : 0;
-		sa = a;
-		part[0] = all;
-	}
-	__syncthreads();
-	if (!verdict) return false;
-	const SegExtremes all = part[0];
-	const int64_t a = sa;
-	const int32_t vmin = val[all.imin], vmax = val[all.imax];
-	__syncthreads();
-	write_distinct(sl, key, val, f, l, all, a, vmin, vmax, tid, kBigThreads);
-	__syncthreads();
-	return true;
-}
-
 __global__ void __launch_bounds__(kBigThreads) seg_cta_kernel(const Seg* __restrict__ segs, double* key, int32_t* val, SortScratch sc,
-                                                             SampleStats* st, SortedLevel sl) {
+                                                             SampleStats* st) {
 	const Seg g = segs[blockIdx.x];
-	if (sl.sk && block_finish_distinct(sl, key, val, g.f, g.l)) return;
 	block_std_sort(key + g.f, val + g.f, g.l - g.f, sc.SL + g.f, sc.SR + g.f, sc.blk + 2 * g.f, st, g.d);
 }
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) seg_warp_kernel(const Seg* __restrict__ segs, int n, double* key, int32_t* val,
-                                                                      SortScratch sc, SampleStats* st, int* next_seg, SortedLevel sl) {
+                                                                      SortScratch sc, SampleStats* st, int* next_seg) {
 	__shared__ Seg stacks[kWarpsPerBlock][kStackDepth];
 	__shared__ int nblk[kWarpsPerBlock];
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -798,7 +775,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) seg_warp_kernel(const Seg
 		if (idx >= n) break;
 		const Seg g = segs[idx];
 		const int64_t len = g.l - g.f;
-		if (sl.sk && warp_finish_distinct(sl, key, val, g.f, g.l)) continue;
 		if (lane == 0) nblk[warp] = 0;
 		__syncwarp();
 		warp_introsort(key + g.f, val + g.f, 0, len, g.d, sc.SL + g.f, sc.SR + g.f, sc.blk + 2 * g.f, &nblk[warp], stacks[warp], st);
@@ -872,31 +848,39 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 	WideLists L;
 	L.cap_seg = M / 16 + 64;
 	L.cap_blk = M / 2 + 64;
+	L.sl = sl;
+	L.wide_min = wide_min();
 	Seg* ping[2] = {mem.alloc<Seg>(L.cap_seg), mem.alloc<Seg>(L.cap_seg)};
+	SegBounds* pingb[2] = {mem.alloc<SegBounds>(L.cap_seg), mem.alloc<SegBounds>(L.cap_seg)};
 	L.cta = mem.alloc<Seg>(L.cap_seg);
 	L.warp = mem.alloc<Seg>(L.cap_seg);
 	L.blk = mem.alloc<int32_t>(2 * L.cap_blk);
-	int* counters = mem.alloc<int>(5);  // next, cta, warp, blk, warp-kernel cursor
+	L.fin = mem.alloc<FinSeg>(L.cap_seg);
+	int* counters = mem.alloc<int>(6);  // next, cta, warp, blk, warp-kernel cursor, fin
 	L.n_next = counters;
 	L.n_cta = counters + 1;
 	L.n_warp = counters + 2;
 	L.n_blk = counters + 3;
-	// the initial segments, classified like the halves of a partition
+	L.n_fin = counters + 5;
+	// the initial segments (whole nodes: every key in range), classified
+	// like the halves of a partition
 	std::vector<Seg> cur, cta, warp;
+	std::vector<SegBounds> curb;
 	std::vector<int32_t> blk;
 	for (const SortSeg& g : segs) {
 		const int64_t n = g.l - g.f;
 		if (n <= 16) {
 			if (n > 1) { blk.push_back((int32_t)g.f); blk.push_back((int32_t)g.l); }
-		} else if (g.d == 0 || (n >= kBigSortMin && n <= kWideMin)) {
+		} else if (g.d == 0 || (n >= kBigSortMin && n <= L.wide_min)) {
 			cta.push_back(g);
-		} else if (n > kWideMin) {
+		} else if (n > L.wide_min) {
 			cur.push_back(g);
+			curb.push_back(SegBounds{-std::numeric_limits<double>::infinity(), std::numeric_limits<double>::infinity(), 0, 0});
 		} else {
 			warp.push_back(g);
 		}
 	}
-	int h_counts[5] = {0, (int)cta.size(), (int)warp.size(), (int)(blk.size() / 2), 0};
+	int h_counts[6] = {0, (int)cta.size(), (int)warp.size(), (int)(blk.size() / 2), 0, 0};
 	if (!cta.empty()) PCG_CUDA(cudaMemcpyAsync(L.cta, cta.data(), cta.size() * sizeof(Seg), cudaMemcpyHostToDevice, s));
 	if (!warp.empty()) PCG_CUDA(cudaMemcpyAsync(L.warp, warp.data(), warp.size() * sizeof(Seg), cudaMemcpyHostToDevice, s));
 	if (!blk.empty()) PCG_CUDA(cudaMemcpyAsync(L.blk, blk.data(), blk.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
@@ -927,8 +911,11 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 		}
 		const int nt = (int)tiles.size();
 		Seg* d_cur = ping[pp];
+		SegBounds* d_curb = pingb[pp];
 		L.next = ping[pp ^ 1];
+		L.next_b = pingb[pp ^ 1];
 		PCG_CUDA(cudaMemcpyAsync(d_cur, cur.data(), n * sizeof(Seg), cudaMemcpyHostToDevice, s));
+		PCG_CUDA(cudaMemcpyAsync(d_curb, curb.data(), n * sizeof(SegBounds), cudaMemcpyHostToDevice, s));
 		WideTile* d_tiles = mem.alloc<WideTile>(nt);
 		PCG_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), nt * sizeof(WideTile), cudaMemcpyHostToDevice, s));
 		int32_t* d_seg_tile = mem.alloc<int32_t>(n);
@@ -949,8 +936,8 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 		exclusive_scan_i64(reinterpret_cast<const int64_t*>(counts), reinterpret_cast<int64_t*>(offs), nt, false, mem);
 		wide_write_kernel<<<nt, kWideThreads, 0, s>>>(d_tiles, d_cur, key, offs, sc.SL, sc.SR);
 		PCG_LAUNCHED();
-		wide_split_kernel<<<(unsigned)ceil_div((int64_t)n * 32, 128), 128, 0, s>>>(d_cur, n, d_tiles, d_seg_tile, counts, offs, sc.SL, sc.SR,
-		                                                                          segK, segCR, L, st);
+		wide_split_kernel<<<(unsigned)ceil_div((int64_t)n * 32, 128), 128, 0, s>>>(d_cur, d_curb, n, d_tiles, d_seg_tile, counts, offs, sc.SL,
+		                                                                          sc.SR, key, segK, segCR, L, st);
 		PCG_LAUNCHED();
 		wide_swap_kernel<<<nt, kWideThreads, 0, s>>>(d_tiles, d_cur, segK, segCR, sc.SL, sc.SR, key, val);
 		PCG_LAUNCHED();
@@ -959,7 +946,11 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 		PCG_CUDA(cudaStreamSynchronize(s));
 		if (n_next > L.cap_seg) throw PcgError(5, "sort replay: segment list overflow");
 		cur.resize(n_next);
-		if (n_next) PCG_CUDA(cudaMemcpyAsync(cur.data(), L.next, n_next * sizeof(Seg), cudaMemcpyDeviceToHost, s));
+		curb.resize(n_next);
+		if (n_next) {
+			PCG_CUDA(cudaMemcpyAsync(cur.data(), L.next, n_next * sizeof(Seg), cudaMemcpyDeviceToHost, s));
+			PCG_CUDA(cudaMemcpyAsync(curb.data(), L.next_b, n_next * sizeof(SegBounds), cudaMemcpyDeviceToHost, s));
+		}
 		PCG_CUDA(cudaStreamSynchronize(s));
 		mem.free(counts);
 		mem.free(offs);
@@ -969,9 +960,30 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 	}
 	PCG_CUDA(cudaMemcpyAsync(h_counts, counters, sizeof(h_counts), cudaMemcpyDeviceToHost, s));
 	PCG_CUDA(cudaStreamSynchronize(s));
-	if (h_counts[1] > L.cap_seg || h_counts[2] > L.cap_seg || h_counts[3] > L.cap_blk) throw PcgError(5, "sort replay: list overflow");
+	if (h_counts[1] > L.cap_seg || h_counts[2] > L.cap_seg || h_counts[3] > L.cap_blk || h_counts[5] > L.cap_seg)
+		throw PcgError(5, "sort replay: list overflow");
+	if (h_counts[5] > 0) {
+		std::vector<FinSeg> fin(h_counts[5]);
+		PCG_CUDA(cudaMemcpyAsync(fin.data(), L.fin, fin.size() * sizeof(FinSeg), cudaMemcpyDeviceToHost, s));
+		PCG_CUDA(cudaStreamSynchronize(s));
+		std::vector<int32_t> ts;
+		std::vector<int64_t> to;
+		for (size_t i = 0; i < fin.size(); i++)
+			for (int64_t o = 0; o < fin[i].l - fin[i].f; o += kFinTile) {
+				ts.push_back((int32_t)i);
+				to.push_back(o);
+			}
+		int32_t* d_ts = mem.alloc<int32_t>(ts.size());
+		int64_t* d_to = mem.alloc<int64_t>(to.size());
+		PCG_CUDA(cudaMemcpyAsync(d_ts, ts.data(), ts.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+		PCG_CUDA(cudaMemcpyAsync(d_to, to.data(), to.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+		fin_copy_kernel<<<(unsigned)ts.size(), 256, 0, s>>>(L.fin, d_ts, d_to, sl, key, val);
+		PCG_LAUNCHED();
+		mem.free(d_to);
+		mem.free(d_ts);
+	}
 	if (h_counts[1] > 0) {
-		seg_cta_kernel<<<h_counts[1], kBigThreads, 0, s>>>(L.cta, key, val, sc, st, sl);
+		seg_cta_kernel<<<h_counts[1], kBigThreads, 0, s>>>(L.cta, key, val, sc, st);
 		PCG_LAUNCHED();
 	}
 	if (h_counts[2] > 0) {
@@ -979,7 +991,7 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 		int blocks = (int)ceil_div(h_counts[2], kWarpsPerBlock);
 		const int cap = sm_count() * 16;
 		if (blocks > cap) blocks = cap;
-		seg_warp_kernel<<<blocks, kWarpsPerBlock * 32, 0, s>>>(L.warp, h_counts[2], key, val, sc, st, counters + 4, sl);
+		seg_warp_kernel<<<blocks, kWarpsPerBlock * 32, 0, s>>>(L.warp, h_counts[2], key, val, sc, st, counters + 4);
 		PCG_LAUNCHED();
 	}
 	if (h_counts[3] > 0) {
@@ -989,6 +1001,9 @@ void replay_segments(double* key, int32_t* val, int64_t M, const std::vector<Sor
 	if (segK) { mem.free(segK); mem.free(segCR); }
 	mem.free(ping[0]);
 	mem.free(ping[1]);
+	mem.free(pingb[0]);
+	mem.free(pingb[1]);
+	mem.free(L.fin);
 	mem.free(L.cta);
 	mem.free(L.warp);
 	mem.free(L.blk);

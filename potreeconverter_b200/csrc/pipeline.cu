@@ -158,6 +158,7 @@ public:
 			void* p = it->second;
 			cached_ -= it->first;
 			free_.erase(it);
+			age_.erase(p);
 			return static_cast<uint8_t*>(p);
 		}
 		void* p = nullptr;
@@ -173,13 +174,20 @@ public:
 		auto it = owned_.find(p);
 		if (it == owned_.end()) return false;
 		free_.insert({it->second, p});
+		age_[p] = ++clock_;
 		cached_ += it->second;
-		while (cached_ > max_cached() && !free_.empty()) {  // drop the largest
-			auto last = std::prev(free_.end());
-			cached_ -= last->first;
-			owned_.erase(last->second);
-			cudaFreeHost(last->second);
-			free_.erase(last);
+		while (cached_ > max_cached() && !free_.empty()) {  // drop the longest unused
+			void* old = nullptr;
+			uint64_t oldest = UINT64_MAX;
+			for (const auto& a : age_)
+				if (a.second < oldest) { oldest = a.second; old = a.first; }
+			const size_t sz = owned_[old];
+			for (auto f = free_.lower_bound(sz); f != free_.end() && f->first == sz; ++f)
+				if (f->second == old) { free_.erase(f); break; }
+			age_.erase(old);
+			cached_ -= sz;
+			owned_.erase(old);
+			cudaFreeHost(old);
 		}
 		return true;
 	}
@@ -198,6 +206,8 @@ private:
 	std::mutex m_;
 	std::multimap<size_t, void*> free_;
 	std::unordered_map<void*, size_t> owned_;
+	std::unordered_map<void*, uint64_t> age_;  // cached buffer -> when it was given back
+	uint64_t clock_ = 0;
 	size_t cached_ = 0;
 };
 
@@ -757,14 +767,18 @@ struct Converter {
 		} else {
 			d_out = mem.alloc<uint8_t>(res.octree_size);
 		}
-		PayloadItem* d_items = upload(items, mem);
-		launch_write_payloads(p, items, d_items, d_out, mem);
-		PCG_CUDA(cudaStreamSynchronize(stream));
-		res.stats.ms_output = ms_since(t_out);
-		// the attribute statistics first (small), then octree.bin, whose copy
-		// runs while the host writes hierarchy.bin and metadata.json
+		// the attribute statistics (final since the counting pass) first;
+		// then the payloads are written and octree.bin copied out while the
+		// host writes hierarchy.bin and metadata.json
 		auto stats_dev = download(co.stats, MAX_ATTRS, stream);
 		auto hist = download(co.histogram, 256, stream);
+		PayloadItem* d_items = upload(items, mem);
+		cudaEvent_t ev_out[2];
+		for (auto& e : ev_out) PCG_CUDA(cudaEventCreate(&e));
+		PCG_CUDA(cudaEventRecord(ev_out[0], stream));
+		launch_write_payloads(p, items, d_items, d_out, mem);
+		PCG_CUDA(cudaEventRecord(ev_out[1], stream));
+		const double ms_out_host = ms_since(t_out);
 		auto t_d2h = Clock::now();
 		if (!keep_on_device) {
 			res.octree = host_buffers ? host_buffers->take(res.octree_size) : nullptr;
@@ -778,7 +792,11 @@ struct Converter {
 		finish_writers(job, s, N, recs, stats_dev, hist, octree_depth, base_spacing, res);
 		res.stats.ms_host_writers = ms_since(t_w);
 		PCG_CUDA(cudaStreamSynchronize(stream));
-		res.stats.ms_d2h = ms_since(t_d2h);  // the copy, overlapped with the host writers
+		res.stats.ms_d2h = ms_since(t_d2h);  // payloads and copy, overlapped with the host writers
+		float ms_payloads = 0.f;
+		PCG_CUDA(cudaEventElapsedTime(&ms_payloads, ev_out[0], ev_out[1]));
+		for (auto& e : ev_out) cudaEventDestroy(e);
+		res.stats.ms_output = ms_out_host + ms_payloads;  // order and records on the host, then the payload kernel
 		res.stats.num_nodes = num_nodes;
 		res.stats.output_points = out_points;
 		res.stats.gpu_launches = g_launch_count;
