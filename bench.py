@@ -490,7 +490,9 @@ def main():
     # parts (config-3 shape), single GPU runs only
     parts = None
     if world == 1 and not args.no_parts:
-        pts = args.parts_points or min(3_000_000_000, host_points_budget(34 + 35 * 1.7))
+        # page-locked input (34 B) and octree.bin pieces (about 1.9 output
+        # points of 34 B per input point) in half the available host memory
+        pts = args.parts_points or min(3_000_000_000, host_points_budget(34 + 34 * 1.9))
         parts = leg(parts_leg, local, stream, pts, 1)
     serving = None
     if world == 1 and not args.no_serving:

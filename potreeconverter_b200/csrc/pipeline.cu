@@ -161,6 +161,10 @@ public:
 			age_.erase(p);
 			return static_cast<uint8_t*>(p);
 		}
+		// a new buffer first frees at least as many cached bytes (longest
+		// unused first), so cached plus handed-out memory does not grow
+		// past what a previous job held
+		for (size_t freed = 0; freed < n && !free_.empty();) freed += drop_oldest();
 		void* p = nullptr;
 		if (cudaMallocHost(&p, n) != cudaSuccess) {
 			cudaGetLastError();
@@ -176,23 +180,27 @@ public:
 		free_.insert({it->second, p});
 		age_[p] = ++clock_;
 		cached_ += it->second;
-		while (cached_ > max_cached() && !free_.empty()) {  // drop the longest unused
-			void* old = nullptr;
-			uint64_t oldest = UINT64_MAX;
-			for (const auto& a : age_)
-				if (a.second < oldest) { oldest = a.second; old = a.first; }
-			const size_t sz = owned_[old];
-			for (auto f = free_.lower_bound(sz); f != free_.end() && f->first == sz; ++f)
-				if (f->second == old) { free_.erase(f); break; }
-			age_.erase(old);
-			cached_ -= sz;
-			owned_.erase(old);
-			cudaFreeHost(old);
-		}
+		while (cached_ > max_cached() && !free_.empty()) drop_oldest();
 		return true;
 	}
 
 private:
+	// frees the cached buffer given back longest ago; returns its size
+	size_t drop_oldest() {
+		void* old = nullptr;
+		uint64_t oldest = UINT64_MAX;
+		for (const auto& a : age_)
+			if (a.second < oldest) { oldest = a.second; old = a.first; }
+		if (!old) return 0;
+		const size_t sz = owned_[old];
+		for (auto f = free_.lower_bound(sz); f != free_.end() && f->first == sz; ++f)
+			if (f->second == old) { free_.erase(f); break; }
+		age_.erase(old);
+		cached_ -= sz;
+		owned_.erase(old);
+		cudaFreeHost(old);
+		return sz;
+	}
 	// pinned memory kept for reuse: a third of the host's memory, at most
 	// 64 GiB (the pieces of a large conversion are reused by the next one)
 	static size_t max_cached() {
