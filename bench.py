@@ -488,15 +488,15 @@ def main():
 
     # ---- the request-loop replay (config-4 shape) and the conversion in
     # parts (config-3 shape), single GPU runs only
+    serving = None
+    if world == 1 and not args.no_serving:
+        serving = leg(serving_leg, local, args.serving_jobs, args.serving_rate)
     parts = None
     if world == 1 and not args.no_parts:
         # page-locked input (34 B) and octree.bin pieces (about 1.9 output
         # points of 34 B per input point) in half the available host memory
         pts = args.parts_points or min(3_000_000_000, host_points_budget(34 + 34 * 1.9))
         parts = leg(parts_leg, local, stream, pts, 1)
-    serving = None
-    if world == 1 and not args.no_serving:
-        serving = leg(serving_leg, local, args.serving_jobs, args.serving_rate)
 
     if rank == 0:
         cpu = None

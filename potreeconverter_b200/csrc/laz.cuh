@@ -27,8 +27,13 @@
 
 #ifdef __CUDACC__
 #define LAZ_HD __host__ __device__ __forceinline__
+// rarely taken routines stay out of line: one decoder chain per chunk is
+// bound by its own issue latency, and inlining them at every call site
+// multiplies the code the instruction cache has to hold
+#define LAZ_RARE inline __host__ __device__ __noinline__
 #else
 #define LAZ_HD inline
+#define LAZ_RARE inline
 #endif
 
 namespace pcg {
@@ -93,7 +98,7 @@ LAZ_HD uint16_t* model_dist(uint32_t* h) { return reinterpret_cast<uint16_t*>(h 
 
 // counts halved at the limit, cumulative distribution, decoder table, next
 // update interval (5/4 of the last, at most 8 (n + 6))
-LAZ_HD void model_update(uint32_t* h) {
+LAZ_RARE void model_update(uint32_t* h) {
 	const uint32_t n = h[M_N];
 	uint16_t* dist = model_dist(h);
 	uint16_t* cnt = dist + n;
@@ -134,7 +139,7 @@ LAZ_HD void model_update(uint32_t* h) {
 }
 
 // uniform counts, then the first update after (n + 6) / 2 symbols
-LAZ_HD void model_init(uint32_t* h) {
+LAZ_RARE void model_init(uint32_t* h) {
 	const uint32_t n = h[M_N];
 	uint16_t* cnt = model_dist(h) + n;
 	h[M_TOTAL] = 0;
@@ -155,7 +160,7 @@ LAZ_HD void model_header(uint32_t* h, uint32_t n) {
 	}
 }
 
-LAZ_HD uint32_t* model_new(Arena& ar, uint32_t n) {
+LAZ_RARE uint32_t* model_new(Arena& ar, uint32_t n) {
 	uint32_t* h = ar.take(model_words(n));
 	if (h) model_header(h, n);
 	return h;
@@ -171,7 +176,7 @@ LAZ_HD void bit_init(uint32_t* h) {
 	h[B_CYCLE] = h[B_UNTIL] = 4;
 }
 
-LAZ_HD void bit_update(uint32_t* h) {
+LAZ_RARE void bit_update(uint32_t* h) {
 	if ((h[B_COUNT] += h[B_CYCLE]) > kBitMaxCount) {
 		h[B_COUNT] = (h[B_COUNT] + 1) >> 1;
 		h[B_ZERO] = (h[B_ZERO] + 1) >> 1;
@@ -332,14 +337,14 @@ struct IntCoder {
 		arena = nullptr;
 		k = 0;
 	}
-	LAZ_HD void alloc_classes(Arena& ar) {
+	LAZ_RARE void alloc_classes(Arena& ar) {
 		arena = &ar;
 		mbits = ar.take(contexts * mbits_words);
 		if (mbits)
 			for (uint32_t i = 0; i < contexts; i++) model_header(mbits + i * mbits_words, corr_bits + 1);
 		corr0 = ar.take(B_WORDS);
 	}
-	LAZ_HD void alloc_correctors(Arena& ar, uint32_t lo, uint32_t hi) {
+	LAZ_RARE void alloc_correctors(Arena& ar, uint32_t lo, uint32_t hi) {
 		for (uint32_t i = lo; i <= hi && i <= corr_bits; i++) corr[i] = model_new(ar, i <= bits_high ? (1u << i) : (1u << bits_high));
 	}
 	LAZ_HD void init() {
@@ -494,7 +499,7 @@ struct Models {
 	uint32_t* rgb_diff[6];
 	uint32_t* byte_model[kMaxExtraBytes];
 
-	LAZ_HD void create(Arena& ar, const Layout& L) {
+	LAZ_RARE void create(Arena& ar, const Layout& L) {
 		ic_intensity.setup(16, 4);
 		ic_psid.setup(16, 1);
 		ic_dx.setup(32, 2);

@@ -157,20 +157,21 @@ public:
 		if (it != free_.end() && it->first <= 2 * n + (size_t(64) << 20)) {
 			void* p = it->second;
 			cached_ -= it->first;
+			in_use_ += it->first;
 			free_.erase(it);
 			age_.erase(p);
 			return static_cast<uint8_t*>(p);
 		}
-		// a new buffer first frees at least as many cached bytes (longest
-		// unused first), so cached plus handed-out memory does not grow
-		// past what a previous job held
-		for (size_t freed = 0; freed < n && !free_.empty();) freed += drop_oldest();
+		// a new buffer first frees cached ones (longest unused first) while
+		// cached plus handed-out memory would pass half the host's memory
+		while (!free_.empty() && cached_ + in_use_ + n > max_total()) drop_oldest();
 		void* p = nullptr;
 		if (cudaMallocHost(&p, n) != cudaSuccess) {
 			cudaGetLastError();
 			return nullptr;
 		}
 		owned_[p] = n;
+		in_use_ += n;
 		return static_cast<uint8_t*>(p);
 	}
 	bool give(void* p) {
@@ -180,6 +181,7 @@ public:
 		free_.insert({it->second, p});
 		age_[p] = ++clock_;
 		cached_ += it->second;
+		in_use_ -= it->second;
 		while (cached_ > max_cached() && !free_.empty()) drop_oldest();
 		return true;
 	}
@@ -201,14 +203,19 @@ private:
 		cudaFreeHost(old);
 		return sz;
 	}
+	static size_t phys() {
+		const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGE_SIZE);
+		return pages > 0 && page > 0 ? (size_t)pages * (size_t)page : (size_t(32) << 30);
+	}
 	// pinned memory kept for reuse: a third of the host's memory, at most
 	// 64 GiB (the pieces of a large conversion are reused by the next one)
 	static size_t max_cached() {
-		static const size_t m = [] {
-			const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGE_SIZE);
-			const size_t phys = pages > 0 && page > 0 ? (size_t)pages * (size_t)page : (size_t(32) << 30);
-			return std::max(size_t(8) << 30, std::min(size_t(64) << 30, phys / 3));
-		}();
+		static const size_t m = std::max(size_t(8) << 30, std::min(size_t(64) << 30, phys() / 3));
+		return m;
+	}
+	// cached plus handed-out pinned memory before new buffers free cached ones
+	static size_t max_total() {
+		static const size_t m = std::max(size_t(8) << 30, phys() / 2);
 		return m;
 	}
 	std::mutex m_;
@@ -216,7 +223,7 @@ private:
 	std::unordered_map<void*, size_t> owned_;
 	std::unordered_map<void*, uint64_t> age_;  // cached buffer -> when it was given back
 	uint64_t clock_ = 0;
-	size_t cached_ = 0;
+	size_t cached_ = 0, in_use_ = 0;
 };
 
 PinnedPool g_pinned;
