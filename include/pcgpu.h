@@ -82,7 +82,8 @@ typedef struct pcg_opts {
 	   source with more points than group_points is indexed in parts of
 	   consecutive chunks of at most group_points points (a chunk larger than
 	   that is a part by itself). 0 = parts only when the whole cloud would
-	   not fit the device, sized from its free memory. */
+	   not fit the device, sized from its free memory and at most 100M
+	   points each. */
 	int64_t group_points;
 } pcg_opts;
 
