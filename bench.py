@@ -443,8 +443,9 @@ def main():
     rec_len = int.from_bytes(header[105:107], "little")
     bpp = 39
     out_pts = s["output_points"]
-    # roofline: the dominant kernel of a step (ncu launch list) is the
-    # acceptance from conflict lists (greedy_list_kernel and its warp form),
+    # roofline: the largest kernel family of a step (ncu launch list, 25 %)
+    # is the acceptance from conflict lists (greedy_list_cluster_kernel for
+    # the largest nodes, greedy_list_kernel, greedy_list_warp_kernel),
     # launched once per octree level. Algorithmic bytes: per candidate its
     # record (16 B), list length (1 B) and its decision, rank and flag
     # (9 B); per list entry the entry (4 B) and that candidate's decision
@@ -517,7 +518,7 @@ def main():
             "e2e": {"value": e2e, "unit": "Mpts/s", "h2d_bytes_per_step": int(pinned.numel()),
                     "d2h_bytes_per_step": int(octree_bytes)},
             "gpu_launches": int(s["gpu_launches"]) * args.steps,
-            "roofline": {"bound": "hbm", "kernel": "greedy_list_kernel + greedy_list_warp_kernel (all levels of a step)",
+            "roofline": {"bound": "hbm", "kernel": "greedy_list_cluster_kernel + greedy_list_kernel + greedy_list_warp_kernel (list acceptance, all levels of a step)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "traffic_source": "DRAM bytes per candidate from ncu, profiles/accept_hotspots-5M_poisson.md",
                          "algorithmic_bytes": accept_bytes, "kernel_ms": accept_ms,
