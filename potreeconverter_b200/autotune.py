@@ -67,18 +67,18 @@ def sweep(points: int) -> list:
     return rows
 
 
-def write(rows: list, points: int):
+def write(rows: list, points: int, out_dir: str = CSRC):
     ok = [r for r in rows if "total_ms" in r]
     best = min(ok, key=lambda r: r["total_ms"])
     cta, small, clu, warp = best["schedule"]
-    with open(os.path.join(CSRC, "tuned_schedule.h"), "w") as f:
+    with open(os.path.join(out_dir, "tuned_schedule.h"), "w") as f:
         f.write("// Level schedule of the samplers (sampling.h LevelSchedule). Written by\n"
                 "// potreeconverter_b200/autotune.py from a sweep on the target GPU; the\n"
                 "// values below are the sweep's best for the benchmarked workload, or the\n"
                 "// hand-set defaults until a sweep has run.\n#pragma once\n"
                 f"#define PCG_TUNED_CTA_MIN {cta}\n#define PCG_TUNED_SMALL_LEVEL_CTA_MIN {small}\n"
                 f"#define PCG_TUNED_CLUSTER_MIN {clu}\n#define PCG_TUNED_WARP_BLOCKS_PER_SM {warp}\n")
-    with open(os.path.join(CSRC, "tuned_schedule.json"), "w") as f:
+    with open(os.path.join(out_dir, "tuned_schedule.json"), "w") as f:
         json.dump({"points": points, "best": best, "rows": rows}, f, indent=1)
     return best
 

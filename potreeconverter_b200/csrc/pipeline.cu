@@ -718,7 +718,7 @@ struct Converter {
 		if (method != PCG_RANDOM) {
 			// coordinates travel with the ids from here on
 			leaf_rec = mem.alloc<int4>(N);
-			launch_gather_records(leaf_ids, N, co.X, co.Y, co.Z, leaf_rec, mem);
+			launch_gather_records(leaf_ids, N, co.X, co.Y, co.Z, leaf_rec, mem, N);
 		}
 		for (auto& n : tree.nodes) {
 			if (!n.has_children()) {
@@ -1104,7 +1104,7 @@ struct Converter {
 		int4* leaf_rec = nullptr;
 		if (method != PCG_RANDOM) {
 			leaf_rec = mem.alloc<int4>(std::max<int64_t>(n, 1));
-			launch_gather_records(leaf_ids, n, co.X, co.Y, co.Z, leaf_rec, mem);
+			launch_gather_records(leaf_ids, n, co.X, co.Y, co.Z, leaf_rec, mem, n);
 		}
 		for (int ni : nodes) {
 			TNode& t = tree.nodes[ni];

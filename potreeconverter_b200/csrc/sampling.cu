@@ -99,6 +99,19 @@ __global__ void gather_records_kernel(const uint32_t* __restrict__ ids, int64_t 
 	rec[i] = make_int4(X[id], Y[id], Z[id], 0);
 }
 
+// (X, Y, Z, 0) of every point, so that a gather in a scattered order reads
+// one 16-byte record per point instead of three 4-byte words from three arrays
+__global__ void pack_records_kernel(int64_t n, const int32_t* __restrict__ X, const int32_t* __restrict__ Y, const int32_t* __restrict__ Z,
+                                    int4* __restrict__ xyz) {
+	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) xyz[i] = make_int4(X[i], Y[i], Z[i], 0);
+}
+
+__global__ void gather_packed_kernel(const uint32_t* __restrict__ ids, int64_t n, const int4* __restrict__ xyz, int4* __restrict__ rec) {
+	const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) rec[i] = xyz[ids[i]];
+}
+
 // sorted candidate records: (X, Y, Z, local index) at each sorted position
 __global__ void cand_records_kernel(const LevelNode* __restrict__ nodes, const int32_t* __restrict__ X, const int32_t* __restrict__ Y,
                                     const int32_t* __restrict__ Z, LevelBuffers lb) {
@@ -1598,7 +1611,18 @@ void launch_keys(const LevelNode* nodes, const PosParamsS& pp, LevelBuffers& lb,
 	PCG_LAUNCHED();
 }
 
-void launch_gather_records(const uint32_t* ids, int64_t n, const int32_t* X, const int32_t* Y, const int32_t* Z, int4* rec, DeviceMem& mem) {
+void launch_gather_records(const uint32_t* ids, int64_t n, const int32_t* X, const int32_t* Y, const int32_t* Z, int4* rec, DeviceMem& mem,
+                           int64_t n_src) {
+	if (n > 0 && n_src >= (int64_t(1) << 20)) {
+		// a permutation of many points: pack first, then one load per point
+		int4* xyz = mem.alloc<int4>(n_src);
+		pack_records_kernel<<<(unsigned)ceil_div(n_src, 256), 256, 0, mem.stream()>>>(n_src, X, Y, Z, xyz);
+		PCG_LAUNCHED();
+		gather_packed_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(ids, n, xyz, rec);
+		PCG_LAUNCHED();
+		mem.free(xyz);
+		return;
+	}
 	if (n == 0) return;
 	gather_records_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, mem.stream()>>>(ids, n, X, Y, Z, rec);
 	PCG_LAUNCHED();

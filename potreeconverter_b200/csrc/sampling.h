@@ -74,7 +74,10 @@ void launch_gather(const std::vector<GatherItem>& h_items, const GatherItem* ite
 // keys from the gathered records lb.rec
 void launch_keys(const LevelNode* nodes, const PosParamsS& pp, LevelBuffers& lb, DeviceMem& mem);
 // records (X, Y, Z, -) of ids[0..n)
-void launch_gather_records(const uint32_t* ids, int64_t n, const int32_t* X, const int32_t* Y, const int32_t* Z, int4* rec, DeviceMem& mem);
+// n_src > 0: X, Y, Z hold n_src points and ids are spread over all of them
+// (packed first when there are many)
+void launch_gather_records(const uint32_t* ids, int64_t n, const int32_t* X, const int32_t* Y, const int32_t* Z, int4* rec, DeviceMem& mem,
+                           int64_t n_src = 0);
 // std::sort emulation per node; `order` lists node indices, largest first.
 // Nodes order[0..num_big) (the largest) get one CTA each, the rest one warp.
 // Which kernel shape samples which node of a level: nodes of at least
