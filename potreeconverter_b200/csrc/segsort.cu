@@ -39,8 +39,11 @@ namespace {
 
 constexpr int kSegThreads = 256;
 constexpr int kSegWarps = kSegThreads / 32;
-constexpr int kSegSteps = 16;
-constexpr int kSegTile = kSegThreads * kSegSteps;  // 4096
+// 2048-element tiles: the downsweep keeps a tile's keys, values and ranks in
+// registers, and at 8 per thread it fits 64 registers, four blocks per SM
+// (16 per thread took 106 registers, two blocks, and waited on memory)
+constexpr int kSegSteps = 8;
+constexpr int kSegTile = kSegThreads * kSegSteps;  // 2048
 constexpr int kSegDigits = 256;
 static_assert(kSegThreads == kSegDigits, "one thread per digit");
 
@@ -79,7 +82,7 @@ __global__ void __launch_bounds__(kSegThreads) seg_upsweep(const SegTile* __rest
 }
 
 // vals_in == nullptr: first pass, the value is the candidate's index in its node
-__global__ void __launch_bounds__(kSegThreads) seg_downsweep(const SegTile* __restrict__ tiles, const uint64_t* __restrict__ keys_in,
+__global__ void __launch_bounds__(kSegThreads, 4) seg_downsweep(const SegTile* __restrict__ tiles, const uint64_t* __restrict__ keys_in,
                                                            const uint32_t* __restrict__ vals_in, uint64_t* __restrict__ keys_out,
                                                            uint32_t* __restrict__ vals_out, int shift, const uint32_t* __restrict__ offsets) {
 	extern __shared__ __align__(16) unsigned char seg_smem[];
